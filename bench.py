@@ -1,0 +1,400 @@
+"""Benchmark of the channel-DNS hot path on B200: RK3 steps/s and grid-point updates/s,
+FP32-mixed vs FP64, with the error of the mixed path against the FP64 path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config re550] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1).  The path does not shard (each channel lives on
+one GPU), so N > 1 runs N independent replicas ("scaling": "weak"); `value` is the
+aggregate over ranks, timed as the max over ranks.  Inputs (GBs of spectral state) are far
+larger than the 126 MB L2, so no flush is needed between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK3 steps/s and grid-pt updates/s: FP32-mixed vs FP64 on 1 B200 at stated error"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------------------------------------
+# algorithmic bytes per launch of each kernel (compulsory traffic: every operand read once,
+# every result written once)
+# ------------------------------------------------------------------------------------------
+def kernel_bytes(name, setup, mixed):
+    cfg, g = setup.cfg, setup.grid
+    ncol, nyu, nyv, nyp = cfg.ncol, g.nyu, g.nyv, g.nyp
+    cs, ct = 16, (8 if mixed else 16)
+    hpl = cfg.ngal2 * cfg.nkx                 # half-physical plane (complex values)
+    nslot = nyu + nyv
+    nplu = sum(max(0, min(h, g.ju1 - 1) - max(l, g.ju0 + 1) + 1) for l, h in zip(setup.ibu.jlo, setup.ibu.jhi))
+    nplv = sum(max(0, min(h, g.jv1 - 1) - max(l, g.jv0 + 1) + 1) for l, h in zip(setup.ibv.jlo, setup.ibv.jhi))
+    phys = cfg.ngal1 * cfg.ngal2
+    rt = 4 if mixed else 8
+    b = {
+        "k_zinv": (2 * nyu + nyv) * ncol * cs + 3 * nslot * hpl * ct,
+        "k_xline": (3 * nslot + 4 * nyu + 2 * nyv) * hpl * ct,
+        "k_zfwd": (4 * nyu + 2 * nyv) * (hpl + ncol) * ct,
+        "k_rhs": ncol * ((2 * nyu + nyv + nyp) * cs + (2 * nyu + nyv) * ct + (4 * nyu + 2 * nyv) * ct
+                         + (2 * nyu + nyv) * cs + (2 * nyu + nyv) * ct),
+        "k_solve_uvw": ncol * 2 * (2 * nyu + nyv) * cs,
+        "k_solve_p": ncol * (2 * nyu + nyv + nyp + 2 * nyp) * cs,
+        "k_vcorr": ncol * (2 * (2 * nyu + nyv) + nyp) * cs,
+    }
+    # IB kernels: average over the u-grid (2 batches) and v-grid (1 batch) launches
+    ib = []
+    for npl, nb in ((nplu, 2), (nplv, 1)):
+        if npl:
+            ib.append({"k_ib_zinv": npl * 2 * nb * (ncol * cs + hpl * ct),
+                       "k_ib_xinv": npl * nb * (2 * hpl * ct + 2 * phys * rt),
+                       "k_ib_xfwd": npl * nb * (phys * rt + hpl * ct),
+                       "k_ib_zfwd": npl * nb * (hpl * ct + ncol * cs)})
+    for k in ("k_ib_zinv", "k_ib_xinv", "k_ib_xfwd", "k_ib_zfwd"):
+        if ib:
+            b[k] = sum(x[k] for x in ib) / len(ib)
+    return b.get(name)
+
+
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.index), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+            os.unlink(self.f.name)
+        except OSError:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(rows), "reasons": reasons}
+
+
+# ------------------------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v, device):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_steps(torch, ch, stream, nsteps, ws, device):
+    barrier(ws)
+    torch.cuda.synchronize(device)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    ch.step(nsteps)
+    e.record(stream)
+    e.synchronize()
+    torch.cuda.synchronize(device)
+    barrier(ws)
+    return max_over_ranks(ws, s.elapsed_time(e) / 1e3, device)
+
+
+def profile_step(ch):
+    """One RK3 step through the stage entry points with per-kernel CUDA events."""
+    lib = ch.lib
+    lib.cfd_profile(ch.ctx, 1)
+    for k in (1, 2, 3):
+        ch.rk_substep(k)
+    lib.cfd_profile(ch.ctx, 0)
+    buf = C.create_string_buffer(1 << 16)
+    lib.cfd_profile_read(ch.ctx, buf, len(buf))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, calls, ms = line.split()
+        out[name] = (int(calls), float(ms))
+    return out
+
+
+def rel_err(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def cpu_baseline(setup, budget_s=30.0):
+    """FP64 oracle (C++ port of the reference step, all host threads) on a bounded sample."""
+    from oracle import oracle as O
+    O.build()
+    nthreads = os.cpu_count() or 1
+    O.set_threads(nthreads)
+    o = O.OracleChannel(setup)
+    o.upload_state()
+    t0 = time.perf_counter()
+    o.rk_substep(1)
+    t_sub = time.perf_counter() - t0
+    if 2 * t_sub < budget_s:
+        t0 = time.perf_counter()
+        o.rk_substep(2)
+        o.rk_substep(3)
+        t_step = t_sub + (time.perf_counter() - t0)
+        sample = f"one full RK3 step of the {setup.cfg.name} grid (3 substeps)"
+    else:
+        t_step = 3.0 * t_sub
+        sample = f"one RK3 substep (kRK=1) of the {setup.cfg.name} grid, x3 for a step"
+    o.close()
+    return {"value": 1.0 / t_step, "unit": "RK3 steps/s", "cores": nthreads, "kind": "port",
+            "sample": sample, "seconds": t_step}
+
+
+# ------------------------------------------------------------------------------------------
+def run_reference(args, setup, ws, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build()
+    nth = os.cpu_count() or 1
+    O.set_threads(nth)
+    o = O.OracleChannel(setup)
+    o.upload_state()
+    budget = 120.0
+    # warm-up: one substep at most (the oracle has no caches to warm beyond first touch)
+    o.rk_substep(1)
+    done = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for k in (1, 2, 3):
+            o.rk_substep(k)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    v = done / el
+    line = {"metric": METRIC, "value": v, "unit": "RK3 steps/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": setup.cfg.name, "grid": f"{setup.cfg.ngal1}x{setup.cfg.ny}x{setup.cfg.ngal2}",
+                       "ny_tot": setup.grid.nyv},
+            "grid_pt_updates_per_s": v * setup.grid_points,
+            "cpu_baseline": {"value": v, "unit": "RK3 steps/s", "cores": nth, "kind": "port",
+                             "sample": f"{done} full RK3 steps of the {setup.cfg.name} grid "
+                                       f"(capped at {budget:.0f} s of timed work)"},
+            "e2e": {"value": v, "unit": "RK3 steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="re550")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--error-steps", type=int, default=10)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    from cfd_b200.channel import build_channel
+    from cfd_b200.config import preset
+    cfg = preset(args.config)
+    ws, rank, local = dist_init() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                              int(os.environ.get("RANK", "0")), 0)
+    setup = build_channel(cfg.with_(seed=cfg.seed + rank))
+    if args.impl == "reference":
+        run_reference(args, setup, ws, rank)
+        return
+
+    import torch
+    from cfd_b200.channel import Channel
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream(device)
+    results = {}
+    chans = {}
+    for prec in ("mixed", "fp64"):
+        ch = Channel(setup, device=local, precision=prec)
+        ch.set_stream(stream.cuda_stream)
+        ch.upload_state()
+        ch.step(args.warmup)
+        n0 = ch.launch_count()
+        with ClockSampler(local) as cs:
+            t = time_steps(torch, ch, stream, args.steps, ws, device)
+        results[prec] = {"seconds": t, "steps_per_s": ws * args.steps / t, "clocks": cs.summary(),
+                         "launches": ch.launch_count() - n0}
+        chans[prec] = ch
+
+    # error of the mixed path against the FP64 path after the same number of steps
+    err = {}
+    states = {}
+    for prec, ch in chans.items():
+        ch.upload_state()
+        ch.step(args.error_steps)
+        states[prec] = ch.download_state()
+    for k in ("u1", "u2", "u3", "p"):
+        err[k] = rel_err(states["mixed"][k], states["fp64"][k])
+    fp64_div = chans["fp64"].divergence_max()
+
+    # per-kernel timing (CUDA events on the launching stream) for the roofline
+    hbm, peak_kind = peaks()
+    prof = profile_step(chans["mixed"])
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    tot = sum(v[1] for v in prof.values())
+    kname, (kcalls, kms) = top
+    kb = kernel_bytes(kname, setup, True)
+    per_launch_s = kms / kcalls / 1e3
+    achieved = kb / per_launch_s / 1e9 if kb else None
+    prof64 = profile_step(chans["fp64"])
+
+    # end-to-end through the C ABI with pinned host buffers: H2D state, step, D2H state
+    ch = chans["mixed"]
+    host = {}
+    nbytes = 0
+    for k in ("u1", "u2", "u3", "p"):
+        a = torch.from_numpy(np.ascontiguousarray(setup.state()[k]).view(np.float64).copy()).pin_memory()
+        host[k] = a
+        nbytes += a.numel() * 8
+    lib = ch.lib
+    fid = {"u1": 0, "u2": 1, "u3": 2, "p": 3}
+
+    def e2e_step():
+        for k in host:
+            lib.cfd_upload_field(ch.ctx, fid[k], C.cast(host[k].data_ptr(), C.POINTER(C.c_double)), 0)
+        ch.step(1)
+        for k in host:
+            lib.cfd_download_field(ch.ctx, fid[k], C.cast(host[k].data_ptr(), C.POINTER(C.c_double)), 0)
+        ch.synchronize()
+
+    for _ in range(args.warmup):
+        e2e_step()
+    ne2e = max(3, min(args.steps, 10))
+    barrier(ws)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(ne2e):
+        e2e_step()
+    e.record(stream)
+    e.synchronize()
+    barrier(ws)
+    te2e = max_over_ranks(ws, s.elapsed_time(e) / 1e3, device)
+    e2e_val = ws * ne2e / te2e
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(setup)
+
+    gp = setup.grid_points
+    mixed, fp64 = results["mixed"], results["fp64"]
+    line = {
+        "metric": METRIC,
+        "value": mixed["steps_per_s"],
+        "unit": "RK3 steps/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * mixed["seconds"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32-mixed (FP32 transforms/products, FP64 solves/state)",
+        "data": "synthetic (seeded perturbed Poiseuille, cylinder lattice)",
+        "config": {"workload": f"{cfg.name}: Re_tau {cfg.re_tau:g}, {cfg.ngal1}x{cfg.ny}x{cfg.ngal2} "
+                               f"(+{2 * setup.grid.dny} canopy planes), cylinders H {cfg.posth} D {cfg.cyl_diameter} "
+                               f"s {cfg.cyl_spacing}",
+                   "ny_tot": setup.grid.nyv, "ib_points_u": setup.ibu.n, "ib_points_v": setup.ibv.n,
+                   "dt": setup.dt, "parallelism": f"replicas x{ws}",
+                   "l2": "state and work buffers are GBs, far above the 126 MB L2 (no flush)"},
+        "grid_pt_updates_per_s": mixed["steps_per_s"] * gp,
+        "fp64": {"steps_per_s": fp64["steps_per_s"], "grid_pt_updates_per_s": fp64["steps_per_s"] * gp,
+                 "ms_per_step": 1e3 * fp64["seconds"] / args.steps, "clocks": fp64["clocks"],
+                 "max_divergence": fp64_div},
+        "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
+        "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+                     "traffic": None, "algorithmic_bytes_per_launch": kb,
+                     "avg_launch_ms": kms / kcalls, "share_of_step": kms / tot},
+        "kernels_mixed": {k: {"calls": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "kernels_fp64": {k: {"calls": v[0], "ms": v[1]} for k, v in sorted(prof64.items(), key=lambda kv: -kv[1][1])},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_val, "unit": "RK3 steps/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                "path": "cfd_upload_field x4 (pinned host, reference layout) + cfd_step + cfd_download_field x4"},
+        "gpu_launches": mixed["launches"],
+        "launches_per_step": mixed["launches"] // max(args.steps, 1),
+        "clocks": mixed["clocks"],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for ch in chans.values():
+        ch.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

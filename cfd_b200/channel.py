@@ -1,0 +1,180 @@
+"""Host-side driver of the B200 hot path, mirroring the reference's main loop.
+
+``Channel`` exposes the subroutine entry points of littleharsh.f90 (RHS0_u1..3,
+nonlinear, solveU/solveV, meanflow_ctU/ctP, solveP, v_corr; littleharsh.f90:163-196)
+over the C ABI of ``libcfdb200.so``.  State lives on the GPU; host arrays use the
+reference's cfield layout f(j,column) as complex128 arrays of shape [column, plane].
+
+``build_channel`` produces everything the step consumes from a ChannelConfig: the
+y-grid, the IB lists, the seeded initial fields and the fixed time step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import capi
+from .config import ChannelConfig
+from .geometry import IBList, ib_lists
+from .grid import YGrid, y_grid_rough
+from .initial import cfl_dt, initial_state
+
+
+@dataclass
+class ChannelSetup:
+    cfg: ChannelConfig
+    grid: YGrid
+    ibu: IBList
+    ibv: IBList
+    dt: float
+    u1: np.ndarray
+    u2: np.ndarray
+    u3: np.ndarray
+    p: np.ndarray
+
+    def state(self):
+        return {"u1": self.u1, "u2": self.u2, "u3": self.u3, "p": self.p}
+
+    @property
+    def grid_points(self) -> int:
+        """Ngal1 * Ngal2 * ny_tot (faces, walls included) - the unit of grid-pt updates."""
+        return self.cfg.ngal1 * self.cfg.ngal2 * self.grid.nyv
+
+
+def build_channel(cfg: ChannelConfig, with_fields: bool = True) -> ChannelSetup:
+    grid = y_grid_rough(cfg.ny, cfg.dyq, cfg.ppp, cfg.posth)
+    ibu, ibv = ib_lists(cfg, grid)
+    if with_fields:
+        u1, u2, u3, p = initial_state(cfg, grid)
+        dt = cfg.dt if cfg.dt is not None else cfl_dt(cfg, grid, u1, u2, u3)
+    else:
+        u1 = u2 = u3 = p = None
+        dt = cfg.dt if cfg.dt is not None else 1e-4
+    return ChannelSetup(cfg=cfg, grid=grid, ibu=ibu, ibv=ibv, dt=float(dt),
+                        u1=u1, u2=u2, u3=u3, p=p)
+
+
+def field_planes(setup: ChannelSetup, name: str) -> int:
+    g = setup.grid
+    return {"u1": g.nyu, "u3": g.nyu, "nu1": g.nyu, "nu3": g.nyu, "du1": g.nyu, "du3": g.nyu,
+            "u2": g.nyv, "nu2": g.nyv, "du2": g.nyv,
+            "p": g.nyp, "div": g.nyp, "psi": g.nyp}[name]
+
+
+class Channel:
+    """One channel on one GPU, driven through the C ABI."""
+
+    def __init__(self, setup: ChannelSetup, device: int = 0, precision: Optional[str] = None):
+        self.setup = setup
+        self.lib = capi.load()
+        self._keep = []
+        cfg = setup.cfg if precision is None else setup.cfg.with_(precision=precision)
+        self.cfg = cfg
+        c = capi.make_config(cfg, setup.grid, setup.dt, self._keep)
+        ibu = capi.make_iblist(setup.ibu, self._keep)
+        ibv = capi.make_iblist(setup.ibv, self._keep)
+        ctx = C.c_void_p()
+        st = self.lib.cfd_create(C.byref(c), C.byref(ibu) if ibu else None,
+                                 C.byref(ibv) if ibv else None, device, C.byref(ctx))
+        if st != capi.CFD_OK:
+            msg = self.lib.cfd_last_error(ctx).decode() if ctx else ""
+            if ctx:
+                self.lib.cfd_destroy(ctx)
+            raise capi.CfdError(f"cfd_create failed: {capi.ERRORS.get(st, st)}: {msg}")
+        self.ctx = ctx
+
+    # -- lifetime -----------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.cfd_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st, what):
+        capi.check(self.lib, self.ctx, st, what)
+
+    # -- state ----------------------------------------------------------------------------
+    def upload(self, name: str, arr: np.ndarray, layout: int = capi.LAYOUT_REF):
+        a = np.ascontiguousarray(arr, dtype=np.complex128)
+        self._chk(self.lib.cfd_upload_field(self.ctx, capi.FIELDS[name],
+                                            a.ctypes.data_as(C.POINTER(C.c_double)), layout),
+                  f"upload {name}")
+        self.synchronize()
+
+    def download(self, name: str, layout: int = capi.LAYOUT_REF) -> np.ndarray:
+        n = field_planes(self.setup, name)
+        out = np.empty((self.cfg.ncol, n) if layout == capi.LAYOUT_REF else (n, self.cfg.ncol),
+                       np.complex128)
+        self._chk(self.lib.cfd_download_field(self.ctx, capi.FIELDS[name],
+                                              out.ctypes.data_as(C.POINTER(C.c_double)), layout),
+                  f"download {name}")
+        self.synchronize()
+        return out
+
+    def upload_state(self, state=None):
+        st = state if state is not None else self.setup.state()
+        for k in ("u1", "u2", "u3", "p"):
+            self.upload(k, st[k])
+
+    def download_state(self):
+        return {k: self.download(k) for k in ("u1", "u2", "u3", "p")}
+
+    def synchronize(self):
+        self._chk(self.lib.cfd_synchronize(self.ctx), "synchronize")
+
+    def device_ptr(self, name: str) -> int:
+        p = C.c_void_p()
+        self._chk(self.lib.cfd_field_device_ptr(self.ctx, capi.FIELDS[name], C.byref(p)), "ptr")
+        return p.value
+
+    def set_stream(self, stream_handle: int):
+        self._chk(self.lib.cfd_set_stream(self.ctx, C.c_void_p(stream_handle)), "set_stream")
+
+    # -- the step (littleharsh.f90:163-196) -----------------------------------------------
+    def rhs0(self, krk: int):
+        self._chk(self.lib.cfd_rhs0(self.ctx, krk), "rhs0")
+
+    def nonlinear(self, krk: int):
+        self._chk(self.lib.cfd_nonlinear(self.ctx, krk), "nonlinear")
+
+    def solve_uvw(self, krk: int):
+        self._chk(self.lib.cfd_solve_uvw(self.ctx, krk), "solve_uvw")
+
+    def meanflow(self, krk: int):
+        self._chk(self.lib.cfd_meanflow(self.ctx, krk), "meanflow")
+
+    def solve_p(self, krk: int):
+        self._chk(self.lib.cfd_solve_p(self.ctx, krk), "solve_p")
+
+    def vcorr(self, krk: int):
+        self._chk(self.lib.cfd_vcorr(self.ctx, krk), "vcorr")
+
+    def rk_substep(self, krk: int):
+        self._chk(self.lib.cfd_rk_substep(self.ctx, krk), "rk_substep")
+
+    def step(self, nsteps: int = 1):
+        self._chk(self.lib.cfd_step(self.ctx, nsteps), "step")
+
+    def scalars(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self._chk(self.lib.cfd_get_scalars(self.ctx, C.byref(a), C.byref(b), C.byref(c)),
+                  "scalars")
+        return {"mpgx": a.value, "qx": b.value, "dgx": c.value}
+
+    def divergence_max(self) -> float:
+        e = C.c_double()
+        self._chk(self.lib.cfd_divergence_max(self.ctx, C.byref(e)), "divergence_max")
+        return e.value
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._chk(self.lib.cfd_launch_count(self.ctx, C.byref(n)), "launch_count")
+        return n.value

@@ -1,0 +1,948 @@
+// cfd_capi.cu - C ABI (include/cfd_b200.h) of the B200 hot path: context set-up,
+// device buffers, kernel orchestration of one RK3 substep, CUDA-graph replay of whole
+// steps, layout conversion for the reference's f(j,column) arrays, and the reference's
+// FFT entry points on device memory.
+//
+// Build: nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo -shared -Xcompiler -fPIC
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cfd_b200.h"
+#include "channel_kernels.cuh"
+
+using namespace cfd;
+
+#define CFD_VERSION_STR "cfd_b200 0.1.0 (sm_100a)"
+
+namespace {
+
+const double kRKa[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+const double kRKb[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+const double kRKg[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+const double kRKc[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+const double kRKd[3] = {8.0 / 15.0, 2.0 / 15.0, 1.0 / 3.0};
+
+bool fft_plan(int n, FFTDesc& d) {
+    d.n = n;
+    d.nrad = 0;
+    int m = n;
+    while (m % 4 == 0 && d.nrad < 10) { d.rad[d.nrad++] = 4; m /= 4; }
+    while (m % 2 == 0 && d.nrad < 10) { d.rad[d.nrad++] = 2; m /= 2; }
+    while (m % 3 == 0 && d.nrad < 10) { d.rad[d.nrad++] = 3; m /= 3; }
+    return m == 1 && n >= 2;
+}
+
+struct IBDev {
+    int n = 0;
+    int npl = 0;
+    int* idx = nullptr;
+    double* w = nullptr;
+    int* planes = nullptr;
+    int* slot_of_j = nullptr;
+    std::vector<int> h_planes;
+};
+
+}  // namespace
+
+struct cfd_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    Dims d{};
+    Geo g{};
+    int ny = 0, dsty = 0;
+    int precision = CFD_PREC_FP64;
+    double re = 0, alp = 0, bet = 0, dt = 0, qxt = 0, mpgx0 = 0, mean_diag = 0;
+    int ctpress = 1;
+    double* geo = nullptr;
+    // fields
+    double2 *u1 = nullptr, *u2 = nullptr, *u3 = nullptr, *p = nullptr, *psi = nullptr, *div = nullptr;
+    double2 *du1 = nullptr, *du2 = nullptr, *du3 = nullptr;
+    void *Nu1 = nullptr, *Nu2 = nullptr, *Nu3 = nullptr;
+    void* H[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* S[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* cs = nullptr;
+    double* scal = nullptr;
+    double* mf_work = nullptr;
+    double2* stage0 = nullptr;
+    double2* stage1 = nullptr;
+    double* part = nullptr;
+    int npart = 0;
+    IBDev ibu, ibv;
+    void* Hib = nullptr;
+    void* phys = nullptr;
+    // FFT
+    FFTDesc fx{}, fz{};
+    double2 *twx_d = nullptr, *twz_d = nullptr;
+    float2 *twx_f = nullptr, *twz_f = nullptr;
+    int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
+    bool state_loaded = false;
+    // graph of one RK3 step
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int64_t graph_launches = 0;
+    int64_t launches = 0;
+    bool capturing = false;
+    bool profiling = false;
+    cudaEvent_t prof_last = nullptr;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> prof;
+    std::string err;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+int fail(cfd_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+int cuda_check(cfd_ctx* c, cudaError_t e, const char* what) {
+    if (e != cudaSuccess) return fail(c, CFD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return CFD_OK;
+}
+
+#define CK(call)                                                   \
+    do {                                                           \
+        int _s = cuda_check(c, (call), #call);                     \
+        if (_s != CFD_OK) return _s;                               \
+    } while (0)
+
+int launched(cfd_ctx* c, const char* name) {
+    c->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(c, CFD_ERR_CUDA, "launch %s: %s", name, cudaGetErrorString(e));
+    if (c->profiling && !c->capturing) {
+        cudaEvent_t ev;
+        if (cudaEventCreate(&ev) == cudaSuccess) {
+            cudaEventRecord(ev, c->stream);
+            c->prof.push_back({name, {c->prof_last, ev}});
+            c->prof_last = ev;
+        }
+    }
+    return CFD_OK;
+}
+
+// start event of the next profiled launch: recorded right before it is enqueued
+void prof_mark(cfd_ctx* c) {
+    if (c->profiling && !c->capturing) {
+        cudaEvent_t ev;
+        if (cudaEventCreate(&ev) == cudaSuccess) {
+            cudaEventRecord(ev, c->stream);
+            c->prof_last = ev;
+            c->prof.push_back({"", {ev, ev}});
+        }
+    }
+}
+
+#define LK(name)                                    \
+    do {                                            \
+        int _s = launched(c, name);                 \
+        if (_s != CFD_OK) return _s;                \
+    } while (0)
+
+template <typename T>
+int dalloc(cfd_ctx* c, T** p, size_t n) {
+    void* q = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    if (e != cudaSuccess) return fail(c, CFD_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    c->allocs.push_back(q);
+    *p = (T*)q;
+    return CFD_OK;
+}
+
+#define AL(ptr, type, n)                                     \
+    do {                                                     \
+        int _s = dalloc<type>(c, (type**)&(ptr), (n));       \
+        if (_s != CFD_OK) return _s;                         \
+    } while (0)
+
+size_t zsmem(int n, int CH, size_t esz) { return (size_t)(2 * n * CH + n) * esz; }
+
+// ---------------------------------------------------------------------------------------
+template <typename T2>
+int set_smem_attrs(cfd_ctx* c) {
+    const size_t e = sizeof(T2);
+    const int n2 = c->d.ngal2, n1 = c->d.ngal1;
+    size_t sz = zsmem(n2, c->CHz, e);
+    size_t sx = (size_t)(2 * (2 * c->RWx) * n1 + n1) * e;
+    size_t si = (size_t)(2 * c->RWib * n1 + n1) * e;
+    size_t sf = (size_t)(2 * (c->RWibf / 2) * n1 + n1) * e;
+    CK(cudaFuncSetAttribute(k_zinv<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
+    CK(cudaFuncSetAttribute(k_zfwd<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
+    CK(cudaFuncSetAttribute(k_ib_zinv<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
+    CK(cudaFuncSetAttribute(k_ib_zfwd<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
+    CK(cudaFuncSetAttribute(k_xline<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx));
+    CK(cudaFuncSetAttribute(k_ib_xinv<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)si));
+    CK(cudaFuncSetAttribute(k_ib_xfwd<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf));
+    return CFD_OK;
+}
+
+template <typename T2> const T2* twx(cfd_ctx* c);
+template <typename T2> const T2* twz(cfd_ctx* c);
+template <> const double2* twx<double2>(cfd_ctx* c) { return c->twx_d; }
+template <> const double2* twz<double2>(cfd_ctx* c) { return c->twz_d; }
+template <> const float2* twx<float2>(cfd_ctx* c) { return c->twx_f; }
+template <> const float2* twz<float2>(cfd_ctx* c) { return c->twz_f; }
+
+RKCoef coef(cfd_ctx* c, int krk) {
+    RKCoef k;
+    const int r = krk - 1;
+    k.C1 = kRKa[r] / c->re;
+    k.C2 = -kRKc[r];
+    k.dRK = kRKd[r];
+    k.mg = -kRKg[r];
+    k.dt = c->dt;
+    k.krk = krk;
+    return k;
+}
+
+// nonlinear passes 1-3 (FOU3D.f90:79-155)
+template <typename T2>
+int nl_transforms(cfd_ctx* c) {
+    const Dims& d = c->d;
+    const int CH = c->CHz;
+    const size_t e = sizeof(T2);
+    dim3 gz((d.nkx + CH - 1) / CH, d.nslot, 3);
+    prof_mark(c);
+    k_zinv<T2><<<gz, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0], (T2*)c->H[1],
+                                                             (T2*)c->H[2], c->fz, twz<T2>(c), CH);
+    LK("k_zinv");
+    dim3 gx(d.ngal2 / c->RWx, d.nslot);
+    prof_mark(c);
+    k_xline<T2><<<gx, 256, (size_t)(2 * (2 * c->RWx) * d.ngal1 + d.ngal1) * e, c->stream>>>(
+        d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], c->fx, twx<T2>(c), c->RWx);
+    LK("k_xline");
+    dim3 gf((d.nkx + CH - 1) / CH, d.nslot, 4);
+    prof_mark(c);
+    k_zfwd<T2><<<gf, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
+                                                             (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2], (T2*)c->S[3],
+                                                             c->fz, twz<T2>(c), CH);
+    LK("k_zfwd");
+    return CFD_OK;
+}
+
+template <typename T2, int MODE>
+int rhs_kernel(cfd_ctx* c, int krk) {
+    const Dims& d = c->d;
+    dim3 gb((d.ncol + 255) / 256);
+    prof_mark(c);
+    k_rhs<T2, MODE><<<gb, 256, 0, c->stream>>>(d, c->g, coef(c, krk), c->scal, c->u1, c->u2, c->u3, c->p, (T2*)c->Nu1,
+                                               (T2*)c->Nu2, (T2*)c->Nu3, c->du1, c->du2, c->du3, (const T2*)c->S[0],
+                                               (const T2*)c->S[1], (const T2*)c->S[2], (const T2*)c->S[3]);
+    LK("k_rhs");
+    return CFD_OK;
+}
+
+// immersed_boundaries_U (u1,u3) and immersed_boundaries_V (u2)
+template <typename T2>
+int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2* u_a, double2* rhs_b, double2* u_b) {
+    if (ib.npl == 0) return CFD_OK;
+    using R = decltype(T2::x);
+    const Dims& d = c->d;
+    const int CH = c->CHz;
+    const size_t e = sizeof(T2);
+    IBSrc src;
+    src.f[0] = rhs_a; src.f[1] = u_a; src.f[2] = rhs_b; src.f[3] = u_b;
+    IBDst dst;
+    dst.f[0] = rhs_a; dst.f[1] = rhs_b;
+    dim3 g1((d.nkx + CH - 1) / CH, ib.npl, 2 * nb);
+    prof_mark(c);
+    k_ib_zinv<T2><<<g1, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib, c->fz,
+                                                                twz<T2>(c), CH);
+    LK("k_ib_zinv");
+    dim3 g2(d.ngal2 / c->RWib, ib.npl, nb);
+    prof_mark(c);
+    k_ib_xinv<T2><<<g2, 256, (size_t)(2 * c->RWib * d.ngal1 + d.ngal1) * e, c->stream>>>(d, (T2*)c->Hib, ib.npl, (R*)c->phys,
+                                                                                      c->fx, twx<T2>(c), c->RWib);
+    LK("k_ib_xinv");
+    if (ib.n > 0) {
+        dim3 g3((ib.n + 255) / 256, nb);
+        prof_mark(c);
+        k_ib_force<R><<<g3, 256, 0, c->stream>>>(d, ib.idx, ib.w, ib.n, ib.slot_of_j, j0, ib.npl, (R*)c->phys);
+        LK("k_ib_force");
+    }
+    dim3 g4(d.ngal2 / c->RWibf, ib.npl, nb);
+    prof_mark(c);
+    k_ib_xfwd<T2><<<g4, 256, (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * e, c->stream>>>(
+        d, (T2*)c->Hib, ib.npl, (const R*)c->phys, c->fx, twx<T2>(c), c->RWibf);
+    LK("k_ib_xfwd");
+    dim3 g5((d.nkx + CH - 1) / CH, ib.npl, nb);
+    prof_mark(c);
+    k_ib_zfwd<T2><<<g5, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0, ib.planes, c->fz,
+                                                                twz<T2>(c), CH);
+    LK("k_ib_zfwd");
+    return CFD_OK;
+}
+
+template <typename T2>
+int ib_all(cfd_ctx* c) {
+    int s = ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3);
+    if (s != CFD_OK) return s;
+    return ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr);
+}
+
+int solve_kernel(cfd_ctx* c, int krk) {
+    const Dims& d = c->d;
+    const double beta = kRKb[krk - 1] * c->dt / c->re;
+    dim3 gb((d.ncol + 255) / 256);
+    prof_mark(c);
+    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, 1, 1);
+    LK("k_solve_uvw");
+    return CFD_OK;
+}
+
+int meanflow_kernel(cfd_ctx* c, int krk) {
+    const double beta = kRKb[krk - 1] * c->dt / c->re;
+    const double bdt = -kRKd[krk - 1] * c->dt;
+    prof_mark(c);
+    k_meanflow<<<1, 32, 0, c->stream>>>(c->d, c->g, beta, bdt, c->qxt, c->ctpress, c->u1, c->scal, c->mf_work);
+    LK("k_meanflow");
+    return CFD_OK;
+}
+
+int solvep_kernel(cfd_ctx* c, int krk, bool with_div) {
+    const Dims& d = c->d;
+    const double dtirk = (1.0 / c->dt) / (kRKa[krk - 1] + kRKb[krk - 1]);
+    dim3 gb((d.ncol + 255) / 256);
+    prof_mark(c);
+    k_solve_p<<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, with_div ? c->div : nullptr,
+                                         c->cs, c->mean_diag);
+    LK("k_solve_p");
+    return CFD_OK;
+}
+
+int vcorr_kernel(cfd_ctx* c, int krk, bool with_div) {
+    const Dims& d = c->d;
+    const double dtrk = c->dt * (kRKa[krk - 1] + kRKb[krk - 1]);
+    dim3 gb((d.ncol + 255) / 256);
+    prof_mark(c);
+    k_vcorr<<<gb, 256, 0, c->stream>>>(d, c->g, dtrk, c->u1, c->u2, c->u3, c->psi, with_div ? c->div : nullptr);
+    LK("k_vcorr");
+    return CFD_OK;
+}
+
+template <typename T2>
+int substep(cfd_ctx* c, int krk) {
+    int s;
+    if ((s = nl_transforms<T2>(c)) != CFD_OK) return s;
+    if ((s = rhs_kernel<T2, 7>(c, krk)) != CFD_OK) return s;
+    if ((s = ib_all<T2>(c)) != CFD_OK) return s;
+    if ((s = solve_kernel(c, krk)) != CFD_OK) return s;
+    if (c->ctpress == 0 && (s = meanflow_kernel(c, krk)) != CFD_OK) return s;
+    if ((s = solvep_kernel(c, krk, false)) != CFD_OK) return s;
+    return vcorr_kernel(c, krk, false);
+}
+
+int substep_any(cfd_ctx* c, int krk) {
+    return c->precision == CFD_PREC_MIXED ? substep<float2>(c, krk) : substep<double2>(c, krk);
+}
+
+int check_krk(cfd_ctx* c, int krk) {
+    if (!c) return CFD_ERR_ARG;
+    if (krk < 1 || krk > 3) return fail(c, CFD_ERR_ARG, "krk must be 1..3 (got %d)", krk);
+    if (!c->state_loaded) return fail(c, CFD_ERR_STATE, "state not uploaded");
+    return CFD_OK;
+}
+
+struct FieldInfo {
+    void* ptr;
+    int j0;
+    int nplanes;
+    bool single;  // stored as float2
+};
+
+bool field_info(const cfd_ctx* c, int f, FieldInfo& fi) {
+    const Dims& d = c->d;
+    const bool mixed = c->precision == CFD_PREC_MIXED;
+    switch (f) {
+        case CFD_FIELD_U1: fi = {c->u1, d.ju0, d.nyu, false}; return true;
+        case CFD_FIELD_U2: fi = {c->u2, d.jv0, d.nyv, false}; return true;
+        case CFD_FIELD_U3: fi = {c->u3, d.ju0, d.nyu, false}; return true;
+        case CFD_FIELD_P: fi = {c->p, d.jp0, d.nyp, false}; return true;
+        case CFD_FIELD_NU1: fi = {c->Nu1, d.ju0, d.nyu, mixed}; return true;
+        case CFD_FIELD_NU2: fi = {c->Nu2, d.jv0, d.nyv, mixed}; return true;
+        case CFD_FIELD_NU3: fi = {c->Nu3, d.ju0, d.nyu, mixed}; return true;
+        case CFD_FIELD_DIV: fi = {c->div, d.jp0, d.nyp, false}; return true;
+        case CFD_FIELD_PSI: fi = {c->psi, d.jp0, d.nyp, false}; return true;
+        case CFD_FIELD_DU1: fi = {c->du1, d.ju0, d.nyu, false}; return true;
+        case CFD_FIELD_DU2: fi = {c->du2, d.jv0, d.nyv, false}; return true;
+        case CFD_FIELD_DU3: fi = {c->du3, d.ju0, d.nyu, false}; return true;
+    }
+    return false;
+}
+
+__global__ void k_d2f(const double2* __restrict__ a, float2* __restrict__ b, size_t n) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        b[t] = make_float2((float)a[t].x, (float)a[t].y);
+}
+__global__ void k_f2d(const float2* __restrict__ a, double2* __restrict__ b, size_t n) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        b[t] = make_double2((double)a[t].x, (double)a[t].y);
+}
+
+void destroy_graph(cfd_ctx* c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+}
+
+int fill_tw(cfd_ctx* c, int n, double2** dd, float2** df) {
+    std::vector<double2> hd(n);
+    std::vector<float2> hf(n);
+    const long double PI_L = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < n; ++k) {
+        long double a = -2.0L * PI_L * (long double)k / (long double)n;
+        long double cr = cosl(a), ci = sinl(a);
+        hd[k] = make_double2((double)cr, (double)ci);
+        hf[k] = make_float2((float)cr, (float)ci);
+    }
+    AL(*dd, double2, n);
+    AL(*df, float2, n);
+    CK(cudaMemcpy(*dd, hd.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(*df, hf.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    return CFD_OK;
+}
+
+int setup_ib(cfd_ctx* c, const cfd_ib_list* l, int j0, int j1, IBDev& ib, const char* name) {
+    if (!l) return CFD_OK;
+    if (l->n < 0) return fail(c, CFD_ERR_ARG, "%s: negative point count", name);
+    if (l->n > 0 && (!l->idx || !l->w)) return fail(c, CFD_ERR_ARG, "%s: null list arrays", name);
+    // round-trip planes: interior planes inside either range (modes_to_planes_dU, FOU3D.f90:1318-1319)
+    std::vector<int> slot(j1 - j0 + 1, -1);
+    for (int s = 0; s < 2; ++s)
+        for (int j = std::max(l->jlo[s], j0 + 1); j <= std::min(l->jhi[s], j1 - 1); ++j)
+            if (slot[j - j0] < 0) {
+                slot[j - j0] = (int)ib.h_planes.size();
+                ib.h_planes.push_back(j);
+            }
+    ib.npl = (int)ib.h_planes.size();
+    const int ng1 = c->d.ngal1, ng2 = c->d.ngal2;
+    for (int p = 0; p < l->n; ++p) {
+        const int32_t* id = l->idx + 9 * (size_t)p;
+        for (int t = 0; t < 3; ++t) {
+            const int i = id[3 * t], k = id[3 * t + 1], j = id[3 * t + 2];
+            if (i < 1 || i > ng1 || k < 1 || k > ng2)
+                return fail(c, CFD_ERR_ARG, "%s: point %d has (i,k)=(%d,%d) outside 1..%d x 1..%d", name, p, i, k, ng1, ng2);
+            if (j < j0 || j > j1 || slot[j - j0] < 0)
+                return fail(c, CFD_ERR_ARG, "%s: point %d references plane %d outside the round-trip ranges", name, p, j);
+        }
+        if (p > 0) {
+            const int32_t* pv = id - 9;
+            const long a = ((long)pv[2] * ng2 + pv[1]) * ng1 + pv[0], b = ((long)id[2] * ng2 + id[1]) * ng1 + id[0];
+            if (b < a) return fail(c, CFD_ERR_ARG, "%s: points must be sorted by (j,k,i) (point %d)", name, p);
+        }
+    }
+    ib.n = l->n;
+    AL(ib.idx, int, 9 * (size_t)l->n);
+    AL(ib.w, double, 3 * (size_t)l->n);
+    AL(ib.planes, int, ib.npl);
+    AL(ib.slot_of_j, int, slot.size());
+    if (l->n > 0) {
+        CK(cudaMemcpy(ib.idx, l->idx, 9 * sizeof(int) * (size_t)l->n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ib.w, l->w, 3 * sizeof(double) * (size_t)l->n, cudaMemcpyHostToDevice));
+    }
+    if (ib.npl > 0) CK(cudaMemcpy(ib.planes, ib.h_planes.data(), sizeof(int) * ib.npl, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ib.slot_of_j, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
+    return CFD_OK;
+}
+
+int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list* ibv, int device, cfd_ctx* c) {
+    if (!cfg || !cfg->yu || !cfg->yv || !cfg->dthdyu || !cfg->dthdyv || !cfg->dyu2i || !cfg->dyv2i)
+        return fail(c, CFD_ERR_ARG, "null config or grid array");
+    if (cfg->precision != CFD_PREC_FP64 && cfg->precision != CFD_PREC_MIXED)
+        return fail(c, CFD_ERR_ARG, "precision must be CFD_PREC_FP64 or CFD_PREC_MIXED");
+    if (cfg->flag_ctpress != 0 && cfg->flag_ctpress != 1) return fail(c, CFD_ERR_ARG, "flag_ctpress must be 0 or 1");
+    if (!(cfg->re > 0) || !(cfg->dt > 0)) return fail(c, CFD_ERR_ARG, "Re and dt must be positive");
+    FFTDesc fx, fz;
+    if (!fft_plan(cfg->ngal1, fx) || !fft_plan(cfg->ngal2, fz) || cfg->ngal1 < 6 || cfg->ngal2 < 6 || (cfg->ngal1 & 1) ||
+        (cfg->ngal2 & 1))
+        return fail(c, CFD_ERR_SIZE, "Ngal1=%d, Ngal2=%d must be even 2^a*3^b >= 6 (rft_buff.f:303-310)", cfg->ngal1, cfg->ngal2);
+    if (cfg->ngal1 > 1536 || cfg->ngal2 > 1536) return fail(c, CFD_ERR_SIZE, "Ngal above 1536 not supported");
+    if (cfg->ny < 4 || cfg->dsty < 0) return fail(c, CFD_ERR_SIZE, "ny must be >= 4 and dsty >= 0");
+    c->device = device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    c->fx = fx;
+    c->fz = fz;
+    Dims& d = c->d;
+    d.ngal1 = cfg->ngal1; d.ngal2 = cfg->ngal2;
+    d.n1 = 2 * (cfg->ngal1 / 3); d.n2 = 2 * (cfg->ngal2 / 3);
+    d.nkx = d.n1 / 2 + 1; d.ncol = d.nkx * d.n2;
+    c->ny = cfg->ny; c->dsty = cfg->dsty;
+    d.ny = cfg->ny;
+    d.ju0 = -cfg->dsty; d.ju1 = cfg->ny + cfg->dsty;
+    d.jv0 = -cfg->dsty; d.jv1 = cfg->ny + cfg->dsty - 1;
+    d.jp0 = -cfg->dsty + 1; d.jp1 = cfg->ny + cfg->dsty - 1;
+    d.nyu = d.ju1 - d.ju0 + 1; d.nyv = d.jv1 - d.jv0 + 1; d.nyp = d.jp1 - d.jp0 + 1;
+    d.nslot = d.nyu + d.nyv;
+    c->precision = cfg->precision;
+    c->re = cfg->re; c->alp = cfg->alp; c->bet = cfg->bet; c->dt = cfg->dt; c->qxt = cfg->qxt;
+    c->mpgx0 = cfg->mpgx; c->ctpress = cfg->flag_ctpress;
+
+    // grid + wavenumbers in one allocation
+    const int nyu = d.nyu, nyv = d.nyv;
+    std::vector<double> hg;
+    auto push = [&](const double* a, size_t n) { hg.insert(hg.end(), a, a + n); };
+    push(cfg->yu, nyu); push(cfg->yv, nyv); push(cfg->dthdyu, nyu); push(cfg->dthdyv, nyv);
+    push(cfg->dyu2i, 3 * (size_t)nyu); push(cfg->dyv2i, 3 * (size_t)nyv);
+    const size_t okx = hg.size();
+    for (int i = 0; i < d.nkx; ++i) hg.push_back(cfg->alp * i);
+    const size_t okz = hg.size();
+    for (int q = 0; q < d.n2; ++q) hg.push_back(q < d.n2 / 2 ? cfg->bet * q : -cfg->bet * (d.n2 - q));
+    for (double v : hg)
+        if (!std::isfinite(v)) return fail(c, CFD_ERR_ARG, "non-finite grid value");
+    AL(c->geo, double, hg.size());
+    CK(cudaMemcpy(c->geo, hg.data(), hg.size() * sizeof(double), cudaMemcpyHostToDevice));
+    Geo& g = c->g;
+    g.yu = c->geo;
+    g.yv = g.yu + nyu;
+    g.dthdyu = g.yv + nyv;
+    g.dthdyv = g.dthdyu + nyu;
+    g.dyu2i = g.dthdyv + nyv;
+    g.dyv2i = g.dyu2i + 3 * nyu;
+    g.kx = c->geo + okx;
+    g.kz = c->geo + okz;
+    auto YU = [&](int j) { return cfg->yu[j - d.ju0]; };
+    auto YV = [&](int j) { return cfg->yv[j - d.jv0]; };
+    g.gwb = -(YV(d.jv0) - YU(d.ju0)) / (YV(d.jv0) - YU(d.ju0 + 1));
+    g.gwt = (YU(d.ju1) - YV(d.jv1)) / (YV(d.jv1) - YU(d.ju1 - 1));
+    g.gwib = (YU(d.ju0) - YU(d.ju0 + 1)) / (YV(d.jv0) - YU(d.ju0 + 1));
+    g.gwit = (YU(d.ju1) - YU(d.ju1 - 1)) / (YV(d.jv1) - YU(d.ju1 - 1));
+    // mean-mode Poisson row (tridLU_3D_IB.f90:468-474): 1/(yu(2)-yu(1))^2
+    if (d.ju0 > 1 || d.ju1 < 2) return fail(c, CFD_ERR_SIZE, "grid too small");
+    c->mean_diag = 1.0 / ((YU(2) - YU(1)) * (YU(2) - YU(1)));
+
+    // launch shapes
+    const bool mixed = c->precision == CFD_PREC_MIXED;
+    const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
+    const size_t budget = 110 * 1024;
+    c->CHz = 8;
+    while (c->CHz > 1 && zsmem(d.ngal2, c->CHz, esz) > budget) c->CHz /= 2;
+    c->RWx = 8;
+    while (c->RWx > 1 && ((d.ngal2 % c->RWx) || (size_t)(2 * (2 * c->RWx) * d.ngal1 + d.ngal1) * esz > budget)) c->RWx /= 2;
+    c->RWib = 8;
+    while (c->RWib > 1 && ((d.ngal2 % c->RWib) || (size_t)(2 * c->RWib * d.ngal1 + d.ngal1) * esz > budget)) c->RWib /= 2;
+    c->RWibf = 8;
+    while (c->RWibf > 2 && ((d.ngal2 % c->RWibf) || (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * esz > budget))
+        c->RWibf /= 2;
+    if (d.ngal2 % c->RWibf) return fail(c, CFD_ERR_SIZE, "Ngal2 must be even");
+    int s = mixed ? set_smem_attrs<float2>(c) : set_smem_attrs<double2>(c);
+    if (s != CFD_OK) return s;
+    if ((s = fill_tw(c, d.ngal1, &c->twx_d, &c->twx_f)) != CFD_OK) return s;
+    if ((s = fill_tw(c, d.ngal2, &c->twz_d, &c->twz_f)) != CFD_OK) return s;
+
+    // fields
+    const size_t nc = d.ncol;
+    AL(c->u1, double2, nc * nyu); AL(c->u3, double2, nc * nyu); AL(c->u2, double2, nc * nyv);
+    AL(c->p, double2, nc * d.nyp); AL(c->psi, double2, nc * d.nyp); AL(c->div, double2, nc * d.nyp);
+    AL(c->du1, double2, nc * nyu); AL(c->du3, double2, nc * nyu); AL(c->du2, double2, nc * nyv);
+    if (mixed) {
+        AL(c->Nu1, float2, nc * nyu); AL(c->Nu3, float2, nc * nyu); AL(c->Nu2, float2, nc * nyv);
+    } else {
+        AL(c->Nu1, double2, nc * nyu); AL(c->Nu3, double2, nc * nyu); AL(c->Nu2, double2, nc * nyv);
+    }
+    const size_t hsz = (size_t)d.nslot * d.ngal2 * d.nkx;
+    for (int k = 0; k < 4; ++k) {
+        if (mixed) { AL(c->H[k], float2, hsz); AL(c->S[k], float2, (size_t)d.nslot * nc); }
+        else { AL(c->H[k], double2, hsz); AL(c->S[k], double2, (size_t)d.nslot * nc); }
+    }
+    AL(c->cs, double, nc * nyu);
+    AL(c->scal, double, 4);
+    AL(c->mf_work, double, 4 * (size_t)(cfg->ny + 4));
+    AL(c->stage0, double2, nc * nyu);
+    AL(c->stage1, double2, nc * nyu);
+    c->npart = 1024;
+    AL(c->part, double, c->npart);
+    CK(cudaMemset(c->Nu1, 0, nc * nyu * esz));
+    CK(cudaMemset(c->Nu3, 0, nc * nyu * esz));
+    CK(cudaMemset(c->Nu2, 0, nc * nyv * esz));
+    for (double2* f : {c->u1, c->u3, c->du1, c->du3}) CK(cudaMemset(f, 0, nc * nyu * sizeof(double2)));
+    for (double2* f : {c->u2, c->du2}) CK(cudaMemset(f, 0, nc * nyv * sizeof(double2)));
+    for (double2* f : {c->p, c->psi, c->div}) CK(cudaMemset(f, 0, nc * d.nyp * sizeof(double2)));
+    double sc[4] = {cfg->mpgx, 0.0, 0.0, 0.0};
+    CK(cudaMemcpy(c->scal, sc, sizeof(sc), cudaMemcpyHostToDevice));
+
+    // immersed boundaries
+    if ((s = setup_ib(c, ibu, d.ju0, d.ju1, c->ibu, "ibu")) != CFD_OK) return s;
+    if ((s = setup_ib(c, ibv, d.jv0, d.jv1, c->ibv, "ibv")) != CFD_OK) return s;
+    const size_t nibp = std::max((size_t)4 * c->ibu.npl, (size_t)2 * c->ibv.npl);
+    if (nibp > 0) {
+        if (mixed) {
+            AL(c->Hib, float2, nibp * d.ngal2 * d.nkx);
+            AL(c->phys, float, nibp * d.ngal2 * d.ngal1);
+        } else {
+            AL(c->Hib, double2, nibp * d.ngal2 * d.nkx);
+            AL(c->phys, double, nibp * d.ngal2 * d.ngal1);
+        }
+    }
+    CK(cudaDeviceSynchronize());
+    return CFD_OK;
+}
+
+int fft_generic_smem(int n, int CH) { return (2 * n * CH + n) * (int)sizeof(double2); }
+
+int strided_cft(cfd_ctx* c, double* dptr, int n, int ise, int isa, int m, long long bstride, int nb, int iopt) {
+    FFTDesc fd;
+    if (!fft_plan(n, fd)) return fail(c, CFD_ERR_SIZE, "length %d not 2^a*3^b", n);
+    const double2* tw = n == c->d.ngal2 ? c->twz_d : (n == c->d.ngal1 ? c->twx_d : nullptr);
+    if (!tw) return fail(c, CFD_ERR_SIZE, "cft length must be Ngal2 or Ngal1");
+    const int CH = 8;
+    const int sm = fft_generic_smem(n, CH);
+    CK(cudaFuncSetAttribute(k_cft_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    dim3 grid((m + CH - 1) / CH, nb);
+    prof_mark(c);
+    k_cft_strided<<<grid, 256, sm, c->stream>>>(dptr, ise, isa, m, bstride, fd, tw, iopt, CH);
+    LK("k_cft_strided");
+    return CFD_OK;
+}
+
+int strided_rft(cfd_ctx* c, double* dptr, int n, int isa, int m, long long bstride, int nb, int iopt) {
+    FFTDesc fd;
+    if (!fft_plan(n, fd) || (n & 1)) return fail(c, CFD_ERR_SIZE, "length %d not even 2^a*3^b", n);
+    const double2* tw = n == c->d.ngal1 ? c->twx_d : (n == c->d.ngal2 ? c->twz_d : nullptr);
+    if (!tw) return fail(c, CFD_ERR_SIZE, "rft length must be Ngal1 or Ngal2");
+    const int CH = 8;
+    const int sm = fft_generic_smem(n, CH);
+    CK(cudaFuncSetAttribute(k_rft_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    dim3 grid((m + CH - 1) / CH, nb);
+    prof_mark(c);
+    k_rft_strided<<<grid, 256, sm, c->stream>>>(dptr, isa, m, bstride, fd, tw, iopt, CH);
+    LK("k_rft_strided");
+    return CFD_OK;
+}
+
+}  // namespace
+
+// =======================================================================================
+extern "C" {
+
+const char* cfd_version(void) { return CFD_VERSION_STR; }
+
+const char* cfd_last_error(const cfd_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int cfd_create(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list* ibv, int32_t device, cfd_ctx** out) {
+    if (!out) return CFD_ERR_ARG;
+    *out = nullptr;
+    cfd_ctx* c = new cfd_ctx();
+    int s = create_impl(cfg, ibu, ibv, device, c);
+    *out = c;  // returned even on failure so cfd_last_error can report; caller destroys
+    return s;
+}
+
+int cfd_destroy(cfd_ctx* c) {
+    if (!c) return CFD_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    destroy_graph(c);
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return CFD_OK;
+}
+
+int cfd_set_stream(cfd_ctx* c, void* stream) {
+    if (!c) return CFD_ERR_ARG;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->own_stream;
+    if (s != c->stream) destroy_graph(c);
+    c->stream = s;
+    return CFD_OK;
+}
+
+int cfd_synchronize(cfd_ctx* c) {
+    if (!c) return CFD_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return CFD_OK;
+}
+
+int cfd_field_shape(const cfd_ctx* c, int32_t field, int64_t* ncomplex, int32_t* j0, int32_t* nplanes, int32_t* ncolumns) {
+    if (!c) return CFD_ERR_ARG;
+    FieldInfo fi;
+    if (!field_info(c, field, fi)) return CFD_ERR_ARG;
+    if (ncomplex) *ncomplex = (int64_t)fi.nplanes * c->d.ncol;
+    if (j0) *j0 = fi.j0;
+    if (nplanes) *nplanes = fi.nplanes;
+    if (ncolumns) *ncolumns = c->d.ncol;
+    return CFD_OK;
+}
+
+int cfd_upload_field(cfd_ctx* c, int32_t field, const double* host, int32_t layout) {
+    if (!c || !host) return fail(c, CFD_ERR_ARG, "null argument");
+    FieldInfo fi;
+    if (!field_info(c, field, fi)) return fail(c, CFD_ERR_ARG, "bad field %d", field);
+    if (layout != CFD_LAYOUT_REF && layout != CFD_LAYOUT_PLANE) return fail(c, CFD_ERR_ARG, "bad layout %d", layout);
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)fi.nplanes * c->d.ncol;
+    double2* dst = fi.single ? c->stage1 : (double2*)fi.ptr;
+    if (layout == CFD_LAYOUT_PLANE) {
+        CK(cudaMemcpyAsync(dst, host, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    } else {
+        CK(cudaMemcpyAsync(c->stage0, host, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        dim3 grid((fi.nplanes + 31) / 32, (c->d.ncol + 31) / 32);
+        prof_mark(c);
+        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(c->stage0, dst, c->d.ncol, fi.nplanes);
+        LK("k_transpose");
+    }
+    if (fi.single) {
+        prof_mark(c);
+        k_d2f<<<1024, 256, 0, c->stream>>>(dst, (float2*)fi.ptr, n);
+        LK("k_d2f");
+    }
+    if (field <= CFD_FIELD_P) c->state_loaded = true;
+    return CFD_OK;
+}
+
+int cfd_download_field(cfd_ctx* c, int32_t field, double* host, int32_t layout) {
+    if (!c || !host) return fail(c, CFD_ERR_ARG, "null argument");
+    FieldInfo fi;
+    if (!field_info(c, field, fi)) return fail(c, CFD_ERR_ARG, "bad field %d", field);
+    if (layout != CFD_LAYOUT_REF && layout != CFD_LAYOUT_PLANE) return fail(c, CFD_ERR_ARG, "bad layout %d", layout);
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)fi.nplanes * c->d.ncol;
+    const double2* src = (const double2*)fi.ptr;
+    if (fi.single) {
+        prof_mark(c);
+        k_f2d<<<1024, 256, 0, c->stream>>>((const float2*)fi.ptr, c->stage1, n);
+        LK("k_f2d");
+        src = c->stage1;
+    }
+    if (layout == CFD_LAYOUT_PLANE) {
+        CK(cudaMemcpyAsync(host, src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        dim3 grid((c->d.ncol + 31) / 32, (fi.nplanes + 31) / 32);
+        prof_mark(c);
+        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(src, c->stage0, fi.nplanes, c->d.ncol);
+        LK("k_transpose");
+        CK(cudaMemcpyAsync(host, c->stage0, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    }
+    return CFD_OK;
+}
+
+int cfd_field_device_ptr(cfd_ctx* c, int32_t field, void** dev_ptr) {
+    if (!c || !dev_ptr) return CFD_ERR_ARG;
+    FieldInfo fi;
+    if (!field_info(c, field, fi)) return fail(c, CFD_ERR_ARG, "bad field %d", field);
+    *dev_ptr = fi.ptr;
+    if (field <= CFD_FIELD_P) c->state_loaded = true;
+    return CFD_OK;
+}
+
+int cfd_rhs0(cfd_ctx* c, int32_t krk) {
+    int s = check_krk(c, krk);
+    if (s) return s;
+    return c->precision == CFD_PREC_MIXED ? rhs_kernel<float2, 1>(c, krk) : rhs_kernel<double2, 1>(c, krk);
+}
+
+int cfd_nonlinear(cfd_ctx* c, int32_t krk) {
+    int s = check_krk(c, krk);
+    if (s) return s;
+    if (c->precision == CFD_PREC_MIXED) {
+        if ((s = nl_transforms<float2>(c))) return s;
+        return rhs_kernel<float2, 2>(c, krk);
+    }
+    if ((s = nl_transforms<double2>(c))) return s;
+    return rhs_kernel<double2, 2>(c, krk);
+}
+
+int cfd_solve_uvw(cfd_ctx* c, int32_t krk) {
+    int s = check_krk(c, krk);
+    if (s) return s;
+    if (c->precision == CFD_PREC_MIXED) {
+        if ((s = rhs_kernel<float2, 4>(c, krk))) return s;
+        if ((s = ib_all<float2>(c))) return s;
+    } else {
+        if ((s = rhs_kernel<double2, 4>(c, krk))) return s;
+        if ((s = ib_all<double2>(c))) return s;
+    }
+    return solve_kernel(c, krk);
+}
+
+int cfd_meanflow(cfd_ctx* c, int32_t krk) {
+    int s = check_krk(c, krk);
+    if (s) return s;
+    return meanflow_kernel(c, krk);
+}
+
+int cfd_solve_p(cfd_ctx* c, int32_t krk) {
+    int s = check_krk(c, krk);
+    if (s) return s;
+    return solvep_kernel(c, krk, true);
+}
+
+int cfd_vcorr(cfd_ctx* c, int32_t krk) {
+    int s = check_krk(c, krk);
+    if (s) return s;
+    return vcorr_kernel(c, krk, true);
+}
+
+int cfd_rk_substep(cfd_ctx* c, int32_t krk) {
+    int s = check_krk(c, krk);
+    if (s) return s;
+    return substep_any(c, krk);
+}
+
+int cfd_step(cfd_ctx* c, int32_t nsteps) {
+    int s = check_krk(c, 1);
+    if (s) return s;
+    if (nsteps < 0) return fail(c, CFD_ERR_ARG, "nsteps < 0");
+    CK(cudaSetDevice(c->device));
+    if (!c->gexec) {
+        const int64_t before = c->launches;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->capturing = true;
+        int st = CFD_OK;
+        for (int k = 1; k <= 3 && st == CFD_OK; ++k) st = substep_any(c, k);
+        if (st == CFD_OK && c->ctpress == 1) st = meanflow_kernel(c, 1);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        c->capturing = false;
+        if (st != CFD_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) return fail(c, CFD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        c->graph = graph;
+        CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+        c->graph_launches = c->launches - before;
+        c->launches = before;
+    }
+    for (int n = 0; n < nsteps; ++n) {
+        CK(cudaGraphLaunch(c->gexec, c->stream));
+        c->launches += c->graph_launches;
+    }
+    return CFD_OK;
+}
+
+int cfd_get_scalars(cfd_ctx* c, double* mpgx, double* qx, double* dgx) {
+    if (!c) return CFD_ERR_ARG;
+    double h[4];
+    CK(cudaMemcpyAsync(h, c->scal, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (mpgx) *mpgx = h[0];
+    if (qx) *qx = h[1];
+    if (dgx) *dgx = h[2];
+    return CFD_OK;
+}
+
+int cfd_divergence_max(cfd_ctx* c, double* errmax) {
+    if (!c || !errmax) return CFD_ERR_ARG;
+    const Dims& d = c->d;
+    // recompute div from the current state (divergence, littleharsh.f90:209-244)
+    prof_mark(c);
+    k_divergence<<<(d.ncol + 255) / 256, 256, 0, c->stream>>>(d, c->g, c->u1, c->u2, c->u3, c->div);
+    LK("k_divergence");
+    prof_mark(c);
+    k_absmax<<<c->npart, 256, 0, c->stream>>>(c->div, (size_t)d.ncol * d.nyp, c->part);
+    LK("k_absmax");
+    std::vector<double> h(c->npart);
+    CK(cudaMemcpyAsync(h.data(), c->part, sizeof(double) * c->npart, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double m = 0.0;
+    bool bad = false;
+    for (double v : h) {
+        if (!std::isfinite(v)) bad = true;
+        m = std::max(m, v);
+    }
+    *errmax = bad ? NAN : m;
+    if (bad) return fail(c, CFD_ERR_NONFINITE, "non-finite divergence");
+    return CFD_OK;
+}
+
+int cfd_four_to_phys(cfd_ctx* c, double* planes, int32_t nplanes, int32_t zero_oddball) {
+    if (!c || !planes || nplanes < 0) return fail(c, CFD_ERR_ARG, "bad arguments");
+    const Dims& d = c->d;
+    const long long ps = (long long)(d.ngal1 + 2) * d.ngal2;
+    if (nplanes == 0) return CFD_OK;
+    if (zero_oddball)
+        CK(cudaMemset2DAsync(planes + (size_t)(d.ngal2 / 2) * (d.ngal1 + 2), ps * sizeof(double), 0,
+                             (d.ngal1 + 2) * sizeof(double), nplanes, c->stream));
+    int s = strided_cft(c, planes, d.ngal2, d.ngal1 + 2, 2, d.nkx, ps, nplanes, +1);
+    if (s) return s;
+    return strided_rft(c, planes, d.ngal1, d.ngal1 + 2, d.ngal2, ps, nplanes, +1);
+}
+
+int cfd_phys_to_four(cfd_ctx* c, double* planes, int32_t nplanes) {
+    if (!c || !planes || nplanes < 0) return fail(c, CFD_ERR_ARG, "bad arguments");
+    const Dims& d = c->d;
+    const long long ps = (long long)(d.ngal1 + 2) * d.ngal2;
+    if (nplanes == 0) return CFD_OK;
+    int s = strided_rft(c, planes, d.ngal1, d.ngal1 + 2, d.ngal2, ps, nplanes, -1);
+    if (s) return s;
+    return strided_cft(c, planes, d.ngal2, d.ngal1 + 2, 2, d.nkx, ps, nplanes, -1);
+}
+
+int cfd_rft(cfd_ctx* c, double* cdev, int32_t isa, int32_t m, int32_t iopt) {
+    if (!c || !cdev || m < 0 || isa < c->d.ngal1 + 2) return fail(c, CFD_ERR_ARG, "bad arguments (isa >= Ngal1+2)");
+    if (m == 0) return CFD_OK;
+    return strided_rft(c, cdev, c->d.ngal1, isa, m, 0, 1, iopt);
+}
+
+int cfd_cft(cfd_ctx* c, double* cdev, int32_t ise, int32_t isa, int32_t m, int32_t iopt) {
+    if (!c || !cdev || m < 0 || ise < 2) return fail(c, CFD_ERR_ARG, "bad arguments (ise >= 2)");
+    if (m == 0) return CFD_OK;
+    return strided_cft(c, cdev, c->d.ngal2, ise, isa, m, 0, 1, iopt);
+}
+
+int cfd_profile(cfd_ctx* c, int32_t enable) {
+    if (!c) return CFD_ERR_ARG;
+    c->profiling = enable != 0;
+    return CFD_OK;
+}
+
+int cfd_profile_read(cfd_ctx* c, char* buf, int32_t buflen) {
+    if (!c || !buf || buflen <= 0) return CFD_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<std::string> names;
+    std::vector<double> ms;
+    std::vector<long> calls;
+    std::vector<cudaEvent_t> all;
+    for (auto& r : c->prof) {
+        all.push_back(r.second.second);
+        if (r.first.empty()) continue;
+        float t = 0.f;
+        if (r.second.first && cudaEventElapsedTime(&t, r.second.first, r.second.second) != cudaSuccess) t = 0.f;
+        size_t k = 0;
+        while (k < names.size() && names[k] != r.first) ++k;
+        if (k == names.size()) { names.push_back(r.first); ms.push_back(0.0); calls.push_back(0); }
+        ms[k] += t;
+        calls[k] += 1;
+    }
+    std::sort(all.begin(), all.end());
+    all.erase(std::unique(all.begin(), all.end()), all.end());
+    for (cudaEvent_t e : all) cudaEventDestroy(e);
+    c->prof.clear();
+    c->prof_last = nullptr;
+    std::string out;
+    char line[256];
+    for (size_t k = 0; k < names.size(); ++k) {
+        snprintf(line, sizeof(line), "%s %ld %.6f\n", names[k].c_str(), calls[k], ms[k]);
+        out += line;
+    }
+    strncpy(buf, out.c_str(), (size_t)buflen - 1);
+    buf[buflen - 1] = 0;
+    return CFD_OK;
+}
+
+int cfd_launch_count(const cfd_ctx* c, int64_t* count) {
+    if (!c || !count) return CFD_ERR_ARG;
+    *count = c->launches;
+    return CFD_OK;
+}
+
+}  // extern "C"

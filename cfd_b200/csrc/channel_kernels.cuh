@@ -1,0 +1,954 @@
+// channel_kernels.cuh - sm_100a kernels of one RK3 substep of the LittleHarsh channel DNS.
+//
+// Device layout (HBM): a spectral field is [plane][column] complex, column = q*nkx + i
+// (kx-mode i fastest, then kz-mode q), i.e. every y-plane is a contiguous (N2 x N1/2+1)
+// array.  Thread-per-column kernels that march in y therefore read/write coalesced rows,
+// and per-plane FFT kernels read contiguous planes: the reference's MPI transposes
+// (modes_to_planes_* / planes_to_modes_*, FOU3D.f90:808-906, 1662-2170) disappear into
+// this layout.
+//
+// Nonlinear term (FOU3D.f90:41-259, 1529-1617) in three passes over "half-physical"
+// buffers H[slot][z][kx] (z physical, x still spectral; slot = u-plane or v-plane):
+//   k_zinv  : y-interpolation (interp_u/v) + zero-padded inverse z transform
+//   k_xline : inverse x transform, velocity products, forward x transform (fused)
+//   k_zfwd  : forward z transform + truncation to the N2 retained modes
+// and the column kernel k_rhs forms x/z/y derivatives and the RK right-hand side.
+#pragma once
+
+#include "fft_smem.cuh"
+
+namespace cfd {
+
+struct Dims {
+    int ngal1, ngal2, n1, n2, nkx, ncol;
+    int ju0, ju1, jv0, jv1, jp0, jp1, nyu, nyv, nyp;
+    int nslot;  // nyu + nyv
+    int ny;     // faces from y=-1 to y=1 (input.in ny)
+};
+
+// Grid and wavenumber tables on the device (array index = j - j0 of the grid).
+struct Geo {
+    const double* yu;
+    const double* yv;
+    const double* dthdyu;
+    const double* dthdyv;
+    const double* dyu2i;  // [nyu][3]
+    const double* dyv2i;  // [nyv][3]
+    const double* kx;     // [nkx]
+    const double* kz;     // [n2]
+    double gwb, gwt, gwib, gwit;
+};
+
+__device__ __forceinline__ int row_of(const Dims& d, int q) { return q < d.n2 / 2 ? q : q + (d.ngal2 - d.n2); }
+
+__device__ __forceinline__ double2 dc(double a, double b) { double2 r; r.x = a; r.y = b; return r; }
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return dc(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 dsub(double2 a, double2 b) { return dc(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 dscl(double s, double2 a) { return dc(s * a.x, s * a.y); }
+// (i*k) * a
+__device__ __forceinline__ double2 dik(double k, double2 a) { return dc(-k * a.y, k * a.x); }
+
+template <typename T2> __device__ __forceinline__ T2 to_t2(double2 a);
+template <> __device__ __forceinline__ float2 to_t2<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __device__ __forceinline__ double2 to_t2<double2>(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d2(float2 a) { return dc((double)a.x, (double)a.y); }
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+
+// --------------------------------------------------------------------------------------
+// Pass 1: y-interpolation + inverse z transform (interp_u/interp_v FOU3D.f90:261-308,
+// modes_to_planes_UVP, cft inverse of four_to_phys_u FOU3D.f90:546-572).
+// grid: x = kx chunk of CH modes, y = slot (u-planes then v-planes), z = field 0..2
+//   u-plane j: U = u1(j), W = u3(j), V = v interpolated to the centre (with ghost rows)
+//   v-plane j: U = u1 interpolated to the face, W = u3 interpolated, V = u2(j)
+// --------------------------------------------------------------------------------------
+template <typename T2>
+__global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __restrict__ u1,
+                                              const double2* __restrict__ u2, const double2* __restrict__ u3,
+                                              T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+                                              FFTDesc fz, const T2* __restrict__ twz, int CH) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* buf0 = reinterpret_cast<T2*>(smem_raw);
+    T2* buf1 = buf0 + (size_t)d.ngal2 * CH;
+    T2* tw = buf1 + (size_t)d.ngal2 * CH;
+    const int kx0 = blockIdx.x * CH;
+    const int slot = blockIdx.y;
+    const int f = blockIdx.z;
+    const int n = d.ngal2;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) buf0[t] = cx<T2>(0, 0);
+    __syncthreads();
+    const bool uplane = slot < d.nyu;
+    const int j = uplane ? d.ju0 + slot : d.jv0 + (slot - d.nyu);
+    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
+        const int b = t % CH, q = t / CH;
+        const int i = kx0 + b;
+        if (i >= d.nkx) continue;
+        const size_t col = (size_t)q * d.nkx + i;
+        double2 val;
+        if (uplane) {
+            if (f == 0) val = u1[(size_t)(j - d.ju0) * d.ncol + col];
+            else if (f == 1) val = u3[(size_t)(j - d.ju0) * d.ncol + col];
+            else {
+                // interp_v (FOU3D.f90:296-304): v at centre j from faces j-1, j; ghosts extrapolated
+                auto itp = [&](int jj) {
+                    const double2 va = u2[(size_t)(jj - d.jv0) * d.ncol + col];
+                    const double2 vb = u2[(size_t)(jj - 1 - d.jv0) * d.ncol + col];
+                    const double yuj = g.yu[jj - d.ju0], yvj = g.yv[jj - d.jv0], yvm = g.yv[jj - 1 - d.jv0];
+                    return dc(((yuj - yvm) * va.x + (yvj - yuj) * vb.x) / (yvj - yvm),
+                              ((yuj - yvm) * va.y + (yvj - yuj) * vb.y) / (yvj - yvm));
+                };
+                if (j == d.ju0) {
+                    const double2 vi = itp(d.ju0 + 1);
+                    const double2 vw = u2[(size_t)0 * d.ncol + col];
+                    val = dadd(dscl(g.gwib, dsub(vw, vi)), vi);
+                } else if (j == d.ju1) {
+                    const double2 vi = itp(d.ju1 - 1);
+                    const double2 vw = u2[(size_t)(d.jv1 - d.jv0) * d.ncol + col];
+                    val = dadd(dscl(g.gwit, dsub(vw, vi)), vi);
+                } else {
+                    val = itp(j);
+                }
+            }
+        } else {
+            if (f == 2) val = u2[(size_t)(j - d.jv0) * d.ncol + col];
+            else {
+                // interp_u (FOU3D.f90:272-279): u at face j from centres j, j+1
+                const double2* s = f == 0 ? u1 : u3;
+                const double2 ua = s[(size_t)(j + 1 - d.ju0) * d.ncol + col];
+                const double2 ub = s[(size_t)(j - d.ju0) * d.ncol + col];
+                const double yvj = g.yv[j - d.jv0], yuj = g.yu[j - d.ju0], yup = g.yu[j + 1 - d.ju0];
+                val = dc(((yvj - yuj) * ua.x + (yup - yvj) * ub.x) / (yup - yuj),
+                         ((yvj - yuj) * ua.y + (yup - yvj) * ub.y) / (yup - yuj));
+            }
+        }
+        buf0[(size_t)row_of(d, q) * CH + b] = to_t2<T2>(val);
+    }
+    __syncthreads();
+    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, +1);
+    T2* H = f == 0 ? H0 : (f == 1 ? H1 : H2);
+    const size_t base = (size_t)slot * n * d.nkx;
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+        const int b = t % CH, z = t / CH;
+        const int i = kx0 + b;
+        if (i < d.nkx) H[base + (size_t)z * d.nkx + i] = res[(size_t)z * CH + b];
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// Pass 2: per z-row of a plane, inverse real x transform (rft inverse), products, forward
+// real x transform (rft forward, x 1/Ngal1), truncation to kx <= N1/2
+// (ops_in_planes FOU3D.f90:1553-1569, 1588-1600).  Two real rows share one complex
+// transform: line = A + i*B with A, B the Hermitian spectra of two real signals.
+// u-plane: (u + i w), (v + i 0) -> (uu + i uw), (vv + i ww)
+// v-plane: (u + i w), (v + i 0) -> (uv + i vw)
+// grid: x = chunk of RW rows, y = slot
+// --------------------------------------------------------------------------------------
+template <typename T2>
+__device__ __forceinline__ T2 herm_line(const Dims& d, const T2* A, const T2* B, int k) {
+    // entry k (0..Ngal1-1) of the complex line A + iB from kx-spectra A, B (i = 0..N1/2);
+    // the rft inverse ignores Im of the kx = 0 entry (rft_buff.f:78-80)
+    using R = decltype(T2::x);
+    const int h = d.n1 / 2;
+    if (k <= h) {
+        T2 a = A ? A[k] : cx<T2>(0, 0);
+        T2 b = B ? B[k] : cx<T2>(0, 0);
+        if (k == 0) { a.y = 0; b.y = 0; }
+        return cx<T2>(a.x - b.y, a.y + b.x);
+    }
+    if (k >= d.ngal1 - h) {
+        const int kk = d.ngal1 - k;
+        T2 a = A ? A[kk] : cx<T2>(0, 0);
+        T2 b = B ? B[kk] : cx<T2>(0, 0);
+        return cx<T2>(a.x + b.y, -a.y + b.x);
+    }
+    return cx<T2>((R)0, (R)0);
+}
+
+template <typename T2>
+__global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+                                               T2* __restrict__ H3, FFTDesc fx, const T2* __restrict__ twx, int RW) {
+    using R = decltype(T2::x);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = d.ngal1;
+    const int B = 2 * RW;
+    T2* buf0 = reinterpret_cast<T2*>(smem_raw);
+    T2* buf1 = buf0 + (size_t)n * B;
+    T2* tw = buf1 + (size_t)n * B;
+    const int slot = blockIdx.y;
+    const int z0 = blockIdx.x * RW;
+    const bool uplane = slot < d.nyu;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twx[t];
+    const size_t pbase = (size_t)slot * d.ngal2 * d.nkx;
+    for (int t = threadIdx.x; t < n * B; t += blockDim.x) {
+        const int b = t % B, k = t / B;
+        const int rr = b >> 1, which = b & 1;
+        const size_t rb = pbase + (size_t)(z0 + rr) * d.nkx;
+        T2 v = which == 0 ? herm_line<T2>(d, H0 + rb, H1 + rb, k) : herm_line<T2>(d, H2 + rb, (const T2*)nullptr, k);
+        buf0[(size_t)k * B + b] = v;
+    }
+    __syncthreads();
+    T2* P = fft_lines<T2>(buf0, buf1, B, fx, tw, +1);
+    T2* Q = P == buf0 ? buf1 : buf0;
+    for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
+        const int rr = t % RW, k = t / RW;
+        T2 l0 = P[(size_t)k * B + 2 * rr];
+        T2 l1 = P[(size_t)k * B + 2 * rr + 1];
+        const R u = l0.x, w = l0.y, v = l1.x;
+        if (uplane) {
+            P[(size_t)k * B + 2 * rr] = cx<T2>(u * u, u * w);
+            P[(size_t)k * B + 2 * rr + 1] = cx<T2>(v * v, w * w);
+        } else {
+            P[(size_t)k * B + 2 * rr] = cx<T2>(u * v, w * v);
+            P[(size_t)k * B + 2 * rr + 1] = cx<T2>((R)0, (R)0);
+        }
+    }
+    __syncthreads();
+    T2* F = fft_lines<T2>(P, Q, B, fx, tw, -1);
+    const R s = (R)1 / (R)n;
+    const int nl = uplane ? B : RW;  // v-planes carry one output line per row
+    for (int t = threadIdx.x; t < d.nkx * nl; t += blockDim.x) {
+        const int k = t % d.nkx, bl = t / d.nkx;
+        const int b = uplane ? bl : 2 * bl;
+        const int rr = b >> 1, which = b & 1;
+        const T2 Pk = F[(size_t)k * B + b];
+        const T2 Qc = cconj(F[(size_t)((n - k) % n) * B + b]);
+        const T2 A = cx<T2>((Pk.x + Qc.x) * (R)0.5 * s, (Pk.y + Qc.y) * (R)0.5 * s);
+        const T2 Bv = cx<T2>((Pk.y - Qc.y) * (R)0.5 * s, -(Pk.x - Qc.x) * (R)0.5 * s);
+        const size_t o = pbase + (size_t)(z0 + rr) * d.nkx + k;
+        if (which == 0) { H0[o] = A; H1[o] = Bv; }
+        else { H2[o] = A; H3[o] = Bv; }
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// Pass 3: forward z transform (cft forward of phys_to_four_du, x 1/Ngal2) and truncation
+// to the retained kz modes (planes_to_modes_UVP/NUVP picks rows k and k+Ngal2-N2).
+// Output spectral products S_f[slot][column]:  u-plane: S0=uu S1=uw S2=vv S3=ww;
+// v-plane: S0=uv S1=vw.   grid: x = kx chunk, y = slot, z = field 0..3
+// --------------------------------------------------------------------------------------
+template <typename T2>
+__global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1,
+                                              const T2* __restrict__ H2, const T2* __restrict__ H3,
+                                              T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
+                                              T2* __restrict__ S3, FFTDesc fz, const T2* __restrict__ twz, int CH) {
+    using R = decltype(T2::x);
+    const int slot = blockIdx.y;
+    const int f = blockIdx.z;
+    if (slot >= d.nyu && f >= 2) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = d.ngal2;
+    T2* buf0 = reinterpret_cast<T2*>(smem_raw);
+    T2* buf1 = buf0 + (size_t)n * CH;
+    T2* tw = buf1 + (size_t)n * CH;
+    const int kx0 = blockIdx.x * CH;
+    const T2* H = f == 0 ? H0 : (f == 1 ? H1 : (f == 2 ? H2 : H3));
+    T2* S = f == 0 ? S0 : (f == 1 ? S1 : (f == 2 ? S2 : S3));
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
+    const size_t base = (size_t)slot * n * d.nkx;
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+        const int b = t % CH, z = t / CH;
+        const int i = kx0 + b;
+        buf0[t] = i < d.nkx ? H[base + (size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
+    }
+    __syncthreads();
+    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, -1);
+    const R s = (R)1 / (R)n;
+    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
+        const int b = t % CH, q = t / CH;
+        const int i = kx0 + b;
+        if (i < d.nkx) S[(size_t)slot * d.ncol + (size_t)q * d.nkx + i] = cscale(res[(size_t)row_of(d, q) * CH + b], s);
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// Column kernel: RHS0_u1/u2/u3 (littleharsh.f90:613-730), the tail of nonlinear
+// (der_x/der_z FOU3D.f90:310-414 as ik products with the kz = -N2/2 row zeroed,
+// der_yu_h/der_yv_h :453-493, du += -g Nu :233-244) and the solveU/solveV prologue
+// (du = u + dt du, wall/ghost rows 0; littleharsh.f90:744-786).
+// MODE bits: 1 = RHS0, 2 = nonlinear tail, 4 = solve prologue.
+// --------------------------------------------------------------------------------------
+struct RKCoef {
+    double C1;    // a/Re
+    double C2;    // -c
+    double dRK;   // d = g + c
+    double mg;    // -g
+    double dt;
+    int krk;
+};
+
+template <typename T2> __device__ __forceinline__ T2 ldT(const T2* p) { return *p; }
+
+template <typename T2, int MODE>
+__global__ void __launch_bounds__(256) k_rhs(Dims d, Geo g, RKCoef c, const double* __restrict__ scal,
+                                             const double2* __restrict__ u1, const double2* __restrict__ u2,
+                                             const double2* __restrict__ u3, const double2* __restrict__ p,
+                                             T2* __restrict__ Nu1, T2* __restrict__ Nu2, T2* __restrict__ Nu3,
+                                             double2* __restrict__ du1, double2* __restrict__ du2,
+                                             double2* __restrict__ du3, const T2* __restrict__ S0,
+                                             const T2* __restrict__ S1, const T2* __restrict__ S2,
+                                             const T2* __restrict__ S3) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol) return;
+    const int i = col % d.nkx, q = col / d.nkx;
+    const double kxv = g.kx[i], kzv = g.kz[q];
+    const double k2 = (-kxv * kxv) + (-kzv * kzv);
+    const bool zrow = (q == d.n2 / 2);  // der_x/der_z zero the kz = -N2/2 mode
+    const size_t nc = d.ncol;
+    const double mpgx = scal[0];
+    constexpr bool RHS0 = (MODE & 1) != 0, NL = (MODE & 2) != 0, PRO = (MODE & 4) != 0;
+
+    // ---- u and w (ugrid), j = ju0+1 .. ju1-1
+    {
+        double2 a_m = u1[col], a_0 = u1[nc + col];
+        double2 w_m = u3[col], w_0 = u3[nc + col];
+        const size_t vs = (size_t)d.nyu * nc;  // first v-slot
+        double2 uv_m = NL ? to_d2(ldT(S0 + vs + col)) : dc(0, 0);  // uv at face ju0 (= jv0)
+        double2 vw_m = NL ? to_d2(ldT(S1 + vs + col)) : dc(0, 0);
+        for (int j = d.ju0 + 1; j <= d.ju1 - 1; ++j) {
+            const size_t ju = (size_t)(j - d.ju0);
+            const double2 a_p = u1[(ju + 1) * nc + col];
+            const double2 w_p = u3[(ju + 1) * nc + col];
+            const size_t jp = (size_t)(j - d.jp0);
+            double2 r1, r3;
+            if (RHS0) {
+                const double c0 = g.dyu2i[3 * ju + 0], c1 = g.dyu2i[3 * ju + 1], c2 = g.dyu2i[3 * ju + 2];
+                const double dg = k2 + c1;
+                const double2 Lu = dadd(dadd(dscl(c0, a_m), dscl(dg, a_0)), dscl(c2, a_p));
+                const double2 Lw = dadd(dadd(dscl(c0, w_m), dscl(dg, w_0)), dscl(c2, w_p));
+                const double2 pp = p[jp * nc + col];
+                const double2 n1o = to_d2(Nu1[ju * nc + col]);
+                const double2 n3o = to_d2(Nu3[ju * nc + col]);
+                r1 = dadd(dadd(dscl(c.C1, Lu), dscl(c.C2, n1o)), dik(-c.dRK * kxv, pp));
+                r3 = dadd(dadd(dscl(c.C1, Lw), dscl(c.C2, n3o)), dik(-c.dRK * kzv, pp));
+                if (col == 0) r1.x += -c.dRK * mpgx;
+            } else {
+                r1 = du1[ju * nc + col];
+                r3 = du3[ju * nc + col];
+            }
+            if (NL) {
+                const size_t su = ju * nc + col;
+                const size_t sv = vs + (size_t)(j - d.jv0) * nc + col;
+                const double2 uv_p = to_d2(ldT(S0 + sv)), vw_p = to_d2(ldT(S1 + sv));
+                const double dth = g.dthdyu[ju];
+                double2 n1 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(ldT(S0 + su))), dik(kzv, to_d2(ldT(S1 + su))));
+                double2 n3 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(ldT(S1 + su))), dik(kzv, to_d2(ldT(S3 + su))));
+                n1 = dadd(n1, dscl(dth, dsub(uv_p, uv_m)));
+                n3 = dadd(n3, dscl(dth, dsub(vw_p, vw_m)));
+                Nu1[su] = to_t2<T2>(n1);
+                Nu3[su] = to_t2<T2>(n3);
+                r1 = dadd(r1, dscl(c.mg, n1));
+                r3 = dadd(r3, dscl(c.mg, n3));
+                uv_m = uv_p;
+                vw_m = vw_p;
+            }
+            if (PRO) {
+                r1 = dadd(a_0, dscl(c.dt, r1));
+                r3 = dadd(w_0, dscl(c.dt, r3));
+            }
+            du1[ju * nc + col] = r1;
+            du3[ju * nc + col] = r3;
+            a_m = a_0; a_0 = a_p;
+            w_m = w_0; w_0 = w_p;
+        }
+        if (PRO) {
+            du1[col] = dc(0, 0);
+            du3[col] = dc(0, 0);
+            du1[(size_t)(d.nyu - 1) * nc + col] = dc(0, 0);
+            du3[(size_t)(d.nyu - 1) * nc + col] = dc(0, 0);
+        }
+    }
+    // ---- v (vgrid), j = jv0+1 .. jv1-1
+    {
+        double2 v_m = u2[col], v_0 = u2[nc + col];
+        double2 vv_0 = NL ? to_d2(ldT(S2 + (size_t)(d.jv0 + 1 - d.ju0) * nc + col)) : dc(0, 0);
+        const size_t vs = (size_t)d.nyu * nc;
+        for (int j = d.jv0 + 1; j <= d.jv1 - 1; ++j) {
+            const size_t jv = (size_t)(j - d.jv0);
+            const double2 v_p = u2[(jv + 1) * nc + col];
+            double2 r2;
+            if (RHS0) {
+                const double c0 = g.dyv2i[3 * jv + 0], c1 = g.dyv2i[3 * jv + 1], c2 = g.dyv2i[3 * jv + 2];
+                const double2 Lv = dadd(dadd(dscl(c0, v_m), dscl(k2 + c1, v_0)), dscl(c2, v_p));
+                const double C3 = -c.dRK * g.dthdyv[jv];
+                const double2 pa = p[(size_t)(j + 1 - d.jp0) * nc + col];
+                const double2 pb = p[(size_t)(j - d.jp0) * nc + col];
+                const double2 n2o = to_d2(Nu2[jv * nc + col]);
+                r2 = dadd(dadd(dscl(c.C1, Lv), dscl(c.C2, n2o)), dscl(C3, dsub(pa, pb)));
+            } else {
+                r2 = du2[jv * nc + col];
+            }
+            if (NL) {
+                const size_t sv = vs + jv * nc + col;
+                const double2 vv_p = to_d2(ldT(S2 + (size_t)(j + 1 - d.ju0) * nc + col));
+                double2 n2 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(ldT(S0 + sv))), dik(kzv, to_d2(ldT(S1 + sv))));
+                n2 = dadd(n2, dscl(g.dthdyv[jv], dsub(vv_p, vv_0)));
+                Nu2[jv * nc + col] = to_t2<T2>(n2);
+                r2 = dadd(r2, dscl(c.mg, n2));
+                vv_0 = vv_p;
+            }
+            if (PRO) r2 = dadd(v_0, dscl(c.dt, r2));
+            du2[jv * nc + col] = r2;
+            v_m = v_0; v_0 = v_p;
+        }
+        if (PRO) {
+            du2[col] = dc(0, 0);
+            du2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// Immersed-boundary forcing (immersed_boundaries_U/V, tridLU_3D_IB.f90:163-281) on the
+// canopy planes only: inverse 2-D transform of rhs and u, point forcing, forward
+// transform of rhs back to every column of those planes.
+// Sources are (rhs, u) pairs; src[2*fb] = rhs of batch fb, src[2*fb+1] = its u.
+// --------------------------------------------------------------------------------------
+struct IBSrc {
+    const double2* f[4];
+};
+struct IBDst {
+    double2* f[2];
+};
+
+// inverse z transform of the IB planes of every source.  grid: x = kx chunk, y = plane,
+// z = source.  Hib[(s*npl + p)][z][kx]
+template <typename T2>
+__global__ void __launch_bounds__(256) k_ib_zinv(Dims d, IBSrc src, int j0, const int* __restrict__ planes, int npl,
+                                                 T2* __restrict__ Hib, FFTDesc fz, const T2* __restrict__ twz, int CH) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = d.ngal2;
+    T2* buf0 = reinterpret_cast<T2*>(smem_raw);
+    T2* buf1 = buf0 + (size_t)n * CH;
+    T2* tw = buf1 + (size_t)n * CH;
+    const int kx0 = blockIdx.x * CH, p = blockIdx.y, s = blockIdx.z;
+    const int j = planes[p];
+    const double2* f = src.f[s];
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) buf0[t] = cx<T2>(0, 0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
+        const int b = t % CH, q = t / CH, i = kx0 + b;
+        if (i >= d.nkx) continue;
+        buf0[(size_t)row_of(d, q) * CH + b] = to_t2<T2>(f[(size_t)(j - j0) * d.ncol + (size_t)q * d.nkx + i]);
+    }
+    __syncthreads();
+    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, +1);
+    const size_t base = ((size_t)s * npl + p) * n * d.nkx;
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+        const int b = t % CH, z = t / CH, i = kx0 + b;
+        if (i < d.nkx) Hib[base + (size_t)z * d.nkx + i] = res[(size_t)z * CH + b];
+    }
+}
+
+// inverse x transform: line (rhs + i u) of one row -> physical rhs, u.
+// grid: x = row chunk (RW rows), y = plane, z = batch fb.  Phys[(fb*2+which)*npl + p][z][x]
+template <typename T2>
+__global__ void __launch_bounds__(256) k_ib_xinv(Dims d, const T2* __restrict__ Hib, int npl, decltype(T2::x)* __restrict__ phys,
+                                                 FFTDesc fx, const T2* __restrict__ twx, int RW) {
+    using R = decltype(T2::x);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = d.ngal1;
+    T2* buf0 = reinterpret_cast<T2*>(smem_raw);
+    T2* buf1 = buf0 + (size_t)n * RW;
+    T2* tw = buf1 + (size_t)n * RW;
+    const int z0 = blockIdx.x * RW, p = blockIdx.y, fb = blockIdx.z;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twx[t];
+    const size_t pl = (size_t)d.ngal2 * d.nkx;
+    const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl;
+    const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl;
+    for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
+        const int b = t % RW, k = t / RW;
+        const size_t rb = (size_t)(z0 + b) * d.nkx;
+        buf0[(size_t)k * RW + b] = herm_line<T2>(d, Hr + rb, Hu + rb, k);
+    }
+    __syncthreads();
+    T2* res = fft_lines<T2>(buf0, buf1, RW, fx, tw, +1);
+    const size_t ppl = (size_t)d.ngal2 * n;
+    R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl;
+    R* pu = phys + ((size_t)(2 * fb + 1) * npl + p) * ppl;
+    for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
+        const int k = t % n, b = t / n;
+        const T2 v = res[(size_t)k * RW + b];
+        pr[(size_t)(z0 + b) * n + k] = v.x;
+        pu[(size_t)(z0 + b) * n + k] = v.y;
+    }
+}
+
+// point forcing rhs(p) = Lap*(w2 u(p2) + w3 u(p3) - u(p) + rhs(p)) (tridLU_3D_IB.f90:193-211);
+// points are sorted by (j,k,i): the first point of a run of equal targets applies the
+// whole run in list order, so repeated targets behave as the reference's serial loop.
+// grid: x = points, y = batch fb
+template <typename R>
+__global__ void k_ib_force(Dims d, const int* __restrict__ idx, const double* __restrict__ w, int npts,
+                           const int* __restrict__ slot_of_j, int j0, int npl, R* __restrict__ phys) {
+    const int pt = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pt >= npts) return;
+    const int fb = blockIdx.y;
+    const int* id = idx + 9 * (size_t)pt;
+    if (pt > 0) {
+        const int* pv = id - 9;
+        if (pv[0] == id[0] && pv[1] == id[1] && pv[2] == id[2]) return;
+    }
+    const size_t ppl = (size_t)d.ngal2 * d.ngal1;
+    R* pr = phys + (size_t)(2 * fb) * npl * ppl;
+    const R* pu = phys + (size_t)(2 * fb + 1) * npl * ppl;
+    auto off = [&](int i, int k, int j) -> size_t {
+        return (size_t)slot_of_j[j - j0] * ppl + (size_t)(k - 1) * d.ngal1 + (i - 1);
+    };
+    const size_t tgt = off(id[0], id[1], id[2]);
+    R r = pr[tgt];
+    const R u0 = pu[tgt];
+    for (int q = pt; q < npts; ++q) {
+        const int* iq = idx + 9 * (size_t)q;
+        if (q > pt && !(iq[0] == id[0] && iq[1] == id[1] && iq[2] == id[2])) break;
+        const double* wq = w + 3 * (size_t)q;
+        const R vf = (R)wq[1] * pu[off(iq[3], iq[4], iq[5])] + (R)wq[2] * pu[off(iq[6], iq[7], iq[8])];
+        r = (R)wq[0] * (vf - u0 + r);
+    }
+    pr[tgt] = r;
+}
+
+// forward x transform of physical rhs rows (two rows per complex line), truncated to
+// kx <= N1/2, x 1/Ngal1.  grid: x = row chunk (RW rows, RW even), y = plane, z = batch.
+// Output into Hib[(fb*2)*npl + p] (the rhs slot).
+template <typename T2>
+__global__ void __launch_bounds__(256) k_ib_xfwd(Dims d, T2* __restrict__ Hib, int npl, const decltype(T2::x)* __restrict__ phys,
+                                                 FFTDesc fx, const T2* __restrict__ twx, int RW) {
+    using R = decltype(T2::x);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = d.ngal1;
+    const int B = RW / 2;
+    T2* buf0 = reinterpret_cast<T2*>(smem_raw);
+    T2* buf1 = buf0 + (size_t)n * B;
+    T2* tw = buf1 + (size_t)n * B;
+    const int z0 = blockIdx.x * RW, p = blockIdx.y, fb = blockIdx.z;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twx[t];
+    const size_t ppl = (size_t)d.ngal2 * n;
+    const R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl;
+    for (int t = threadIdx.x; t < n * B; t += blockDim.x) {
+        const int k = t % n, b = t / n;
+        buf0[(size_t)k * B + b] = cx<T2>(pr[(size_t)(z0 + 2 * b) * n + k], pr[(size_t)(z0 + 2 * b + 1) * n + k]);
+    }
+    __syncthreads();
+    T2* F = fft_lines<T2>(buf0, buf1, B, fx, tw, -1);
+    const R s = (R)1 / (R)n;
+    T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)d.ngal2 * d.nkx;
+    for (int t = threadIdx.x; t < d.nkx * B; t += blockDim.x) {
+        const int k = t % d.nkx, b = t / d.nkx;
+        const T2 Pk = F[(size_t)k * B + b];
+        const T2 Qc = cconj(F[(size_t)((n - k) % n) * B + b]);
+        Hr[(size_t)(z0 + 2 * b) * d.nkx + k] = cx<T2>((Pk.x + Qc.x) * (R)0.5 * s, (Pk.y + Qc.y) * (R)0.5 * s);
+        Hr[(size_t)(z0 + 2 * b + 1) * d.nkx + k] = cx<T2>((Pk.y - Qc.y) * (R)0.5 * s, -(Pk.x - Qc.x) * (R)0.5 * s);
+    }
+}
+
+// forward z transform of the rhs slot and write-back to every column of the plane
+// (planes_to_modes_dU/dV).  grid: x = kx chunk, y = plane, z = batch fb
+template <typename T2>
+__global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ Hib, int npl, IBDst dst, int j0,
+                                                 const int* __restrict__ planes, FFTDesc fz, const T2* __restrict__ twz,
+                                                 int CH) {
+    using R = decltype(T2::x);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = d.ngal2;
+    T2* buf0 = reinterpret_cast<T2*>(smem_raw);
+    T2* buf1 = buf0 + (size_t)n * CH;
+    T2* tw = buf1 + (size_t)n * CH;
+    const int kx0 = blockIdx.x * CH, p = blockIdx.y, fb = blockIdx.z;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
+    const T2* H = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)n * d.nkx;
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+        const int b = t % CH, z = t / CH, i = kx0 + b;
+        buf0[t] = i < d.nkx ? H[(size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
+    }
+    __syncthreads();
+    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, -1);
+    const R s = (R)1 / (R)n;
+    double2* out = dst.f[fb] + (size_t)(planes[p] - j0) * d.ncol;
+    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
+        const int b = t % CH, q = t / CH, i = kx0 + b;
+        if (i < d.nkx) out[(size_t)q * d.nkx + i] = to_d2(cscale(res[(size_t)row_of(d, q) * CH + b], s));
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// Implicit Helmholtz solves: LUsolU/LUsolV with LU_buildU/V + LU_dec computed on the fly
+// (tridLU_3D_IB.f90:50-160, 349-413, 521-559).  One thread per (kx,kz) column; the
+// forward sweep leaves y_j in the solution array and the scaled upper diagonal in `cs`.
+// u and w share the matrix and its factorisation.
+// --------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_solve_uvw(Dims d, Geo g, double beta, double2* __restrict__ u1,
+                                                   double2* __restrict__ u2, double2* __restrict__ u3,
+                                                   const double2* __restrict__ r1, const double2* __restrict__ r2,
+                                                   const double2* __restrict__ r3, double* __restrict__ cs,
+                                                   int do_uw, int do_v) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol) return;
+    const int i = col % d.nkx, q = col / d.nkx;
+    const double k2x = -g.kx[i] * g.kx[i], k2z = -g.kz[q] * g.kz[q];
+    const size_t nc = d.ncol;
+    if (do_uw) {
+        const int n = d.nyu;
+        // row 0: (0, 1, gwb)
+        double dinv = 1.0 / 1.0;
+        double a3prev = g.gwb;
+        double2 y1 = dscl(dinv, r1[col]);
+        double2 y3 = dscl(dinv, r3[col]);
+        u1[col] = y1;
+        u3[col] = y3;
+        double dprev = dinv;
+        for (int jj = 1; jj < n; ++jj) {
+            double a1, a2, a3;
+            if (jj < n - 1) {
+                const double b = beta;
+                a1 = -b * g.dyu2i[3 * jj + 0];
+                a2 = 1.0 - b * (g.dyu2i[3 * jj + 1] + k2x + k2z);
+                a3 = -b * g.dyu2i[3 * jj + 2];
+            } else {
+                a1 = g.gwt; a2 = 1.0; a3 = 0.0;
+            }
+            const double csm = a3prev * dprev;  // a(3,j-1) * a(2,j-1)
+            cs[(size_t)(jj - 1) * nc + col] = csm;
+            const double dj = 1.0 / (a2 - a1 * csm);
+            const double2 ra = r1[(size_t)jj * nc + col], rc = r3[(size_t)jj * nc + col];
+            y1 = dscl(dj, dsub(ra, dscl(a1, y1)));
+            y3 = dscl(dj, dsub(rc, dscl(a1, y3)));
+            u1[(size_t)jj * nc + col] = y1;
+            u3[(size_t)jj * nc + col] = y3;
+            dprev = dj;
+            a3prev = a3;
+        }
+        double2 x1 = y1, x3 = y3;
+        for (int jj = n - 2; jj >= 0; --jj) {
+            const double csj = cs[(size_t)jj * nc + col];
+            x1 = dsub(u1[(size_t)jj * nc + col], dscl(csj, x1));
+            x3 = dsub(u3[(size_t)jj * nc + col], dscl(csj, x3));
+            u1[(size_t)jj * nc + col] = x1;
+            u3[(size_t)jj * nc + col] = x3;
+        }
+    }
+    if (do_v) {
+        const int n = d.nyv;
+        double dprev = 1.0;
+        double a3prev = 0.0;
+        double2 y = r2[col];
+        u2[col] = y;
+        for (int jj = 1; jj < n; ++jj) {
+            double a1, a2, a3;
+            if (jj < n - 1) {
+                a1 = -beta * g.dyv2i[3 * jj + 0];
+                a2 = 1.0 - beta * (g.dyv2i[3 * jj + 1] + k2x + k2z);
+                a3 = -beta * g.dyv2i[3 * jj + 2];
+            } else {
+                a1 = 0.0; a2 = 1.0; a3 = 0.0;
+            }
+            const double csm = a3prev * dprev;
+            cs[(size_t)(jj - 1) * nc + col] = csm;
+            const double dj = 1.0 / (a2 - a1 * csm);
+            y = dscl(dj, dsub(r2[(size_t)jj * nc + col], dscl(a1, y)));
+            u2[(size_t)jj * nc + col] = y;
+            dprev = dj;
+            a3prev = a3;
+        }
+        double2 x = y;
+        for (int jj = n - 2; jj >= 0; --jj) {
+            x = dsub(u2[(size_t)jj * nc + col], dscl(cs[(size_t)jj * nc + col], x));
+            u2[(size_t)jj * nc + col] = x;
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// solveP (littleharsh.f90:556-611): divergence (:209-244), psi = div/(dt(a+b)),
+// psi(mean, bottom) = 0, LUsolP with the D.G matrix of LU_buildP/LU_decP computed on
+// the fly (tridLU_3D_IB.f90:284-318, 417-491, 562-603), p += psi.
+// --------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_solve_p(Dims d, Geo g, double dtirk, const double2* __restrict__ u1,
+                                                 const double2* __restrict__ u2, const double2* __restrict__ u3,
+                                                 double2* __restrict__ p, double2* __restrict__ psi,
+                                                 double2* __restrict__ divo, double* __restrict__ cs, double mean_diag) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol) return;
+    const int i = col % d.nkx, q = col / d.nkx;
+    const double kxv = g.kx[i], kzv = g.kz[q];
+    const double k2x = -kxv * kxv, k2z = -kzv * kzv;
+    const size_t nc = d.ncol;
+    const int n = d.nyp;
+    // D.G coefficients: D_b(m) = -dthdyu(m+1), G_b(m) = -dthdyv(m), D_t(m) = dthdyu(m), G_t(m) = dthdyv(m-1)
+    auto DTHU = [&](int j) { return g.dthdyu[j - d.ju0]; };
+    auto DTHV = [&](int j) { return g.dthdyv[j - d.jv0]; };
+    double dprev = 0.0, a3prev = 0.0;
+    double2 y = dc(0, 0);
+    for (int jj = 0; jj < n; ++jj) {
+        const int j = d.jp0 + jj;
+        // divergence at p-point j
+        const double2 a = u1[(size_t)(j - d.ju0) * nc + col];
+        const double2 w = u3[(size_t)(j - d.ju0) * nc + col];
+        const double2 va = u2[(size_t)(j - d.jv0) * nc + col];
+        const double2 vb = u2[(size_t)(j - 1 - d.jv0) * nc + col];
+        const double2 dv = dadd(dadd(dik(kxv, a), dik(kzv, w)), dscl(DTHU(j), dsub(va, vb)));
+        if (divo) divo[(size_t)jj * nc + col] = dv;
+        double2 r = dscl(dtirk, dv);
+        double a1, a2, a3;
+        if (jj == 0) {
+            a1 = 0.0;
+            a2 = (DTHU(j) * -DTHV(j)) + k2x + k2z;
+            a3 = (DTHU(j) * DTHV(j));
+            if (col == 0) { a2 = mean_diag; a3 = 0.0; r = dc(0, 0); }
+        } else if (jj == n - 1) {
+            a1 = (-DTHU(j)) * (-DTHV(j - 1));
+            a2 = ((-DTHU(j)) * DTHV(j - 1)) + k2x + k2z;
+            a3 = 0.0;
+        } else {
+            a2 = ((-DTHU(j)) * DTHV(j - 1)) + (DTHU(j) * -DTHV(j)) + k2x + k2z;
+            a1 = ((-DTHU(j)) * (-DTHV(j - 1)));
+            a3 = (DTHU(j) * DTHV(j));
+        }
+        double dj;
+        if (jj == 0) {
+            dj = 1.0 / a2;
+            y = dscl(dj, r);
+        } else {
+            const double csm = a3prev * dprev;
+            cs[(size_t)(jj - 1) * nc + col] = csm;
+            dj = 1.0 / (a2 - a1 * csm);
+            y = dscl(dj, dsub(r, dscl(a1, y)));
+        }
+        psi[(size_t)jj * nc + col] = y;
+        dprev = dj;
+        a3prev = a3;
+    }
+    double2 x = y;
+    p[(size_t)(n - 1) * nc + col] = dadd(p[(size_t)(n - 1) * nc + col], x);
+    for (int jj = n - 2; jj >= 0; --jj) {
+        x = dsub(psi[(size_t)jj * nc + col], dscl(cs[(size_t)jj * nc + col], x));
+        psi[(size_t)jj * nc + col] = x;
+        p[(size_t)jj * nc + col] = dadd(p[(size_t)jj * nc + col], x);
+    }
+}
+
+// v_corr (littleharsh.f90:796-907): u -= dt(a+b) ikx psi, w -= dt(a+b) ikz psi,
+// v -= dt(a+b) dthdyv (psi(j+1)-psi(j)), ghost rows by gridweighting, v walls 0, and the
+// closing divergence (optional).
+__global__ void __launch_bounds__(256) k_vcorr(Dims d, Geo g, double dtrk, double2* __restrict__ u1,
+                                               double2* __restrict__ u2, double2* __restrict__ u3,
+                                               const double2* __restrict__ psi, double2* __restrict__ divo) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol) return;
+    const int i = col % d.nkx, q = col / d.nkx;
+    const double kxv = g.kx[i], kzv = g.kz[q];
+    const size_t nc = d.ncol;
+    double2 psim = dc(0, 0);
+    double2 vprev = dc(0, 0);
+    for (int j = d.ju0 + 1; j <= d.ju1 - 1; ++j) {
+        const size_t ju = (size_t)(j - d.ju0), jp = (size_t)(j - d.jp0), jv = (size_t)(j - d.jv0);
+        const double2 ps = psi[jp * nc + col];
+        const double2 a = dsub(u1[ju * nc + col], dik(dtrk * kxv, ps));
+        const double2 w = dsub(u3[ju * nc + col], dik(dtrk * kzv, ps));
+        u1[ju * nc + col] = a;
+        u3[ju * nc + col] = w;
+        // v at face j-1 (interior faces jv0+1..jv1-1) uses psi(j) - psi(j-1)
+        if (j - 1 >= d.jv0 + 1) {
+            const size_t jvm = jv - 1;
+            const double2 vn = dsub(u2[jvm * nc + col], dscl(dtrk * g.dthdyv[jvm], dsub(ps, psim)));
+            u2[jvm * nc + col] = vn;
+            if (divo) {
+                // divergence at p-point j-1 now that u(j-1), w(j-1), v(j-1), v(j-2) are final
+                const double2 am = u1[(ju - 1) * nc + col], wm = u3[(ju - 1) * nc + col];
+                divo[(jp - 1) * nc + col] = dadd(dadd(dik(kxv, am), dik(kzv, wm)), dscl(g.dthdyu[ju - 1], dsub(vn, vprev)));
+            }
+            vprev = vn;
+        } else {
+            vprev = dc(0, 0);  // wall v(jv0) = 0
+        }
+        psim = ps;
+    }
+    u2[col] = dc(0, 0);
+    u2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
+    u1[col] = dscl(-g.gwb, u1[nc + col]);
+    u3[col] = dscl(-g.gwb, u3[nc + col]);
+    u1[(size_t)(d.nyu - 1) * nc + col] = dscl(-g.gwt, u1[(size_t)(d.nyu - 2) * nc + col]);
+    u3[(size_t)(d.nyu - 1) * nc + col] = dscl(-g.gwt, u3[(size_t)(d.nyu - 2) * nc + col]);
+    if (divo) {
+        // last p-point j = jp1: v(jv1) = 0 (wall)
+        const int j = d.jp1;
+        const size_t ju = (size_t)(j - d.ju0), jp = (size_t)(j - d.jp0);
+        const double2 am = u1[ju * nc + col], wm = u3[ju * nc + col];
+        divo[jp * nc + col] = dadd(dadd(dik(kxv, am), dik(kzv, wm)), dscl(g.dthdyu[ju], dsub(dc(0, 0), vprev)));
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// Mean mode: flowrate_corr with LUsol0/LU_build0/LU_dec0 (littleharsh.f90:452-484,
+// tridLU_3D_IB.f90:320-346, 493-519, 605-622) and flowrateIm (littleharsh.f90:411-430).
+// scal[0] = mpgx, scal[1] = Qx, scal[2] = dgx.  One thread.  The unit-response column
+// spans j = 0..ny (cells between the crests plus one each side), as in the reference.
+// --------------------------------------------------------------------------------------
+__global__ void k_meanflow(Dims d, Geo g, double beta, double bdt, double qxt, int ctpress, double2* __restrict__ u1,
+                           double* __restrict__ scal, double* __restrict__ work) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nn = d.ny - 2;
+    auto YV = [&](int j) { return g.yv[j - d.jv0]; };
+    double Qx0 = 0.0;
+    for (int j = 1; j <= nn + 1; ++j) Qx0 += (YV(j) - YV(j - 1)) * u1[(size_t)(j - d.ju0) * d.ncol].x;
+    if (ctpress == 1) { scal[1] = Qx0; return; }
+    const int n = nn + 3;
+    double* a1 = work;
+    double* a2 = work + n;
+    double* a3 = work + 2 * n;
+    double* x = work + 3 * n;
+    a1[0] = 0.0; a2[0] = 1.0; a3[0] = g.gwb;
+    for (int j = 1; j <= nn + 1; ++j) {
+        const int jj = j - d.ju0;
+        a1[j] = -beta * g.dyu2i[3 * jj + 0];
+        a2[j] = 1.0 - beta * g.dyu2i[3 * jj + 1];
+        a3[j] = -beta * g.dyu2i[3 * jj + 2];
+    }
+    a1[nn + 2] = g.gwt; a2[nn + 2] = 1.0; a3[nn + 2] = 0.0;
+    a2[0] = 1.0 / a2[0];
+    for (int j = 1; j < n; ++j) {
+        a3[j - 1] = a3[j - 1] * a2[j - 1];
+        a2[j] = 1.0 / (a2[j] - a1[j] * a3[j - 1]);
+    }
+    x[0] = 0.0 * a2[0];
+    for (int j = 1; j < n; ++j) {
+        const double rj = (j <= nn + 1) ? bdt : 0.0;
+        x[j] = (rj - a1[j] * x[j - 1]) * a2[j];
+    }
+    for (int j = n - 2; j >= 0; --j) x[j] = x[j] - a3[j] * x[j + 1];
+    double Qx1 = 0.0;
+    for (int j = 1; j <= nn + 1; ++j) Qx1 += (YV(j) - YV(j - 1)) * x[j];
+    const double gg = (qxt - Qx0) / Qx1;
+    scal[0] = scal[0] + gg;
+    scal[2] = gg;
+    for (int j = 0; j <= nn + 2; ++j) u1[(size_t)(j - d.ju0) * d.ncol].x += gg * x[j];
+}
+
+// --------------------------------------------------------------------------------------
+// Layout conversion f(j,column) <-> [j][column] (32x32 tiles through shared memory).
+// --------------------------------------------------------------------------------------
+__global__ void k_transpose(const double2* __restrict__ in, double2* __restrict__ out, int rows, int cols) {
+    // in: [rows][cols] -> out: [cols][rows]
+    __shared__ double2 tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const int r = by + yy, c = bx + threadIdx.x;
+        if (r < rows && c < cols) tile[yy][threadIdx.x] = in[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const int c = bx + yy, r = by + threadIdx.x;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][yy];
+    }
+}
+
+// divergence at every p-point (littleharsh.f90:209-244), no state change
+__global__ void __launch_bounds__(256) k_divergence(Dims d, Geo g, const double2* __restrict__ u1,
+                                                    const double2* __restrict__ u2, const double2* __restrict__ u3,
+                                                    double2* __restrict__ divo) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol) return;
+    const double kxv = g.kx[col % d.nkx], kzv = g.kz[col / d.nkx];
+    const size_t nc = d.ncol;
+    for (int j = d.jp0; j <= d.jp1; ++j) {
+        const size_t ju = (size_t)(j - d.ju0), jv = (size_t)(j - d.jv0);
+        divo[(size_t)(j - d.jp0) * nc + col] =
+            dadd(dadd(dik(kxv, u1[ju * nc + col]), dik(kzv, u3[ju * nc + col])),
+                 dscl(g.dthdyu[ju], dsub(u2[jv * nc + col], u2[(jv - 1) * nc + col])));
+    }
+}
+
+// per-block max |z| of a complex array (error(), littleharsh.f90:322-351)
+__global__ void k_absmax(const double2* __restrict__ a, size_t n, double* __restrict__ part) {
+    __shared__ double sm[256];
+    double m = 0.0;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+        const double2 v = a[t];
+        m = fmax(m, sqrt(v.x * v.x + v.y * v.y));
+    }
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+
+// --------------------------------------------------------------------------------------
+// Generic strided transforms with the reference wrapper semantics (cft_buff.f:1-65,
+// rft_buff.f:24-86), FP64.  Lines are gathered into shared memory, transformed, scattered.
+// grid: x = chunk of CH lines, y = batch (plane) with stride `bstride` doubles.
+// --------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_cft_strided(double* __restrict__ c, int ise, int isa, int m, long long bstride,
+                                                     FFTDesc fd, const double2* __restrict__ tw_g, int iopt, int CH) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = fd.n;
+    double2* buf0 = reinterpret_cast<double2*>(smem_raw);
+    double2* buf1 = buf0 + (size_t)n * CH;
+    double2* tw = buf1 + (size_t)n * CH;
+    double* base = c + (size_t)blockIdx.y * bstride;
+    const int l0 = blockIdx.x * CH;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = tw_g[t];
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+        const int b = t % CH, e = t / CH, l = l0 + b;
+        buf0[t] = l < m ? dc(base[(size_t)l * isa + (size_t)e * ise], base[(size_t)l * isa + (size_t)e * ise + 1]) : dc(0, 0);
+    }
+    __syncthreads();
+    double2* res = fft_lines<double2>(buf0, buf1, CH, fd, tw, iopt < 0 ? -1 : +1);
+    const double s = iopt < 0 ? 1.0 / n : 1.0;
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+        const int b = t % CH, e = t / CH, l = l0 + b;
+        if (l < m) {
+            const double2 v = res[t];
+            base[(size_t)l * isa + (size_t)e * ise] = s * v.x;
+            base[(size_t)l * isa + (size_t)e * ise + 1] = s * v.y;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_rft_strided(double* __restrict__ c, int isa, int m, long long bstride,
+                                                     FFTDesc fd, const double2* __restrict__ tw_g, int iopt, int CH) {
+    // each line: complex transform of length n of (real, 0) data; FFTPACK storage
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = fd.n;
+    double2* buf0 = reinterpret_cast<double2*>(smem_raw);
+    double2* buf1 = buf0 + (size_t)n * CH;
+    double2* tw = buf1 + (size_t)n * CH;
+    double* base = c + (size_t)blockIdx.y * bstride;
+    const int l0 = blockIdx.x * CH;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = tw_g[t];
+    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+        const int b = t % CH, k = t / CH, l = l0 + b;
+        double2 v = dc(0, 0);
+        if (l < m) {
+            const double* x = base + (size_t)l * isa;
+            if (iopt < 0) {
+                v = dc(x[k], 0.0);
+            } else {
+                // Hermitian extension of cc(0..n/2); Im cc(0), Im cc(n/2) ignored
+                if (k <= n / 2) v = dc(x[2 * k], (k == 0 || k == n / 2) ? 0.0 : x[2 * k + 1]);
+                else v = dc(x[2 * (n - k)], -x[2 * (n - k) + 1]);
+            }
+        }
+        buf0[t] = v;
+    }
+    __syncthreads();
+    double2* res = fft_lines<double2>(buf0, buf1, CH, fd, tw, iopt < 0 ? -1 : +1);
+    for (int t = threadIdx.x; t < (n + 2) * CH; t += blockDim.x) {
+        const int b = t % CH, e = t / CH, l = l0 + b;
+        if (l >= m) continue;
+        double* x = base + (size_t)l * isa;
+        if (iopt < 0) {
+            const int k = e >> 1;
+            const double2 v = res[(size_t)k * CH + b];
+            double val = (e & 1) ? v.y : v.x;
+            if ((e & 1) && (k == 0 || k == n / 2)) val = 0.0;
+            x[e] = val / n;
+        } else if (e < n) {
+            x[e] = res[(size_t)e * CH + b].x;
+        }
+    }
+}
+
+}  // namespace cfd

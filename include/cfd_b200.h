@@ -1,0 +1,212 @@
+/*
+ * cfd_b200.h - C ABI of the B200 (sm_100a) hot path of the LittleHarsh channel DNS
+ * (Fourier x/z, staggered 2nd-order finite differences in y, Kim & Moin fractional
+ * step with low-storage RK3 / Crank-Nicolson, direct-forcing immersed boundaries).
+ *
+ * Every entry point takes plain pointers, sizes and int32/int64/double scalars so it can
+ * be bound from Fortran with iso_c_binding, from C, or from Python ctypes.  All
+ * functions return an int status (CFD_OK = 0) and never abort the process; the text of
+ * the last error of a context is available from cfd_last_error().
+ *
+ * Citations are file:line in the reference Fortran tree (Mel222/CFD).
+ *
+ * Conventions shared with the reference
+ *  - A spectral field is the reference's cfield%f(j,column) (declaration.f90:140-142):
+ *    complex(8), one y-profile per (kx,kz) column.  With a single y-band the column list
+ *    is k-major, i-minor: column = (k-1)*(N1/2+1) + i + 1, i = 0..N1/2 (kx = alp*i),
+ *    k = 1..N2 (kz = bet*(k-1) for k <= N2/2, -bet*(N2-k+1) above; start.f90:965-986,
+ *    start.f90:1488-1501).  N1 = 2*(Ngal1/3), N2 = 2*(Ngal2/3) (start.f90:108-111).
+ *  - y indices are absolute as in the reference: u/w live on j = -dsty .. ny+dsty
+ *    (ghosts included), v on j = -dsty .. ny+dsty-1 (walls included), p on
+ *    j = -dsty+1 .. ny+dsty-1 (start.f90:1538-1557 with y_grid_rough.f90:46-52).
+ *  - Host arrays passed to cfd_upload_field/cfd_download_field are interleaved
+ *    (re,im) doubles in one of two orders: CFD_LAYOUT_REF is f(j,column) with j fastest
+ *    (the Fortran array itself), CFD_LAYOUT_PLANE is [j][column] with column fastest
+ *    (the device layout, no reordering needed).
+ *  - A physical plane is the reference's xPL(Ngal1+2, Ngal2): Re/Im of kx-mode i at
+ *    entries 2i+1/2i+2 of row k (FOU3D.f90:842-848); after the inverse transform entries
+ *    1..Ngal1 of each row are samples at x=(i-1)Lx/Ngal1.  Forward transforms scale by
+ *    1/(Ngal1*Ngal2), inverse transforms do not (rft_buff.f:60-70, cft_buff.f:41-51).
+ */
+#ifndef CFD_B200_H
+#define CFD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CFD_OK              0
+#define CFD_ERR_ARG         1   /* null pointer, bad enum, out-of-range index           */
+#define CFD_ERR_SIZE        2   /* FFT length not 2^a*3^b, grid too small, list too big  */
+#define CFD_ERR_CUDA        3   /* a CUDA runtime call failed                            */
+#define CFD_ERR_NONFINITE   4   /* NaN/Inf found by the watchdog                         */
+#define CFD_ERR_STATE       5   /* call out of order (e.g. before state upload)          */
+#define CFD_ERR_NOMEM       6   /* device allocation failed at create                    */
+
+/* arithmetic of the transforms and nonlinear products */
+#define CFD_PREC_FP64   0       /* everything in FP64 (the reference's real(8))          */
+#define CFD_PREC_MIXED  1       /* FFTs/products/Nu history in FP32; y-solves, state,
+                                   mean mode, bulk correction in FP64                   */
+
+/* field identifiers */
+#define CFD_FIELD_U1    0       /* u  (ugrid)                       */
+#define CFD_FIELD_U2    1       /* v  (vgrid)                       */
+#define CFD_FIELD_U3    2       /* w  (ugrid)                       */
+#define CFD_FIELD_P     3       /* p  (pgrid)                       */
+#define CFD_FIELD_NU1   4       /* RK nonlinear history, ugrid      */
+#define CFD_FIELD_NU2   5       /* RK nonlinear history, vgrid      */
+#define CFD_FIELD_NU3   6       /* RK nonlinear history, ugrid      */
+#define CFD_FIELD_DIV   7       /* divergence (pgrid, diagnostic)   */
+#define CFD_FIELD_PSI   8       /* pressure increment (pgrid)       */
+#define CFD_FIELD_DU1   9       /* RHS / Helmholtz right-hand side  */
+#define CFD_FIELD_DU2   10
+#define CFD_FIELD_DU3   11
+
+#define CFD_LAYOUT_REF   0      /* f(j,column), j fastest (Fortran cfield%f)             */
+#define CFD_LAYOUT_PLANE 1      /* [j][column], column fastest                           */
+
+/* Problem definition.  Replaces the module globals of declaration.f90 that the hot path
+ * reads (Re, alp, bet, dt, mpgx, QxT, flag_ctpress, N/Ngal, yu, yv, dthdyu, dthdyv,
+ * dyu2i, dyv2i).  Grid arrays start at j = -dsty. */
+typedef struct cfd_config {
+    int32_t ngal1;          /* Ngal(1,1): collocation points in x (2^a*3^b)         */
+    int32_t ngal2;          /* Ngal(2,1): collocation points in z (2^a*3^b)         */
+    int32_t ny;             /* input.in ny: faces from y=-1 to y=1                 */
+    int32_t dsty;           /* in-canopy planes below each crest (dny)             */
+    double  re;             /* Re (bulk)                                           */
+    double  alp, bet;       /* Lx = 2*pi/alp, Lz = 2*pi/bet                        */
+    double  dt;             /* fixed time step                                     */
+    double  mpgx;           /* mean pressure gradient (initial value if ctpress=0) */
+    double  qxt;            /* target flow rate QxT (flag_ctpress = 0)             */
+    int32_t flag_ctpress;   /* 1 = constant pressure gradient, 0 = constant flow   */
+    int32_t precision;      /* CFD_PREC_FP64 or CFD_PREC_MIXED                     */
+    const double *yu;       /* [ny+2*dsty+1]                                       */
+    const double *yv;       /* [ny+2*dsty]                                         */
+    const double *dthdyu;   /* [ny+2*dsty+1]                                       */
+    const double *dthdyv;   /* [ny+2*dsty]                                         */
+    const double *dyu2i;    /* [ny+2*dsty+1][3]  (Fortran dyu2i(3,j))              */
+    const double *dyv2i;    /* [ny+2*dsty][3]                                      */
+} cfd_config;
+
+/* Immersed-boundary forcing list of one grid (start.f90:1133-1145 f_list_ib_u/w_list_ib_u).
+ * idx[p*9 + 0..8] = i,k,j,i2,k2,j2,i3,k3,j3 (i,k 1-based physical indices, j absolute);
+ * w[p*3 + 0..2] = Lap coefficient, w2, w3.  Points act in list order: the reference sorts
+ * them by (j,k,i) (geom_circ_rough_mixed_forcing_24pt.f90:578-606).  jlo/jhi are the plane
+ * ranges that go through the physical round trip (nyuIB1..nyuIB2 / nyvIB1..nyvIB2 of the
+ * bottom [0] and top [1] canopy, start.f90:1091-1101); a range with jhi < jlo is empty.
+ * Every j, j2, j3 must lie inside one of the ranges. */
+typedef struct cfd_ib_list {
+    int32_t        n;
+    const int32_t *idx;
+    const double  *w;
+    int32_t        jlo[2];
+    int32_t        jhi[2];
+} cfd_ib_list;
+
+typedef struct cfd_ctx cfd_ctx;
+
+/* ---- lifetime ------------------------------------------------------------------- */
+
+/* Build a context on CUDA device `device`: validates sizes, uploads the grid, the
+ * wavenumbers and the IB lists, and allocates every device buffer the step needs (no
+ * allocation happens inside a step).  Replaces start() + getbounds() + LU_buildP()
+ * set-up (start.f90:36-649, start.f90:1020-1380, tridLU_3D_IB.f90:417-491).
+ * ibu: list for u and w (ugrid), ibv: list for v (vgrid); either may be NULL. */
+int cfd_create(const cfd_config *cfg, const cfd_ib_list *ibu, const cfd_ib_list *ibv,
+               int32_t device, cfd_ctx **out);
+int cfd_destroy(cfd_ctx *ctx);
+const char *cfd_last_error(const cfd_ctx *ctx);
+
+/* Work on a caller-provided cudaStream_t (NULL = the context's own stream). */
+int cfd_set_stream(cfd_ctx *ctx, void *stream);
+int cfd_synchronize(cfd_ctx *ctx);
+
+/* Sizes: number of complex values of a field (columns * planes), its first absolute j
+ * and its plane count. */
+int cfd_field_shape(const cfd_ctx *ctx, int32_t field, int64_t *ncomplex,
+                    int32_t *j0, int32_t *nplanes, int32_t *ncolumns);
+
+/* ---- state transfer (littleharsh.f90:103-147 arrays) ---------------------------- */
+
+/* Host <-> device copy of one field (complex(8) interleaved).  host must hold
+ * ncomplex complex values in `layout` order.  Stream-ordered; call cfd_synchronize
+ * before reading a downloaded buffer.  Pinned host memory makes the copy async. */
+int cfd_upload_field(cfd_ctx *ctx, int32_t field, const double *host, int32_t layout);
+int cfd_download_field(cfd_ctx *ctx, int32_t field, double *host, int32_t layout);
+/* Device pointer of a field (FP64 [j][column] complex; NU* are FP32 complex in
+ * CFD_PREC_MIXED).  Lets a caller fill state in place. */
+int cfd_field_device_ptr(cfd_ctx *ctx, int32_t field, void **dev_ptr);
+
+/* ---- one RK substep, stage by stage (littleharsh.f90:163-189) -------------------- */
+/* krk = 1, 2, 3 selects the Le & Moin coefficients (start.f90:395-409). */
+
+/* RHS0_u1/u2/u3 (littleharsh.f90:613-730): du = a/Re*L(u) - c*Nu_old - d*grad p
+ * (+ -d*mpgx on the (0,0) mode). */
+int cfd_rhs0(cfd_ctx *ctx, int32_t krk);
+/* nonlinear (FOU3D.f90:41-259): y-interpolation, inverse FFTs, products, forward FFTs,
+ * x/z and y derivatives; Nu <- new advective term; du += -g*Nu. */
+int cfd_nonlinear(cfd_ctx *ctx, int32_t krk);
+/* solveU(u1), solveV(u2), solveU(u3) (littleharsh.f90:172-174, 732-794): du = u + dt*du,
+ * immersed_boundaries_U/V (tridLU_3D_IB.f90:163-281), LUsolU/LUsolV (:50-160). */
+int cfd_solve_uvw(cfd_ctx *ctx, int32_t krk);
+/* meanflow_ctU / flowrate_corr (littleharsh.f90:452-484, 522-537) if flag_ctpress = 0;
+ * meanflow_ctP (littleharsh.f90:504-520) otherwise. */
+int cfd_meanflow(cfd_ctx *ctx, int32_t krk);
+/* solveP (littleharsh.f90:556-611): divergence, psi = div/(dt(a+b)), LUsolP, p += psi. */
+int cfd_solve_p(cfd_ctx *ctx, int32_t krk);
+/* v_corr (littleharsh.f90:796-907): u -= dt(a+b) grad psi, ghost/wall rows. */
+int cfd_vcorr(cfd_ctx *ctx, int32_t krk);
+
+/* The whole substep (all of the above in order) and whole RK3 steps.  cfd_step captures
+ * one RK3 step in a CUDA graph on first use and replays it. */
+int cfd_rk_substep(cfd_ctx *ctx, int32_t krk);
+int cfd_step(cfd_ctx *ctx, int32_t nsteps);
+
+/* Scalars of the mean mode: mpgx, Qx (flow rate between the crests), dgx (last
+ * correction).  Synchronises the context stream. */
+int cfd_get_scalars(cfd_ctx *ctx, double *mpgx, double *qx, double *dgx);
+
+/* Largest |div| over all columns and p-planes (error(), littleharsh.f90:322-351).
+ * Synchronises. */
+int cfd_divergence_max(cfd_ctx *ctx, double *errmax);
+
+/* ---- transforms (four_to_phys_du / phys_to_four_du, FOU3D.f90:574-592, 1619-1639) -- */
+
+/* In-place batched 2-D transforms of `nplanes` device planes laid out as the reference's
+ * xPL(Ngal1+2, Ngal2) (plane stride (Ngal1+2)*Ngal2 doubles).  Inverse: complex z
+ * transform of kx-modes 0..N1/2 then real x transform of every row; forward: the reverse,
+ * scaled by 1/(Ngal1*Ngal2).  If zero_oddball, row Ngal2/2+1 is zeroed first
+ * (four_to_phys_u, FOU3D.f90:561-563). */
+int cfd_four_to_phys(cfd_ctx *ctx, double *planes_dev, int32_t nplanes, int32_t zero_oddball);
+int cfd_phys_to_four(cfd_ctx *ctx, double *planes_dev, int32_t nplanes);
+
+/* Batched strided transforms with the FFTPACK-wrapper semantics of the reference, on
+ * device memory.  rft: m real vectors of length Ngal1 at stride isa (rft_buff.f:24-86);
+ * cft: m complex vectors of length Ngal2, element stride ise, vector stride isa, both in
+ * doubles (cft_buff.f:1-65).  iopt >= 0 inverse (unscaled), iopt < 0 forward (x 1/n).
+ * n must be the context's Ngal1 (rft) or Ngal2 (cft). */
+int cfd_rft(cfd_ctx *ctx, double *c_dev, int32_t isa, int32_t m, int32_t iopt);
+int cfd_cft(cfd_ctx *ctx, double *c_dev, int32_t ise, int32_t isa, int32_t m, int32_t iopt);
+
+/* ---- introspection ---------------------------------------------------------------- */
+
+/* Per-kernel timing: while enabled, every kernel launched by a stage entry point (not by
+ * a graph replay) is bracketed by CUDA events on the context stream.  cfd_profile_read
+ * synchronises and writes one line "name calls total_ms" per kernel into buf (NUL
+ * terminated, truncated to buflen) and clears the records. */
+int cfd_profile(cfd_ctx *ctx, int32_t enable);
+int cfd_profile_read(cfd_ctx *ctx, char *buf, int32_t buflen);
+
+/* Number of kernel launches issued by this context since creation (all entry points). */
+int cfd_launch_count(const cfd_ctx *ctx, int64_t *count);
+/* Library version string. */
+const char *cfd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFD_B200_H */

