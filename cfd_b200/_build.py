@@ -5,8 +5,8 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(HERE, "csrc", "cfd_capi.cu")
-DEPS = [os.path.join(HERE, "csrc", f) for f in ("cfd_capi.cu", "channel_kernels.cuh", "fft_smem.cuh")] + \
+SRCS = [os.path.join(HERE, "csrc", f) for f in ("cfd_capi.cu", "cfd_noalloc.cu")]
+DEPS = SRCS + [os.path.join(HERE, "csrc", f) for f in ("channel_kernels.cuh", "fft_smem.cuh")] + \
     [os.path.join(os.path.dirname(HERE), "include", "cfd_b200.h")]
 OUT = os.path.join(HERE, "_lib", "libcfdb200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
@@ -26,7 +26,7 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     stale = force or not os.path.exists(OUT) or \
         any(os.path.getmtime(d) > os.path.getmtime(OUT) for d in DEPS)
     if stale:
-        cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT, SRC]
+        cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT] + SRCS
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

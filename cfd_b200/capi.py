@@ -104,6 +104,8 @@ SIGNATURES = {
     "cfd_launch_count": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "cfd_profile": (C.c_int, [_VP, C.c_int32]),
     "cfd_profile_read": (C.c_int, [_VP, C.c_char_p, C.c_int32]),
+    "cfd_lusol_u_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                      _VP, _VP, _VP, _VP, _VP, _VP]),
     "cfd_version": (C.c_char_p, []),
 }
 

@@ -191,6 +191,30 @@ int cfd_phys_to_four(cfd_ctx *ctx, double *planes_dev, int32_t nplanes);
 int cfd_rft(cfd_ctx *ctx, double *c_dev, int32_t isa, int32_t m, int32_t iopt);
 int cfd_cft(cfd_ctx *ctx, double *c_dev, int32_t ise, int32_t isa, int32_t m, int32_t iopt);
 
+/* ---- allocation-free solve ----------------------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc/cudaFree: a
+ * driver whose device memory belongs to another allocator or sits under a hard cap, or a
+ * loop that must not take cudaFree's implicit device synchronisation.  Solves the u/w
+ * Helmholtz system of LUsolU (ghost rows (0,1,gw_bot) and (gw_top,1,0), interior rows
+ * -beta*dyu2i(1), 1-beta*(dyu2i(2)+k2x+k2z), -beta*dyu2i(3)) for one complex right-hand
+ * side on caller-owned device memory, with no context and no allocation.
+ *   rhs_dev, u_dev : [nplanes][nkx*n2] complex (interleaved doubles, CFD_LAYOUT_PLANE order)
+ *   kx_dev [nkx], kz_dev [n2], dyu2i_dev [nplanes][3] : device arrays
+ * Its Thomas scratch is one file-scope device array of CFD_NOALLOC_MAX_SCRATCH doubles
+ * (128 MiB) that every GPU loading the library holds until exit; (nplanes-1)*nkx*n2 above
+ * that returns CFD_ERR_SIZE before any GPU work.  The first call on a device looks up that
+ * device's copy of the array (with the device current), so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other streams, other
+ * host threads) race on it and give wrong results.  Nothing in it needs to start at zero.
+ * Enqueued on `stream` (NULL = legacy default stream); returns CFD_ERR_CUDA on a launch
+ * failure. */
+#define CFD_NOALLOC_MAX_SCRATCH (16u * 1024u * 1024u)
+int cfd_lusol_u_noalloc(int32_t nkx, int32_t n2, int32_t nplanes, double beta,
+                        double gw_bot, double gw_top, const double *kx_dev,
+                        const double *kz_dev, const double *dyu2i_dev,
+                        const double *rhs_dev, double *u_dev, void *stream);
+
 /* ---- introspection ---------------------------------------------------------------- */
 
 /* Per-kernel timing: while enabled, every kernel launched by a stage entry point (not by
