@@ -173,22 +173,46 @@ int dalloc(cfd_ctx* c, T** p, size_t n) {
 
 size_t zsmem(int n, int CH, size_t esz) { return (size_t)(2 * n * CH + n) * esz; }
 
+int ilog2(int b) {
+    int s = 0;
+    while ((1 << s) < b) ++s;
+    return s;
+}
+
+// Run BODY with NF = the fixed transform length of n (or 0 = runtime plan).
+#define FFT_SWITCH(n, ...)                                \
+    switch (n) {                                           \
+        case 64: { constexpr int NF = 64; __VA_ARGS__; } break;   \
+        case 96: { constexpr int NF = 96; __VA_ARGS__; } break;   \
+        case 128: { constexpr int NF = 128; __VA_ARGS__; } break; \
+        case 192: { constexpr int NF = 192; __VA_ARGS__; } break; \
+        case 384: { constexpr int NF = 384; __VA_ARGS__; } break; \
+        case 768: { constexpr int NF = 768; __VA_ARGS__; } break; \
+        default: { constexpr int NF = 0; __VA_ARGS__; } break;    \
+    }
+
 // ---------------------------------------------------------------------------------------
 template <typename T2>
 int set_smem_attrs(cfd_ctx* c) {
-    const size_t e = sizeof(T2);
+    const size_t esz = sizeof(T2);
     const int n2 = c->d.ngal2, n1 = c->d.ngal1;
-    size_t sz = zsmem(n2, c->CHz, e);
-    size_t sx = (size_t)(2 * (2 * c->RWx) * n1 + n1) * e;
-    size_t si = (size_t)(2 * c->RWib * n1 + n1) * e;
-    size_t sf = (size_t)(2 * (c->RWibf / 2) * n1 + n1) * e;
-    CK(cudaFuncSetAttribute(k_zinv<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
-    CK(cudaFuncSetAttribute(k_zfwd<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
-    CK(cudaFuncSetAttribute(k_ib_zinv<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
-    CK(cudaFuncSetAttribute(k_ib_zfwd<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
-    CK(cudaFuncSetAttribute(k_xline<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx));
-    CK(cudaFuncSetAttribute(k_ib_xinv<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)si));
-    CK(cudaFuncSetAttribute(k_ib_xfwd<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf));
+    size_t sz = zsmem(n2, c->CHz, esz);
+    size_t sx = (size_t)(2 * (2 * c->RWx) * n1 + n1) * esz;
+    size_t si = (size_t)(2 * c->RWib * n1 + n1) * esz;
+    size_t sf = (size_t)(2 * (c->RWibf / 2) * n1 + n1) * esz;
+    cudaError_t e = cudaSuccess;
+    FFT_SWITCH(n2, {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_zinv<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_zfwd<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ib_zinv<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ib_zfwd<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz);
+    });
+    FFT_SWITCH(n1, {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xline<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ib_xinv<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)si);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ib_xfwd<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
+    });
+    CK(e);
     return CFD_OK;
 }
 
@@ -219,19 +243,26 @@ int nl_transforms(cfd_ctx* c) {
     const size_t e = sizeof(T2);
     dim3 gz((d.nkx + CH - 1) / CH, d.nslot, 3);
     prof_mark(c);
-    k_zinv<T2><<<gz, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0], (T2*)c->H[1],
-                                                             (T2*)c->H[2], c->fz, twz<T2>(c), CH);
+    FFT_SWITCH(d.ngal2, {
+        k_zinv<T2, NF><<<gz, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0],
+                                                                     (T2*)c->H[1], (T2*)c->H[2], c->fz, twz<T2>(c), CH,
+                                                                     ilog2(CH));
+    });
     LK("k_zinv");
     dim3 gx(d.ngal2 / c->RWx, d.nslot);
     prof_mark(c);
-    k_xline<T2><<<gx, 256, (size_t)(2 * (2 * c->RWx) * d.ngal1 + d.ngal1) * e, c->stream>>>(
-        d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], c->fx, twx<T2>(c), c->RWx);
+    FFT_SWITCH(d.ngal1, {
+        k_xline<T2, NF><<<gx, 256, (size_t)(2 * (2 * c->RWx) * d.ngal1 + d.ngal1) * e, c->stream>>>(
+            d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], c->fx, twx<T2>(c), c->RWx, ilog2(2 * c->RWx));
+    });
     LK("k_xline");
     dim3 gf((d.nkx + CH - 1) / CH, d.nslot, 4);
     prof_mark(c);
-    k_zfwd<T2><<<gf, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
-                                                             (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2], (T2*)c->S[3],
-                                                             c->fz, twz<T2>(c), CH);
+    FFT_SWITCH(d.ngal2, {
+        k_zfwd<T2, NF><<<gf, 256, zsmem(d.ngal2, CH, e), c->stream>>>(
+            d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
+            (T2*)c->S[3], c->fz, twz<T2>(c), CH, ilog2(CH));
+    });
     LK("k_zfwd");
     return CFD_OK;
 }
@@ -262,13 +293,17 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     dst.f[0] = rhs_a; dst.f[1] = rhs_b;
     dim3 g1((d.nkx + CH - 1) / CH, ib.npl, 2 * nb);
     prof_mark(c);
-    k_ib_zinv<T2><<<g1, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib, c->fz,
-                                                                twz<T2>(c), CH);
+    FFT_SWITCH(d.ngal2, {
+        k_ib_zinv<T2, NF><<<g1, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib,
+                                                                        c->fz, twz<T2>(c), CH, ilog2(CH));
+    });
     LK("k_ib_zinv");
     dim3 g2(d.ngal2 / c->RWib, ib.npl, nb);
     prof_mark(c);
-    k_ib_xinv<T2><<<g2, 256, (size_t)(2 * c->RWib * d.ngal1 + d.ngal1) * e, c->stream>>>(d, (T2*)c->Hib, ib.npl, (R*)c->phys,
-                                                                                      c->fx, twx<T2>(c), c->RWib);
+    FFT_SWITCH(d.ngal1, {
+        k_ib_xinv<T2, NF><<<g2, 256, (size_t)(2 * c->RWib * d.ngal1 + d.ngal1) * e, c->stream>>>(
+            d, (T2*)c->Hib, ib.npl, (R*)c->phys, c->fx, twx<T2>(c), c->RWib, ilog2(c->RWib));
+    });
     LK("k_ib_xinv");
     if (ib.n > 0) {
         dim3 g3((ib.n + 255) / 256, nb);
@@ -278,13 +313,17 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     }
     dim3 g4(d.ngal2 / c->RWibf, ib.npl, nb);
     prof_mark(c);
-    k_ib_xfwd<T2><<<g4, 256, (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * e, c->stream>>>(
-        d, (T2*)c->Hib, ib.npl, (const R*)c->phys, c->fx, twx<T2>(c), c->RWibf);
+    FFT_SWITCH(d.ngal1, {
+        k_ib_xfwd<T2, NF><<<g4, 256, (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * e, c->stream>>>(
+            d, (T2*)c->Hib, ib.npl, (const R*)c->phys, c->fx, twx<T2>(c), c->RWibf, ilog2(c->RWibf / 2));
+    });
     LK("k_ib_xfwd");
     dim3 g5((d.nkx + CH - 1) / CH, ib.npl, nb);
     prof_mark(c);
-    k_ib_zfwd<T2><<<g5, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0, ib.planes, c->fz,
-                                                                twz<T2>(c), CH);
+    FFT_SWITCH(d.ngal2, {
+        k_ib_zfwd<T2, NF><<<g5, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0, ib.planes,
+                                                                        c->fz, twz<T2>(c), CH, ilog2(CH));
+    });
     LK("k_ib_zfwd");
     return CFD_OK;
 }

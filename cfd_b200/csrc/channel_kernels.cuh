@@ -61,11 +61,11 @@ __device__ __forceinline__ double2 to_d2(double2 a) { return a; }
 //   u-plane j: U = u1(j), W = u3(j), V = v interpolated to the centre (with ghost rows)
 //   v-plane j: U = u1 interpolated to the face, W = u3 interpolated, V = u2(j)
 // --------------------------------------------------------------------------------------
-template <typename T2>
+template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __restrict__ u1,
                                               const double2* __restrict__ u2, const double2* __restrict__ u3,
                                               T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
-                                              FFTDesc fz, const T2* __restrict__ twz, int CH) {
+                                              FFTDesc fz, const T2* __restrict__ twz, int CH, int bshift) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* buf0 = reinterpret_cast<T2*>(smem_raw);
     T2* buf1 = buf0 + (size_t)d.ngal2 * CH;
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __re
         buf0[(size_t)row_of(d, q) * CH + b] = to_t2<T2>(val);
     }
     __syncthreads();
-    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, +1);
+    T2* res = fft_batch<T2, NF, +1>(buf0, buf1, CH, bshift, fz, tw);
     T2* H = f == 0 ? H0 : (f == 1 ? H1 : H2);
     const size_t base = (size_t)slot * n * d.nkx;
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
@@ -164,9 +164,9 @@ __device__ __forceinline__ T2 herm_line(const Dims& d, const T2* A, const T2* B,
     return cx<T2>((R)0, (R)0);
 }
 
-template <typename T2>
+template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
-                                               T2* __restrict__ H3, FFTDesc fx, const T2* __restrict__ twx, int RW) {
+                                               T2* __restrict__ H3, FFTDesc fx, const T2* __restrict__ twx, int RW, int bshift) {
     using R = decltype(T2::x);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = d.ngal1;
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
         buf0[(size_t)k * B + b] = v;
     }
     __syncthreads();
-    T2* P = fft_lines<T2>(buf0, buf1, B, fx, tw, +1);
+    T2* P = fft_batch<T2, NF, +1>(buf0, buf1, B, bshift, fx, tw);
     T2* Q = P == buf0 ? buf1 : buf0;
     for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
         const int rr = t % RW, k = t / RW;
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
         }
     }
     __syncthreads();
-    T2* F = fft_lines<T2>(P, Q, B, fx, tw, -1);
+    T2* F = fft_batch<T2, NF, -1>(P, Q, B, bshift, fx, tw);
     const R s = (R)1 / (R)n;
     const int nl = uplane ? B : RW;  // v-planes carry one output line per row
     for (int t = threadIdx.x; t < d.nkx * nl; t += blockDim.x) {
@@ -226,11 +226,11 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // Output spectral products S_f[slot][column]:  u-plane: S0=uu S1=uw S2=vv S3=ww;
 // v-plane: S0=uv S1=vw.   grid: x = kx chunk, y = slot, z = field 0..3
 // --------------------------------------------------------------------------------------
-template <typename T2>
+template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1,
                                               const T2* __restrict__ H2, const T2* __restrict__ H3,
                                               T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
-                                              T2* __restrict__ S3, FFTDesc fz, const T2* __restrict__ twz, int CH) {
+                                              T2* __restrict__ S3, FFTDesc fz, const T2* __restrict__ twz, int CH, int bshift) {
     using R = decltype(T2::x);
     const int slot = blockIdx.y;
     const int f = blockIdx.z;
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0,
         buf0[t] = i < d.nkx ? H[base + (size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
     }
     __syncthreads();
-    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, -1);
+    T2* res = fft_batch<T2, NF, -1>(buf0, buf1, CH, bshift, fz, tw);
     const R s = (R)1 / (R)n;
     for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
         const int b = t % CH, q = t / CH;
@@ -412,9 +412,9 @@ struct IBDst {
 
 // inverse z transform of the IB planes of every source.  grid: x = kx chunk, y = plane,
 // z = source.  Hib[(s*npl + p)][z][kx]
-template <typename T2>
+template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_ib_zinv(Dims d, IBSrc src, int j0, const int* __restrict__ planes, int npl,
-                                                 T2* __restrict__ Hib, FFTDesc fz, const T2* __restrict__ twz, int CH) {
+                                                 T2* __restrict__ Hib, FFTDesc fz, const T2* __restrict__ twz, int CH, int bshift) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = d.ngal2;
     T2* buf0 = reinterpret_cast<T2*>(smem_raw);
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(256) k_ib_zinv(Dims d, IBSrc src, int j0, cons
         buf0[(size_t)row_of(d, q) * CH + b] = to_t2<T2>(f[(size_t)(j - j0) * d.ncol + (size_t)q * d.nkx + i]);
     }
     __syncthreads();
-    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, +1);
+    T2* res = fft_batch<T2, NF, +1>(buf0, buf1, CH, bshift, fz, tw);
     const size_t base = ((size_t)s * npl + p) * n * d.nkx;
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, z = t / CH, i = kx0 + b;
@@ -442,9 +442,9 @@ __global__ void __launch_bounds__(256) k_ib_zinv(Dims d, IBSrc src, int j0, cons
 
 // inverse x transform: line (rhs + i u) of one row -> physical rhs, u.
 // grid: x = row chunk (RW rows), y = plane, z = batch fb.  Phys[(fb*2+which)*npl + p][z][x]
-template <typename T2>
+template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_ib_xinv(Dims d, const T2* __restrict__ Hib, int npl, decltype(T2::x)* __restrict__ phys,
-                                                 FFTDesc fx, const T2* __restrict__ twx, int RW) {
+                                                 FFTDesc fx, const T2* __restrict__ twx, int RW, int bshift) {
     using R = decltype(T2::x);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = d.ngal1;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(256) k_ib_xinv(Dims d, const T2* __restrict__ 
         buf0[(size_t)k * RW + b] = herm_line<T2>(d, Hr + rb, Hu + rb, k);
     }
     __syncthreads();
-    T2* res = fft_lines<T2>(buf0, buf1, RW, fx, tw, +1);
+    T2* res = fft_batch<T2, NF, +1>(buf0, buf1, RW, bshift, fx, tw);
     const size_t ppl = (size_t)d.ngal2 * n;
     R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl;
     R* pu = phys + ((size_t)(2 * fb + 1) * npl + p) * ppl;
@@ -511,9 +511,9 @@ __global__ void k_ib_force(Dims d, const int* __restrict__ idx, const double* __
 // forward x transform of physical rhs rows (two rows per complex line), truncated to
 // kx <= N1/2, x 1/Ngal1.  grid: x = row chunk (RW rows, RW even), y = plane, z = batch.
 // Output into Hib[(fb*2)*npl + p] (the rhs slot).
-template <typename T2>
+template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_ib_xfwd(Dims d, T2* __restrict__ Hib, int npl, const decltype(T2::x)* __restrict__ phys,
-                                                 FFTDesc fx, const T2* __restrict__ twx, int RW) {
+                                                 FFTDesc fx, const T2* __restrict__ twx, int RW, int bshift) {
     using R = decltype(T2::x);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = d.ngal1;
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(256) k_ib_xfwd(Dims d, T2* __restrict__ Hib, i
         buf0[(size_t)k * B + b] = cx<T2>(pr[(size_t)(z0 + 2 * b) * n + k], pr[(size_t)(z0 + 2 * b + 1) * n + k]);
     }
     __syncthreads();
-    T2* F = fft_lines<T2>(buf0, buf1, B, fx, tw, -1);
+    T2* F = fft_batch<T2, NF, -1>(buf0, buf1, B, bshift, fx, tw);
     const R s = (R)1 / (R)n;
     T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)d.ngal2 * d.nkx;
     for (int t = threadIdx.x; t < d.nkx * B; t += blockDim.x) {
@@ -544,10 +544,10 @@ __global__ void __launch_bounds__(256) k_ib_xfwd(Dims d, T2* __restrict__ Hib, i
 
 // forward z transform of the rhs slot and write-back to every column of the plane
 // (planes_to_modes_dU/dV).  grid: x = kx chunk, y = plane, z = batch fb
-template <typename T2>
+template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ Hib, int npl, IBDst dst, int j0,
                                                  const int* __restrict__ planes, FFTDesc fz, const T2* __restrict__ twz,
-                                                 int CH) {
+                                                 int CH, int bshift) {
     using R = decltype(T2::x);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = d.ngal2;
@@ -562,7 +562,7 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
         buf0[t] = i < d.nkx ? H[(size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
     }
     __syncthreads();
-    T2* res = fft_lines<T2>(buf0, buf1, CH, fz, tw, -1);
+    T2* res = fft_batch<T2, NF, -1>(buf0, buf1, CH, bshift, fz, tw);
     const R s = (R)1 / (R)n;
     double2* out = dst.f[fb] + (size_t)(planes[p] - j0) * d.ncol;
     for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {

@@ -115,3 +115,149 @@ __device__ T2* fft_lines(T2* a, T2* b, int B, const FFTDesc& d, const T2* __rest
 }
 
 }  // namespace cfd
+
+// ======================================================================================
+// Fixed-length engine for the production lengths (64, 96, 128, 192, 384, 768): the radix
+// plan is a compile-time constant (radix 8 first, then 4/6/3), so every index of a pass is
+// a constant-folded multiply/shift; the batch count B is a power of two (B = 1 << bshift).
+// ======================================================================================
+namespace cfd {
+
+template <int N> struct RadixPlan { static constexpr int P = 0; static constexpr int R[1] = {1}; };
+template <> struct RadixPlan<64> { static constexpr int P = 2; static constexpr int R[2] = {8, 8}; };
+template <> struct RadixPlan<96> { static constexpr int P = 3; static constexpr int R[3] = {8, 4, 3}; };
+template <> struct RadixPlan<128> { static constexpr int P = 3; static constexpr int R[3] = {8, 4, 4}; };
+template <> struct RadixPlan<192> { static constexpr int P = 3; static constexpr int R[3] = {8, 8, 3}; };
+template <> struct RadixPlan<384> { static constexpr int P = 3; static constexpr int R[3] = {8, 8, 6}; };
+template <> struct RadixPlan<768> { static constexpr int P = 4; static constexpr int R[4] = {8, 8, 4, 3}; };
+
+template <int N> struct IsFixed { static constexpr bool value = RadixPlan<N>::P > 0; };
+
+// multiply by SIGN*i
+template <int SIGN, typename T2> __device__ __forceinline__ T2 mul_si(T2 a) {
+    return SIGN < 0 ? cx<T2>(a.y, -a.x) : cx<T2>(-a.y, a.x);
+}
+
+template <int SIGN, typename T2> __device__ __forceinline__ void dft2(T2& a, T2& b) {
+    T2 t = csub(a, b);
+    a = cadd(a, b);
+    b = t;
+}
+
+template <int SIGN, typename T2> __device__ __forceinline__ void dft3(T2& x0, T2& x1, T2& x2) {
+    using R_t = decltype(T2::x);
+    const R_t s3 = (R_t)0.86602540378443864676 * (R_t)SIGN;
+    T2 t1 = cadd(x1, x2);
+    T2 t2 = csub(x0, cscale(t1, (R_t)0.5));
+    T2 d = csub(x1, x2);
+    T2 t3 = cx<T2>(-s3 * d.y, s3 * d.x);
+    x0 = cadd(x0, t1);
+    x1 = cadd(t2, t3);
+    x2 = csub(t2, t3);
+}
+
+template <int SIGN, typename T2> __device__ __forceinline__ void dft4(T2& x0, T2& x1, T2& x2, T2& x3) {
+    T2 a0 = cadd(x0, x2), a1 = csub(x0, x2);
+    T2 b0 = cadd(x1, x3), b1 = mul_si<SIGN>(csub(x1, x3));
+    x0 = cadd(a0, b0);
+    x2 = csub(a0, b0);
+    x1 = cadd(a1, b1);
+    x3 = csub(a1, b1);
+}
+
+// radix-6 = even/odd split into two DFT3: X_k = E_{k%3} + w6^k O_{k%3}
+template <int SIGN, typename T2> __device__ __forceinline__ void dft6(T2* v) {
+    using R_t = decltype(T2::x);
+    T2 e0 = v[0], e1 = v[2], e2 = v[4], o0 = v[1], o1 = v[3], o2 = v[5];
+    dft3<SIGN>(e0, e1, e2);
+    dft3<SIGN>(o0, o1, o2);
+    const R_t h = (R_t)0.5, s = (R_t)0.86602540378443864676 * (R_t)SIGN;
+    const T2 w1 = cx<T2>(h, s), w2 = cx<T2>(-h, s);  // w6^1, w6^2
+    const T2 p1 = cmul(o1, w1), p2 = cmul(o2, w2);
+    v[0] = cadd(e0, o0); v[3] = csub(e0, o0);
+    v[1] = cadd(e1, p1); v[4] = csub(e1, p1);
+    v[2] = cadd(e2, p2); v[5] = csub(e2, p2);
+}
+
+// radix-8 = even/odd split into two DFT4: X_k = A_{k%4} + w8^k B_{k%4}
+template <int SIGN, typename T2> __device__ __forceinline__ void dft8(T2* v) {
+    using R_t = decltype(T2::x);
+    T2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];
+    T2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];
+    dft4<SIGN>(a0, a1, a2, a3);
+    dft4<SIGN>(b0, b1, b2, b3);
+    const R_t r = (R_t)0.70710678118654752440;
+    // w8^1 = r(1 + SIGN i), w8^2 = SIGN i, w8^3 = r(-1 + SIGN i)
+    const T2 q1 = cmul(b1, cx<T2>(r, (R_t)SIGN * r));
+    const T2 q2 = mul_si<SIGN>(b2);
+    const T2 q3 = cmul(b3, cx<T2>(-r, (R_t)SIGN * r));
+    v[0] = cadd(a0, b0); v[4] = csub(a0, b0);
+    v[1] = cadd(a1, q1); v[5] = csub(a1, q1);
+    v[2] = cadd(a2, q2); v[6] = csub(a2, q2);
+    v[3] = cadd(a3, q3); v[7] = csub(a3, q3);
+}
+
+template <int R, int SIGN, typename T2> __device__ __forceinline__ void dftR(T2* v) {
+    if constexpr (R == 2) dft2<SIGN>(v[0], v[1]);
+    else if constexpr (R == 3) dft3<SIGN>(v[0], v[1], v[2]);
+    else if constexpr (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+    else if constexpr (R == 6) dft6<SIGN>(v);
+    else dft8<SIGN>(v);
+}
+
+// one Stockham pass: B lines at buf[e*B + b], Ns = product of the previous radices
+template <typename T2, int N, int PASS, int NS, int SIGN>
+__device__ __forceinline__ void fixed_pass(const T2* __restrict__ in, T2* __restrict__ out, int bshift,
+                                           const T2* __restrict__ tw) {
+    constexpr int R = RadixPlan<N>::R[PASS];
+    constexpr int NR = N / R;
+    constexpr int TSTEP = N / (NS * R);
+    const int B = 1 << bshift;
+    const int ntask = NR << bshift;
+    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
+        const int bb = t & (B - 1);
+        const int i = t >> bshift;
+        const int k = i % NS;
+        T2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = in[((i + r * NR) << bshift) + bb];
+        if constexpr (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const T2 w = tw[r * k * TSTEP];
+                v[r] = SIGN < 0 ? cmul(v[r], w) : cmulc(v[r], w);
+            }
+        }
+        dftR<R, SIGN>(v);
+        const int idxD = (i / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) out[((idxD + r * NS) << bshift) + bb] = v[r];
+    }
+    __syncthreads();
+}
+
+template <typename T2, int N, int PASS, int NS, int SIGN>
+__device__ __forceinline__ T2* fixed_passes(T2* a, T2* b, int bshift, const T2* tw) {
+    if constexpr (PASS == RadixPlan<N>::P) {
+        return a;
+    } else {
+        fixed_pass<T2, N, PASS, NS, SIGN>(a, b, bshift, tw);
+        return fixed_passes<T2, N, PASS + 1, NS * RadixPlan<N>::R[PASS], SIGN>(b, a, bshift, tw);
+    }
+}
+
+// Batched transform dispatch: NF = 0 uses the runtime plan `d` (any 2^a*3^b), otherwise
+// the fixed engine for length NF (B must then be a power of two, B = 1 << bshift).
+template <typename T2, int NF, int SIGN>
+__device__ __forceinline__ T2* fft_batch(T2* a, T2* b, int B, int bshift, const FFTDesc& d, const T2* tw) {
+    if constexpr (NF == 0) {
+        (void)bshift;
+        return fft_lines<T2>(a, b, B, d, tw, SIGN);
+    } else {
+        (void)d;
+        (void)B;
+        return fixed_passes<T2, NF, 0, 1, SIGN>(a, b, bshift, tw);
+    }
+}
+
+}  // namespace cfd

@@ -190,3 +190,38 @@ def test_errors_are_codes_not_crashes(torch_cuda):
     g.close()
     with pytest.raises(capi.CfdError, match="2\\^a\\*3\\^b"):
         Channel(build_channel(tiny(ngal1=20, posth=0.0, cyl_diameter=0.0)))   # 20 is not 2^a 3^b
+
+
+# grids whose x and z lengths cover every fixed-length transform (64, 96, 128, 192, 384, 768)
+FIXED_GRIDS = [(64, 96, 17), (96, 192, 13), (128, 64, 13), (192, 128, 11), (384, 768, 9), (768, 384, 9)]
+
+
+@pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
+def test_fixed_length_transforms(torch_cuda, ng1, ng2, ny):
+    from cfd_b200.channel import build_channel
+    from cfd_b200.config import tiny
+    s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=ng1 + ng2))
+    assert s.ibu.n > 0
+    o = oracle(s)
+    o.rk_substep(1)
+    ref1 = o.download_state()
+    o.rk_substep(2)
+    o.rk_substep(3)
+    ref = o.download_state()
+    g = make(s, "fp64")
+    g.rk_substep(1)
+    st = g.download_state()
+    for k in ("u1", "u2", "u3", "p"):
+        assert rel(st[k], ref1[k]) < 1e-11, (k, rel(st[k], ref1[k]))
+    g.rk_substep(2)
+    g.rk_substep(3)
+    st = g.download_state()
+    for k in ("u1", "u2", "u3", "p"):
+        assert rel(st[k], ref[k]) < 1e-10, (k, rel(st[k], ref[k]))
+    g.close()
+    m = make(s, "mixed")
+    m.step(1)
+    st = m.download_state()
+    for k in ("u1", "u2", "u3"):
+        assert rel(st[k], ref[k]) < 1e-5, (k, rel(st[k], ref[k]))
+    m.close()
