@@ -70,6 +70,9 @@ struct cfd_ctx {
     void* H[4] = {nullptr, nullptr, nullptr, nullptr};
     void* S[4] = {nullptr, nullptr, nullptr, nullptr};
     double* cs = nullptr;
+    double* cs_v = nullptr;
+    int JC = 16;
+    int nch = 1;
     double* scal = nullptr;
     double* mf_work = nullptr;
     double2* stage0 = nullptr;
@@ -272,9 +275,10 @@ int rhs_kernel(cfd_ctx* c, int krk) {
     const Dims& d = c->d;
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
+    gb.y = c->nch;
     k_rhs<T2, MODE><<<gb, 256, 0, c->stream>>>(d, c->g, coef(c, krk), c->scal, c->u1, c->u2, c->u3, c->p, (T2*)c->Nu1,
                                                (T2*)c->Nu2, (T2*)c->Nu3, c->du1, c->du2, c->du3, (const T2*)c->S[0],
-                                               (const T2*)c->S[1], (const T2*)c->S[2], (const T2*)c->S[3]);
+                                               (const T2*)c->S[1], (const T2*)c->S[2], (const T2*)c->S[3], c->JC);
     LK("k_rhs");
     return CFD_OK;
 }
@@ -340,7 +344,8 @@ int solve_kernel(cfd_ctx* c, int krk) {
     const double beta = kRKb[krk - 1] * c->dt / c->re;
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
-    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, 1, 1);
+    gb.y = 2;
+    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v);
     LK("k_solve_uvw");
     return CFD_OK;
 }
@@ -370,8 +375,14 @@ int vcorr_kernel(cfd_ctx* c, int krk, bool with_div) {
     const double dtrk = c->dt * (kRKa[krk - 1] + kRKb[krk - 1]);
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
-    k_vcorr<<<gb, 256, 0, c->stream>>>(d, c->g, dtrk, c->u1, c->u2, c->u3, c->psi, with_div ? c->div : nullptr);
-    LK("k_vcorr");
+    if (with_div) {
+        k_vcorr<<<gb, 256, 0, c->stream>>>(d, c->g, dtrk, c->u1, c->u2, c->u3, c->psi, c->div);
+        LK("k_vcorr");
+    } else {
+        gb.y = c->nch;
+        k_vcorr_chunk<<<gb, 256, 0, c->stream>>>(d, c->g, dtrk, c->u1, c->u2, c->u3, c->psi, c->JC);
+        LK("k_vcorr_chunk");
+    }
     return CFD_OK;
 }
 
@@ -603,6 +614,9 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         else { AL(c->H[k], double2, hsz); AL(c->S[k], double2, (size_t)d.nslot * nc); }
     }
     AL(c->cs, double, nc * nyu);
+    AL(c->cs_v, double, nc * nyv);
+    c->JC = 16;
+    c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;
     AL(c->scal, double, 4);
     AL(c->mf_work, double, 4 * (size_t)(cfg->ny + 4));
     AL(c->stage0, double2, nc * nyu);

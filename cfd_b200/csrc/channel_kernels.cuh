@@ -286,7 +286,8 @@ __global__ void __launch_bounds__(256) k_rhs(Dims d, Geo g, RKCoef c, const doub
                                              double2* __restrict__ du1, double2* __restrict__ du2,
                                              double2* __restrict__ du3, const T2* __restrict__ S0,
                                              const T2* __restrict__ S1, const T2* __restrict__ S2,
-                                             const T2* __restrict__ S3) {
+                                             const T2* __restrict__ S3, int JC) {
+    // one thread = one column and a chunk of JC planes (blockIdx.y); no recurrence in y
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
     const int i = col % d.nkx, q = col / d.nkx;
@@ -296,104 +297,113 @@ __global__ void __launch_bounds__(256) k_rhs(Dims d, Geo g, RKCoef c, const doub
     const size_t nc = d.ncol;
     const double mpgx = scal[0];
     constexpr bool RHS0 = (MODE & 1) != 0, NL = (MODE & 2) != 0, PRO = (MODE & 4) != 0;
+    const int cb = blockIdx.y;
 
     // ---- u and w (ugrid), j = ju0+1 .. ju1-1
     {
-        double2 a_m = u1[col], a_0 = u1[nc + col];
-        double2 w_m = u3[col], w_0 = u3[nc + col];
-        const size_t vs = (size_t)d.nyu * nc;  // first v-slot
-        double2 uv_m = NL ? to_d2(ldT(S0 + vs + col)) : dc(0, 0);  // uv at face ju0 (= jv0)
-        double2 vw_m = NL ? to_d2(ldT(S1 + vs + col)) : dc(0, 0);
-        for (int j = d.ju0 + 1; j <= d.ju1 - 1; ++j) {
-            const size_t ju = (size_t)(j - d.ju0);
-            const double2 a_p = u1[(ju + 1) * nc + col];
-            const double2 w_p = u3[(ju + 1) * nc + col];
-            const size_t jp = (size_t)(j - d.jp0);
-            double2 r1, r3;
-            if (RHS0) {
-                const double c0 = g.dyu2i[3 * ju + 0], c1 = g.dyu2i[3 * ju + 1], c2 = g.dyu2i[3 * ju + 2];
-                const double dg = k2 + c1;
-                const double2 Lu = dadd(dadd(dscl(c0, a_m), dscl(dg, a_0)), dscl(c2, a_p));
-                const double2 Lw = dadd(dadd(dscl(c0, w_m), dscl(dg, w_0)), dscl(c2, w_p));
-                const double2 pp = p[jp * nc + col];
-                const double2 n1o = to_d2(Nu1[ju * nc + col]);
-                const double2 n3o = to_d2(Nu3[ju * nc + col]);
-                r1 = dadd(dadd(dscl(c.C1, Lu), dscl(c.C2, n1o)), dik(-c.dRK * kxv, pp));
-                r3 = dadd(dadd(dscl(c.C1, Lw), dscl(c.C2, n3o)), dik(-c.dRK * kzv, pp));
-                if (col == 0) r1.x += -c.dRK * mpgx;
-            } else {
-                r1 = du1[ju * nc + col];
-                r3 = du3[ju * nc + col];
+        const int jb = d.ju0 + 1 + cb * JC;
+        const int je = min(jb + JC, d.ju1);
+        if (jb < je) {
+            const size_t ju = (size_t)(jb - d.ju0);
+            double2 a_m = u1[(ju - 1) * nc + col], a_0 = u1[ju * nc + col];
+            double2 w_m = u3[(ju - 1) * nc + col], w_0 = u3[ju * nc + col];
+            const size_t vs = (size_t)d.nyu * nc;  // first v-slot
+            double2 uv_m = NL ? to_d2(S0[vs + (size_t)(jb - 1 - d.jv0) * nc + col]) : dc(0, 0);
+            double2 vw_m = NL ? to_d2(S1[vs + (size_t)(jb - 1 - d.jv0) * nc + col]) : dc(0, 0);
+            for (int j = jb; j < je; ++j) {
+                const size_t ju = (size_t)(j - d.ju0);
+                const double2 a_p = u1[(ju + 1) * nc + col];
+                const double2 w_p = u3[(ju + 1) * nc + col];
+                const size_t jp = (size_t)(j - d.jp0);
+                double2 r1, r3;
+                if (RHS0) {
+                    const double c0 = g.dyu2i[3 * ju + 0], c1 = g.dyu2i[3 * ju + 1], c2 = g.dyu2i[3 * ju + 2];
+                    const double dg = k2 + c1;
+                    const double2 Lu = dadd(dadd(dscl(c0, a_m), dscl(dg, a_0)), dscl(c2, a_p));
+                    const double2 Lw = dadd(dadd(dscl(c0, w_m), dscl(dg, w_0)), dscl(c2, w_p));
+                    const double2 pp = p[jp * nc + col];
+                    const double2 n1o = to_d2(Nu1[ju * nc + col]);
+                    const double2 n3o = to_d2(Nu3[ju * nc + col]);
+                    r1 = dadd(dadd(dscl(c.C1, Lu), dscl(c.C2, n1o)), dik(-c.dRK * kxv, pp));
+                    r3 = dadd(dadd(dscl(c.C1, Lw), dscl(c.C2, n3o)), dik(-c.dRK * kzv, pp));
+                    if (col == 0) r1.x += -c.dRK * mpgx;
+                } else {
+                    r1 = du1[ju * nc + col];
+                    r3 = du3[ju * nc + col];
+                }
+                if (NL) {
+                    const size_t su = ju * nc + col;
+                    const size_t sv = vs + (size_t)(j - d.jv0) * nc + col;
+                    const double2 uv_p = to_d2(S0[sv]), vw_p = to_d2(S1[sv]);
+                    const double dth = g.dthdyu[ju];
+                    double2 n1 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(S0[su])), dik(kzv, to_d2(S1[su])));
+                    double2 n3 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(S1[su])), dik(kzv, to_d2(S3[su])));
+                    n1 = dadd(n1, dscl(dth, dsub(uv_p, uv_m)));
+                    n3 = dadd(n3, dscl(dth, dsub(vw_p, vw_m)));
+                    Nu1[su] = to_t2<T2>(n1);
+                    Nu3[su] = to_t2<T2>(n3);
+                    r1 = dadd(r1, dscl(c.mg, n1));
+                    r3 = dadd(r3, dscl(c.mg, n3));
+                    uv_m = uv_p;
+                    vw_m = vw_p;
+                }
+                if (PRO) {
+                    r1 = dadd(a_0, dscl(c.dt, r1));
+                    r3 = dadd(w_0, dscl(c.dt, r3));
+                }
+                du1[ju * nc + col] = r1;
+                du3[ju * nc + col] = r3;
+                a_m = a_0; a_0 = a_p;
+                w_m = w_0; w_0 = w_p;
             }
-            if (NL) {
-                const size_t su = ju * nc + col;
-                const size_t sv = vs + (size_t)(j - d.jv0) * nc + col;
-                const double2 uv_p = to_d2(ldT(S0 + sv)), vw_p = to_d2(ldT(S1 + sv));
-                const double dth = g.dthdyu[ju];
-                double2 n1 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(ldT(S0 + su))), dik(kzv, to_d2(ldT(S1 + su))));
-                double2 n3 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(ldT(S1 + su))), dik(kzv, to_d2(ldT(S3 + su))));
-                n1 = dadd(n1, dscl(dth, dsub(uv_p, uv_m)));
-                n3 = dadd(n3, dscl(dth, dsub(vw_p, vw_m)));
-                Nu1[su] = to_t2<T2>(n1);
-                Nu3[su] = to_t2<T2>(n3);
-                r1 = dadd(r1, dscl(c.mg, n1));
-                r3 = dadd(r3, dscl(c.mg, n3));
-                uv_m = uv_p;
-                vw_m = vw_p;
-            }
-            if (PRO) {
-                r1 = dadd(a_0, dscl(c.dt, r1));
-                r3 = dadd(w_0, dscl(c.dt, r3));
-            }
-            du1[ju * nc + col] = r1;
-            du3[ju * nc + col] = r3;
-            a_m = a_0; a_0 = a_p;
-            w_m = w_0; w_0 = w_p;
-        }
-        if (PRO) {
-            du1[col] = dc(0, 0);
-            du3[col] = dc(0, 0);
-            du1[(size_t)(d.nyu - 1) * nc + col] = dc(0, 0);
-            du3[(size_t)(d.nyu - 1) * nc + col] = dc(0, 0);
         }
     }
     // ---- v (vgrid), j = jv0+1 .. jv1-1
     {
-        double2 v_m = u2[col], v_0 = u2[nc + col];
-        double2 vv_0 = NL ? to_d2(ldT(S2 + (size_t)(d.jv0 + 1 - d.ju0) * nc + col)) : dc(0, 0);
-        const size_t vs = (size_t)d.nyu * nc;
-        for (int j = d.jv0 + 1; j <= d.jv1 - 1; ++j) {
-            const size_t jv = (size_t)(j - d.jv0);
-            const double2 v_p = u2[(jv + 1) * nc + col];
-            double2 r2;
-            if (RHS0) {
-                const double c0 = g.dyv2i[3 * jv + 0], c1 = g.dyv2i[3 * jv + 1], c2 = g.dyv2i[3 * jv + 2];
-                const double2 Lv = dadd(dadd(dscl(c0, v_m), dscl(k2 + c1, v_0)), dscl(c2, v_p));
-                const double C3 = -c.dRK * g.dthdyv[jv];
-                const double2 pa = p[(size_t)(j + 1 - d.jp0) * nc + col];
-                const double2 pb = p[(size_t)(j - d.jp0) * nc + col];
-                const double2 n2o = to_d2(Nu2[jv * nc + col]);
-                r2 = dadd(dadd(dscl(c.C1, Lv), dscl(c.C2, n2o)), dscl(C3, dsub(pa, pb)));
-            } else {
-                r2 = du2[jv * nc + col];
+        const int jb = d.jv0 + 1 + cb * JC;
+        const int je = min(jb + JC, d.jv1);
+        if (jb < je) {
+            const size_t jv = (size_t)(jb - d.jv0);
+            double2 v_m = u2[(jv - 1) * nc + col], v_0 = u2[jv * nc + col];
+            double2 vv_0 = NL ? to_d2(S2[(size_t)(jb - d.ju0) * nc + col]) : dc(0, 0);
+            const size_t vs = (size_t)d.nyu * nc;
+            for (int j = jb; j < je; ++j) {
+                const size_t jv = (size_t)(j - d.jv0);
+                const double2 v_p = u2[(jv + 1) * nc + col];
+                double2 r2;
+                if (RHS0) {
+                    const double c0 = g.dyv2i[3 * jv + 0], c1 = g.dyv2i[3 * jv + 1], c2 = g.dyv2i[3 * jv + 2];
+                    const double2 Lv = dadd(dadd(dscl(c0, v_m), dscl(k2 + c1, v_0)), dscl(c2, v_p));
+                    const double C3 = -c.dRK * g.dthdyv[jv];
+                    const double2 pa = p[(size_t)(j + 1 - d.jp0) * nc + col];
+                    const double2 pb = p[(size_t)(j - d.jp0) * nc + col];
+                    const double2 n2o = to_d2(Nu2[jv * nc + col]);
+                    r2 = dadd(dadd(dscl(c.C1, Lv), dscl(c.C2, n2o)), dscl(C3, dsub(pa, pb)));
+                } else {
+                    r2 = du2[jv * nc + col];
+                }
+                if (NL) {
+                    const size_t sv = vs + jv * nc + col;
+                    const double2 vv_p = to_d2(S2[(size_t)(j + 1 - d.ju0) * nc + col]);
+                    double2 n2 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(S0[sv])), dik(kzv, to_d2(S1[sv])));
+                    n2 = dadd(n2, dscl(g.dthdyv[jv], dsub(vv_p, vv_0)));
+                    Nu2[jv * nc + col] = to_t2<T2>(n2);
+                    r2 = dadd(r2, dscl(c.mg, n2));
+                    vv_0 = vv_p;
+                }
+                if (PRO) r2 = dadd(v_0, dscl(c.dt, r2));
+                du2[jv * nc + col] = r2;
+                v_m = v_0; v_0 = v_p;
             }
-            if (NL) {
-                const size_t sv = vs + jv * nc + col;
-                const double2 vv_p = to_d2(ldT(S2 + (size_t)(j + 1 - d.ju0) * nc + col));
-                double2 n2 = zrow ? dc(0, 0) : dadd(dik(kxv, to_d2(ldT(S0 + sv))), dik(kzv, to_d2(ldT(S1 + sv))));
-                n2 = dadd(n2, dscl(g.dthdyv[jv], dsub(vv_p, vv_0)));
-                Nu2[jv * nc + col] = to_t2<T2>(n2);
-                r2 = dadd(r2, dscl(c.mg, n2));
-                vv_0 = vv_p;
-            }
-            if (PRO) r2 = dadd(v_0, dscl(c.dt, r2));
-            du2[jv * nc + col] = r2;
-            v_m = v_0; v_0 = v_p;
         }
-        if (PRO) {
-            du2[col] = dc(0, 0);
-            du2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
-        }
+    }
+    if (PRO && cb == 0) {
+        du1[col] = dc(0, 0);
+        du3[col] = dc(0, 0);
+        du1[(size_t)(d.nyu - 1) * nc + col] = dc(0, 0);
+        du3[(size_t)(d.nyu - 1) * nc + col] = dc(0, 0);
+        du2[col] = dc(0, 0);
+        du2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
     }
 }
 
@@ -577,83 +587,123 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
 // forward sweep leaves y_j in the solution array and the scaled upper diagonal in `cs`.
 // u and w share the matrix and its factorisation.
 // --------------------------------------------------------------------------------------
+// Loads of the sweeps are batched UB planes at a time so that each thread keeps several
+// independent loads in flight while the recurrence runs on registers.
+#define CFD_UB 8
+
 __global__ void __launch_bounds__(256) k_solve_uvw(Dims d, Geo g, double beta, double2* __restrict__ u1,
                                                    double2* __restrict__ u2, double2* __restrict__ u3,
                                                    const double2* __restrict__ r1, const double2* __restrict__ r2,
-                                                   const double2* __restrict__ r3, double* __restrict__ cs,
-                                                   int do_uw, int do_v) {
+                                                   const double2* __restrict__ r3, double* __restrict__ cs_uw,
+                                                   double* __restrict__ cs_v) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
     const int i = col % d.nkx, q = col / d.nkx;
     const double k2x = -g.kx[i] * g.kx[i], k2z = -g.kz[q] * g.kz[q];
     const size_t nc = d.ncol;
-    if (do_uw) {
+    if (blockIdx.y == 0) {
+        // u and w share the matrix: rows (0,1,gwb), interior, (gwt,1,0)
         const int n = d.nyu;
-        // row 0: (0, 1, gwb)
-        double dinv = 1.0 / 1.0;
-        double a3prev = g.gwb;
-        double2 y1 = dscl(dinv, r1[col]);
-        double2 y3 = dscl(dinv, r3[col]);
+        double dprev = 1.0, a3prev = g.gwb;
+        double2 y1 = r1[col], y3 = r3[col];
         u1[col] = y1;
         u3[col] = y3;
-        double dprev = dinv;
-        for (int jj = 1; jj < n; ++jj) {
-            double a1, a2, a3;
-            if (jj < n - 1) {
-                const double b = beta;
-                a1 = -b * g.dyu2i[3 * jj + 0];
-                a2 = 1.0 - b * (g.dyu2i[3 * jj + 1] + k2x + k2z);
-                a3 = -b * g.dyu2i[3 * jj + 2];
-            } else {
-                a1 = g.gwt; a2 = 1.0; a3 = 0.0;
+        for (int j0 = 1; j0 < n; j0 += CFD_UB) {
+            double2 ra[CFD_UB], rc[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 + t < n) { ra[t] = r1[(size_t)(j0 + t) * nc + col]; rc[t] = r3[(size_t)(j0 + t) * nc + col]; }
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                const int jj = j0 + t;
+                if (jj >= n) break;
+                double a1, a2, a3;
+                if (jj < n - 1) {
+                    a1 = -beta * g.dyu2i[3 * jj + 0];
+                    a2 = 1.0 - beta * (g.dyu2i[3 * jj + 1] + k2x + k2z);
+                    a3 = -beta * g.dyu2i[3 * jj + 2];
+                } else {
+                    a1 = g.gwt; a2 = 1.0; a3 = 0.0;
+                }
+                const double csm = a3prev * dprev;  // a(3,j-1) * a(2,j-1)
+                cs_uw[(size_t)(jj - 1) * nc + col] = csm;
+                const double dj = 1.0 / (a2 - a1 * csm);
+                y1 = dscl(dj, dsub(ra[t], dscl(a1, y1)));
+                y3 = dscl(dj, dsub(rc[t], dscl(a1, y3)));
+                u1[(size_t)jj * nc + col] = y1;
+                u3[(size_t)jj * nc + col] = y3;
+                dprev = dj;
+                a3prev = a3;
             }
-            const double csm = a3prev * dprev;  // a(3,j-1) * a(2,j-1)
-            cs[(size_t)(jj - 1) * nc + col] = csm;
-            const double dj = 1.0 / (a2 - a1 * csm);
-            const double2 ra = r1[(size_t)jj * nc + col], rc = r3[(size_t)jj * nc + col];
-            y1 = dscl(dj, dsub(ra, dscl(a1, y1)));
-            y3 = dscl(dj, dsub(rc, dscl(a1, y3)));
-            u1[(size_t)jj * nc + col] = y1;
-            u3[(size_t)jj * nc + col] = y3;
-            dprev = dj;
-            a3prev = a3;
         }
         double2 x1 = y1, x3 = y3;
-        for (int jj = n - 2; jj >= 0; --jj) {
-            const double csj = cs[(size_t)jj * nc + col];
-            x1 = dsub(u1[(size_t)jj * nc + col], dscl(csj, x1));
-            x3 = dsub(u3[(size_t)jj * nc + col], dscl(csj, x3));
-            u1[(size_t)jj * nc + col] = x1;
-            u3[(size_t)jj * nc + col] = x3;
+        for (int j0 = n - 2; j0 >= 0; j0 -= CFD_UB) {
+            double cc[CFD_UB];
+            double2 ya[CFD_UB], yc[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 - t >= 0) {
+                    const size_t o = (size_t)(j0 - t) * nc + col;
+                    cc[t] = cs_uw[o]; ya[t] = u1[o]; yc[t] = u3[o];
+                }
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                if (j0 - t < 0) break;
+                const size_t o = (size_t)(j0 - t) * nc + col;
+                x1 = dsub(ya[t], dscl(cc[t], x1));
+                x3 = dsub(yc[t], dscl(cc[t], x3));
+                u1[o] = x1;
+                u3[o] = x3;
+            }
         }
-    }
-    if (do_v) {
+    } else {
+        // v: identity wall rows
         const int n = d.nyv;
-        double dprev = 1.0;
-        double a3prev = 0.0;
+        double dprev = 1.0, a3prev = 0.0;
         double2 y = r2[col];
         u2[col] = y;
-        for (int jj = 1; jj < n; ++jj) {
-            double a1, a2, a3;
-            if (jj < n - 1) {
-                a1 = -beta * g.dyv2i[3 * jj + 0];
-                a2 = 1.0 - beta * (g.dyv2i[3 * jj + 1] + k2x + k2z);
-                a3 = -beta * g.dyv2i[3 * jj + 2];
-            } else {
-                a1 = 0.0; a2 = 1.0; a3 = 0.0;
+        for (int j0 = 1; j0 < n; j0 += CFD_UB) {
+            double2 ra[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 + t < n) ra[t] = r2[(size_t)(j0 + t) * nc + col];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                const int jj = j0 + t;
+                if (jj >= n) break;
+                double a1, a2, a3;
+                if (jj < n - 1) {
+                    a1 = -beta * g.dyv2i[3 * jj + 0];
+                    a2 = 1.0 - beta * (g.dyv2i[3 * jj + 1] + k2x + k2z);
+                    a3 = -beta * g.dyv2i[3 * jj + 2];
+                } else {
+                    a1 = 0.0; a2 = 1.0; a3 = 0.0;
+                }
+                const double csm = a3prev * dprev;
+                cs_v[(size_t)(jj - 1) * nc + col] = csm;
+                const double dj = 1.0 / (a2 - a1 * csm);
+                y = dscl(dj, dsub(ra[t], dscl(a1, y)));
+                u2[(size_t)jj * nc + col] = y;
+                dprev = dj;
+                a3prev = a3;
             }
-            const double csm = a3prev * dprev;
-            cs[(size_t)(jj - 1) * nc + col] = csm;
-            const double dj = 1.0 / (a2 - a1 * csm);
-            y = dscl(dj, dsub(r2[(size_t)jj * nc + col], dscl(a1, y)));
-            u2[(size_t)jj * nc + col] = y;
-            dprev = dj;
-            a3prev = a3;
         }
         double2 x = y;
-        for (int jj = n - 2; jj >= 0; --jj) {
-            x = dsub(u2[(size_t)jj * nc + col], dscl(cs[(size_t)jj * nc + col], x));
-            u2[(size_t)jj * nc + col] = x;
+        for (int j0 = n - 2; j0 >= 0; j0 -= CFD_UB) {
+            double cc[CFD_UB];
+            double2 ya[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 - t >= 0) {
+                    const size_t o = (size_t)(j0 - t) * nc + col;
+                    cc[t] = cs_v[o]; ya[t] = u2[o];
+                }
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                if (j0 - t < 0) break;
+                x = dsub(ya[t], dscl(cc[t], x));
+                u2[(size_t)(j0 - t) * nc + col] = x;
+            }
         }
     }
 }
@@ -679,51 +729,115 @@ __global__ void __launch_bounds__(256) k_solve_p(Dims d, Geo g, double dtirk, co
     auto DTHV = [&](int j) { return g.dthdyv[j - d.jv0]; };
     double dprev = 0.0, a3prev = 0.0;
     double2 y = dc(0, 0);
-    for (int jj = 0; jj < n; ++jj) {
-        const int j = d.jp0 + jj;
-        // divergence at p-point j
-        const double2 a = u1[(size_t)(j - d.ju0) * nc + col];
-        const double2 w = u3[(size_t)(j - d.ju0) * nc + col];
-        const double2 va = u2[(size_t)(j - d.jv0) * nc + col];
-        const double2 vb = u2[(size_t)(j - 1 - d.jv0) * nc + col];
-        const double2 dv = dadd(dadd(dik(kxv, a), dik(kzv, w)), dscl(DTHU(j), dsub(va, vb)));
-        if (divo) divo[(size_t)jj * nc + col] = dv;
-        double2 r = dscl(dtirk, dv);
-        double a1, a2, a3;
-        if (jj == 0) {
-            a1 = 0.0;
-            a2 = (DTHU(j) * -DTHV(j)) + k2x + k2z;
-            a3 = (DTHU(j) * DTHV(j));
-            if (col == 0) { a2 = mean_diag; a3 = 0.0; r = dc(0, 0); }
-        } else if (jj == n - 1) {
-            a1 = (-DTHU(j)) * (-DTHV(j - 1));
-            a2 = ((-DTHU(j)) * DTHV(j - 1)) + k2x + k2z;
-            a3 = 0.0;
-        } else {
-            a2 = ((-DTHU(j)) * DTHV(j - 1)) + (DTHU(j) * -DTHV(j)) + k2x + k2z;
-            a1 = ((-DTHU(j)) * (-DTHV(j - 1)));
-            a3 = (DTHU(j) * DTHV(j));
+    double2 vb = u2[(size_t)(d.jp0 - 1 - d.jv0) * nc + col];
+    for (int jj0 = 0; jj0 < n; jj0 += CFD_UB) {
+        double2 A[CFD_UB], W[CFD_UB], VA[CFD_UB];
+#pragma unroll
+        for (int t = 0; t < CFD_UB; ++t)
+            if (jj0 + t < n) {
+                const int j = d.jp0 + jj0 + t;
+                A[t] = u1[(size_t)(j - d.ju0) * nc + col];
+                W[t] = u3[(size_t)(j - d.ju0) * nc + col];
+                VA[t] = u2[(size_t)(j - d.jv0) * nc + col];
+            }
+#pragma unroll
+        for (int t = 0; t < CFD_UB; ++t) {
+            const int jj = jj0 + t;
+            if (jj >= n) break;
+            const int j = d.jp0 + jj;
+            // divergence at p-point j
+            const double2 dv = dadd(dadd(dik(kxv, A[t]), dik(kzv, W[t])), dscl(DTHU(j), dsub(VA[t], vb)));
+            vb = VA[t];
+            if (divo) divo[(size_t)jj * nc + col] = dv;
+            double2 r = dscl(dtirk, dv);
+            double a1, a2, a3;
+            if (jj == 0) {
+                a1 = 0.0;
+                a2 = (DTHU(j) * -DTHV(j)) + k2x + k2z;
+                a3 = (DTHU(j) * DTHV(j));
+                if (col == 0) { a2 = mean_diag; a3 = 0.0; r = dc(0, 0); }
+            } else if (jj == n - 1) {
+                a1 = (-DTHU(j)) * (-DTHV(j - 1));
+                a2 = ((-DTHU(j)) * DTHV(j - 1)) + k2x + k2z;
+                a3 = 0.0;
+            } else {
+                a2 = ((-DTHU(j)) * DTHV(j - 1)) + (DTHU(j) * -DTHV(j)) + k2x + k2z;
+                a1 = ((-DTHU(j)) * (-DTHV(j - 1)));
+                a3 = (DTHU(j) * DTHV(j));
+            }
+            double dj;
+            if (jj == 0) {
+                dj = 1.0 / a2;
+                y = dscl(dj, r);
+            } else {
+                const double csm = a3prev * dprev;
+                cs[(size_t)(jj - 1) * nc + col] = csm;
+                dj = 1.0 / (a2 - a1 * csm);
+                y = dscl(dj, dsub(r, dscl(a1, y)));
+            }
+            psi[(size_t)jj * nc + col] = y;
+            dprev = dj;
+            a3prev = a3;
         }
-        double dj;
-        if (jj == 0) {
-            dj = 1.0 / a2;
-            y = dscl(dj, r);
-        } else {
-            const double csm = a3prev * dprev;
-            cs[(size_t)(jj - 1) * nc + col] = csm;
-            dj = 1.0 / (a2 - a1 * csm);
-            y = dscl(dj, dsub(r, dscl(a1, y)));
-        }
-        psi[(size_t)jj * nc + col] = y;
-        dprev = dj;
-        a3prev = a3;
     }
     double2 x = y;
     p[(size_t)(n - 1) * nc + col] = dadd(p[(size_t)(n - 1) * nc + col], x);
-    for (int jj = n - 2; jj >= 0; --jj) {
-        x = dsub(psi[(size_t)jj * nc + col], dscl(cs[(size_t)jj * nc + col], x));
-        psi[(size_t)jj * nc + col] = x;
-        p[(size_t)jj * nc + col] = dadd(p[(size_t)jj * nc + col], x);
+    for (int jj0 = n - 2; jj0 >= 0; jj0 -= CFD_UB) {
+        double cc[CFD_UB];
+        double2 ya[CFD_UB], pa[CFD_UB];
+#pragma unroll
+        for (int t = 0; t < CFD_UB; ++t)
+            if (jj0 - t >= 0) {
+                const size_t o = (size_t)(jj0 - t) * nc + col;
+                cc[t] = cs[o]; ya[t] = psi[o]; pa[t] = p[o];
+            }
+#pragma unroll
+        for (int t = 0; t < CFD_UB; ++t) {
+            if (jj0 - t < 0) break;
+            const size_t o = (size_t)(jj0 - t) * nc + col;
+            x = dsub(ya[t], dscl(cc[t], x));
+            psi[o] = x;
+            p[o] = dadd(pa[t], x);
+        }
+    }
+}
+
+// v_corr without the closing divergence, one thread per column and a chunk of JC planes
+// (the fused substep; cfd_vcorr keeps the sequential k_vcorr that also returns div).
+__global__ void __launch_bounds__(256) k_vcorr_chunk(Dims d, Geo g, double dtrk, double2* __restrict__ u1,
+                                                     double2* __restrict__ u2, double2* __restrict__ u3,
+                                                     const double2* __restrict__ psi, int JC) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol) return;
+    const int i = col % d.nkx, q = col / d.nkx;
+    const double kxv = g.kx[i], kzv = g.kz[q];
+    const size_t nc = d.ncol;
+    const int cb = blockIdx.y;
+    // u, w at centres j = ju0+1..ju1-1 (= p-points)
+    const int jb = d.ju0 + 1 + cb * JC, je = min(jb + JC, d.ju1);
+    for (int j = jb; j < je; ++j) {
+        const size_t ju = (size_t)(j - d.ju0);
+        const double2 ps = psi[(size_t)(j - d.jp0) * nc + col];
+        u1[ju * nc + col] = dsub(u1[ju * nc + col], dik(dtrk * kxv, ps));
+        u3[ju * nc + col] = dsub(u3[ju * nc + col], dik(dtrk * kzv, ps));
+    }
+    // v at faces j = jv0+1..jv1-1: psi(j+1) - psi(j)
+    const int vb = d.jv0 + 1 + cb * JC, ve = min(vb + JC, d.jv1);
+    for (int j = vb; j < ve; ++j) {
+        const size_t jv = (size_t)(j - d.jv0);
+        const double2 pa = psi[(size_t)(j + 1 - d.jp0) * nc + col], pb = psi[(size_t)(j - d.jp0) * nc + col];
+        u2[jv * nc + col] = dsub(u2[jv * nc + col], dscl(dtrk * g.dthdyv[jv], dsub(pa, pb)));
+    }
+    if (cb == 0) {
+        u2[col] = dc(0, 0);
+        u2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
+        // chunk 0 has just corrected u(ju0+1), the row the bottom ghost extrapolates from
+        u1[col] = dscl(-g.gwb, u1[nc + col]);
+        u3[col] = dscl(-g.gwb, u3[nc + col]);
+    }
+    if (je == d.ju1 && jb < je) {
+        u1[(size_t)(d.nyu - 1) * nc + col] = dscl(-g.gwt, u1[(size_t)(d.nyu - 2) * nc + col]);
+        u3[(size_t)(d.nyu - 1) * nc + col] = dscl(-g.gwt, u3[(size_t)(d.nyu - 2) * nc + col]);
     }
 }
 
