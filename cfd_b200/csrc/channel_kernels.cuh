@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __re
                          ((yvj - yuj) * ua.y + (yup - yvj) * ub.y) / (yup - yuj));
             }
         }
-        buf0[(size_t)row_of(d, q) * CH + b] = to_t2<T2>(val);
+        buf0[swz(row_of(d, q), b, bshift)] = to_t2<T2>(val);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, +1>(buf0, buf1, CH, bshift, fz, tw);
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __re
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, z = t / CH;
         const int i = kx0 + b;
-        if (i < d.nkx) H[base + (size_t)z * d.nkx + i] = res[(size_t)z * CH + b];
+        if (i < d.nkx) H[base + (size_t)z * d.nkx + i] = res[swz(z, b, bshift)];
     }
 }
 
@@ -166,55 +166,70 @@ __device__ __forceinline__ T2 herm_line(const Dims& d, const T2* A, const T2* B,
 
 template <typename T2, int NF>
 __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
-                                               T2* __restrict__ H3, FFTDesc fx, const T2* __restrict__ twx, int RW, int bshift) {
+                                               T2* __restrict__ H3, FFTDesc fx, const T2* __restrict__ twx, int RW,
+                                               int bshift) {
     using R = decltype(T2::x);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = d.ngal1;
-    const int B = 2 * RW;
+    const int B = 2 * RW;  // line 2*rr = (u + i w) of row rr, line 2*rr+1 = (v + i 0)
     T2* buf0 = reinterpret_cast<T2*>(smem_raw);
     T2* buf1 = buf0 + (size_t)n * B;
     T2* tw = buf1 + (size_t)n * B;
     const int slot = blockIdx.y;
     const int z0 = blockIdx.x * RW;
     const bool uplane = slot < d.nyu;
+    const int h = d.n1 / 2;  // retained kx modes 0..h
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twx[t];
+    // zero the padding modes h < k < n-h of every line
+    const int ngap = n - 2 * h - 1;
+    for (int t = threadIdx.x; t < ngap * B; t += blockDim.x) {
+        const int b = t & (B - 1), k = h + 1 + (t >> bshift);
+        buf0[swz(k, b, bshift)] = cx<T2>((R)0, (R)0);
+    }
+    // Hermitian lines from the kx spectra, k fastest across threads (coalesced rows);
+    // the rft inverse ignores Im of the kx = 0 entry (rft_buff.f:78-80)
     const size_t pbase = (size_t)slot * d.ngal2 * d.nkx;
-    for (int t = threadIdx.x; t < n * B; t += blockDim.x) {
-        const int b = t % B, k = t / B;
+    const int nk = d.nkx;
+    for (int t = threadIdx.x; t < nk * B; t += blockDim.x) {
+        const int k = t % nk, b = t / nk;
         const int rr = b >> 1, which = b & 1;
-        const size_t rb = pbase + (size_t)(z0 + rr) * d.nkx;
-        T2 v = which == 0 ? herm_line<T2>(d, H0 + rb, H1 + rb, k) : herm_line<T2>(d, H2 + rb, (const T2*)nullptr, k);
-        buf0[(size_t)k * B + b] = v;
+        const size_t o = pbase + (size_t)(z0 + rr) * nk + k;
+        T2 a, c;
+        if (which == 0) { a = H0[o]; c = H1[o]; }
+        else { a = H2[o]; c = cx<T2>((R)0, (R)0); }
+        if (k == 0) { a.y = 0; c.y = 0; }
+        buf0[swz(k, b, bshift)] = cx<T2>(a.x - c.y, a.y + c.x);
+        if (k > 0) buf0[swz(n - k, b, bshift)] = cx<T2>(a.x + c.y, -a.y + c.x);
     }
     __syncthreads();
     T2* P = fft_batch<T2, NF, +1>(buf0, buf1, B, bshift, fx, tw);
     T2* Q = P == buf0 ? buf1 : buf0;
     for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
         const int rr = t % RW, k = t / RW;
-        T2 l0 = P[(size_t)k * B + 2 * rr];
-        T2 l1 = P[(size_t)k * B + 2 * rr + 1];
+        const int a0 = swz(k, 2 * rr, bshift), a1 = swz(k, 2 * rr + 1, bshift);
+        const T2 l0 = P[a0], l1 = P[a1];
         const R u = l0.x, w = l0.y, v = l1.x;
         if (uplane) {
-            P[(size_t)k * B + 2 * rr] = cx<T2>(u * u, u * w);
-            P[(size_t)k * B + 2 * rr + 1] = cx<T2>(v * v, w * w);
+            P[a0] = cx<T2>(u * u, u * w);
+            P[a1] = cx<T2>(v * v, w * w);
         } else {
-            P[(size_t)k * B + 2 * rr] = cx<T2>(u * v, w * v);
-            P[(size_t)k * B + 2 * rr + 1] = cx<T2>((R)0, (R)0);
+            P[a0] = cx<T2>(u * v, w * v);
+            P[a1] = cx<T2>((R)0, (R)0);
         }
     }
     __syncthreads();
     T2* F = fft_batch<T2, NF, -1>(P, Q, B, bshift, fx, tw);
     const R s = (R)1 / (R)n;
     const int nl = uplane ? B : RW;  // v-planes carry one output line per row
-    for (int t = threadIdx.x; t < d.nkx * nl; t += blockDim.x) {
-        const int k = t % d.nkx, bl = t / d.nkx;
+    for (int t = threadIdx.x; t < nk * nl; t += blockDim.x) {
+        const int k = t % nk, bl = t / nk;
         const int b = uplane ? bl : 2 * bl;
         const int rr = b >> 1, which = b & 1;
-        const T2 Pk = F[(size_t)k * B + b];
-        const T2 Qc = cconj(F[(size_t)((n - k) % n) * B + b]);
+        const T2 Pk = F[swz(k, b, bshift)];
+        const T2 Qc = cconj(F[swz((n - k) % n, b, bshift)]);
         const T2 A = cx<T2>((Pk.x + Qc.x) * (R)0.5 * s, (Pk.y + Qc.y) * (R)0.5 * s);
         const T2 Bv = cx<T2>((Pk.y - Qc.y) * (R)0.5 * s, -(Pk.x - Qc.x) * (R)0.5 * s);
-        const size_t o = pbase + (size_t)(z0 + rr) * d.nkx + k;
+        const size_t o = pbase + (size_t)(z0 + rr) * nk + k;
         if (which == 0) { H0[o] = A; H1[o] = Bv; }
         else { H2[o] = A; H3[o] = Bv; }
     }
@@ -248,7 +263,7 @@ __global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0,
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, z = t / CH;
         const int i = kx0 + b;
-        buf0[t] = i < d.nkx ? H[base + (size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
+        buf0[swz(z, b, bshift)] = i < d.nkx ? H[base + (size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, -1>(buf0, buf1, CH, bshift, fz, tw);
@@ -256,7 +271,7 @@ __global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0,
     for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
         const int b = t % CH, q = t / CH;
         const int i = kx0 + b;
-        if (i < d.nkx) S[(size_t)slot * d.ncol + (size_t)q * d.nkx + i] = cscale(res[(size_t)row_of(d, q) * CH + b], s);
+        if (i < d.nkx) S[(size_t)slot * d.ncol + (size_t)q * d.nkx + i] = cscale(res[swz(row_of(d, q), b, bshift)], s);
     }
 }
 
@@ -439,14 +454,14 @@ __global__ void __launch_bounds__(256) k_ib_zinv(Dims d, IBSrc src, int j0, cons
     for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
         const int b = t % CH, q = t / CH, i = kx0 + b;
         if (i >= d.nkx) continue;
-        buf0[(size_t)row_of(d, q) * CH + b] = to_t2<T2>(f[(size_t)(j - j0) * d.ncol + (size_t)q * d.nkx + i]);
+        buf0[swz(row_of(d, q), b, bshift)] = to_t2<T2>(f[(size_t)(j - j0) * d.ncol + (size_t)q * d.nkx + i]);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, +1>(buf0, buf1, CH, bshift, fz, tw);
     const size_t base = ((size_t)s * npl + p) * n * d.nkx;
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, z = t / CH, i = kx0 + b;
-        if (i < d.nkx) Hib[base + (size_t)z * d.nkx + i] = res[(size_t)z * CH + b];
+        if (i < d.nkx) Hib[base + (size_t)z * d.nkx + i] = res[swz(z, b, bshift)];
     }
 }
 
@@ -466,10 +481,19 @@ __global__ void __launch_bounds__(256) k_ib_xinv(Dims d, const T2* __restrict__ 
     const size_t pl = (size_t)d.ngal2 * d.nkx;
     const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl;
     const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl;
-    for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
-        const int b = t % RW, k = t / RW;
-        const size_t rb = (size_t)(z0 + b) * d.nkx;
-        buf0[(size_t)k * RW + b] = herm_line<T2>(d, Hr + rb, Hu + rb, k);
+    // line (rhs + i u) per row, k fastest across threads (coalesced rows); gap modes zero
+    const int h = d.n1 / 2, nk = d.nkx;
+    for (int t = threadIdx.x; t < (n - 2 * h - 1) * RW; t += blockDim.x) {
+        const int b = t & (RW - 1), k = h + 1 + (t >> bshift);
+        buf0[swz(k, b, bshift)] = cx<T2>((R)0, (R)0);
+    }
+    for (int t = threadIdx.x; t < nk * RW; t += blockDim.x) {
+        const int k = t % nk, b = t / nk;
+        const size_t o = (size_t)(z0 + b) * nk + k;
+        T2 a = Hr[o], c = Hu[o];
+        if (k == 0) { a.y = 0; c.y = 0; }
+        buf0[swz(k, b, bshift)] = cx<T2>(a.x - c.y, a.y + c.x);
+        if (k > 0) buf0[swz(n - k, b, bshift)] = cx<T2>(a.x + c.y, -a.y + c.x);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, +1>(buf0, buf1, RW, bshift, fx, tw);
@@ -478,7 +502,7 @@ __global__ void __launch_bounds__(256) k_ib_xinv(Dims d, const T2* __restrict__ 
     R* pu = phys + ((size_t)(2 * fb + 1) * npl + p) * ppl;
     for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
         const int k = t % n, b = t / n;
-        const T2 v = res[(size_t)k * RW + b];
+        const T2 v = res[swz(k, b, bshift)];
         pr[(size_t)(z0 + b) * n + k] = v.x;
         pu[(size_t)(z0 + b) * n + k] = v.y;
     }
@@ -537,7 +561,7 @@ __global__ void __launch_bounds__(256) k_ib_xfwd(Dims d, T2* __restrict__ Hib, i
     const R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl;
     for (int t = threadIdx.x; t < n * B; t += blockDim.x) {
         const int k = t % n, b = t / n;
-        buf0[(size_t)k * B + b] = cx<T2>(pr[(size_t)(z0 + 2 * b) * n + k], pr[(size_t)(z0 + 2 * b + 1) * n + k]);
+        buf0[swz(k, b, bshift)] = cx<T2>(pr[(size_t)(z0 + 2 * b) * n + k], pr[(size_t)(z0 + 2 * b + 1) * n + k]);
     }
     __syncthreads();
     T2* F = fft_batch<T2, NF, -1>(buf0, buf1, B, bshift, fx, tw);
@@ -545,8 +569,8 @@ __global__ void __launch_bounds__(256) k_ib_xfwd(Dims d, T2* __restrict__ Hib, i
     T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)d.ngal2 * d.nkx;
     for (int t = threadIdx.x; t < d.nkx * B; t += blockDim.x) {
         const int k = t % d.nkx, b = t / d.nkx;
-        const T2 Pk = F[(size_t)k * B + b];
-        const T2 Qc = cconj(F[(size_t)((n - k) % n) * B + b]);
+        const T2 Pk = F[swz(k, b, bshift)];
+        const T2 Qc = cconj(F[swz((n - k) % n, b, bshift)]);
         Hr[(size_t)(z0 + 2 * b) * d.nkx + k] = cx<T2>((Pk.x + Qc.x) * (R)0.5 * s, (Pk.y + Qc.y) * (R)0.5 * s);
         Hr[(size_t)(z0 + 2 * b + 1) * d.nkx + k] = cx<T2>((Pk.y - Qc.y) * (R)0.5 * s, -(Pk.x - Qc.x) * (R)0.5 * s);
     }
@@ -569,7 +593,7 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
     const T2* H = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)n * d.nkx;
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, z = t / CH, i = kx0 + b;
-        buf0[t] = i < d.nkx ? H[(size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
+        buf0[swz(z, b, bshift)] = i < d.nkx ? H[(size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, -1>(buf0, buf1, CH, bshift, fz, tw);
@@ -577,7 +601,7 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
     double2* out = dst.f[fb] + (size_t)(planes[p] - j0) * d.ncol;
     for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
         const int b = t % CH, q = t / CH, i = kx0 + b;
-        if (i < d.nkx) out[(size_t)q * d.nkx + i] = to_d2(cscale(res[(size_t)row_of(d, q) * CH + b], s));
+        if (i < d.nkx) out[(size_t)q * d.nkx + i] = to_d2(cscale(res[swz(row_of(d, q), b, bshift)], s));
     }
 }
 
@@ -1006,7 +1030,8 @@ __global__ void __launch_bounds__(256) k_cft_strided(double* __restrict__ c, int
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = tw_g[t];
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, e = t / CH, l = l0 + b;
-        buf0[t] = l < m ? dc(base[(size_t)l * isa + (size_t)e * ise], base[(size_t)l * isa + (size_t)e * ise + 1]) : dc(0, 0);
+        buf0[swz(e, b, __ffs(CH) - 1)] =
+            l < m ? dc(base[(size_t)l * isa + (size_t)e * ise], base[(size_t)l * isa + (size_t)e * ise + 1]) : dc(0, 0);
     }
     __syncthreads();
     double2* res = fft_lines<double2>(buf0, buf1, CH, fd, tw, iopt < 0 ? -1 : +1);
@@ -1014,7 +1039,7 @@ __global__ void __launch_bounds__(256) k_cft_strided(double* __restrict__ c, int
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, e = t / CH, l = l0 + b;
         if (l < m) {
-            const double2 v = res[t];
+            const double2 v = res[swz(e, b, __ffs(CH) - 1)];
             base[(size_t)l * isa + (size_t)e * ise] = s * v.x;
             base[(size_t)l * isa + (size_t)e * ise + 1] = s * v.y;
         }
@@ -1045,7 +1070,7 @@ __global__ void __launch_bounds__(256) k_rft_strided(double* __restrict__ c, int
                 else v = dc(x[2 * (n - k)], -x[2 * (n - k) + 1]);
             }
         }
-        buf0[t] = v;
+        buf0[swz(k, b, __ffs(CH) - 1)] = v;
     }
     __syncthreads();
     double2* res = fft_lines<double2>(buf0, buf1, CH, fd, tw, iopt < 0 ? -1 : +1);
@@ -1055,12 +1080,12 @@ __global__ void __launch_bounds__(256) k_rft_strided(double* __restrict__ c, int
         double* x = base + (size_t)l * isa;
         if (iopt < 0) {
             const int k = e >> 1;
-            const double2 v = res[(size_t)k * CH + b];
+            const double2 v = res[swz(k, b, __ffs(CH) - 1)];
             double val = (e & 1) ? v.y : v.x;
             if ((e & 1) && (k == 0 || k == n / 2)) val = 0.0;
             x[e] = val / n;
         } else if (e < n) {
-            x[e] = res[(size_t)e * CH + b].x;
+            x[e] = res[swz(e, b, __ffs(CH) - 1)].x;
         }
     }
 }

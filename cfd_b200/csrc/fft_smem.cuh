@@ -44,6 +44,14 @@ struct FFTDesc {
     int rad[10];
 };
 
+// Shared-memory address of element e of line b in a batch of B = 1 << bshift lines:
+// element-major with the line index XOR-swizzled by the low bits of e, so that both
+// "consecutive lines, same element" and "consecutive elements, same line" accesses of a
+// warp spread over all banks.
+__device__ __forceinline__ int swz(int e, int b, int bshift) {
+    return (e << bshift) + (b ^ (e & ((1 << bshift) - 1)));
+}
+
 // sign = -1: forward (e^{-i..}), +1: inverse.
 template <typename T2>
 __device__ __forceinline__ void butterfly(T2* v, int R, int sign) {
@@ -79,6 +87,7 @@ __device__ T2* fft_lines(T2* a, T2* b, int B, const FFTDesc& d, const T2* __rest
     T2* in = a;
     T2* out = b;
     const int n = d.n;
+    const int bshift = __ffs(B) - 1;  // B is a power of two
     int Ns = 1;
     for (int p = 0; p < d.nrad; ++p) {
         const int R = d.rad[p];
@@ -86,14 +95,14 @@ __device__ T2* fft_lines(T2* a, T2* b, int B, const FFTDesc& d, const T2* __rest
         const int tstep = n / (Ns * R);
         const int ntask = nr * B;
         for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
-            const int bb = t % B;
-            const int i = t / B;
+            const int bb = t & (B - 1);
+            const int i = t >> bshift;
             const int k = i % Ns;
             T2 v[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 if (r < R) {
-                    T2 x = in[(i + r * nr) * B + bb];
+                    T2 x = in[swz(i + r * nr, bb, bshift)];
                     if (r > 0 && Ns > 1) {
                         const T2 w = tw[r * k * tstep];
                         x = sign < 0 ? cmul(x, w) : cmulc(x, w);
@@ -105,7 +114,7 @@ __device__ T2* fft_lines(T2* a, T2* b, int B, const FFTDesc& d, const T2* __rest
             const int idxD = (i / Ns) * Ns * R + k;
 #pragma unroll
             for (int r = 0; r < 4; ++r)
-                if (r < R) out[(idxD + r * Ns) * B + bb] = v[r];
+                if (r < R) out[swz(idxD + r * Ns, bb, bshift)] = v[r];
         }
         __syncthreads();
         T2* tmp = in; in = out; out = tmp;
@@ -220,7 +229,7 @@ __device__ __forceinline__ void fixed_pass(const T2* __restrict__ in, T2* __rest
         const int k = i % NS;
         T2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = in[((i + r * NR) << bshift) + bb];
+        for (int r = 0; r < R; ++r) v[r] = in[swz(i + r * NR, bb, bshift)];
         if constexpr (NS > 1) {
 #pragma unroll
             for (int r = 1; r < R; ++r) {
@@ -231,7 +240,7 @@ __device__ __forceinline__ void fixed_pass(const T2* __restrict__ in, T2* __rest
         dftR<R, SIGN>(v);
         const int idxD = (i / NS) * NS * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) out[((idxD + r * NS) << bshift) + bb] = v[r];
+        for (int r = 0; r < R; ++r) out[swz(idxD + r * NS, bb, bshift)] = v[r];
     }
     __syncthreads();
 }
