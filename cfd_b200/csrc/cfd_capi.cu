@@ -556,6 +556,21 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     for (int i = 0; i < d.nkx; ++i) hg.push_back(cfg->alp * i);
     const size_t okz = hg.size();
     for (int q = 0; q < d.n2; ++q) hg.push_back(q < d.n2 / 2 ? cfg->bet * q : -cfg->bet * (d.n2 - q));
+    // interpolation weights (interp_v: centres from faces; interp_u: faces from centres)
+    auto YUh = [&](int j) { return cfg->yu[j - d.ju0]; };
+    auto YVh = [&](int j) { return cfg->yv[j - d.jv0]; };
+    const size_t ovc = hg.size();
+    for (int j = d.ju0; j <= d.ju1; ++j) {
+        const bool in = j > d.ju0 && j < d.ju1;
+        hg.push_back(in ? (YUh(j) - YVh(j - 1)) / (YVh(j) - YVh(j - 1)) : 0.0);
+    }
+    for (int j = d.ju0; j <= d.ju1; ++j) {
+        const bool in = j > d.ju0 && j < d.ju1;
+        hg.push_back(in ? (YVh(j) - YUh(j)) / (YVh(j) - YVh(j - 1)) : 0.0);
+    }
+    const size_t ouf = hg.size();
+    for (int j = d.jv0; j <= d.jv1; ++j) hg.push_back((YVh(j) - YUh(j)) / (YUh(j + 1) - YUh(j)));
+    for (int j = d.jv0; j <= d.jv1; ++j) hg.push_back((YUh(j + 1) - YVh(j)) / (YUh(j + 1) - YUh(j)));
     for (double v : hg)
         if (!std::isfinite(v)) return fail(c, CFD_ERR_ARG, "non-finite grid value");
     AL(c->geo, double, hg.size());
@@ -569,6 +584,10 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     g.dyv2i = g.dyu2i + 3 * nyu;
     g.kx = c->geo + okx;
     g.kz = c->geo + okz;
+    g.vca = c->geo + ovc;
+    g.vcb = g.vca + nyu;
+    g.ufa = c->geo + ouf;
+    g.ufb = g.ufa + nyv;
     auto YU = [&](int j) { return cfg->yu[j - d.ju0]; };
     auto YV = [&](int j) { return cfg->yv[j - d.jv0]; };
     g.gwb = -(YV(d.jv0) - YU(d.ju0)) / (YV(d.jv0) - YU(d.ju0 + 1));

@@ -36,6 +36,13 @@ struct Geo {
     const double* dyv2i;  // [nyv][3]
     const double* kx;     // [nkx]
     const double* kz;     // [n2]
+    // linear y-interpolation weights (interp_u/interp_v, FOU3D.f90:261-308):
+    // v at centre j = vca[j]*v(j) + vcb[j]*v(j-1)   (index j - ju0, interior centres)
+    // u at face j   = ufa[j]*u(j+1) + ufb[j]*u(j)   (index j - jv0)
+    const double* vca;
+    const double* vcb;
+    const double* ufa;
+    const double* ufb;
     double gwb, gwt, gwib, gwit;
 };
 
@@ -79,8 +86,8 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __re
     __syncthreads();
     const bool uplane = slot < d.nyu;
     const int j = uplane ? d.ju0 + slot : d.jv0 + (slot - d.nyu);
-    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
-        const int b = t % CH, q = t / CH;
+    for (int t = threadIdx.x; t < (d.n2 << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), q = t >> bshift;
         const int i = kx0 + b;
         if (i >= d.nkx) continue;
         const size_t col = (size_t)q * d.nkx + i;
@@ -93,9 +100,8 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __re
                 auto itp = [&](int jj) {
                     const double2 va = u2[(size_t)(jj - d.jv0) * d.ncol + col];
                     const double2 vb = u2[(size_t)(jj - 1 - d.jv0) * d.ncol + col];
-                    const double yuj = g.yu[jj - d.ju0], yvj = g.yv[jj - d.jv0], yvm = g.yv[jj - 1 - d.jv0];
-                    return dc(((yuj - yvm) * va.x + (yvj - yuj) * vb.x) / (yvj - yvm),
-                              ((yuj - yvm) * va.y + (yvj - yuj) * vb.y) / (yvj - yvm));
+                    const double wa = g.vca[jj - d.ju0], wb = g.vcb[jj - d.ju0];
+                    return dc(wa * va.x + wb * vb.x, wa * va.y + wb * vb.y);
                 };
                 if (j == d.ju0) {
                     const double2 vi = itp(d.ju0 + 1);
@@ -116,9 +122,8 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __re
                 const double2* s = f == 0 ? u1 : u3;
                 const double2 ua = s[(size_t)(j + 1 - d.ju0) * d.ncol + col];
                 const double2 ub = s[(size_t)(j - d.ju0) * d.ncol + col];
-                const double yvj = g.yv[j - d.jv0], yuj = g.yu[j - d.ju0], yup = g.yu[j + 1 - d.ju0];
-                val = dc(((yvj - yuj) * ua.x + (yup - yvj) * ub.x) / (yup - yuj),
-                         ((yvj - yuj) * ua.y + (yup - yvj) * ub.y) / (yup - yuj));
+                const double wa = g.ufa[j - d.jv0], wb = g.ufb[j - d.jv0];
+                val = dc(wa * ua.x + wb * ub.x, wa * ua.y + wb * ub.y);
             }
         }
         buf0[swz(row_of(d, q), b, bshift)] = to_t2<T2>(val);
@@ -127,8 +132,8 @@ __global__ void __launch_bounds__(256) k_zinv(Dims d, Geo g, const double2* __re
     T2* res = fft_batch<T2, NF, +1>(buf0, buf1, CH, bshift, fz, tw);
     T2* H = f == 0 ? H0 : (f == 1 ? H1 : H2);
     const size_t base = (size_t)slot * n * d.nkx;
-    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
-        const int b = t % CH, z = t / CH;
+    for (int t = threadIdx.x; t < (n << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), z = t >> bshift;
         const int i = kx0 + b;
         if (i < d.nkx) H[base + (size_t)z * d.nkx + i] = res[swz(z, b, bshift)];
     }
@@ -190,22 +195,24 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
     // the rft inverse ignores Im of the kx = 0 entry (rft_buff.f:78-80)
     const size_t pbase = (size_t)slot * d.ngal2 * d.nkx;
     const int nk = d.nkx;
-    for (int t = threadIdx.x; t < nk * B; t += blockDim.x) {
-        const int k = t % nk, b = t / nk;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int b = warp; b < B; b += nwarp) {
         const int rr = b >> 1, which = b & 1;
-        const size_t o = pbase + (size_t)(z0 + rr) * nk + k;
-        T2 a, c;
-        if (which == 0) { a = H0[o]; c = H1[o]; }
-        else { a = H2[o]; c = cx<T2>((R)0, (R)0); }
-        if (k == 0) { a.y = 0; c.y = 0; }
-        buf0[swz(k, b, bshift)] = cx<T2>(a.x - c.y, a.y + c.x);
-        if (k > 0) buf0[swz(n - k, b, bshift)] = cx<T2>(a.x + c.y, -a.y + c.x);
+        const T2* ra = (which == 0 ? H0 : H2) + pbase + (size_t)(z0 + rr) * nk;
+        const T2* rc = H1 + pbase + (size_t)(z0 + rr) * nk;
+        for (int k = lane; k < nk; k += 32) {
+            T2 a = ra[k];
+            T2 c = which == 0 ? rc[k] : cx<T2>((R)0, (R)0);
+            if (k == 0) { a.y = 0; c.y = 0; }
+            buf0[swz(k, b, bshift)] = cx<T2>(a.x - c.y, a.y + c.x);
+            if (k > 0) buf0[swz(n - k, b, bshift)] = cx<T2>(a.x + c.y, -a.y + c.x);
+        }
     }
     __syncthreads();
     T2* P = fft_batch<T2, NF, +1>(buf0, buf1, B, bshift, fx, tw);
     T2* Q = P == buf0 ? buf1 : buf0;
     for (int t = threadIdx.x; t < n * RW; t += blockDim.x) {
-        const int rr = t % RW, k = t / RW;
+        const int rr = t & (RW - 1), k = t >> (bshift - 1);
         const int a0 = swz(k, 2 * rr, bshift), a1 = swz(k, 2 * rr + 1, bshift);
         const T2 l0 = P[a0], l1 = P[a1];
         const R u = l0.x, w = l0.y, v = l1.x;
@@ -221,17 +228,18 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
     T2* F = fft_batch<T2, NF, -1>(P, Q, B, bshift, fx, tw);
     const R s = (R)1 / (R)n;
     const int nl = uplane ? B : RW;  // v-planes carry one output line per row
-    for (int t = threadIdx.x; t < nk * nl; t += blockDim.x) {
-        const int k = t % nk, bl = t / nk;
+    const R hs = (R)0.5 * s;
+    for (int bl = warp; bl < nl; bl += nwarp) {
         const int b = uplane ? bl : 2 * bl;
         const int rr = b >> 1, which = b & 1;
-        const T2 Pk = F[swz(k, b, bshift)];
-        const T2 Qc = cconj(F[swz((n - k) % n, b, bshift)]);
-        const T2 A = cx<T2>((Pk.x + Qc.x) * (R)0.5 * s, (Pk.y + Qc.y) * (R)0.5 * s);
-        const T2 Bv = cx<T2>((Pk.y - Qc.y) * (R)0.5 * s, -(Pk.x - Qc.x) * (R)0.5 * s);
-        const size_t o = pbase + (size_t)(z0 + rr) * nk + k;
-        if (which == 0) { H0[o] = A; H1[o] = Bv; }
-        else { H2[o] = A; H3[o] = Bv; }
+        T2* oa = (which == 0 ? H0 : H2) + pbase + (size_t)(z0 + rr) * nk;
+        T2* ob = (which == 0 ? H1 : H3) + pbase + (size_t)(z0 + rr) * nk;
+        for (int k = lane; k < nk; k += 32) {
+            const T2 Pk = F[swz(k, b, bshift)];
+            const T2 Qc = cconj(F[swz(k == 0 ? 0 : n - k, b, bshift)]);
+            oa[k] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+            ob[k] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
+        }
     }
 }
 
@@ -260,16 +268,16 @@ __global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0,
     T2* S = f == 0 ? S0 : (f == 1 ? S1 : (f == 2 ? S2 : S3));
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
     const size_t base = (size_t)slot * n * d.nkx;
-    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
-        const int b = t % CH, z = t / CH;
+    for (int t = threadIdx.x; t < (n << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), z = t >> bshift;
         const int i = kx0 + b;
         buf0[swz(z, b, bshift)] = i < d.nkx ? H[base + (size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, -1>(buf0, buf1, CH, bshift, fz, tw);
     const R s = (R)1 / (R)n;
-    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
-        const int b = t % CH, q = t / CH;
+    for (int t = threadIdx.x; t < (d.n2 << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), q = t >> bshift;
         const int i = kx0 + b;
         if (i < d.nkx) S[(size_t)slot * d.ncol + (size_t)q * d.nkx + i] = cscale(res[swz(row_of(d, q), b, bshift)], s);
     }
@@ -451,16 +459,16 @@ __global__ void __launch_bounds__(256) k_ib_zinv(Dims d, IBSrc src, int j0, cons
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) buf0[t] = cx<T2>(0, 0);
     __syncthreads();
-    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
-        const int b = t % CH, q = t / CH, i = kx0 + b;
+    for (int t = threadIdx.x; t < (d.n2 << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), q = t >> bshift, i = kx0 + b;
         if (i >= d.nkx) continue;
         buf0[swz(row_of(d, q), b, bshift)] = to_t2<T2>(f[(size_t)(j - j0) * d.ncol + (size_t)q * d.nkx + i]);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, +1>(buf0, buf1, CH, bshift, fz, tw);
     const size_t base = ((size_t)s * npl + p) * n * d.nkx;
-    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
-        const int b = t % CH, z = t / CH, i = kx0 + b;
+    for (int t = threadIdx.x; t < (n << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), z = t >> bshift, i = kx0 + b;
         if (i < d.nkx) Hib[base + (size_t)z * d.nkx + i] = res[swz(z, b, bshift)];
     }
 }
@@ -591,16 +599,16 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
     const int kx0 = blockIdx.x * CH, p = blockIdx.y, fb = blockIdx.z;
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = twz[t];
     const T2* H = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)n * d.nkx;
-    for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
-        const int b = t % CH, z = t / CH, i = kx0 + b;
+    for (int t = threadIdx.x; t < (n << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), z = t >> bshift, i = kx0 + b;
         buf0[swz(z, b, bshift)] = i < d.nkx ? H[(size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
     }
     __syncthreads();
     T2* res = fft_batch<T2, NF, -1>(buf0, buf1, CH, bshift, fz, tw);
     const R s = (R)1 / (R)n;
     double2* out = dst.f[fb] + (size_t)(planes[p] - j0) * d.ncol;
-    for (int t = threadIdx.x; t < d.n2 * CH; t += blockDim.x) {
-        const int b = t % CH, q = t / CH, i = kx0 + b;
+    for (int t = threadIdx.x; t < (d.n2 << bshift); t += blockDim.x) {
+        const int b = t & (CH - 1), q = t >> bshift, i = kx0 + b;
         if (i < d.nkx) out[(size_t)q * d.nkx + i] = to_d2(cscale(res[swz(row_of(d, q), b, bshift)], s));
     }
 }
