@@ -87,6 +87,13 @@ struct cfd_ctx {
     double2 *twx_d = nullptr, *twz_d = nullptr;
     float2 *twx_f = nullptr, *twz_f = nullptr;
     int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
+    int RW2 = 0, NT2 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
+    int LZ2 = -1, NTZ2 = 0; // two-step z kernels: log2(columns per CTA) (-1 = not used), threads
+    size_t SMZ2 = 0;
+    int RWIX2 = 0, RWFX2 = 0;  // two-step IB x kernels: rows per CTA (0 = not used)
+    int NTIX2 = 0, NTFX2 = 0;
+    size_t SMIX2 = 0, SMFX2 = 0;
+    size_t SM2 = 0;
     bool state_loaded = false;
     // graph of one RK3 step
     cudaGraph_t graph = nullptr;
@@ -194,6 +201,26 @@ int ilog2(int b) {
         default: { constexpr int NF = 0; __VA_ARGS__; } break;    \
     }
 
+// Run BODY with (TN1, TN2) = the two-step split of n; sets ok = false if n has none.
+#define TWO_SWITCH(n, ok, ...)                                               \
+    switch (n) {                                                             \
+        case 64: { constexpr int TN1 = 8, TN2 = 8; __VA_ARGS__; } break;     \
+        case 96: { constexpr int TN1 = 8, TN2 = 12; __VA_ARGS__; } break;    \
+        case 128: { constexpr int TN1 = 8, TN2 = 16; __VA_ARGS__; } break;   \
+        case 192: { constexpr int TN1 = 16, TN2 = 12; __VA_ARGS__; } break;  \
+        case 384: { constexpr int TN1 = 16, TN2 = 24; __VA_ARGS__; } break;  \
+        case 768: { constexpr int TN1 = 32, TN2 = 24; __VA_ARGS__; } break;  \
+        default: ok = false; break;                                          \
+    }
+
+// shared memory of k_xline2 (elements): B*LX + N + RW*3*nk
+size_t xline2_smem(int n1s, int n2s, int rw, int nk, size_t esz) {
+    const int N = n1s * n2s;
+    const int L1 = n1s * (n2s + 1) + 1, L2 = n2s * (n1s + 1) + 1, LU = N + 1;
+    const int LX = std::max(L1, std::max(L2, LU));
+    return ((size_t)2 * rw * LX + N + (size_t)rw * 3 * nk) * esz;
+}
+
 // ---------------------------------------------------------------------------------------
 template <typename T2>
 int set_smem_attrs(cfd_ctx* c) {
@@ -215,6 +242,40 @@ int set_smem_attrs(cfd_ctx* c) {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ib_xinv<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)si);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ib_xfwd<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
     });
+    if (c->LZ2 >= 0) {
+        bool ok = true;
+        TWO_SWITCH(n2, ok, {
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_zinv2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_zfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
+        });
+    }
+    if (c->LZ2 >= 0) {
+        bool ok = true;
+        TWO_SWITCH(n2, ok, {
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_ib_zinv2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_ib_zfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
+        });
+    }
+    if (c->RWIX2) {
+        bool ok = true;
+        TWO_SWITCH(n1, ok, {
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_ib_xinv2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMIX2);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_ib_xfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMFX2);
+        });
+    }
+    if (c->RW2) {
+        bool ok = true;
+        TWO_SWITCH(n1, ok, {
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
+        });
+    }
     CK(e);
     return CFD_OK;
 }
@@ -244,29 +305,62 @@ int nl_transforms(cfd_ctx* c) {
     const Dims& d = c->d;
     const int CH = c->CHz;
     const size_t e = sizeof(T2);
-    dim3 gz((d.nkx + CH - 1) / CH, d.nslot, 3);
     prof_mark(c);
-    FFT_SWITCH(d.ngal2, {
-        k_zinv<T2, NF><<<gz, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0],
-                                                                     (T2*)c->H[1], (T2*)c->H[2], c->fz, twz<T2>(c), CH,
-                                                                     ilog2(CH));
-    });
-    LK("k_zinv");
-    dim3 gx(d.ngal2 / c->RWx, d.nslot);
+    if (c->LZ2 >= 0) {
+        const int CH2 = 1 << c->LZ2;
+        dim3 gz2((d.nkx + CH2 - 1) / CH2, d.nslot, 3);
+        bool ok = true;
+        TWO_SWITCH(d.ngal2, ok, {
+            k_zinv2<T2, TN1, TN2><<<gz2, c->NTZ2, c->SMZ2, c->stream>>>(d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0],
+                                                                     (T2*)c->H[1], (T2*)c->H[2], twz<T2>(c), c->LZ2);
+        });
+        LK("k_zinv2");
+    } else {
+        dim3 gz((d.nkx + CH - 1) / CH, d.nslot, 3);
+        FFT_SWITCH(d.ngal2, {
+            k_zinv<T2, NF><<<gz, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0],
+                                                                         (T2*)c->H[1], (T2*)c->H[2], c->fz, twz<T2>(c),
+                                                                         CH, ilog2(CH));
+        });
+        LK("k_zinv");
+    }
     prof_mark(c);
-    FFT_SWITCH(d.ngal1, {
-        k_xline<T2, NF><<<gx, 256, (size_t)(2 * (2 * c->RWx) * d.ngal1 + d.ngal1) * e, c->stream>>>(
-            d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], c->fx, twx<T2>(c), c->RWx, ilog2(2 * c->RWx));
-    });
-    LK("k_xline");
-    dim3 gf((d.nkx + CH - 1) / CH, d.nslot, 4);
+    if (c->RW2) {
+        dim3 gx2(d.ngal2 / c->RW2, d.nslot);
+        bool ok = true;
+        TWO_SWITCH(d.ngal1, ok, {
+            k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2],
+                                                                    (T2*)c->H[3], twx<T2>(c), c->RW2, ilog2(c->RW2));
+        });
+        LK("k_xline2");
+    } else {
+        dim3 gx(d.ngal2 / c->RWx, d.nslot);
+        FFT_SWITCH(d.ngal1, {
+            k_xline<T2, NF><<<gx, 256, (size_t)(2 * (2 * c->RWx) * d.ngal1 + d.ngal1) * e, c->stream>>>(
+                d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], c->fx, twx<T2>(c), c->RWx, ilog2(2 * c->RWx));
+        });
+        LK("k_xline");
+    }
     prof_mark(c);
-    FFT_SWITCH(d.ngal2, {
-        k_zfwd<T2, NF><<<gf, 256, zsmem(d.ngal2, CH, e), c->stream>>>(
-            d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
-            (T2*)c->S[3], c->fz, twz<T2>(c), CH, ilog2(CH));
-    });
-    LK("k_zfwd");
+    if (c->LZ2 >= 0) {
+        const int CH2 = 1 << c->LZ2;
+        dim3 gf2((d.nkx + CH2 - 1) / CH2, d.nslot, 4);
+        bool ok = true;
+        TWO_SWITCH(d.ngal2, ok, {
+            k_zfwd2<T2, TN1, TN2><<<gf2, c->NTZ2, c->SMZ2, c->stream>>>(
+                d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
+                (T2*)c->S[3], twz<T2>(c), c->LZ2);
+        });
+        LK("k_zfwd2");
+    } else {
+        dim3 gf((d.nkx + CH - 1) / CH, d.nslot, 4);
+        FFT_SWITCH(d.ngal2, {
+            k_zfwd<T2, NF><<<gf, 256, zsmem(d.ngal2, CH, e), c->stream>>>(
+                d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
+                (T2*)c->S[3], c->fz, twz<T2>(c), CH, ilog2(CH));
+        });
+        LK("k_zfwd");
+    }
     return CFD_OK;
 }
 
@@ -295,40 +389,82 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     src.f[0] = rhs_a; src.f[1] = u_a; src.f[2] = rhs_b; src.f[3] = u_b;
     IBDst dst;
     dst.f[0] = rhs_a; dst.f[1] = rhs_b;
-    dim3 g1((d.nkx + CH - 1) / CH, ib.npl, 2 * nb);
     prof_mark(c);
-    FFT_SWITCH(d.ngal2, {
-        k_ib_zinv<T2, NF><<<g1, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib,
-                                                                        c->fz, twz<T2>(c), CH, ilog2(CH));
-    });
-    LK("k_ib_zinv");
-    dim3 g2(d.ngal2 / c->RWib, ib.npl, nb);
+    if (c->LZ2 >= 0) {
+        const int CH2 = 1 << c->LZ2;
+        dim3 g1((d.nkx + CH2 - 1) / CH2, ib.npl, 2 * nb);
+        bool ok = true;
+        TWO_SWITCH(d.ngal2, ok, {
+            k_ib_zinv2<T2, TN1, TN2><<<g1, c->NTZ2, c->SMZ2, c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib,
+                                                                        twz<T2>(c), c->LZ2);
+        });
+        LK("k_ib_zinv2");
+    } else {
+        dim3 g1((d.nkx + CH - 1) / CH, ib.npl, 2 * nb);
+        FFT_SWITCH(d.ngal2, {
+            k_ib_zinv<T2, NF><<<g1, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib,
+                                                                            c->fz, twz<T2>(c), CH, ilog2(CH));
+        });
+        LK("k_ib_zinv");
+    }
     prof_mark(c);
-    FFT_SWITCH(d.ngal1, {
-        k_ib_xinv<T2, NF><<<g2, 256, (size_t)(2 * c->RWib * d.ngal1 + d.ngal1) * e, c->stream>>>(
-            d, (T2*)c->Hib, ib.npl, (R*)c->phys, c->fx, twx<T2>(c), c->RWib, ilog2(c->RWib));
-    });
-    LK("k_ib_xinv");
+    if (c->RWIX2) {
+        dim3 g2(d.ngal2 / c->RWIX2, ib.npl, nb);
+        bool ok = true;
+        TWO_SWITCH(d.ngal1, ok, {
+            k_ib_xinv2<T2, TN1, TN2><<<g2, c->NTIX2, c->SMIX2, c->stream>>>(d, (T2*)c->Hib, ib.npl, (R*)c->phys,
+                                                                          twx<T2>(c), c->RWIX2);
+        });
+        LK("k_ib_xinv2");
+    } else {
+        dim3 g2(d.ngal2 / c->RWib, ib.npl, nb);
+        FFT_SWITCH(d.ngal1, {
+            k_ib_xinv<T2, NF><<<g2, 256, (size_t)(2 * c->RWib * d.ngal1 + d.ngal1) * e, c->stream>>>(
+                d, (T2*)c->Hib, ib.npl, (R*)c->phys, c->fx, twx<T2>(c), c->RWib, ilog2(c->RWib));
+        });
+        LK("k_ib_xinv");
+    }
     if (ib.n > 0) {
         dim3 g3((ib.n + 255) / 256, nb);
         prof_mark(c);
         k_ib_force<R><<<g3, 256, 0, c->stream>>>(d, ib.idx, ib.w, ib.n, ib.slot_of_j, j0, ib.npl, (R*)c->phys);
         LK("k_ib_force");
     }
-    dim3 g4(d.ngal2 / c->RWibf, ib.npl, nb);
     prof_mark(c);
-    FFT_SWITCH(d.ngal1, {
-        k_ib_xfwd<T2, NF><<<g4, 256, (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * e, c->stream>>>(
-            d, (T2*)c->Hib, ib.npl, (const R*)c->phys, c->fx, twx<T2>(c), c->RWibf, ilog2(c->RWibf / 2));
-    });
-    LK("k_ib_xfwd");
-    dim3 g5((d.nkx + CH - 1) / CH, ib.npl, nb);
+    if (c->RWIX2) {
+        dim3 g4(d.ngal2 / c->RWFX2, ib.npl, nb);
+        bool ok = true;
+        TWO_SWITCH(d.ngal1, ok, {
+            k_ib_xfwd2<T2, TN1, TN2><<<g4, c->NTFX2, c->SMFX2, c->stream>>>(d, (T2*)c->Hib, ib.npl, (const R*)c->phys,
+                                                                          twx<T2>(c), c->RWFX2);
+        });
+        LK("k_ib_xfwd2");
+    } else {
+        dim3 g4(d.ngal2 / c->RWibf, ib.npl, nb);
+        FFT_SWITCH(d.ngal1, {
+            k_ib_xfwd<T2, NF><<<g4, 256, (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * e, c->stream>>>(
+                d, (T2*)c->Hib, ib.npl, (const R*)c->phys, c->fx, twx<T2>(c), c->RWibf, ilog2(c->RWibf / 2));
+        });
+        LK("k_ib_xfwd");
+    }
     prof_mark(c);
-    FFT_SWITCH(d.ngal2, {
-        k_ib_zfwd<T2, NF><<<g5, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0, ib.planes,
-                                                                        c->fz, twz<T2>(c), CH, ilog2(CH));
-    });
-    LK("k_ib_zfwd");
+    if (c->LZ2 >= 0) {
+        const int CH2 = 1 << c->LZ2;
+        dim3 g5((d.nkx + CH2 - 1) / CH2, ib.npl, nb);
+        bool ok = true;
+        TWO_SWITCH(d.ngal2, ok, {
+            k_ib_zfwd2<T2, TN1, TN2><<<g5, c->NTZ2, c->SMZ2, c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0,
+                                                                        ib.planes, twz<T2>(c), c->LZ2);
+        });
+        LK("k_ib_zfwd2");
+    } else {
+        dim3 g5((d.nkx + CH - 1) / CH, ib.npl, nb);
+        FFT_SWITCH(d.ngal2, {
+            k_ib_zfwd<T2, NF><<<g5, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0,
+                                                                            ib.planes, c->fz, twz<T2>(c), CH, ilog2(CH));
+        });
+        LK("k_ib_zfwd");
+    }
     return CFD_OK;
 }
 
@@ -612,6 +748,49 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     while (c->RWibf > 2 && ((d.ngal2 % c->RWibf) || (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * esz > budget))
         c->RWibf /= 2;
     if (d.ngal2 % c->RWibf) return fail(c, CFD_ERR_SIZE, "Ngal2 must be even");
+    {
+        bool ok = true;
+        int n1s = 0, n2s = 0;
+        TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
+        if (ok) {
+            int rw = 8;
+            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, d.nkx, esz) > budget)) rw /= 2;
+            if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
+                c->RW2 = rw;
+                c->NT2 = 2 * rw * std::max(n1s, n2s);
+                c->SM2 = xline2_smem(n1s, n2s, rw, d.nkx, esz);
+            }
+        }
+    }
+    if (!mixed) c->RW2 = 0;  // FP64: the Stockham x-line kernel is faster (register pressure)
+    {
+        bool ok = true;
+        int n1s = 0, n2s = 0;
+        TWO_SWITCH(d.ngal2, ok, { n1s = TN1; n2s = TN2; });
+        if (ok) {
+            const int lb = mixed ? 4 : 3;
+            c->LZ2 = lb;
+            c->NTZ2 = (1 << lb) * std::max(n1s, n2s);
+            c->SMZ2 = ((size_t)(1 << lb) * ((n1s * (n2s + 1)) | 1) + (size_t)n1s * n2s) * esz;
+        }
+    }
+    {
+        bool ok = true;
+        int n1s = 0, n2s = 0;
+        TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
+        if (ok) {
+            const int N = n1s * n2s, L1 = (n1s * (n2s + 1)) | 1, mx = std::max(n1s, n2s);
+            for (int rw = 16; rw >= 1; rw /= 2) {
+                const size_t sm = ((size_t)N + 2 * rw * d.nkx + (size_t)rw * L1) * esz;
+                if (d.ngal2 % rw == 0 && sm <= budget && rw * mx <= 1024) { c->RWIX2 = rw; c->SMIX2 = sm; c->NTIX2 = rw * mx; break; }
+            }
+            for (int rw = 16; rw >= 2; rw /= 2) {
+                const size_t sm = ((size_t)N + (size_t)(rw / 2) * (N + 1) + (size_t)(rw / 2) * L1) * esz;
+                if (d.ngal2 % rw == 0 && sm <= budget && (rw / 2) * mx <= 1024) { c->RWFX2 = rw; c->SMFX2 = sm; c->NTFX2 = (rw / 2) * mx; break; }
+            }
+            if (!c->RWIX2 || !c->RWFX2) c->RWIX2 = c->RWFX2 = 0;
+        }
+    }
     int s = mixed ? set_smem_attrs<float2>(c) : set_smem_attrs<double2>(c);
     if (s != CFD_OK) return s;
     if ((s = fill_tw(c, d.ngal1, &c->twx_d, &c->twx_f)) != CFD_OK) return s;

@@ -16,6 +16,7 @@
 #pragma once
 
 #include "fft_smem.cuh"
+#include "fft_reg.cuh"
 
 namespace cfd {
 
@@ -243,6 +244,154 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
     }
 }
 
+// Pass 2 with the register-resident two-step transform (N = N1*N2, fft_reg.cuh).  A CTA
+// holds RW rows = B = 2*RW lines (line 2r = u + i w, line 2r+1 = v + i 0) and runs with
+// B*max(N1,N2) threads:
+//   step 1  thread (b, n2): N1-point DFT of the stride-N2 subsequence, twiddle, exchange
+//   step 2  thread (b, k1): N2-point DFT -> physical x = k1 + N1*k2 in registers; the two
+//           lines of a row sit in adjacent lanes and swap w / v with one shuffle, form the
+//           products, and start the forward transform from registers (N2-point DFT)
+//   step 2' thread (b, kb): N1-point DFT -> X[kb + N2*ka]; unpack the two real spectra.
+template <typename T2, int N1, int N2>
+__global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+                         T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
+    using R = decltype(T2::x);
+    constexpr int N = N1 * N2;
+    constexpr int L1 = N1 * (N2 + 1) + 1;  // inverse exchange, per line: [k1][n2]
+    constexpr int L2 = N2 * (N1 + 1) + 1;  // forward exchange, per line: [kb][na]
+    constexpr int LU = N + 1;               // unpack buffer, per line
+    constexpr int LX = (L1 > L2 ? (L1 > LU ? L1 : LU) : (L2 > LU ? L2 : LU));
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int B = 2 * RW;
+    const int nk = d.nkx;
+    const int h = d.n1 / 2;
+    T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX
+    T2* twt = ex + (size_t)B * LX;                   // N1 * N2: twt[b*N2 + a] = w^(a*b), a < N2, b < N1
+    T2* stg = twt + N;                               // RW * 3 * nk staged spectra
+    const int slot = blockIdx.y;
+    const int z0 = blockIdx.x * RW;
+    const bool uplane = slot < d.nyu;
+    const int t = threadIdx.x;
+    for (int i = t; i < N; i += blockDim.x) {
+        const int b = i / N2, a = i - b * N2;
+        twt[i] = twx[(a * b) % N];
+    }
+    const size_t pbase = (size_t)slot * d.ngal2 * nk;
+    {
+        const int lane = t & 31, warp = t >> 5, nwarp = blockDim.x >> 5;
+        for (int rf = warp; rf < 3 * RW; rf += nwarp) {
+            const int rr = rf / 3, f = rf - 3 * rr;
+            const T2* src = (f == 0 ? H0 : (f == 1 ? H1 : H2)) + pbase + (size_t)(z0 + rr) * nk;
+            T2* dst = stg + (size_t)rf * nk;
+            for (int k = lane; k < nk; k += 32) dst[k] = src[k];
+        }
+    }
+    __syncthreads();
+
+    // ---- step 1: inverse, thread (b, n2)
+    if (t < B * N2) {
+        const int n2 = t % N2, b = t / N2;
+        const int rr = b >> 1, which = b & 1;
+        const T2* A = stg + (size_t)(3 * rr + (which == 0 ? 0 : 2)) * nk;
+        const T2* C = stg + (size_t)(3 * rr + 1) * nk;
+        T2 v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int e = n1 * N2 + n2;
+            T2 val = cx<T2>((R)0, (R)0);
+            if (e <= h) {
+                T2 a = A[e];
+                T2 c = which == 0 ? C[e] : cx<T2>((R)0, (R)0);
+                if (e == 0) { a.y = 0; c.y = 0; }
+                val = cx<T2>(a.x - c.y, a.y + c.x);
+            } else if (e >= N - h) {
+                const int k = N - e;
+                const T2 a = A[k];
+                const T2 c = which == 0 ? C[k] : cx<T2>((R)0, (R)0);
+                val = cx<T2>(a.x + c.y, -a.y + c.x);
+            }
+            v[n1] = val;
+        }
+        rdft<N1, +1>(v);
+        T2* o = ex + (size_t)b * L1 + n2;
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) o[k1 * (N2 + 1)] = k1 == 0 ? v[0] : cmulc(v[k1], twt[k1 * N2 + n2]);
+    }
+    __syncthreads();
+
+    // ---- step 2: inverse N2-point DFT, products, forward N2-point DFT; thread (b, k1)
+    T2 y[N2];
+    const bool act2 = t < B * N1;
+    const int par = t & 1, rest = t >> 1;
+    const int rr2 = rest & (RW - 1), k1 = rest >> lrw;
+    const int b2 = 2 * rr2 + par;
+    if (act2) {
+        const T2* o = ex + (size_t)b2 * L1 + k1 * (N2 + 1);
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) y[n2] = o[n2];
+        rdft<N2, +1>(y);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            // lane pair (u + i w, v + i 0): even lane sends w, odd lane sends v
+            const R send = par ? y[k2].x : y[k2].y;
+            const R recv = __shfl_xor_sync(0xffffffffu, send, 1);
+            if (par == 0) {
+                const R u = y[k2].x, w = y[k2].y, v = recv;
+                y[k2] = uplane ? cx<T2>(u * u, u * w) : cx<T2>(u * v, w * v);
+            } else {
+                const R v = y[k2].x, w = recv;
+                y[k2] = uplane ? cx<T2>(v * v, w * w) : cx<T2>((R)0, (R)0);
+            }
+        }
+        rdft<N2, -1>(y);
+#pragma unroll
+        for (int kb = 1; kb < N2; ++kb) y[kb] = cmul(y[kb], twt[k1 * N2 + kb]);
+    }
+    __syncthreads();  // every lane has read the inverse exchange
+    if (act2) {
+        T2* o = ex + (size_t)b2 * L2 + k1;
+#pragma unroll
+        for (int kb = 0; kb < N2; ++kb) o[kb * (N1 + 1)] = y[kb];
+    }
+    __syncthreads();
+
+    // ---- step 2': forward N1-point DFT, thread (b, kb) -> X[kb + N2*ka]
+    T2 z[N1];
+    const bool act3 = t < B * N2;
+    const int kb = t % N2, b3 = t / N2;
+    if (act3) {
+        const T2* o = ex + (size_t)b3 * L2 + kb * (N1 + 1);
+#pragma unroll
+        for (int na = 0; na < N1; ++na) z[na] = o[na];
+        rdft<N1, -1>(z);
+    }
+    __syncthreads();
+    if (act3) {
+        T2* o = ex + (size_t)b3 * LU + kb;
+#pragma unroll
+        for (int ka = 0; ka < N1; ++ka) o[N2 * ka] = z[ka];
+    }
+    __syncthreads();
+
+    // ---- unpack A_k = (P_k + conj P_{N-k})/2, B_k = (P_k - conj P_{N-k})/(2i), x 1/N
+    const R hs = (R)0.5 / (R)N;
+    const int lane = t & 31, warp = t >> 5, nwarp = blockDim.x >> 5;
+    const int nl = uplane ? B : RW;
+    for (int bl = warp; bl < nl; bl += nwarp) {
+        const int b = uplane ? bl : 2 * bl;
+        const int rr = b >> 1, which = b & 1;
+        T2* oa = (which == 0 ? H0 : H2) + pbase + (size_t)(z0 + rr) * nk;
+        T2* ob = (which == 0 ? H1 : H3) + pbase + (size_t)(z0 + rr) * nk;
+        const T2* line = ex + (size_t)b * LU;
+        for (int k = lane; k < nk; k += 32) {
+            const T2 Pk = line[k];
+            const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
+            oa[k] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+            ob[k] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
+        }
+    }
+}
+
 // --------------------------------------------------------------------------------------
 // Pass 3: forward z transform (cft forward of phys_to_four_du, x 1/Ngal2) and truncation
 // to the retained kz modes (planes_to_modes_UVP/NUVP picks rows k and k+Ngal2-N2).
@@ -281,6 +430,107 @@ __global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0,
         const int i = kx0 + b;
         if (i < d.nkx) S[(size_t)slot * d.ncol + (size_t)q * d.nkx + i] = cscale(res[swz(row_of(d, q), b, bshift)], s);
     }
+}
+
+// Passes 1 and 3 with the two-step transform: CH = 1 << lb kx-columns per CTA.
+template <typename T2, int TN1, int TN2>
+__global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const double2* __restrict__ u2,
+                        const double2* __restrict__ u3, T2* __restrict__ H0, T2* __restrict__ H1,
+                        T2* __restrict__ H2, const T2* __restrict__ twz, int lb) {
+    using R = decltype(T2::x);
+    constexpr int N = TN1 * TN2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int CH = 1 << lb;
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* ex = twt + N;
+    load_twiddles<T2, TN1, TN2>(twt, twz);
+    const int kx0 = blockIdx.x * CH, slot = blockIdx.y, f = blockIdx.z;
+    const bool uplane = slot < d.nyu;
+    const int j = uplane ? d.ju0 + slot : d.jv0 + (slot - d.nyu);
+    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    const size_t nc = d.ncol;
+    __syncthreads();
+    auto load = [&](int e, int b) -> T2 {
+        const int i = kx0 + b;
+        int q = -1;
+        if (e < hq) q = e;
+        else if (e >= d.ngal2 - hq) q = e - gap;
+        if (q < 0 || i >= d.nkx) return cx<T2>((R)0, (R)0);
+        const size_t col = (size_t)q * d.nkx + i;
+        double2 val;
+        if (uplane) {
+            if (f == 0) val = u1[(size_t)(j - d.ju0) * nc + col];
+            else if (f == 1) val = u3[(size_t)(j - d.ju0) * nc + col];
+            else {
+                auto itp = [&](int jj) {
+                    const double2 va = u2[(size_t)(jj - d.jv0) * nc + col];
+                    const double2 vb = u2[(size_t)(jj - 1 - d.jv0) * nc + col];
+                    const double wa = g.vca[jj - d.ju0], wb = g.vcb[jj - d.ju0];
+                    return dc(wa * va.x + wb * vb.x, wa * va.y + wb * vb.y);
+                };
+                if (j == d.ju0) {
+                    const double2 vi = itp(d.ju0 + 1);
+                    val = dadd(dscl(g.gwib, dsub(u2[col], vi)), vi);
+                } else if (j == d.ju1) {
+                    const double2 vi = itp(d.ju1 - 1);
+                    val = dadd(dscl(g.gwit, dsub(u2[(size_t)(d.jv1 - d.jv0) * nc + col], vi)), vi);
+                } else {
+                    val = itp(j);
+                }
+            }
+        } else {
+            if (f == 2) val = u2[(size_t)(j - d.jv0) * nc + col];
+            else {
+                const double2* sf = f == 0 ? u1 : u3;
+                const double2 ua = sf[(size_t)(j + 1 - d.ju0) * nc + col];
+                const double2 ub = sf[(size_t)(j - d.ju0) * nc + col];
+                const double wa = g.ufa[j - d.jv0], wb = g.ufb[j - d.jv0];
+                val = dc(wa * ua.x + wb * ub.x, wa * ua.y + wb * ub.y);
+            }
+        }
+        return to_t2<T2>(val);
+    };
+    T2* H = f == 0 ? H0 : (f == 1 ? H1 : H2);
+    const size_t base = (size_t)slot * N * d.nkx;
+    auto store = [&](int z, int b, T2 v) {
+        const int i = kx0 + b;
+        if (i < d.nkx) H[base + (size_t)z * d.nkx + i] = v;
+    };
+    two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
+}
+
+template <typename T2, int TN1, int TN2>
+__global__ void k_zfwd2(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
+                        const T2* __restrict__ H3, T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
+                        T2* __restrict__ S3, const T2* __restrict__ twz, int lb) {
+    using R = decltype(T2::x);
+    constexpr int N = TN1 * TN2;
+    const int slot = blockIdx.y, f = blockIdx.z;
+    if (slot >= d.nyu && f >= 2) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int CH = 1 << lb;
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* ex = twt + N;
+    load_twiddles<T2, TN1, TN2>(twt, twz);
+    const int kx0 = blockIdx.x * CH;
+    const T2* H = f == 0 ? H0 : (f == 1 ? H1 : (f == 2 ? H2 : H3));
+    T2* S = f == 0 ? S0 : (f == 1 ? S1 : (f == 2 ? S2 : S3));
+    const size_t base = (size_t)slot * N * d.nkx;
+    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    const R sc = (R)1 / (R)N;
+    __syncthreads();
+    auto load = [&](int z, int b) -> T2 {
+        const int i = kx0 + b;
+        return i < d.nkx ? H[base + (size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
+    };
+    auto store = [&](int e, int b, T2 v) {
+        const int i = kx0 + b;
+        int q = -1;
+        if (e < hq) q = e;
+        else if (e >= d.ngal2 - hq) q = e - gap;
+        if (q >= 0 && i < d.nkx) S[(size_t)slot * d.ncol + (size_t)q * d.nkx + i] = cscale(v, sc);
+    };
+    two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
 }
 
 // --------------------------------------------------------------------------------------
@@ -611,6 +861,151 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
         const int b = t & (CH - 1), q = t >> bshift, i = kx0 + b;
         if (i < d.nkx) out[(size_t)q * d.nkx + i] = to_d2(cscale(res[swz(row_of(d, q), b, bshift)], s));
     }
+}
+
+// IB round trip with the two-step transform (same data flow as k_ib_zinv/xinv/xfwd/zfwd).
+template <typename T2, int TN1, int TN2>
+__global__ void k_ib_zinv2(Dims d, IBSrc src, int j0, const int* __restrict__ planes, int npl, T2* __restrict__ Hib,
+                           const T2* __restrict__ twz, int lb) {
+    using R = decltype(T2::x);
+    constexpr int N = TN1 * TN2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* ex = twt + N;
+    load_twiddles<T2, TN1, TN2>(twt, twz);
+    const int CH = 1 << lb;
+    const int kx0 = blockIdx.x * CH, p = blockIdx.y, sidx = blockIdx.z;
+    const int j = planes[p];
+    const double2* f = src.f[sidx] + (size_t)(j - j0) * d.ncol;
+    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    __syncthreads();
+    auto load = [&](int e, int b) -> T2 {
+        const int i = kx0 + b;
+        int q = -1;
+        if (e < hq) q = e;
+        else if (e >= d.ngal2 - hq) q = e - gap;
+        if (q < 0 || i >= d.nkx) return cx<T2>((R)0, (R)0);
+        return to_t2<T2>(f[(size_t)q * d.nkx + i]);
+    };
+    T2* H = Hib + ((size_t)sidx * npl + p) * N * d.nkx;
+    auto store = [&](int z, int b, T2 v) {
+        const int i = kx0 + b;
+        if (i < d.nkx) H[(size_t)z * d.nkx + i] = v;
+    };
+    two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
+}
+
+// inverse x: line (rhs + i u) of each of RW rows -> physical rhs, u (rows coalesced in x)
+template <typename T2, int TN1, int TN2>
+__global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype(T2::x)* __restrict__ phys,
+                           const T2* __restrict__ twx, int RW) {
+    using R = decltype(T2::x);
+    constexpr int N = TN1 * TN2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* stg = twt + N;                       // [RW][2][nk]
+    T2* ex = stg + (size_t)RW * 2 * d.nkx;
+    load_twiddles<T2, TN1, TN2>(twt, twx);
+    const int z0 = blockIdx.x * RW, p = blockIdx.y, fb = blockIdx.z;
+    const int nk = d.nkx, h = d.n1 / 2;
+    const size_t pl = (size_t)d.ngal2 * nk;
+    const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl;
+    const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl;
+    for (int t = threadIdx.x; t < 2 * RW * nk; t += blockDim.x) {
+        const int rf = t / nk, k = t - rf * nk;
+        const int rr = rf >> 1, which = rf & 1;
+        stg[t] = (which == 0 ? Hr : Hu)[(size_t)(z0 + rr) * nk + k];
+    }
+    __syncthreads();
+    auto load = [&](int e, int b) -> T2 {
+        const T2* A = stg + (size_t)(2 * b) * nk;
+        const T2* C = A + nk;
+        if (e <= h) {
+            T2 a = A[e], c = C[e];
+            if (e == 0) { a.y = 0; c.y = 0; }
+            return cx<T2>(a.x - c.y, a.y + c.x);
+        }
+        if (e >= N - h) {
+            const T2 a = A[N - e], c = C[N - e];
+            return cx<T2>(a.x + c.y, -a.y + c.x);
+        }
+        return cx<T2>((R)0, (R)0);
+    };
+    const size_t ppl = (size_t)d.ngal2 * N;
+    R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl + (size_t)z0 * N;
+    R* pu = phys + ((size_t)(2 * fb + 1) * npl + p) * ppl + (size_t)z0 * N;
+    auto store = [&](int x, int b, T2 v) {
+        pr[(size_t)b * N + x] = v.x;
+        pu[(size_t)b * N + x] = v.y;
+    };
+    two_step_lines<T2, TN1, TN2, +1, false>(0, ex, twt, load, store, RW);
+}
+
+// forward x of physical rhs rows (two rows per complex line), unpack, truncate, x 1/Ngal1
+template <typename T2, int TN1, int TN2>
+__global__ void k_ib_xfwd2(Dims d, T2* __restrict__ Hib, int npl, const decltype(T2::x)* __restrict__ phys,
+                           const T2* __restrict__ twx, int RW) {
+    using R = decltype(T2::x);
+    constexpr int N = TN1 * TN2;
+    constexpr int LU = N + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nl = RW / 2;
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* ub = twt + N;                                  // [nl][LU]
+    T2* ex = ub + (size_t)nl * LU;
+    load_twiddles<T2, TN1, TN2>(twt, twx);
+    const int z0 = blockIdx.x * RW, p = blockIdx.y, fb = blockIdx.z;
+    const size_t ppl = (size_t)d.ngal2 * N;
+    const R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl + (size_t)z0 * N;
+    __syncthreads();
+    auto load = [&](int x, int b) -> T2 { return cx<T2>(pr[(size_t)(2 * b) * N + x], pr[(size_t)(2 * b + 1) * N + x]); };
+    auto store = [&](int k, int b, T2 v) { ub[(size_t)b * LU + k] = v; };
+    two_step_lines<T2, TN1, TN2, -1, false>(0, ex, twt, load, store, nl);
+    const R hs = (R)0.5 / (R)N;
+    const int nk = d.nkx;
+    T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)d.ngal2 * nk;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int b = warp; b < nl; b += nwarp) {
+        const T2* line = ub + (size_t)b * LU;
+        T2* o0 = Hr + (size_t)(z0 + 2 * b) * nk;
+        T2* o1 = o0 + nk;
+        for (int k = lane; k < nk; k += 32) {
+            const T2 Pk = line[k];
+            const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
+            o0[k] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+            o1[k] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
+        }
+    }
+}
+
+template <typename T2, int TN1, int TN2>
+__global__ void k_ib_zfwd2(Dims d, const T2* __restrict__ Hib, int npl, IBDst dst, int j0,
+                           const int* __restrict__ planes, const T2* __restrict__ twz, int lb) {
+    using R = decltype(T2::x);
+    constexpr int N = TN1 * TN2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* ex = twt + N;
+    load_twiddles<T2, TN1, TN2>(twt, twz);
+    const int CH = 1 << lb;
+    const int kx0 = blockIdx.x * CH, p = blockIdx.y, fb = blockIdx.z;
+    const T2* H = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)N * d.nkx;
+    double2* out = dst.f[fb] + (size_t)(planes[p] - j0) * d.ncol;
+    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    const R sc = (R)1 / (R)N;
+    __syncthreads();
+    auto load = [&](int z, int b) -> T2 {
+        const int i = kx0 + b;
+        return i < d.nkx ? H[(size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
+    };
+    auto store = [&](int e, int b, T2 v) {
+        const int i = kx0 + b;
+        int q = -1;
+        if (e < hq) q = e;
+        else if (e >= d.ngal2 - hq) q = e - gap;
+        if (q >= 0 && i < d.nkx) out[(size_t)q * d.nkx + i] = to_d2(cscale(v, sc));
+    };
+    two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
 }
 
 // --------------------------------------------------------------------------------------

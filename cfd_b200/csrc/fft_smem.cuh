@@ -20,12 +20,12 @@ template <typename R> struct CxT;
 template <> struct CxT<float> { using T = float2; };
 template <> struct CxT<double> { using T = double2; };
 
-template <typename T2> __device__ __forceinline__ T2 cx(decltype(T2::x) a, decltype(T2::x) b) {
+template <typename T2> __host__ __device__ __forceinline__ T2 cx(decltype(T2::x) a, decltype(T2::x) b) {
     T2 r; r.x = a; r.y = b; return r;
 }
-template <typename T2> __device__ __forceinline__ T2 cadd(T2 a, T2 b) { return cx<T2>(a.x + b.x, a.y + b.y); }
-template <typename T2> __device__ __forceinline__ T2 csub(T2 a, T2 b) { return cx<T2>(a.x - b.x, a.y - b.y); }
-template <typename T2> __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
+template <typename T2> __host__ __device__ __forceinline__ T2 cadd(T2 a, T2 b) { return cx<T2>(a.x + b.x, a.y + b.y); }
+template <typename T2> __host__ __device__ __forceinline__ T2 csub(T2 a, T2 b) { return cx<T2>(a.x - b.x, a.y - b.y); }
+template <typename T2> __host__ __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
     return cx<T2>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 // a * conj(b)
@@ -33,7 +33,7 @@ template <typename T2> __device__ __forceinline__ T2 cmulc(T2 a, T2 b) {
     return cx<T2>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 template <typename T2> __device__ __forceinline__ T2 cconj(T2 a) { return cx<T2>(a.x, -a.y); }
-template <typename T2> __device__ __forceinline__ T2 cscale(T2 a, decltype(T2::x) s) { return cx<T2>(a.x * s, a.y * s); }
+template <typename T2> __host__ __device__ __forceinline__ T2 cscale(T2 a, decltype(T2::x) s) { return cx<T2>(a.x * s, a.y * s); }
 // i * a
 template <typename T2> __device__ __forceinline__ T2 cmuli(T2 a) { return cx<T2>(-a.y, a.x); }
 
@@ -143,17 +143,17 @@ template <> struct RadixPlan<768> { static constexpr int P = 4; static constexpr
 template <int N> struct IsFixed { static constexpr bool value = RadixPlan<N>::P > 0; };
 
 // multiply by SIGN*i
-template <int SIGN, typename T2> __device__ __forceinline__ T2 mul_si(T2 a) {
+template <int SIGN, typename T2> __host__ __device__ __forceinline__ T2 mul_si(T2 a) {
     return SIGN < 0 ? cx<T2>(a.y, -a.x) : cx<T2>(-a.y, a.x);
 }
 
-template <int SIGN, typename T2> __device__ __forceinline__ void dft2(T2& a, T2& b) {
+template <int SIGN, typename T2> __host__ __device__ __forceinline__ void dft2(T2& a, T2& b) {
     T2 t = csub(a, b);
     a = cadd(a, b);
     b = t;
 }
 
-template <int SIGN, typename T2> __device__ __forceinline__ void dft3(T2& x0, T2& x1, T2& x2) {
+template <int SIGN, typename T2> __host__ __device__ __forceinline__ void dft3(T2& x0, T2& x1, T2& x2) {
     using R_t = decltype(T2::x);
     const R_t s3 = (R_t)0.86602540378443864676 * (R_t)SIGN;
     T2 t1 = cadd(x1, x2);
@@ -165,7 +165,7 @@ template <int SIGN, typename T2> __device__ __forceinline__ void dft3(T2& x0, T2
     x2 = csub(t2, t3);
 }
 
-template <int SIGN, typename T2> __device__ __forceinline__ void dft4(T2& x0, T2& x1, T2& x2, T2& x3) {
+template <int SIGN, typename T2> __host__ __device__ __forceinline__ void dft4(T2& x0, T2& x1, T2& x2, T2& x3) {
     T2 a0 = cadd(x0, x2), a1 = csub(x0, x2);
     T2 b0 = cadd(x1, x3), b1 = mul_si<SIGN>(csub(x1, x3));
     x0 = cadd(a0, b0);
@@ -175,7 +175,7 @@ template <int SIGN, typename T2> __device__ __forceinline__ void dft4(T2& x0, T2
 }
 
 // radix-6 = even/odd split into two DFT3: X_k = E_{k%3} + w6^k O_{k%3}
-template <int SIGN, typename T2> __device__ __forceinline__ void dft6(T2* v) {
+template <int SIGN, typename T2> __host__ __device__ __forceinline__ void dft6(T2* v) {
     using R_t = decltype(T2::x);
     T2 e0 = v[0], e1 = v[2], e2 = v[4], o0 = v[1], o1 = v[3], o2 = v[5];
     dft3<SIGN>(e0, e1, e2);
@@ -189,7 +189,7 @@ template <int SIGN, typename T2> __device__ __forceinline__ void dft6(T2* v) {
 }
 
 // radix-8 = even/odd split into two DFT4: X_k = A_{k%4} + w8^k B_{k%4}
-template <int SIGN, typename T2> __device__ __forceinline__ void dft8(T2* v) {
+template <int SIGN, typename T2> __host__ __device__ __forceinline__ void dft8(T2* v) {
     using R_t = decltype(T2::x);
     T2 a0 = v[0], a1 = v[2], a2 = v[4], a3 = v[6];
     T2 b0 = v[1], b1 = v[3], b2 = v[5], b3 = v[7];
