@@ -500,8 +500,8 @@ int solvep_kernel(cfd_ctx* c, int krk, bool with_div) {
     const double dtirk = (1.0 / c->dt) / (kRKa[krk - 1] + kRKb[krk - 1]);
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
-    k_solve_p<<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, with_div ? c->div : nullptr,
-                                         c->cs, c->mean_diag);
+    k_solve_p<false><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi,
+                                                with_div ? c->div : nullptr, c->cs, c->mean_diag, 0.0);
     LK("k_solve_p");
     return CFD_OK;
 }
@@ -530,8 +530,16 @@ int substep(cfd_ctx* c, int krk) {
     if ((s = ib_all<T2>(c)) != CFD_OK) return s;
     if ((s = solve_kernel(c, krk)) != CFD_OK) return s;
     if (c->ctpress == 0 && (s = meanflow_kernel(c, krk)) != CFD_OK) return s;
-    if ((s = solvep_kernel(c, krk, false)) != CFD_OK) return s;
-    return vcorr_kernel(c, krk, false);
+    // solveP + v_corr in one column sweep (psi is not stored on this path)
+    const Dims& d = c->d;
+    const double dtirk = (1.0 / c->dt) / (kRKa[krk - 1] + kRKb[krk - 1]);
+    const double dtrk = c->dt * (kRKa[krk - 1] + kRKb[krk - 1]);
+    dim3 gb((d.ncol + 255) / 256);
+    prof_mark(c);
+    k_solve_p<true><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, nullptr, c->cs,
+                                               c->mean_diag, dtrk);
+    LK("k_solve_p_vcorr");
+    return CFD_OK;
 }
 
 int substep_any(cfd_ctx* c, int krk) {
@@ -780,7 +788,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
             const int N = n1s * n2s, L1 = (n1s * (n2s + 1)) | 1, mx = std::max(n1s, n2s);
-            for (int rw = 16; rw >= 1; rw /= 2) {
+            for (int rw = 8; rw >= 1; rw /= 2) {
                 const size_t sm = ((size_t)N + 2 * rw * d.nkx + (size_t)rw * L1) * esz;
                 if (d.ngal2 % rw == 0 && sm <= budget && rw * mx <= 1024) { c->RWIX2 = rw; c->SMIX2 = sm; c->NTIX2 = rw * mx; break; }
             }

@@ -1140,10 +1140,12 @@ __global__ void __launch_bounds__(256) k_solve_uvw(Dims d, Geo g, double beta, d
 // psi(mean, bottom) = 0, LUsolP with the D.G matrix of LU_buildP/LU_decP computed on
 // the fly (tridLU_3D_IB.f90:284-318, 417-491, 562-603), p += psi.
 // --------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_solve_p(Dims d, Geo g, double dtirk, const double2* __restrict__ u1,
-                                                 const double2* __restrict__ u2, const double2* __restrict__ u3,
+template <bool FUSE>
+__global__ void __launch_bounds__(256) k_solve_p(Dims d, Geo g, double dtirk, double2* __restrict__ u1,
+                                                 double2* __restrict__ u2, double2* __restrict__ u3,
                                                  double2* __restrict__ p, double2* __restrict__ psi,
-                                                 double2* __restrict__ divo, double* __restrict__ cs, double mean_diag) {
+                                                 double2* __restrict__ divo, double* __restrict__ cs, double mean_diag,
+                                                 double dtrk) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
     const int i = col % d.nkx, q = col / d.nkx;
@@ -1209,23 +1211,52 @@ __global__ void __launch_bounds__(256) k_solve_p(Dims d, Geo g, double dtirk, co
     }
     double2 x = y;
     p[(size_t)(n - 1) * nc + col] = dadd(p[(size_t)(n - 1) * nc + col], x);
+    if (FUSE) {
+        // v_corr (littleharsh.f90:796-907) in the back sweep: centre j = jp0 + jj takes
+        // psi(j); face j takes psi(j+1) - psi(j) (faces jv0+1..jv1-1); ghost/wall rows last
+        const size_t ju = (size_t)(d.jp1 - d.ju0);
+        u1[ju * nc + col] = dsub(u1[ju * nc + col], dik(dtrk * kxv, x));
+        u3[ju * nc + col] = dsub(u3[ju * nc + col], dik(dtrk * kzv, x));
+        u1[(ju + 1) * nc + col] = dscl(-g.gwt, u1[ju * nc + col]);
+        u3[(ju + 1) * nc + col] = dscl(-g.gwt, u3[ju * nc + col]);
+    }
     for (int jj0 = n - 2; jj0 >= 0; jj0 -= CFD_UB) {
         double cc[CFD_UB];
-        double2 ya[CFD_UB], pa[CFD_UB];
+        double2 ya[CFD_UB], pa[CFD_UB], ua[CFD_UB], wa[CFD_UB], va[CFD_UB];
 #pragma unroll
         for (int t = 0; t < CFD_UB; ++t)
             if (jj0 - t >= 0) {
                 const size_t o = (size_t)(jj0 - t) * nc + col;
                 cc[t] = cs[o]; ya[t] = psi[o]; pa[t] = p[o];
+                if (FUSE) {
+                    const int j = d.jp0 + jj0 - t;
+                    ua[t] = u1[(size_t)(j - d.ju0) * nc + col];
+                    wa[t] = u3[(size_t)(j - d.ju0) * nc + col];
+                    va[t] = u2[(size_t)(j - d.jv0) * nc + col];
+                }
             }
 #pragma unroll
         for (int t = 0; t < CFD_UB; ++t) {
             if (jj0 - t < 0) break;
             const size_t o = (size_t)(jj0 - t) * nc + col;
+            const double2 xp = x;  // psi(j+1)
             x = dsub(ya[t], dscl(cc[t], x));
-            psi[o] = x;
+            if (!FUSE) psi[o] = x;
             p[o] = dadd(pa[t], x);
+            if (FUSE) {
+                const int j = d.jp0 + jj0 - t;
+                u1[(size_t)(j - d.ju0) * nc + col] = dsub(ua[t], dik(dtrk * kxv, x));
+                u3[(size_t)(j - d.ju0) * nc + col] = dsub(wa[t], dik(dtrk * kzv, x));
+                const size_t jv = (size_t)(j - d.jv0);
+                u2[jv * nc + col] = dsub(va[t], dscl(dtrk * g.dthdyv[jv], dsub(xp, x)));
+            }
         }
+    }
+    if (FUSE) {
+        u1[col] = dscl(-g.gwb, u1[nc + col]);
+        u3[col] = dscl(-g.gwb, u3[nc + col]);
+        u2[col] = dc(0, 0);
+        u2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
     }
 }
 
