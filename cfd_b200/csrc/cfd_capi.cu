@@ -214,11 +214,11 @@ int ilog2(int b) {
     }
 
 // shared memory of k_xline2 (elements): B*LX + N + RW*3*nk
-size_t xline2_smem(int n1s, int n2s, int rw, int nk, size_t esz) {
+size_t xline2_smem(int n1s, int n2s, int rw, size_t esz) {
     const int N = n1s * n2s;
     const int L1 = n1s * (n2s + 1) + 1, L2 = n2s * (n1s + 1) + 1, LU = N + 1;
     const int LX = std::max(L1, std::max(L2, LU));
-    return ((size_t)2 * rw * LX + N + (size_t)rw * 3 * nk) * esz;
+    return ((size_t)2 * rw * LX + N) * esz;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -308,7 +308,7 @@ int nl_transforms(cfd_ctx* c) {
     prof_mark(c);
     if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
-        dim3 gz2((d.nkx + CH2 - 1) / CH2, d.nslot, 3);
+        dim3 gz2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 3, 2);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
             k_zinv2<T2, TN1, TN2><<<gz2, c->NTZ2, c->SMZ2, c->stream>>>(d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0],
@@ -344,7 +344,7 @@ int nl_transforms(cfd_ctx* c) {
     prof_mark(c);
     if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
-        dim3 gf2((d.nkx + CH2 - 1) / CH2, d.nslot, 4);
+        dim3 gf2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 4, 2);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
             k_zfwd2<T2, TN1, TN2><<<gf2, c->NTZ2, c->SMZ2, c->stream>>>(
@@ -392,7 +392,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     prof_mark(c);
     if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
-        dim3 g1((d.nkx + CH2 - 1) / CH2, ib.npl, 2 * nb);
+        dim3 g1((ib.npl * d.nkx + CH2 - 1) / CH2, 1, 2 * nb);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
             k_ib_zinv2<T2, TN1, TN2><<<g1, c->NTZ2, c->SMZ2, c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib,
@@ -450,7 +450,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     prof_mark(c);
     if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
-        dim3 g5((d.nkx + CH2 - 1) / CH2, ib.npl, nb);
+        dim3 g5((ib.npl * d.nkx + CH2 - 1) / CH2, 1, nb);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
             k_ib_zfwd2<T2, TN1, TN2><<<g5, c->NTZ2, c->SMZ2, c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0,
@@ -762,11 +762,11 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
             int rw = 8;
-            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, d.nkx, esz) > budget)) rw /= 2;
+            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
             if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
                 c->RW2 = rw;
                 c->NT2 = 2 * rw * std::max(n1s, n2s);
-                c->SM2 = xline2_smem(n1s, n2s, rw, d.nkx, esz);
+                c->SM2 = xline2_smem(n1s, n2s, rw, esz);
             }
         }
     }

@@ -247,27 +247,30 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // Pass 2 with the register-resident two-step transform (N = N1*N2, fft_reg.cuh).  A CTA
 // holds RW rows = B = 2*RW lines (line 2r = u + i w, line 2r+1 = v + i 0) and runs with
 // B*max(N1,N2) threads:
-//   step 1  thread (b, n2): N1-point DFT of the stride-N2 subsequence, twiddle, exchange
+//   step 1  thread (b, n2): reads its stride-N2 subsequence of the Hermitian-extended
+//           spectrum straight from global memory, N1-point DFT, twiddle, exchange
 //   step 2  thread (b, k1): N2-point DFT -> physical x = k1 + N1*k2 in registers; the two
 //           lines of a row sit in adjacent lanes and swap w / v with one shuffle, form the
 //           products, and start the forward transform from registers (N2-point DFT)
 //   step 2' thread (b, kb): N1-point DFT -> X[kb + N2*ka]; unpack the two real spectra.
+// The retained modes are kx = 0..N/3 (N1 = 2*(Ngal1/3)), a compile-time bound, so which
+// elements of a subsequence are zero, direct or conjugated is resolved at compile time
+// except in the two blocks that straddle a boundary.
 template <typename T2, int N1, int N2>
 __global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
     using R = decltype(T2::x);
     constexpr int N = N1 * N2;
+    constexpr int HX = N / 3;               // highest retained kx
+    constexpr int NK = HX + 1;              // kx columns per row (= d.nkx)
     constexpr int L1 = N1 * (N2 + 1) + 1;  // inverse exchange, per line: [k1][n2]
     constexpr int L2 = N2 * (N1 + 1) + 1;  // forward exchange, per line: [kb][na]
     constexpr int LU = N + 1;               // unpack buffer, per line
     constexpr int LX = (L1 > L2 ? (L1 > LU ? L1 : LU) : (L2 > LU ? L2 : LU));
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = 2 * RW;
-    const int nk = d.nkx;
-    const int h = d.n1 / 2;
     T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX
     T2* twt = ex + (size_t)B * LX;                   // N1 * N2: twt[b*N2 + a] = w^(a*b), a < N2, b < N1
-    T2* stg = twt + N;                               // RW * 3 * nk staged spectra
     const int slot = blockIdx.y;
     const int z0 = blockIdx.x * RW;
     const bool uplane = slot < d.nyu;
@@ -276,38 +279,30 @@ __global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* _
         const int b = i / N2, a = i - b * N2;
         twt[i] = twx[(a * b) % N];
     }
-    const size_t pbase = (size_t)slot * d.ngal2 * nk;
-    {
-        const int lane = t & 31, warp = t >> 5, nwarp = blockDim.x >> 5;
-        for (int rf = warp; rf < 3 * RW; rf += nwarp) {
-            const int rr = rf / 3, f = rf - 3 * rr;
-            const T2* src = (f == 0 ? H0 : (f == 1 ? H1 : H2)) + pbase + (size_t)(z0 + rr) * nk;
-            T2* dst = stg + (size_t)rf * nk;
-            for (int k = lane; k < nk; k += 32) dst[k] = src[k];
-        }
-    }
+    const size_t pbase = (size_t)slot * d.ngal2 * NK;
     __syncthreads();
 
     // ---- step 1: inverse, thread (b, n2)
     if (t < B * N2) {
-        const int n2 = t % N2, b = t / N2;
+        const int b = (unsigned)t / N2, n2 = t - b * N2;
         const int rr = b >> 1, which = b & 1;
-        const T2* A = stg + (size_t)(3 * rr + (which == 0 ? 0 : 2)) * nk;
-        const T2* C = stg + (size_t)(3 * rr + 1) * nk;
+        const T2* A = (which == 0 ? H0 : H2) + pbase + (size_t)(z0 + rr) * NK;
+        const T2* C = H1 + pbase + (size_t)(z0 + rr) * NK;
         T2 v[N1];
 #pragma unroll
         for (int n1 = 0; n1 < N1; ++n1) {
-            const int e = n1 * N2 + n2;
+            const int e0 = n1 * N2, e = e0 + n2;
+            const bool lo = (e0 + N2 - 1 <= HX) || (e0 <= HX && e <= HX);
+            const bool hi = (e0 >= N - HX) || (e0 + N2 - 1 >= N - HX && e >= N - HX);
             T2 val = cx<T2>((R)0, (R)0);
-            if (e <= h) {
+            if (lo) {
                 T2 a = A[e];
                 T2 c = which == 0 ? C[e] : cx<T2>((R)0, (R)0);
-                if (e == 0) { a.y = 0; c.y = 0; }
+                if (n1 == 0 && n2 == 0) { a.y = 0; c.y = 0; }
                 val = cx<T2>(a.x - c.y, a.y + c.x);
-            } else if (e >= N - h) {
-                const int k = N - e;
-                const T2 a = A[k];
-                const T2 c = which == 0 ? C[k] : cx<T2>((R)0, (R)0);
+            } else if (hi) {
+                const T2 a = A[N - e];
+                const T2 c = which == 0 ? C[N - e] : cx<T2>((R)0, (R)0);
                 val = cx<T2>(a.x + c.y, -a.y + c.x);
             }
             v[n1] = val;
@@ -355,10 +350,12 @@ __global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* _
     }
     __syncthreads();
 
-    // ---- step 2': forward N1-point DFT, thread (b, kb) -> X[kb + N2*ka]
+    // ---- step 2': forward N1-point DFT, thread (b, kb) -> X[kb + N2*ka]; even lines take
+    // the first RW*N2 threads, so on v-planes (odd lines are zero) whole warps drop out
     T2 z[N1];
-    const bool act3 = t < B * N2;
-    const int kb = t % N2, b3 = t / N2;
+    const int kb = t % N2, i3 = t / N2;
+    const int b3 = i3 < RW ? 2 * i3 : 2 * (i3 - RW) + 1;
+    const bool act3 = t < B * N2 && (uplane || i3 < RW);
     if (act3) {
         const T2* o = ex + (size_t)b3 * L2 + kb * (N1 + 1);
 #pragma unroll
@@ -373,22 +370,20 @@ __global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* _
     }
     __syncthreads();
 
-    // ---- unpack A_k = (P_k + conj P_{N-k})/2, B_k = (P_k - conj P_{N-k})/(2i), x 1/N
+    // ---- unpack A_k = (P_k + conj P_{N-k})/2, B_k = (P_k - conj P_{N-k})/(2i), x 1/N;
+    // work items (line, k) flattened so that no lane idles on a partial last chunk
     const R hs = (R)0.5 / (R)N;
-    const int lane = t & 31, warp = t >> 5, nwarp = blockDim.x >> 5;
     const int nl = uplane ? B : RW;
-    for (int bl = warp; bl < nl; bl += nwarp) {
+    for (int it = t; it < nl * NK; it += blockDim.x) {
+        const int bl = (unsigned)it / NK, k = it - bl * NK;
         const int b = uplane ? bl : 2 * bl;
         const int rr = b >> 1, which = b & 1;
-        T2* oa = (which == 0 ? H0 : H2) + pbase + (size_t)(z0 + rr) * nk;
-        T2* ob = (which == 0 ? H1 : H3) + pbase + (size_t)(z0 + rr) * nk;
+        const size_t o = pbase + (size_t)(z0 + rr) * NK + k;
         const T2* line = ex + (size_t)b * LU;
-        for (int k = lane; k < nk; k += 32) {
-            const T2 Pk = line[k];
-            const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
-            oa[k] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
-            ob[k] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
-        }
+        const T2 Pk = line[k];
+        const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
+        (which == 0 ? H0 : H2)[o] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+        (which == 0 ? H1 : H3)[o] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
     }
 }
 
@@ -432,103 +427,141 @@ __global__ void __launch_bounds__(256) k_zfwd(Dims d, const T2* __restrict__ H0,
     }
 }
 
-// Passes 1 and 3 with the two-step transform: CH = 1 << lb kx-columns per CTA.
+// Retained-row index q of z element e = e0 + r of a two-step line, where r (0 <= r < W) is
+// the thread's own offset and e0 a compile-time constant once the element loop is
+// unrolled; -1 inside the truncated band.  Rows 0..N/3-1 hold kz >= 0, rows N-N/3..N-1 the
+// negative kz (N2 = 2*(Ngal2/3) modes kept), so only blocks straddling a band edge test e.
+template <int N, int W>
+__device__ __forceinline__ int zrow_q(int e, int r) {
+    constexpr int HQ = N / 3, GAP = N - 2 * (N / 3);
+    const int e0 = e - r;
+    if (e0 + W - 1 < HQ) return e;
+    if (e0 >= N - HQ) return e - GAP;
+    if (e0 >= HQ && e0 + W - 1 < N - HQ) return -1;
+    return e < HQ ? e : (e >= N - HQ ? e - GAP : -1);
+}
+
+// Passes 1 and 3 with the two-step transform.  Lines are numbered across a slot group
+// (group 0: the nyu u-planes, group 1: the nyv v-planes) as line = slot-in-group * nkx + kx,
+// and a CTA takes CH = 1 << lb consecutive lines, so no CTA is left with a partial kx chunk.
+// grid: x = line chunk, y = field, z = group.
+//
+// Pass 1 source of every line: ca * A[col] + cb * B[col] with planes A, B and weights fixed
+// per line, so the element loop has no branches and its loads issue back to back.  On the
+// two wall centres the ghost extrapolation of v (FOU3D.f90:261-283) is folded into the
+// two weights (A = v(1), B = v(0) at the bottom; A = v(ny), B = v(ny-1) at the top; the
+// u and v index ranges start at the same j).
 template <typename T2, int TN1, int TN2>
 __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const double2* __restrict__ u2,
                         const double2* __restrict__ u3, T2* __restrict__ H0, T2* __restrict__ H1,
                         T2* __restrict__ H2, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
+    const int grp = blockIdx.z, f = blockIdx.y;
+    const int nsl = grp ? d.nyv : d.nyu;
+    const int nlines = nsl * d.nkx;
+    const int line0 = blockIdx.x << lb;
+    if (line0 >= nlines) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int CH = 1 << lb;
     T2* twt = reinterpret_cast<T2*>(smem_raw);
     T2* ex = twt + N;
     load_twiddles<T2, TN1, TN2>(twt, twz);
-    const int kx0 = blockIdx.x * CH, slot = blockIdx.y, f = blockIdx.z;
-    const bool uplane = slot < d.nyu;
-    const int j = uplane ? d.ju0 + slot : d.jv0 + (slot - d.nyu);
-    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    const int b = threadIdx.x & ((1 << lb) - 1);
+    const bool live = line0 + b < nlines;
+    const int line = live ? line0 + b : nlines - 1;
+    const int sl = line / d.nkx, i = line - sl * d.nkx;
     const size_t nc = d.ncol;
-    __syncthreads();
-    auto load = [&](int e, int b) -> T2 {
-        const int i = kx0 + b;
-        int q = -1;
-        if (e < hq) q = e;
-        else if (e >= d.ngal2 - hq) q = e - gap;
-        if (q < 0 || i >= d.nkx) return cx<T2>((R)0, (R)0);
-        const size_t col = (size_t)q * d.nkx + i;
-        double2 val;
-        if (uplane) {
-            if (f == 0) val = u1[(size_t)(j - d.ju0) * nc + col];
-            else if (f == 1) val = u3[(size_t)(j - d.ju0) * nc + col];
-            else {
-                auto itp = [&](int jj) {
-                    const double2 va = u2[(size_t)(jj - d.jv0) * nc + col];
-                    const double2 vb = u2[(size_t)(jj - 1 - d.jv0) * nc + col];
-                    const double wa = g.vca[jj - d.ju0], wb = g.vcb[jj - d.ju0];
-                    return dc(wa * va.x + wb * vb.x, wa * va.y + wb * vb.y);
-                };
-                if (j == d.ju0) {
-                    const double2 vi = itp(d.ju0 + 1);
-                    val = dadd(dscl(g.gwib, dsub(u2[col], vi)), vi);
-                } else if (j == d.ju1) {
-                    const double2 vi = itp(d.ju1 - 1);
-                    val = dadd(dscl(g.gwit, dsub(u2[(size_t)(d.jv1 - d.jv0) * nc + col], vi)), vi);
-                } else {
-                    val = itp(j);
-                }
-            }
+    const double2* pa;
+    const double2* pb;
+    double ca = 1.0, cb = 0.0;
+    bool two;
+    if (grp == 0) {
+        two = f == 2;
+        if (!two) {
+            pa = (f == 0 ? u1 : u3) + (size_t)sl * nc;
+        } else if (sl == 0) {
+            pa = u2 + nc;
+            ca = (1.0 - g.gwib) * g.vca[1];
+            cb = g.gwib + (1.0 - g.gwib) * g.vcb[1];
+        } else if (sl == nsl - 1) {
+            pa = u2 + (size_t)(sl - 1) * nc;
+            ca = g.gwit + (1.0 - g.gwit) * g.vca[sl - 1];
+            cb = (1.0 - g.gwit) * g.vcb[sl - 1];
         } else {
-            if (f == 2) val = u2[(size_t)(j - d.jv0) * nc + col];
-            else {
-                const double2* sf = f == 0 ? u1 : u3;
-                const double2 ua = sf[(size_t)(j + 1 - d.ju0) * nc + col];
-                const double2 ub = sf[(size_t)(j - d.ju0) * nc + col];
-                const double wa = g.ufa[j - d.jv0], wb = g.ufb[j - d.jv0];
-                val = dc(wa * ua.x + wb * ub.x, wa * ua.y + wb * ub.y);
-            }
+            pa = u2 + (size_t)sl * nc;
+            ca = g.vca[sl];
+            cb = g.vcb[sl];
         }
-        return to_t2<T2>(val);
+    } else {
+        two = f != 2;
+        if (!two) {
+            pa = u2 + (size_t)sl * nc;
+        } else {
+            pa = (f == 0 ? u1 : u3) + (size_t)(sl + 1) * nc;
+            ca = g.ufa[sl];
+            cb = g.ufb[sl];
+        }
+    }
+    pa += i;
+    pb = two ? pa - nc : pa;
+    const int r = threadIdx.x >> lb;
+    T2* H = (f == 0 ? H0 : (f == 1 ? H1 : H2)) + (size_t)(grp ? d.nyu + sl : sl) * N * d.nkx + i;
+    __syncthreads();
+    auto qof = [&](int e) { return zrow_q<N, TN2>(e, r); };
+    auto store = [&](int z, int, T2 v) {
+        if (live) H[(size_t)z * d.nkx] = v;
     };
-    T2* H = f == 0 ? H0 : (f == 1 ? H1 : H2);
-    const size_t base = (size_t)slot * N * d.nkx;
-    auto store = [&](int z, int b, T2 v) {
-        const int i = kx0 + b;
-        if (i < d.nkx) H[base + (size_t)z * d.nkx + i] = v;
-    };
-    two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
+    if (two) {
+        auto load = [&](int e, int) -> T2 {
+            const int q = qof(e);
+            double2 va = dc(0.0, 0.0), vb = dc(0.0, 0.0);
+            if (q >= 0) {
+                va = pa[(size_t)q * d.nkx];
+                vb = pb[(size_t)q * d.nkx];
+            }
+            return to_t2<T2>(dc(ca * va.x + cb * vb.x, ca * va.y + cb * vb.y));
+        };
+        two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
+    } else {
+        auto load = [&](int e, int) -> T2 {
+            const int q = qof(e);
+            return q >= 0 ? to_t2<T2>(pa[(size_t)q * d.nkx]) : cx<T2>((R)0, (R)0);
+        };
+        two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
+    }
 }
 
+// Pass 3: grid x = line chunk, y = field 0..3, z = group (v-planes carry fields 0, 1 only).
 template <typename T2, int TN1, int TN2>
 __global__ void k_zfwd2(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
                         const T2* __restrict__ H3, T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
                         T2* __restrict__ S3, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
-    const int slot = blockIdx.y, f = blockIdx.z;
-    if (slot >= d.nyu && f >= 2) return;
+    const int grp = blockIdx.z, f = blockIdx.y;
+    if (grp == 1 && f >= 2) return;
+    const int nsl = grp ? d.nyv : d.nyu;
+    const int nlines = nsl * d.nkx;
+    const int line0 = blockIdx.x << lb;
+    if (line0 >= nlines) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int CH = 1 << lb;
     T2* twt = reinterpret_cast<T2*>(smem_raw);
     T2* ex = twt + N;
     load_twiddles<T2, TN1, TN2>(twt, twz);
-    const int kx0 = blockIdx.x * CH;
-    const T2* H = f == 0 ? H0 : (f == 1 ? H1 : (f == 2 ? H2 : H3));
-    T2* S = f == 0 ? S0 : (f == 1 ? S1 : (f == 2 ? S2 : S3));
-    const size_t base = (size_t)slot * N * d.nkx;
-    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    const int b = threadIdx.x & ((1 << lb) - 1);
+    const bool live = line0 + b < nlines;
+    const int line = live ? line0 + b : nlines - 1;
+    const int sl = line / d.nkx, i = line - sl * d.nkx;
+    const int slot = grp ? d.nyu + sl : sl;
+    const T2* H = (f == 0 ? H0 : (f == 1 ? H1 : (f == 2 ? H2 : H3))) + (size_t)slot * N * d.nkx + i;
+    T2* S = (f == 0 ? S0 : (f == 1 ? S1 : (f == 2 ? S2 : S3))) + (size_t)slot * d.ncol + i;
+    const int r = threadIdx.x >> lb;
     const R sc = (R)1 / (R)N;
     __syncthreads();
-    auto load = [&](int z, int b) -> T2 {
-        const int i = kx0 + b;
-        return i < d.nkx ? H[base + (size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
-    };
-    auto store = [&](int e, int b, T2 v) {
-        const int i = kx0 + b;
-        int q = -1;
-        if (e < hq) q = e;
-        else if (e >= d.ngal2 - hq) q = e - gap;
-        if (q >= 0 && i < d.nkx) S[(size_t)slot * d.ncol + (size_t)q * d.nkx + i] = cscale(v, sc);
+    auto load = [&](int z, int) -> T2 { return H[(size_t)z * d.nkx]; };
+    auto store = [&](int e, int, T2 v) {
+        const int q = zrow_q<N, TN1>(e, r);
+        if (q >= 0 && live) S[(size_t)q * d.nkx] = cscale(v, sc);
     };
     two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
 }
@@ -869,28 +902,27 @@ __global__ void k_ib_zinv2(Dims d, IBSrc src, int j0, const int* __restrict__ pl
                            const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
+    const int nlines = npl * d.nkx;
+    const int line0 = blockIdx.x << lb, sidx = blockIdx.z;
+    if (line0 >= nlines) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* twt = reinterpret_cast<T2*>(smem_raw);
     T2* ex = twt + N;
     load_twiddles<T2, TN1, TN2>(twt, twz);
-    const int CH = 1 << lb;
-    const int kx0 = blockIdx.x * CH, p = blockIdx.y, sidx = blockIdx.z;
-    const int j = planes[p];
-    const double2* f = src.f[sidx] + (size_t)(j - j0) * d.ncol;
-    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    const int b = threadIdx.x & ((1 << lb) - 1);
+    const bool live = line0 + b < nlines;
+    const int line = live ? line0 + b : nlines - 1;
+    const int p = line / d.nkx, i = line - p * d.nkx;
+    const double2* f = src.f[sidx] + (size_t)(planes[p] - j0) * d.ncol + i;
+    T2* H = Hib + ((size_t)sidx * npl + p) * N * d.nkx + i;
+    const int r = threadIdx.x >> lb;
     __syncthreads();
-    auto load = [&](int e, int b) -> T2 {
-        const int i = kx0 + b;
-        int q = -1;
-        if (e < hq) q = e;
-        else if (e >= d.ngal2 - hq) q = e - gap;
-        if (q < 0 || i >= d.nkx) return cx<T2>((R)0, (R)0);
-        return to_t2<T2>(f[(size_t)q * d.nkx + i]);
+    auto load = [&](int e, int) -> T2 {
+        const int q = zrow_q<N, TN2>(e, r);
+        return q >= 0 ? to_t2<T2>(f[(size_t)q * d.nkx]) : cx<T2>((R)0, (R)0);
     };
-    T2* H = Hib + ((size_t)sidx * npl + p) * N * d.nkx;
-    auto store = [&](int z, int b, T2 v) {
-        const int i = kx0 + b;
-        if (i < d.nkx) H[(size_t)z * d.nkx + i] = v;
+    auto store = [&](int z, int, T2 v) {
+        if (live) H[(size_t)z * d.nkx] = v;
     };
     two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
 }
@@ -983,27 +1015,26 @@ __global__ void k_ib_zfwd2(Dims d, const T2* __restrict__ Hib, int npl, IBDst ds
                            const int* __restrict__ planes, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
+    const int nlines = npl * d.nkx;
+    const int line0 = blockIdx.x << lb, fb = blockIdx.z;
+    if (line0 >= nlines) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* twt = reinterpret_cast<T2*>(smem_raw);
     T2* ex = twt + N;
     load_twiddles<T2, TN1, TN2>(twt, twz);
-    const int CH = 1 << lb;
-    const int kx0 = blockIdx.x * CH, p = blockIdx.y, fb = blockIdx.z;
-    const T2* H = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)N * d.nkx;
-    double2* out = dst.f[fb] + (size_t)(planes[p] - j0) * d.ncol;
-    const int hq = d.n2 / 2, gap = d.ngal2 - d.n2;
+    const int b = threadIdx.x & ((1 << lb) - 1);
+    const bool live = line0 + b < nlines;
+    const int line = live ? line0 + b : nlines - 1;
+    const int p = line / d.nkx, i = line - p * d.nkx;
+    const T2* H = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)N * d.nkx + i;
+    double2* out = dst.f[fb] + (size_t)(planes[p] - j0) * d.ncol + i;
+    const int r = threadIdx.x >> lb;
     const R sc = (R)1 / (R)N;
     __syncthreads();
-    auto load = [&](int z, int b) -> T2 {
-        const int i = kx0 + b;
-        return i < d.nkx ? H[(size_t)z * d.nkx + i] : cx<T2>((R)0, (R)0);
-    };
-    auto store = [&](int e, int b, T2 v) {
-        const int i = kx0 + b;
-        int q = -1;
-        if (e < hq) q = e;
-        else if (e >= d.ngal2 - hq) q = e - gap;
-        if (q >= 0 && i < d.nkx) out[(size_t)q * d.nkx + i] = to_d2(cscale(v, sc));
+    auto load = [&](int z, int) -> T2 { return H[(size_t)z * d.nkx]; };
+    auto store = [&](int e, int, T2 v) {
+        const int q = zrow_q<N, TN1>(e, r);
+        if (q >= 0 && live) out[(size_t)q * d.nkx] = to_d2(cscale(v, sc));
     };
     two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
 }
