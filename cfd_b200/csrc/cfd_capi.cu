@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -214,6 +215,16 @@ int ilog2(int b) {
     }
 
 // shared memory of k_xline2 (elements): B*LX + N + RW*3*nk
+// Launch-shape overrides for tuning runs (unset: the built-in choice).
+//   CFD_XLINE_ROWS   rows per CTA of the two-step x-line kernel (power of two, 2..8)
+//   CFD_ZLINES_LOG2  log2 of the lines per CTA of the two-step z kernels (2..4)
+int env_int(const char* name, int dflt, int lo, int hi) {
+    const char* v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    const int x = std::atoi(v);
+    return (x >= lo && x <= hi) ? x : dflt;
+}
+
 size_t xline2_smem(int n1s, int n2s, int rw, size_t esz) {
     const int N = n1s * n2s;
     const int L1 = n1s * (n2s + 1) + 1, L2 = n2s * (n1s + 1) + 1, LU = N + 1;
@@ -761,7 +772,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
-            int rw = 8;
+            int rw = env_int("CFD_XLINE_ROWS", 8, 2, 8);
             while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
             if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
                 c->RW2 = rw;
@@ -776,7 +787,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal2, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
-            const int lb = mixed ? 4 : 3;
+            const int lb = env_int("CFD_ZLINES_LOG2", mixed ? 4 : 3, 2, 4);
             c->LZ2 = lb;
             c->NTZ2 = (1 << lb) * std::max(n1s, n2s);
             c->SMZ2 = ((size_t)(1 << lb) * ((n1s * (n2s + 1)) | 1) + (size_t)n1s * n2s) * esz;

@@ -245,19 +245,21 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 }
 
 // Pass 2 with the register-resident two-step transform (N = N1*N2, fft_reg.cuh).  A CTA
-// holds RW rows = B = 2*RW lines (line 2r = u + i w, line 2r+1 = v + i 0) and runs with
+// holds RW rows = B = 2*RW lines (line 2r = u + i v, line 2r+1 = w + i 0) and runs with
 // B*max(N1,N2) threads:
 //   step 1  thread (b, n2): reads its stride-N2 subsequence of the Hermitian-extended
 //           spectrum straight from global memory, N1-point DFT, twiddle, exchange
 //   step 2  thread (b, k1): N2-point DFT -> physical x = k1 + N1*k2 in registers; the two
-//           lines of a row sit in adjacent lanes and swap w / v with one shuffle, form the
-//           products, and start the forward transform from registers (N2-point DFT)
+//           lines of a row sit in adjacent lanes and pass one value with a shuffle, form
+//           the products, and start the forward transform from registers (N2-point DFT):
+//             u-plane: line 2r -> uu + i vv, line 2r+1 -> ww + i uw (u from lane 2r)
+//             v-plane: line 2r -> uv + i vw (w from lane 2r+1), line 2r+1 unused
 //   step 2' thread (b, kb): N1-point DFT -> X[kb + N2*ka]; unpack the two real spectra.
 // The retained modes are kx = 0..N/3 (N1 = 2*(Ngal1/3)), a compile-time bound, so which
 // elements of a subsequence are zero, direct or conjugated is resolved at compile time
 // except in the two blocks that straddle a boundary.
 template <typename T2, int N1, int N2>
-__global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (N1 > N2 ? N1 : N2) <= 24 ? 2 : 1) k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
     using R = decltype(T2::x);
     constexpr int N = N1 * N2;
@@ -286,8 +288,8 @@ __global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* _
     if (t < B * N2) {
         const int b = (unsigned)t / N2, n2 = t - b * N2;
         const int rr = b >> 1, which = b & 1;
-        const T2* A = (which == 0 ? H0 : H2) + pbase + (size_t)(z0 + rr) * NK;
-        const T2* C = H1 + pbase + (size_t)(z0 + rr) * NK;
+        const T2* A = (which == 0 ? H0 : H1) + pbase + (size_t)(z0 + rr) * NK;
+        const T2* C = H2 + pbase + (size_t)(z0 + rr) * NK;
         T2 v[N1];
 #pragma unroll
         for (int n1 = 0; n1 < N1; ++n1) {
@@ -325,18 +327,14 @@ __global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* _
 #pragma unroll
         for (int n2 = 0; n2 < N2; ++n2) y[n2] = o[n2];
         rdft<N2, +1>(y);
+        // lane pair (u + i v, w + i 0); each lane passes its real part to the other:
+        // u-plane (a*a, b*b) on the even lane, (a*a, a*o) on the odd lane; v-plane (a*b, b*o)
+        const bool sa = uplane && par, sb = uplane && !par;
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) {
-            // lane pair (u + i w, v + i 0): even lane sends w, odd lane sends v
-            const R send = par ? y[k2].x : y[k2].y;
-            const R recv = __shfl_xor_sync(0xffffffffu, send, 1);
-            if (par == 0) {
-                const R u = y[k2].x, w = y[k2].y, v = recv;
-                y[k2] = uplane ? cx<T2>(u * u, u * w) : cx<T2>(u * v, w * v);
-            } else {
-                const R v = y[k2].x, w = recv;
-                y[k2] = uplane ? cx<T2>(v * v, w * w) : cx<T2>((R)0, (R)0);
-            }
+            const R a = y[k2].x, b = y[k2].y;
+            const R o = __shfl_xor_sync(0xffffffffu, a, 1);
+            y[k2] = cx<T2>(a * (uplane ? a : b), (sa ? a : b) * (sb ? b : o));
         }
         rdft<N2, -1>(y);
 #pragma unroll
@@ -382,8 +380,11 @@ __global__ void k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* _
         const T2* line = ex + (size_t)b * LU;
         const T2 Pk = line[k];
         const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
-        (which == 0 ? H0 : H2)[o] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
-        (which == 0 ? H1 : H3)[o] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
+        // real parts: u-plane uu / ww, v-plane uv; imaginary parts: u-plane vv / uw, v-plane vw
+        T2* da = which == 0 ? H0 : H3;
+        T2* db = which == 0 ? (uplane ? H2 : H1) : H1;
+        da[o] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+        db[o] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
     }
 }
 
