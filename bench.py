@@ -52,14 +52,21 @@ def kernel_bytes(name, setup, mixed):
     nplv = sum(max(0, min(h, g.jv1 - 1) - max(l, g.jv0 + 1) + 1) for l, h in zip(setup.ibv.jlo, setup.ibv.jhi))
     phys = cfg.ngal1 * cfg.ngal2
     rt = 4 if mixed else 8
+    nfp = 2 * nyu + nyv                       # field planes u, w, v
     b = {
-        "k_zinv": (2 * nyu + nyv) * ncol * cs + 3 * nslot * hpl * ct,
+        "k_zinv": nfp * ncol * cs + 3 * nslot * hpl * ct,
+        "k_zinv2s": nfp * ncol * cs + nfp * hpl * ct,
         "k_xline": (3 * nslot + 4 * nyu + 2 * nyv) * hpl * ct,
+        # reads every transformed field plane once (y-neighbours of the interpolation from L2)
+        "k_xline2": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,
         "k_zfwd": (4 * nyu + 2 * nyv) * (hpl + ncol) * ct,
         "k_rhs": ncol * ((2 * nyu + nyv + nyp) * cs + (2 * nyu + nyv) * ct + (4 * nyu + 2 * nyv) * ct
                          + (2 * nyu + nyv) * cs + (2 * nyu + nyv) * ct),
         "k_solve_uvw": ncol * 2 * (2 * nyu + nyv) * cs,
         "k_solve_p": ncol * (2 * nyu + nyv + nyp + 2 * nyp) * cs,
+        # fused pressure solve + correction: u, v, w read twice and written once; p read and
+        # written; psi and the scaled upper diagonal (FP64 real) written and read once
+        "k_solve_p_vcorr": ncol * (3 * nfp * cs + nyp * (4 * cs + 2 * 8)),
         "k_vcorr": ncol * (2 * (2 * nyu + nyv) + nyp) * cs,
     }
     # IB kernels: average over the u-grid (2 batches) and v-grid (1 batch) launches
@@ -73,7 +80,9 @@ def kernel_bytes(name, setup, mixed):
     for k in ("k_ib_zinv", "k_ib_xinv", "k_ib_xfwd", "k_ib_zfwd"):
         if ib:
             b[k] = sum(x[k] for x in ib) / len(ib)
-    return b.get(name)
+    if name in b:
+        return b[name]
+    return b.get(name[:-1]) if name.endswith("2") else None
 
 
 # ------------------------------------------------------------------------------------------

@@ -82,6 +82,7 @@ struct cfd_ctx {
     int npart = 0;
     IBDev ibu, ibv;
     void* Hib = nullptr;
+    void* Hx = nullptr;     // z-transformed u, w, v on their own planes (two-step x-line path)
     void* phys = nullptr;
     // FFT
     FFTDesc fx{}, fz{};
@@ -259,6 +260,8 @@ int set_smem_attrs(cfd_ctx* c) {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_zinv2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
             if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_zinv2s<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
+            if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_zfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
         });
     }
@@ -317,7 +320,17 @@ int nl_transforms(cfd_ctx* c) {
     const int CH = c->CHz;
     const size_t e = sizeof(T2);
     prof_mark(c);
-    if (c->LZ2 >= 0) {
+    if (c->RW2) {
+        // each field transformed once on its own planes; the x-line kernel interpolates in y
+        const int CH2 = 1 << c->LZ2;
+        dim3 gz2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 3);
+        bool ok = true;
+        TWO_SWITCH(d.ngal2, ok, {
+            k_zinv2s<T2, TN1, TN2><<<gz2, c->NTZ2, c->SMZ2, c->stream>>>(d, c->u1, c->u2, c->u3, (T2*)c->Hx,
+                                                                      twz<T2>(c), c->LZ2);
+        });
+        LK("k_zinv2s");
+    } else if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
         dim3 gz2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 3, 2);
         bool ok = true;
@@ -340,7 +353,7 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
         TWO_SWITCH(d.ngal1, ok, {
-            k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2],
+            k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2],
                                                                     (T2*)c->H[3], twx<T2>(c), c->RW2, ilog2(c->RW2));
         });
         LK("k_xline2");
@@ -793,6 +806,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
             c->SMZ2 = ((size_t)(1 << lb) * ((n1s * (n2s + 1)) | 1) + (size_t)n1s * n2s) * esz;
         }
     }
+    if (c->LZ2 < 0) c->RW2 = 0;  // the two-step x-line kernel reads the output of k_zinv2s
     {
         bool ok = true;
         int n1s = 0, n2s = 0;
@@ -829,6 +843,10 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     for (int k = 0; k < 4; ++k) {
         if (mixed) { AL(c->H[k], float2, hsz); AL(c->S[k], float2, (size_t)d.nslot * nc); }
         else { AL(c->H[k], double2, hsz); AL(c->S[k], double2, (size_t)d.nslot * nc); }
+    }
+    if (c->RW2) {
+        const size_t hxs = (size_t)(2 * nyu + nyv) * d.ngal2 * d.nkx;
+        if (mixed) AL(c->Hx, float2, hxs); else AL(c->Hx, double2, hxs);
     }
     AL(c->cs, double, nc * nyu);
     AL(c->cs_v, double, nc * nyv);

@@ -15,6 +15,8 @@
 // and the column kernel k_rhs forms x/z/y derivatives and the RK right-hand side.
 #pragma once
 
+#include <type_traits>
+
 #include "fft_smem.cuh"
 #include "fft_reg.cuh"
 
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // elements of a subsequence are zero, direct or conjugated is resolved at compile time
 // except in the two blocks that straddle a boundary.
 template <typename T2, int N1, int N2>
-__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (N1 > N2 ? N1 : N2) <= 24 ? 2 : 1) k_xline2(Dims d, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (N1 > N2 ? N1 : N2) <= 24 ? 2 : 1) k_xline2(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
     using R = decltype(T2::x);
     constexpr int N = N1 * N2;
@@ -273,7 +275,9 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (N1 > N2 ? N1 : N2) 
     const int B = 2 * RW;
     T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX
     T2* twt = ex + (size_t)B * LX;                   // N1 * N2: twt[b*N2 + a] = w^(a*b), a < N2, b < N1
-    const int slot = blockIdx.y;
+    // u- and v-slots interleaved in y (nyu = nyv + 1), so that the y-neighbour planes read
+    // by the interpolation are still in L2 from the adjacent slots
+    const int slot = (blockIdx.y & 1) ? d.nyu + (blockIdx.y >> 1) : (blockIdx.y >> 1);
     const int z0 = blockIdx.x * RW;
     const bool uplane = slot < d.nyu;
     const int t = threadIdx.x;
@@ -282,33 +286,86 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (N1 > N2 ? N1 : N2) 
         twt[i] = twx[(a * b) % N];
     }
     const size_t pbase = (size_t)slot * d.ngal2 * NK;
+    // y-interpolated sources of this slot, each ca * plane a + cb * plane b of Hx:
+    // u-plane j: u, w direct; v at the centre (ghost centres: the extrapolation of
+    // FOU3D.f90:261-283 folded into the weights).  v-plane j: v direct; u, w at the face.
+    const size_t pls = (size_t)d.ngal2 * NK;
+    const T2* Hu = Hx;
+    const T2* Hw = Hx + (size_t)d.nyu * pls;
+    const T2* Hv = Hx + (size_t)(2 * d.nyu) * pls;
+    const T2 *ua, *ub, *va, *vb, *wa, *wb;
+    R uca = 1, ucb = 0, vca = 1, vcb = 0;
+    if (uplane) {
+        const int sl = slot;
+        ua = ub = Hu + sl * pls;
+        wa = wb = Hw + sl * pls;
+        double ca, cb;
+        int pa;
+        if (sl == 0) {
+            pa = 1; ca = (1.0 - g.gwib) * g.vca[1]; cb = g.gwib + (1.0 - g.gwib) * g.vcb[1];
+        } else if (sl == d.nyu - 1) {
+            pa = sl - 1; ca = g.gwit + (1.0 - g.gwit) * g.vca[sl - 1]; cb = (1.0 - g.gwit) * g.vcb[sl - 1];
+        } else {
+            pa = sl; ca = g.vca[sl]; cb = g.vcb[sl];
+        }
+        va = Hv + pa * pls; vb = va - pls; vca = (R)ca; vcb = (R)cb;
+    } else {
+        const int sl = slot - d.nyu;
+        va = vb = Hv + sl * pls;
+        ua = Hu + (sl + 1) * pls; ub = ua - pls;
+        wa = Hw + (sl + 1) * pls; wb = wa - pls;
+        uca = (R)g.ufa[sl]; ucb = (R)g.ufb[sl];
+    }
     __syncthreads();
 
     // ---- step 1: inverse, thread (b, n2)
     if (t < B * N2) {
         const int b = (unsigned)t / N2, n2 = t - b * N2;
         const int rr = b >> 1, which = b & 1;
-        const T2* A = (which == 0 ? H0 : H1) + pbase + (size_t)(z0 + rr) * NK;
-        const T2* C = H2 + pbase + (size_t)(z0 + rr) * NK;
+        const size_t ro = (size_t)(z0 + rr) * NK;
+        // line 2r: A = u, C = v; line 2r+1: A = w.  u-plane: C interpolated; v-plane: A
+        const T2* A0 = (which == 0 ? ua : wa) + ro;
+        const T2* A1 = (which == 0 ? ub : wb) + ro;
+        const T2* C0 = va + ro;
+        const T2* C1 = vb + ro;
+        const bool hasc = which == 0;
         T2 v[N1];
+        // the uniform branch on the plane type sits outside the element loop, so that the
+        // loads of all elements are straight-line (predicated) and issue back to back
+        auto fill = [&](auto vplane) {
+            constexpr bool VP = decltype(vplane)::value;
+            auto fetch = [&](int k, T2& a, T2& c) {
+                const T2 z = cx<T2>((R)0, (R)0);
+                if (VP) {
+                    const T2 a0 = A0[k], a1 = A1[k];
+                    a = cx<T2>(uca * a0.x + ucb * a1.x, uca * a0.y + ucb * a1.y);
+                    c = hasc ? C0[k] : z;
+                } else {
+                    a = A0[k];
+                    const T2 c0 = hasc ? C0[k] : z, c1 = hasc ? C1[k] : z;
+                    c = cx<T2>(vca * c0.x + vcb * c1.x, vca * c0.y + vcb * c1.y);
+                }
+            };
 #pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) {
-            const int e0 = n1 * N2, e = e0 + n2;
-            const bool lo = (e0 + N2 - 1 <= HX) || (e0 <= HX && e <= HX);
-            const bool hi = (e0 >= N - HX) || (e0 + N2 - 1 >= N - HX && e >= N - HX);
-            T2 val = cx<T2>((R)0, (R)0);
-            if (lo) {
-                T2 a = A[e];
-                T2 c = which == 0 ? C[e] : cx<T2>((R)0, (R)0);
-                if (n1 == 0 && n2 == 0) { a.y = 0; c.y = 0; }
-                val = cx<T2>(a.x - c.y, a.y + c.x);
-            } else if (hi) {
-                const T2 a = A[N - e];
-                const T2 c = which == 0 ? C[N - e] : cx<T2>((R)0, (R)0);
-                val = cx<T2>(a.x + c.y, -a.y + c.x);
+            for (int n1 = 0; n1 < N1; ++n1) {
+                const int e0 = n1 * N2, e = e0 + n2;
+                const bool lo = (e0 + N2 - 1 <= HX) || (e0 <= HX && e <= HX);
+                const bool hi = (e0 >= N - HX) || (e0 + N2 - 1 >= N - HX && e >= N - HX);
+                T2 val = cx<T2>((R)0, (R)0);
+                T2 a, c;
+                if (lo) {  // A_e + i C_e; the rft inverse ignores Im of the kx = 0 entries
+                    fetch(e, a, c);
+                    if (n1 == 0 && n2 == 0) { a.y = 0; c.y = 0; }
+                    val = cx<T2>(a.x - c.y, a.y + c.x);
+                } else if (hi) {  // conj(A_k) + i conj(C_k), k = N - e
+                    fetch(N - e, a, c);
+                    val = cx<T2>(a.x + c.y, -a.y + c.x);
+                }
+                v[n1] = val;
             }
-            v[n1] = val;
-        }
+        };
+        if (uplane) fill(std::false_type{});
+        else fill(std::true_type{});
         rdft<N1, +1>(v);
         T2* o = ex + (size_t)b * L1 + n2;
 #pragma unroll
@@ -530,6 +587,43 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
         };
         two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
     }
+}
+
+// Pass 1 for the x-line kernel that interpolates in y itself: every field is transformed
+// once on its own planes, Hx = [u planes ju0..ju1 | w planes ju0..ju1 | v planes jv0..jv1].
+// Interpolation in y and the z transform are both linear, so interpolating the transformed
+// planes gives the transform of the interpolated planes (FOU3D.f90:261-308).
+// grid: x = line chunk (line = plane * nkx + kx), y = field (u, w, v).
+template <typename T2, int TN1, int TN2>
+__global__ void k_zinv2s(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
+                         const double2* __restrict__ u3, T2* __restrict__ Hx, const T2* __restrict__ twz, int lb) {
+    using R = decltype(T2::x);
+    constexpr int N = TN1 * TN2;
+    const int f = blockIdx.y;
+    const int npl = f == 2 ? d.nyv : d.nyu;
+    const int nlines = npl * d.nkx;
+    const int line0 = blockIdx.x << lb;
+    if (line0 >= nlines) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* ex = twt + N;
+    load_twiddles<T2, TN1, TN2>(twt, twz);
+    const int b = threadIdx.x & ((1 << lb) - 1);
+    const bool live = line0 + b < nlines;
+    const int line = live ? line0 + b : nlines - 1;
+    const int pl = line / d.nkx, i = line - pl * d.nkx;
+    const double2* src = (f == 0 ? u1 : (f == 1 ? u3 : u2)) + (size_t)pl * d.ncol + i;
+    T2* H = Hx + ((size_t)(f == 0 ? 0 : (f == 1 ? d.nyu : 2 * d.nyu)) + pl) * N * d.nkx + i;
+    const int r = threadIdx.x >> lb;
+    __syncthreads();
+    auto load = [&](int e, int) -> T2 {
+        const int q = zrow_q<N, TN2>(e, r);
+        return q >= 0 ? to_t2<T2>(src[(size_t)q * d.nkx]) : cx<T2>((R)0, (R)0);
+    };
+    auto store = [&](int z, int, T2 v) {
+        if (live) H[(size_t)z * d.nkx] = v;
+    };
+    two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
 }
 
 // Pass 3: grid x = line chunk, y = field 0..3, z = group (v-planes carry fields 0, 1 only).
