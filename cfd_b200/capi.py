@@ -38,8 +38,44 @@ class CfdIBList(C.Structure):
                 ("jlo", C.c_int32 * 2), ("jhi", C.c_int32 * 2)]
 
 
+class CfdStatsConfig(C.Structure):
+    _fields_ = [("jband", C.c_int32), ("dnx", C.c_int32), ("dnz", C.c_int32)]
+
+
 def dptr(a):
     return a.ctypes.data_as(_dp)
+
+
+# statistics quantities in the order of cfd_stats_read (stats.f90:1-106)
+STATS_U = ("Um", "U2m", "Wm", "W2m", "UVm", "UWm")
+STATS_V = ("Vm", "V2m", "wxm", "wx2m", "VWm")
+STATS_P = ("Pm", "P2m")
+
+
+def stats_buffers(nyu, nyv, nyp, nbu, nbv, nbp, dnx, dnz):
+    """Host arrays for cfd_stats_read / orc_stats_read."""
+    import numpy as np
+    return (np.zeros((6, nyu)), np.zeros((5, nyv)), np.zeros((2, nyp)),
+            np.zeros((6, nbu, dnz, dnx)), np.zeros((5, nbv, dnz, dnx)), np.zeros((2, nbp, dnz, dnx)))
+
+
+def stats_dict(bufs, istat):
+    """Name the arrays of stats_buffers: plane sums by quantity, conditional sums as <name>C."""
+    su, sv, sp, cu, cv, cp = bufs
+    out = {"istat": istat}
+    for names, a, c in ((STATS_U, su, cu), (STATS_V, sv, cv), (STATS_P, sp, cp)):
+        for q, n in enumerate(names):
+            out[n] = a[q].copy()
+            out[n + "C"] = c[q].copy()
+    return out
+
+
+def stats_band(nyu, nyv, nyp, jband, j0u, j0v, j0p):
+    """Planes of the bottom band (and of the mirrored top band) for a band ending at v plane
+    jband: u planes j0u..jband+1, v planes j0v..jband, p planes j0p..jband."""
+    if jband < j0v:
+        return 0, 0, 0
+    return jband + 1 - j0u + 1, jband - j0v + 1, jband - j0p + 1
 
 
 def make_config(cfg, grid, dt, keep: list) -> CfdConfig:
@@ -101,6 +137,11 @@ SIGNATURES = {
     "cfd_phys_to_four": (C.c_int, [_VP, _VP, C.c_int32]),
     "cfd_rft": (C.c_int, [_VP, _VP, C.c_int32, C.c_int32, C.c_int32]),
     "cfd_cft": (C.c_int, [_VP, _VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "cfd_stats_configure": (C.c_int, [_VP, C.POINTER(CfdStatsConfig)]),
+    "cfd_stats_accumulate": (C.c_int, [_VP]),
+    "cfd_stats_reset": (C.c_int, [_VP]),
+    "cfd_stats_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, C.POINTER(C.c_int32)]),
+    "cfd_cfl": (C.c_int, [_VP, _dp, _VP]),
     "cfd_launch_count": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "cfd_profile": (C.c_int, [_VP, C.c_int32]),
     "cfd_profile_read": (C.c_int, [_VP, C.c_char_p, C.c_int32]),

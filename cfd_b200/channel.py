@@ -169,6 +169,38 @@ class Channel:
                   "scalars")
         return {"mpgx": a.value, "qx": b.value, "dgx": c.value}
 
+    # -- statistics and CFL (stats.f90, dtc_calc) ------------------------------------------
+    def stats_configure(self, jband: int, dnx: int, dnz: int):
+        """Configure and zero the FP64 statistics accumulators (bottom band up to v plane
+        jband, tiles of dnx x dnz points; jband below the first v plane: plane sums only)."""
+        sc = capi.CfdStatsConfig(int(jband), int(dnx), int(dnz))
+        self._chk(self.lib.cfd_stats_configure(self.ctx, C.byref(sc)), "stats_configure")
+        g = self.setup.grid
+        self._stats_shape = capi.stats_band(g.nyu, g.nyv, g.nyp, int(jband), g.ju0, g.jv0, g.jp0) + \
+            ((int(dnx), int(dnz)) if jband >= g.jv0 else (0, 0))
+
+    def stats_accumulate(self):
+        self._chk(self.lib.cfd_stats_accumulate(self.ctx), "stats_accumulate")
+
+    def stats_reset(self):
+        self._chk(self.lib.cfd_stats_reset(self.ctx), "stats_reset")
+
+    def stats_read(self) -> dict:
+        g = self.setup.grid
+        nbu, nbv, nbp, dnx, dnz = self._stats_shape
+        bufs = capi.stats_buffers(g.nyu, g.nyv, g.nyp, nbu, nbv, nbp, dnx, dnz)
+        ist = C.c_int32()
+        self._chk(self.lib.cfd_stats_read(self.ctx, *[b.ctypes.data for b in bufs], C.byref(ist)),
+                  "stats_read")
+        return capi.stats_dict(bufs, ist.value)
+
+    def cfl(self):
+        """(dtc, [u term, w term, v term]) of dtc_calc on the current state."""
+        dtc = C.c_double()
+        t = np.zeros(3)
+        self._chk(self.lib.cfd_cfl(self.ctx, C.byref(dtc), t.ctypes.data), "cfl")
+        return dtc.value, t
+
     def divergence_max(self) -> float:
         e = C.c_double()
         self._chk(self.lib.cfd_divergence_max(self.ctx, C.byref(e)), "divergence_max")

@@ -18,6 +18,7 @@
 
 #include "../../include/cfd_b200.h"
 #include "channel_kernels.cuh"
+#include "stats_kernels.cuh"
 
 using namespace cfd;
 
@@ -108,6 +109,22 @@ struct cfd_ctx {
     std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> prof;
     std::string err;
     std::vector<void*> allocs;
+    // statistics pass (stats.f90) and CFL maxima (dtc_calc)
+    struct {
+        bool on = false;          // accumulators configured
+        int jband = 0, dnx = 0, dnz = 0, nbu = 0, nbv = 0, nbp = 0;
+        int istat = 0;
+        int cp = 16;              // planes per field in one chunk
+        double* su = nullptr;     // [6][nyu]
+        double* sv = nullptr;     // [5][nyv]
+        double* sp = nullptr;     // [2][nyp]
+        double* cu = nullptr;     // [2 bottom/top][6][nbu][dnz][dnx]
+        double* cv = nullptr;     // [2][5][nbv][dnz][dnx]
+        double* cp_ = nullptr;    // [2][2][nbp][dnz][dnx]
+        double* planes = nullptr; // [3][cp] physical planes
+        double* mx = nullptr;     // [3][nyu]: |u|, |w| per u plane, |v| dthdyv per v plane
+        cfd::PlaneSrc* src = nullptr;  // [3*cp]
+    } st;
 };
 
 namespace {
@@ -916,6 +933,119 @@ int strided_rft(cfd_ctx* c, double* dptr, int n, int isa, int m, long long bstri
     return CFD_OK;
 }
 
+void dfree(cfd_ctx* c, void* p) {
+    if (!p) return;
+    for (auto it = c->allocs.begin(); it != c->allocs.end(); ++it)
+        if (*it == p) { c->allocs.erase(it); break; }
+    cudaFree(p);
+}
+
+// Plane scratch and maxima of the statistics pass (also used by the CFL query alone).
+int stats_scratch(cfd_ctx* c) {
+    if (c->st.planes) return CFD_OK;
+    const Dims& d = c->d;
+    AL(c->st.planes, double, (size_t)3 * c->st.cp * (d.ngal1 + 2) * d.ngal2);
+    AL(c->st.mx, double, (size_t)3 * d.nyu);
+    AL(c->st.src, PlaneSrc, (size_t)3 * c->st.cp);
+    return CFD_OK;
+}
+
+// One pass over the u, v and p planes in chunks of cp planes per field: build the planes
+// of the chunk from the spectral state, transform them to physical space (FP64), reduce.
+// acc = false computes only the CFL maxima (u, w on u planes, v on v planes).
+int stats_pass(cfd_ctx* c, bool acc) {
+    const Dims& d = c->d;
+    const Geo& g = c->g;
+    auto& st = c->st;
+    const size_t nc = d.ncol;
+    const long long ps = (long long)(d.ngal1 + 2) * d.ngal2;
+    const int rowc = (d.ngal1 + 2) / 2;
+    std::vector<PlaneSrc> hs(3 * st.cp);
+    // host copies of the y weights (small, read once per pass)
+    std::vector<double> hvca(d.nyu), hvcb(d.nyu), ufa(d.nyv), ufb(d.nyv), dthv(d.nyv);
+    CK(cudaMemcpy(hvca.data(), g.vca, sizeof(double) * d.nyu, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(hvcb.data(), g.vcb, sizeof(double) * d.nyu, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ufa.data(), g.ufa, sizeof(double) * d.nyv, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ufb.data(), g.ufb, sizeof(double) * d.nyv, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dthv.data(), g.dthdyv, sizeof(double) * d.nyv, cudaMemcpyDeviceToHost));
+    for (int kind = 0; kind < 3; ++kind) {
+        const int nyg = kind == 0 ? d.nyu : (kind == 1 ? d.nyv : d.nyp);
+        const int nf = kind == 2 ? 1 : 3;
+        if (!acc && kind == 2) break;
+        for (int j0 = 0; j0 < nyg; j0 += st.cp) {
+            const int nch = std::min(st.cp, nyg - j0);
+            for (int pl = 0; pl < nch; ++pl) {
+                const int jr = j0 + pl;
+                PlaneSrc* f = &hs[pl];
+                PlaneSrc* f1 = &hs[nch + pl];
+                PlaneSrc* f2 = &hs[2 * nch + pl];
+                *f = *f1 = *f2 = PlaneSrc{nullptr, nullptr, nullptr, 1.0, 0.0, 0.0};
+                if (kind == 0) {  // u, w, v interpolated to the centre (interp_v, FOU3D.f90:285-308)
+                    f->a = c->u1 + (size_t)jr * nc;
+                    f1->a = c->u3 + (size_t)jr * nc;
+                    if (jr == 0) {
+                        f2->a = c->u2 + nc; f2->b = c->u2;
+                        f2->ca = (1.0 - g.gwib) * hvca[1]; f2->cb = g.gwib + (1.0 - g.gwib) * hvcb[1];
+                    } else if (jr == d.nyu - 1) {
+                        f2->a = c->u2 + (size_t)(jr - 1) * nc; f2->b = c->u2 + (size_t)(jr - 2) * nc;
+                        f2->ca = g.gwit + (1.0 - g.gwit) * hvca[jr - 1]; f2->cb = (1.0 - g.gwit) * hvcb[jr - 1];
+                    } else {
+                        f2->a = c->u2 + (size_t)jr * nc; f2->b = c->u2 + (size_t)(jr - 1) * nc;
+                        f2->ca = hvca[jr]; f2->cb = hvcb[jr];
+                    }
+                } else if (kind == 1) {  // v, w at the face (interp_u), omega_x = dw/dy - dv/dz
+                    f->a = c->u2 + (size_t)jr * nc;
+                    f1->a = c->u3 + (size_t)(jr + 1) * nc; f1->b = c->u3 + (size_t)jr * nc;
+                    f1->ca = ufa[jr]; f1->cb = ufb[jr];
+                    f2->a = c->u3 + (size_t)(jr + 1) * nc; f2->b = c->u3 + (size_t)jr * nc;
+                    f2->ca = dthv[jr]; f2->cb = -dthv[jr];
+                    f2->c = c->u2 + (size_t)jr * nc; f2->cc = -1.0;
+                } else {
+                    f->a = c->p + (size_t)jr * nc;
+                }
+            }
+            CK(cudaMemcpyAsync(st.src, hs.data(), sizeof(PlaneSrc) * nf * nch, cudaMemcpyHostToDevice, c->stream));
+            prof_mark(c);
+            dim3 gb((rowc * d.ngal2 + 255) / 256, nf * nch);
+            k_st_build<<<gb, 256, 0, c->stream>>>(d, g, st.src, st.planes);
+            LK("k_st_build");
+            // four_to_phys (the oddball row Ngal2/2 zeroed by four_to_phys_u lies inside the
+            // dealiasing gap, which the build leaves zero)
+            int s = strided_cft(c, st.planes, d.ngal2, d.ngal1 + 2, 2, d.nkx, ps, nf * nch, +1);
+            if (s) return s;
+            s = strided_rft(c, st.planes, d.ngal1, d.ngal1 + 2, d.ngal2, ps, nf * nch, +1);
+            if (s) return s;
+            prof_mark(c);
+            if (kind == 0) {
+                k_st_sums<0><<<nch, 256, 0, c->stream>>>(d, g, st.planes, nch, j0, acc ? st.su : nullptr, d.nyu, st.mx);
+            } else if (kind == 1) {
+                k_st_sums<1><<<nch, 256, 0, c->stream>>>(d, g, st.planes, nch, j0, acc ? st.sv : nullptr, d.nyv,
+                                                        st.mx + 2 * d.nyu);
+            } else {
+                k_st_sums<2><<<nch, 256, 0, c->stream>>>(d, g, st.planes, nch, j0, st.sp, d.nyp, nullptr);
+            }
+            LK("k_st_sums");
+            if (acc && st.dnx > 0) {
+                const int nb = kind == 0 ? st.nbu : (kind == 1 ? st.nbv : st.nbp);
+                const size_t half = (size_t)(kind == 0 ? 6 : (kind == 1 ? 5 : 2)) * nb * st.dnx * st.dnz;
+                double* cb = kind == 0 ? st.cu : (kind == 1 ? st.cv : st.cp_);
+                dim3 gc((st.dnx * st.dnz + 255) / 256, nch);
+                prof_mark(c);
+                if (kind == 0)
+                    k_st_cond<0><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, cb, cb + half);
+                else if (kind == 1)
+                    k_st_cond<1><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, cb, cb + half);
+                else
+                    k_st_cond<2><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, cb, cb + half);
+                LK("k_st_cond");
+            }
+            // the host array hs is reused by the next chunk: wait for the copy
+            CK(cudaStreamSynchronize(c->stream));
+        }
+    }
+    return CFD_OK;
+}
+
 }  // namespace
 
 // =======================================================================================
@@ -1149,6 +1279,109 @@ int cfd_divergence_max(cfd_ctx* c, double* errmax) {
     }
     *errmax = bad ? NAN : m;
     if (bad) return fail(c, CFD_ERR_NONFINITE, "non-finite divergence");
+    return CFD_OK;
+}
+
+int cfd_stats_configure(cfd_ctx* c, const cfd_stats_config* sc) {
+    if (!c || !sc) return fail(c, CFD_ERR_ARG, "bad arguments");
+    const Dims& d = c->d;
+    auto& st = c->st;
+    const bool cond = sc->jband >= d.jv0;
+    if (cond) {
+        if (sc->dnx <= 0 || sc->dnz <= 0 || d.ngal1 % sc->dnx || d.ngal2 % sc->dnz)
+            return fail(c, CFD_ERR_ARG, "tile %d x %d must divide Ngal1 x Ngal2", sc->dnx, sc->dnz);
+        if (sc->jband + 1 > d.ju1) return fail(c, CFD_ERR_ARG, "jband %d above the channel", sc->jband);
+    }
+    for (double* p : {st.su, st.sv, st.sp, st.cu, st.cv, st.cp_}) dfree(c, p);
+    st.su = st.sv = st.sp = st.cu = st.cv = st.cp_ = nullptr;
+    int s = stats_scratch(c);
+    if (s) return s;
+    st.jband = sc->jband;
+    st.dnx = cond ? sc->dnx : 0;
+    st.dnz = cond ? sc->dnz : 0;
+    // bottom band: u planes -dsty..jband+1, v planes -dsty..jband, p planes -dsty+1..jband
+    st.nbu = cond ? sc->jband + 1 - d.ju0 + 1 : 0;
+    st.nbv = cond ? sc->jband - d.jv0 + 1 : 0;
+    st.nbp = cond ? sc->jband - d.jp0 + 1 : 0;
+    AL(st.su, double, (size_t)6 * d.nyu);
+    AL(st.sv, double, (size_t)5 * d.nyv);
+    AL(st.sp, double, (size_t)2 * d.nyp);
+    const size_t tsz = (size_t)st.dnx * st.dnz;
+    AL(st.cu, double, 2 * 6 * st.nbu * tsz);
+    AL(st.cv, double, 2 * 5 * st.nbv * tsz);
+    AL(st.cp_, double, 2 * 2 * st.nbp * tsz);
+    st.on = true;
+    return cfd_stats_reset(c);
+}
+
+int cfd_stats_reset(cfd_ctx* c) {
+    if (!c) return CFD_ERR_ARG;
+    const Dims& d = c->d;
+    auto& st = c->st;
+    if (!st.on) return fail(c, CFD_ERR_STATE, "statistics not configured");
+    const size_t tsz = (size_t)st.dnx * st.dnz;
+    CK(cudaMemsetAsync(st.su, 0, sizeof(double) * 6 * d.nyu, c->stream));
+    CK(cudaMemsetAsync(st.sv, 0, sizeof(double) * 5 * d.nyv, c->stream));
+    CK(cudaMemsetAsync(st.sp, 0, sizeof(double) * 2 * d.nyp, c->stream));
+    if (tsz) {
+        CK(cudaMemsetAsync(st.cu, 0, sizeof(double) * 2 * 6 * st.nbu * tsz, c->stream));
+        CK(cudaMemsetAsync(st.cv, 0, sizeof(double) * 2 * 5 * st.nbv * tsz, c->stream));
+        CK(cudaMemsetAsync(st.cp_, 0, sizeof(double) * 2 * 2 * st.nbp * tsz, c->stream));
+    }
+    st.istat = 0;
+    return CFD_OK;
+}
+
+int cfd_stats_accumulate(cfd_ctx* c) {
+    if (!c) return CFD_ERR_ARG;
+    if (!c->st.on) return fail(c, CFD_ERR_STATE, "statistics not configured");
+    int s = stats_pass(c, true);
+    if (s) return s;
+    c->st.istat += 1;
+    return CFD_OK;
+}
+
+int cfd_stats_read(cfd_ctx* c, double* u_sums, double* v_sums, double* p_sums, double* cu, double* cv, double* cp,
+                   int32_t* istat) {
+    if (!c) return CFD_ERR_ARG;
+    const Dims& d = c->d;
+    auto& st = c->st;
+    if (!st.on) return fail(c, CFD_ERR_STATE, "statistics not configured");
+    CK(cudaStreamSynchronize(c->stream));
+    if (u_sums) CK(cudaMemcpy(u_sums, st.su, sizeof(double) * 6 * d.nyu, cudaMemcpyDeviceToHost));
+    if (v_sums) CK(cudaMemcpy(v_sums, st.sv, sizeof(double) * 5 * d.nyv, cudaMemcpyDeviceToHost));
+    if (p_sums) CK(cudaMemcpy(p_sums, st.sp, sizeof(double) * 2 * d.nyp, cudaMemcpyDeviceToHost));
+    const size_t tsz = (size_t)st.dnx * st.dnz;
+    // bottom band plus mirrored top band (xC + buffC of recvXC, stats.f90:491-509)
+    auto combine = [&](double* out, const double* dev, size_t n) -> int {
+        if (!out || !n) return CFD_OK;
+        std::vector<double> h(2 * n);
+        CK(cudaMemcpy(h.data(), dev, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) out[i] = h[i] + h[n + i];
+        return CFD_OK;
+    };
+    int s = combine(cu, st.cu, (size_t)6 * st.nbu * tsz);
+    if (!s) s = combine(cv, st.cv, (size_t)5 * st.nbv * tsz);
+    if (!s) s = combine(cp, st.cp_, (size_t)2 * st.nbp * tsz);
+    if (s) return s;
+    if (istat) *istat = st.istat;
+    return CFD_OK;
+}
+
+int cfd_cfl(cfd_ctx* c, double* dtc, double* terms) {
+    if (!c || !dtc) return fail(c, CFD_ERR_ARG, "bad arguments");
+    const Dims& d = c->d;
+    int s = stats_scratch(c);
+    if (!s) s = stats_pass(c, false);
+    if (s) return s;
+    std::vector<double> h((size_t)3 * d.nyu);
+    CK(cudaMemcpy(h.data(), c->st.mx, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+    double um = 0.0, wm = 0.0, vm = 1e-6;
+    for (int j = 0; j < d.nyu; ++j) { um = std::max(um, h[j]); wm = std::max(wm, h[d.nyu + j]); }
+    for (int j = 1; j < d.nyv - 1; ++j) vm = std::max(vm, h[2 * d.nyu + j]);
+    const double t0 = 1.0 / (c->alp * (d.n1 / 2) * um), t1 = 1.0 / (c->bet * (d.n2 / 2) * wm), t2 = 1.0 / vm;
+    if (terms) { terms[0] = t0; terms[1] = t1; terms[2] = t2; }
+    *dtc = std::min(t0, t1);
     return CFD_OK;
 }
 

@@ -191,6 +191,55 @@ int cfd_phys_to_four(cfd_ctx *ctx, double *planes_dev, int32_t nplanes);
 int cfd_rft(cfd_ctx *ctx, double *c_dev, int32_t isa, int32_t m, int32_t iopt);
 int cfd_cft(cfd_ctx *ctx, double *c_dev, int32_t ise, int32_t isa, int32_t m, int32_t iopt);
 
+/* ---- statistics and CFL ------------------------------------------------------------- */
+
+/* Statistics accumulation of stats.f90:1-106, called by the reference from nonlinear at
+ * kRK = 1 every nstat steps (FOU3D.f90:58-62, 187-217), on the current state.  All sums
+ * are FP64 on the device whatever the context precision; the physical fields come from
+ * FP64 transforms of the FP64 state.
+ *   plane sums over the Ngal1 x Ngal2 points of each plane, every plane of its grid:
+ *     u planes (j = -dsty..ny+dsty):   Um U2m Wm W2m UVm UWm   (UV: u * v interpolated)
+ *     v planes (j = -dsty..ny+dsty-1): Vm V2m wxm wx2m VWm      (VW: v * w interpolated;
+ *       wx = dw/dy - dv/dz at the faces, FOU3D.f90:187-207, summed over the first N1 x N2
+ *       points of the plane only, as stats.f90:53-60 does)
+ *     p planes (j = -dsty+1..ny+dsty-1): Pm P2m
+ *   conditional (tile-folded) sums, conddown1/2 and condup1/2 (stats.f90:110-253): each
+ *     plane of the bottom band (index j1 counted from the first plane of its grid) and of
+ *     the top band (j1 counted down from the last plane, v and its products sign-flipped)
+ *     is folded onto one dnx x dnz tile, ntilex = Ngal1/dnx by ntilez = Ngal2/dnz copies.
+ *     The bottom band ends at the v plane jband (the reference's N(3,1)); it holds
+ *     jband+dsty+2 u planes, jband+dsty+1 v planes and jband+dsty p planes.
+ */
+typedef struct cfd_stats_config {
+    int32_t jband;      /* last v plane of the bottom band; < -dsty: no conditional sums */
+    int32_t dnx, dnz;   /* tile size in points; must divide Ngal1, Ngal2 */
+} cfd_stats_config;
+
+/* Sets the band and tile, allocates the accumulators (and the plane scratch) and zeroes
+ * them (the reference's allocation in start.f90:2705-2793). */
+int cfd_stats_configure(cfd_ctx *ctx, const cfd_stats_config *sc);
+/* stats() on the current u, v, w, p: istat += 1 and every sum above updated. */
+int cfd_stats_accumulate(cfd_ctx *ctx);
+/* Zeroes every sum and istat (write_stats' reset, stats.f90:411-441). */
+int cfd_stats_reset(cfd_ctx *ctx);
+/* Copies the sums to host arrays (any pointer may be NULL to skip it):
+ *   u_sums [6][nyu]  Um U2m Wm W2m UVm UWm        (nyu = ny+2*dsty+1)
+ *   v_sums [5][nyv]  Vm V2m wxm wx2m VWm          (nyv = ny+2*dsty)
+ *   p_sums [2][nyp]  Pm P2m                       (nyp = ny+2*dsty-1)
+ *   cu [6][nbu][dnz][dnx], cv [5][nbv][dnz][dnx], cp [2][nbp][dnz][dnx]: conditional sums
+ *     in the same quantity order, bottom band plus mirrored top band as write_stats
+ *     stores them (recvXC, stats.f90:473-512); dnx fastest (the Fortran YmC(i,k,j1)).
+ *   istat: number of accumulated calls. */
+int cfd_stats_read(cfd_ctx *ctx, double *u_sums, double *v_sums, double *p_sums,
+                   double *cu, double *cv, double *cp, int32_t *istat);
+/* dtc_calc (FOU3D.f90:516-544) on the current state.  terms (may be NULL) receives
+ *   [0] 1/(alp*(N1/2)*max|u|), [1] 1/(bet*(N2/2)*max|w|), [2] 1/max(1e-6, max|v|*dthdyv)
+ * with the maxima over the physical u, w planes (all) and v planes (walls excluded).
+ * *dtc is the reference's result min(terms[0], terms[1]): its v term divides by
+ * dthetavi, a module variable that nothing assigns (declaration.f90:72; only ddthetavi is
+ * set, start.f90:684), so that term is 1/0 = +Inf and never limits the step. */
+int cfd_cfl(cfd_ctx *ctx, double *dtc, double *terms);
+
 /* ---- allocation-free solve ----------------------------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc/cudaFree: a

@@ -193,6 +193,14 @@ struct Oracle {
     RFFTPlan px;
     FFTPlan pz;
     int quirk_lastplane = 0;
+    // statistics accumulators (stats.f90:1-253, allocated as start.f90:2705-2793):
+    // plane sums [q][j - j0]; conditional sums of the bottom (b) and top (t) band
+    // [q][j1][k][i] (Fortran YmC(i,k,j1))
+    struct {
+        bool on = false;
+        int jband = 0, dnx = 0, dnz = 0, nbu = 0, nbv = 0, nbp = 0, istat = 0;
+        std::vector<double> su, sv, sp, cub, cut, cvb, cvt, cpb, cpt;
+    } st;
 
     // RK coefficients, Le & Moin (start.f90:395-409)
     static constexpr double aRK[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
@@ -719,6 +727,216 @@ static void rk_substep(Oracle& o, int krk) {
 // ------------------------------------------------------------------------------------
 // extern "C" API (ctypes)
 // ------------------------------------------------------------------------------------
+// ------------------------------------------------------------------------------------
+// stats (stats.f90:1-106) with conddown1/2, condup1/2 (:110-253) and the omega_x planes of
+// nonlinear (FOU3D.f90:187-207); dtc_calc (FOU3D.f90:516-544).  Physical planes come from
+// the same plane transforms as ops_in_planes: u, w, v_itp on u planes, v, w_itp, wx on v
+// planes (four_to_phys_u for velocities, four_to_phys_du for wx and p).
+// ------------------------------------------------------------------------------------
+static void stats_configure(Oracle& o, int jband, int dnx, int dnz) {
+    auto& st = o.st;
+    const bool cond = jband >= o.jv0;
+    st.jband = jband;
+    st.dnx = cond ? dnx : 0;
+    st.dnz = cond ? dnz : 0;
+    st.nbu = cond ? jband + 1 - o.ju0 + 1 : 0;
+    st.nbv = cond ? jband - o.jv0 + 1 : 0;
+    st.nbp = cond ? jband - o.jp0 + 1 : 0;
+    const size_t t = (size_t)st.dnx * st.dnz;
+    st.su.assign((size_t)6 * o.nyu, 0.0);
+    st.sv.assign((size_t)5 * o.nyv, 0.0);
+    st.sp.assign((size_t)2 * o.nyp, 0.0);
+    st.cub.assign(6 * st.nbu * t, 0.0); st.cut.assign(6 * st.nbu * t, 0.0);
+    st.cvb.assign(5 * st.nbv * t, 0.0); st.cvt.assign(5 * st.nbv * t, 0.0);
+    st.cpb.assign(2 * st.nbp * t, 0.0); st.cpt.assign(2 * st.nbp * t, 0.0);
+    st.istat = 0;
+    st.on = true;
+}
+
+// conddown1/condup1 (YmC, Y2mC from x) and conddown2/condup2 (YmC from x1*x2) of one plane
+static void cond1(const Oracle& o, double* Ym, double* Y2m, const double* x, double sign) {
+    const int ntx = o.ngal1 / o.st.dnx, ntz = o.ngal2 / o.st.dnz;
+    for (int k = 0; k < o.st.dnz; ++k)
+        for (int i = 0; i < o.st.dnx; ++i) {
+            double& a = Ym[k * o.st.dnx + i];
+            double& b = Y2m[k * o.st.dnx + i];
+            for (int iz = 0; iz < ntz; ++iz)
+                for (int ix = 0; ix < ntx; ++ix) {
+                    const double v = x[(size_t)(k + o.st.dnz * iz) * o.rowlen + i + o.st.dnx * ix];
+                    a = a + v * sign;
+                    b = b + v * v;
+                }
+        }
+}
+static void cond2(const Oracle& o, double* Ym, const double* x1, const double* x2, double s1, double s2) {
+    const int ntx = o.ngal1 / o.st.dnx, ntz = o.ngal2 / o.st.dnz;
+    for (int k = 0; k < o.st.dnz; ++k)
+        for (int i = 0; i < o.st.dnx; ++i) {
+            double& a = Ym[k * o.st.dnx + i];
+            for (int iz = 0; iz < ntz; ++iz)
+                for (int ix = 0; ix < ntx; ++ix) {
+                    const size_t e = (size_t)(k + o.st.dnz * iz) * o.rowlen + i + o.st.dnx * ix;
+                    a = a + x1[e] * s1 * x2[e] * s2;
+                }
+        }
+}
+
+static void stats_accumulate(Oracle& o) {
+    auto& st = o.st;
+    interp(o);
+    const size_t psz = (size_t)o.rowlen * o.ngal2;
+    const size_t tsz = (size_t)st.dnx * st.dnz;
+    const bool cond = tsz > 0;
+#pragma omp parallel
+    {
+        PlaneWork w;
+        w.init(o);
+        std::vector<double> a(psz), b(psz), c(psz);
+#pragma omp for schedule(dynamic)
+        for (int j = o.ju0; j <= o.ju1; ++j) {  // u1PL, u3PL, u2PL_itp
+            const int jr = j - o.ju0;
+            gather_plane(o, o.u1, o.nyu, o.ju0, j, a.data());
+            gather_plane(o, o.u3, o.nyu, o.ju0, j, b.data());
+            gather_plane(o, o.u2i, o.nyu, o.ju0, j, c.data());
+            four_to_phys(o, a.data(), true, w);
+            four_to_phys(o, b.data(), true, w);
+            four_to_phys(o, c.data(), true, w);
+            double s0 = st.su[0 * o.nyu + jr], s1 = st.su[1 * o.nyu + jr], s2 = st.su[2 * o.nyu + jr];
+            double s3 = st.su[3 * o.nyu + jr], s4 = st.su[4 * o.nyu + jr], s5 = st.su[5 * o.nyu + jr];
+            for (int k = 0; k < o.ngal2; ++k)
+                for (int i = 0; i < o.ngal1; ++i) {
+                    const size_t e = (size_t)k * o.rowlen + i;
+                    s0 = s0 + a[e]; s1 = s1 + a[e] * a[e];
+                    s2 = s2 + b[e]; s3 = s3 + b[e] * b[e];
+                    s4 = s4 + a[e] * c[e]; s5 = s5 + a[e] * b[e];
+                }
+            st.su[0 * o.nyu + jr] = s0; st.su[1 * o.nyu + jr] = s1; st.su[2 * o.nyu + jr] = s2;
+            st.su[3 * o.nyu + jr] = s3; st.su[4 * o.nyu + jr] = s4; st.su[5 * o.nyu + jr] = s5;
+            if (!cond) continue;
+            for (int side = 0; side < 2; ++side) {
+                const int j1 = side == 0 ? jr : o.ju1 - j;
+                if (j1 >= st.nbu) continue;
+                double* C = (side == 0 ? st.cub : st.cut).data();
+                const size_t qs = (size_t)st.nbu * tsz;
+                double* at = C + (size_t)j1 * tsz;
+                const double sv = side == 0 ? 1.0 : -1.0;
+                cond1(o, at + 0 * qs, at + 1 * qs, a.data(), 1.0);
+                cond1(o, at + 2 * qs, at + 3 * qs, b.data(), 1.0);
+                cond2(o, at + 4 * qs, a.data(), c.data(), 1.0, sv);
+                cond2(o, at + 5 * qs, a.data(), b.data(), 1.0, 1.0);
+            }
+        }
+#pragma omp for schedule(dynamic)
+        for (int j = o.jv0; j <= o.jv1; ++j) {  // u2PL, u3PL_itp, wx
+            const int jr = j - o.jv0;
+            gather_plane(o, o.u2, o.nyv, o.jv0, j, a.data());
+            gather_plane(o, o.u3i, o.nyv, o.jv0, j, b.data());
+            // wx = -der_z(v) + der_yv_h_wx(w): dw/dy - dv/dz at the face (FOU3D.f90:187-204)
+            std::memset(c.data(), 0, sizeof(double) * psz);
+            for (int col = 0; col < o.ncol; ++col) {
+                const int i = o.col_i(col), q = o.col_q(col);
+                cplx dz = (q == o.n2 / 2) ? cplx(0.0, 0.0) : cplx(0.0, o.kz[q]) * o.V(o.u2, col, j);
+                cplx dy = (o.U(o.u3, col, j + 1) - o.U(o.u3, col, j)) * o.DTHV(j);
+                cplx v = -dz + dy;
+                const size_t e = (size_t)o.row_of(q) * o.rowlen + 2 * i;
+                c[e] = v.real();
+                c[e + 1] = v.imag();
+            }
+            four_to_phys(o, a.data(), true, w);
+            four_to_phys(o, b.data(), true, w);
+            four_to_phys(o, c.data(), false, w);
+            double s0 = st.sv[0 * o.nyv + jr], s1 = st.sv[1 * o.nyv + jr], s2 = st.sv[2 * o.nyv + jr];
+            double s3 = st.sv[3 * o.nyv + jr], s4 = st.sv[4 * o.nyv + jr];
+            for (int k = 0; k < o.ngal2; ++k)
+                for (int i = 0; i < o.ngal1; ++i) {
+                    const size_t e = (size_t)k * o.rowlen + i;
+                    s0 = s0 + a[e]; s1 = s1 + a[e] * a[e];
+                    s4 = s4 + a[e] * b[e];
+                }
+            // wx over the first N1 x N2 points only (stats.f90:53-60)
+            for (int k = 0; k < o.n2; ++k)
+                for (int i = 0; i < o.n1; ++i) {
+                    const size_t e = (size_t)k * o.rowlen + i;
+                    s2 = s2 + c[e]; s3 = s3 + c[e] * c[e];
+                }
+            st.sv[0 * o.nyv + jr] = s0; st.sv[1 * o.nyv + jr] = s1; st.sv[2 * o.nyv + jr] = s2;
+            st.sv[3 * o.nyv + jr] = s3; st.sv[4 * o.nyv + jr] = s4;
+            if (!cond) continue;
+            for (int side = 0; side < 2; ++side) {
+                const int j1 = side == 0 ? jr : o.jv1 - j;
+                if (j1 >= st.nbv) continue;
+                double* C = (side == 0 ? st.cvb : st.cvt).data();
+                const size_t qs = (size_t)st.nbv * tsz;
+                double* at = C + (size_t)j1 * tsz;
+                const double sv = side == 0 ? 1.0 : -1.0;
+                cond1(o, at + 0 * qs, at + 1 * qs, a.data(), sv);
+                cond1(o, at + 2 * qs, at + 3 * qs, c.data(), 1.0);
+                cond2(o, at + 4 * qs, a.data(), b.data(), sv, 1.0);
+            }
+        }
+#pragma omp for schedule(dynamic)
+        for (int j = o.jp0; j <= o.jp1; ++j) {  // ppPL
+            const int jr = j - o.jp0;
+            gather_plane(o, o.p, o.nyp, o.jp0, j, a.data());
+            four_to_phys(o, a.data(), false, w);
+            double s0 = st.sp[jr], s1 = st.sp[o.nyp + jr];
+            for (int k = 0; k < o.ngal2; ++k)
+                for (int i = 0; i < o.ngal1; ++i) {
+                    const size_t e = (size_t)k * o.rowlen + i;
+                    s0 = s0 + a[e]; s1 = s1 + a[e] * a[e];
+                }
+            st.sp[jr] = s0; st.sp[o.nyp + jr] = s1;
+            if (!cond) continue;
+            for (int side = 0; side < 2; ++side) {
+                const int j1 = side == 0 ? jr : o.jp1 - j;
+                if (j1 >= st.nbp) continue;
+                double* C = (side == 0 ? st.cpb : st.cpt).data();
+                const size_t qs = (size_t)st.nbp * tsz;
+                cond1(o, C + (size_t)j1 * tsz, C + qs + (size_t)j1 * tsz, a.data(), 1.0);
+            }
+        }
+    }
+    st.istat += 1;
+}
+
+static void dtc_calc(Oracle& o, double* terms) {
+    double um = 0.0, wm = 0.0, vm = 1e-6;
+#pragma omp parallel
+    {
+        PlaneWork w;
+        w.init(o);
+        const size_t psz = (size_t)o.rowlen * o.ngal2;
+        std::vector<double> a(psz);
+        double lu = 0.0, lw = 0.0, lv = 0.0;
+#pragma omp for schedule(dynamic) nowait
+        for (int j = o.ju0; j <= o.ju1; ++j) {
+            gather_plane(o, o.u1, o.nyu, o.ju0, j, a.data());
+            four_to_phys(o, a.data(), true, w);
+            for (size_t e = 0; e < psz; ++e) lu = std::max(lu, std::fabs(a[e]));
+            gather_plane(o, o.u3, o.nyu, o.ju0, j, a.data());
+            four_to_phys(o, a.data(), true, w);
+            for (size_t e = 0; e < psz; ++e) lw = std::max(lw, std::fabs(a[e]));
+        }
+#pragma omp for schedule(dynamic) nowait
+        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) {
+            gather_plane(o, o.u2, o.nyv, o.jv0, j, a.data());
+            four_to_phys(o, a.data(), true, w);
+            for (int k = 0; k < o.ngal2; ++k)
+                for (int i = 0; i < o.ngal1; ++i)
+                    lv = std::max(lv, std::fabs(a[(size_t)k * o.rowlen + i]) * o.DTHV(j));
+        }
+#pragma omp critical
+        {
+            um = std::max(um, lu);
+            wm = std::max(wm, lw);
+            vm = std::max(vm, lv);
+        }
+    }
+    terms[0] = 1.0 / (o.alp * (o.n1 / 2) * um);
+    terms[1] = 1.0 / (o.bet * (o.n2 / 2) * wm);
+    terms[2] = 1.0 / vm;
+}
+
 static thread_local std::string g_err;
 
 extern "C" {
@@ -829,6 +1047,39 @@ int orc_step(void* h, int nsteps) {
         for (int k = 1; k <= 3; ++k) rk_substep(o, k);
         if (o.ctpress == 1) meanflow(o, 1);
     }
+    return 0;
+}
+int orc_stats_configure(void* h, int jband, int dnx, int dnz) {
+    Oracle& o = *(Oracle*)h;
+    if (jband >= o.jv0 && (dnx <= 0 || dnz <= 0 || o.ngal1 % dnx || o.ngal2 % dnz)) return 1;
+    stats_configure(o, jband, dnx, dnz);
+    return 0;
+}
+int orc_stats_accumulate(void* h) {
+    Oracle& o = *(Oracle*)h;
+    if (!o.st.on) return 5;
+    stats_accumulate(o);
+    return 0;
+}
+// same layout as cfd_stats_read: bottom + top band combined
+int orc_stats_read(void* h, double* su, double* sv, double* sp, double* cu, double* cv, double* cp, int* istat) {
+    Oracle& o = *(Oracle*)h;
+    auto& st = o.st;
+    if (!st.on) return 5;
+    auto cp_ = [](double* dst, const std::vector<double>& a) { if (dst) std::copy(a.begin(), a.end(), dst); };
+    auto comb = [](double* dst, const std::vector<double>& b, const std::vector<double>& t) {
+        if (dst) for (size_t i = 0; i < b.size(); ++i) dst[i] = b[i] + t[i];
+    };
+    cp_(su, st.su); cp_(sv, st.sv); cp_(sp, st.sp);
+    comb(cu, st.cub, st.cut); comb(cv, st.cvb, st.cvt); comb(cp, st.cpb, st.cpt);
+    if (istat) *istat = st.istat;
+    return 0;
+}
+int orc_cfl(void* h, double* dtc, double* terms) {
+    double t[3];
+    dtc_calc(*(Oracle*)h, t);
+    if (terms) { terms[0] = t[0]; terms[1] = t[1]; terms[2] = t[2]; }
+    *dtc = std::min(t[0], t[1]);
     return 0;
 }
 int orc_set_quirk(void* h, int lastplane) { ((Oracle*)h)->quirk_lastplane = lastplane; return 0; }

@@ -50,6 +50,10 @@ def lib():
         L.orc_four_to_phys.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int]
         L.orc_phys_to_four.argtypes = [C.c_void_p, _dp, C.c_int]
         L.orc_set_num_threads.argtypes = [C.c_int]
+        L.orc_stats_configure.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.orc_stats_accumulate.argtypes = [C.c_void_p]
+        L.orc_stats_read.argtypes = [C.c_void_p] + [C.c_void_p] * 6 + [C.POINTER(C.c_int)]
+        L.orc_cfl.argtypes = [C.c_void_p, _dp, C.c_void_p]
         _lib = L
     return _lib
 
@@ -141,6 +145,33 @@ class OracleChannel:
         a, b, c = C.c_double(), C.c_double(), C.c_double()
         lib().orc_get_scalars(self.h, C.byref(a), C.byref(b), C.byref(c))
         return {"mpgx": a.value, "qx": b.value, "dgx": c.value}
+
+    # statistics (stats.f90) and dtc_calc, same interface as Channel
+    def stats_configure(self, jband: int, dnx: int, dnz: int):
+        from cfd_b200 import capi
+        st = lib().orc_stats_configure(self.h, int(jband), int(dnx), int(dnz))
+        assert st == 0, "bad statistics tile"
+        g = self.setup.grid
+        self._stats_shape = capi.stats_band(g.nyu, g.nyv, g.nyp, int(jband), g.ju0, g.jv0, g.jp0) + \
+            ((int(dnx), int(dnz)) if jband >= g.jv0 else (0, 0))
+
+    def stats_accumulate(self):
+        assert lib().orc_stats_accumulate(self.h) == 0
+
+    def stats_read(self) -> dict:
+        from cfd_b200 import capi
+        g = self.setup.grid
+        nbu, nbv, nbp, dnx, dnz = self._stats_shape
+        bufs = capi.stats_buffers(g.nyu, g.nyv, g.nyp, nbu, nbv, nbp, dnx, dnz)
+        ist = C.c_int()
+        lib().orc_stats_read(self.h, *[b.ctypes.data for b in bufs], C.byref(ist))
+        return capi.stats_dict(bufs, ist.value)
+
+    def cfl(self):
+        dtc = C.c_double()
+        t = np.zeros(3)
+        lib().orc_cfl(self.h, C.byref(dtc), t.ctypes.data)
+        return dtc.value, t
 
     def four_to_phys(self, planes: np.ndarray, zero_oddball: bool = False) -> np.ndarray:
         p = np.ascontiguousarray(planes, dtype=np.float64)

@@ -137,6 +137,83 @@ class NumpyChannel:
             self.nu2[:, jj] = nu2[:, jj] + (vvc[:, jj + 1] - vvc[:, jj]) * g.dthdyv[jj]
             self.du2[:, jj] += C1 * self.nu2[:, jj]
 
+    # --- statistics (stats.f90:1-253 with FOU3D.f90:187-207) and dtc_calc (:516-544) ------
+    def _interp(self):
+        g = self.g
+        yu, yv = g.yu, g.yv
+        u3i = np.zeros((self.ncol, g.nyv), np.complex128)
+        for jj in range(g.nyv):
+            u3i[:, jj] = ((yv[jj] - yu[jj]) * self.u3[:, jj + 1] + (yu[jj + 1] - yv[jj]) * self.u3[:, jj]) / \
+                (yu[jj + 1] - yu[jj])
+        u2i = np.zeros((self.ncol, g.nyu), np.complex128)
+        for jj in range(1, g.nyu - 1):
+            u2i[:, jj] = ((yu[jj] - yv[jj - 1]) * self.u2[:, jj] + (yv[jj] - yu[jj]) * self.u2[:, jj - 1]) / \
+                (yv[jj] - yv[jj - 1])
+        u2i[:, 0] = self.gwib * (self.u2[:, 0] - u2i[:, 1]) + u2i[:, 1]
+        u2i[:, -1] = self.gwit * (self.u2[:, -1] - u2i[:, -2]) + u2i[:, -2]
+        return u2i, u3i
+
+    def stats(self, jband, dnx, dnz):
+        """One stats() call on zeroed accumulators: plane sums and the conditional sums of
+        the bottom band plus the mirrored top band (the layout write_stats stores)."""
+        g = self.g
+        u2i, u3i = self._interp()
+        ntx, ntz = self.ng1 // dnx, self.ng2 // dnz
+
+        def fold(x):
+            return x.reshape(ntz, dnz, ntx, dnx).sum(axis=(0, 2))
+        nbu, nbv, nbp = (jband + 1 - g.ju0 + 1, jband - g.jv0 + 1, jband - g.jp0 + 1) if jband >= g.jv0 else (0, 0, 0)
+        out = {}
+        cond = {k: np.zeros((nb, dnz, dnx)) for k, nb in
+                (("UmC", nbu), ("U2mC", nbu), ("WmC", nbu), ("W2mC", nbu), ("UVmC", nbu), ("UWmC", nbu),
+                 ("VmC", nbv), ("V2mC", nbv), ("wxmC", nbv), ("wx2mC", nbv), ("VWmC", nbv),
+                 ("PmC", nbp), ("P2mC", nbp))}
+        su = np.zeros((6, g.nyu))
+        for jj in range(g.nyu):
+            U, W, Vi = self.to_phys(self.u1[:, jj]), self.to_phys(self.u3[:, jj]), self.to_phys(u2i[:, jj])
+            su[:, jj] = [U.sum(), (U * U).sum(), W.sum(), (W * W).sum(), (U * Vi).sum(), (U * W).sum()]
+            for j1, sg in ((jj, 1.0), (g.nyu - 1 - jj, -1.0)):
+                if j1 < nbu:
+                    for k, x in (("UmC", U), ("U2mC", U * U), ("WmC", W), ("W2mC", W * W),
+                                 ("UVmC", U * Vi * sg), ("UWmC", U * W)):
+                        cond[k][j1] += fold(x)
+        sv = np.zeros((5, g.nyv))
+        zrow = self.q == self.n2 // 2
+        for jj in range(g.nyv):
+            V, Wi = self.to_phys(self.u2[:, jj]), self.to_phys(u3i[:, jj])
+            dz = 1j * self.kz * self.u2[:, jj]
+            dz[zrow] = 0.0
+            wx = self.to_phys(-dz + (self.u3[:, jj + 1] - self.u3[:, jj]) * g.dthdyv[jj])
+            wxs = wx[:self.n2, :self.n1]
+            sv[:, jj] = [V.sum(), (V * V).sum(), wxs.sum(), (wxs * wxs).sum(), (V * Wi).sum()]
+            for j1, sg in ((jj, 1.0), (g.nyv - 1 - jj, -1.0)):
+                if j1 < nbv:
+                    for k, x in (("VmC", V * sg), ("V2mC", V * V), ("wxmC", wx), ("wx2mC", wx * wx),
+                                 ("VWmC", V * sg * Wi)):
+                        cond[k][j1] += fold(x)
+        sp = np.zeros((2, g.nyp))
+        for jj in range(g.nyp):
+            P = self.to_phys(self.p[:, jj])
+            sp[:, jj] = [P.sum(), (P * P).sum()]
+            for j1 in (jj, g.nyp - 1 - jj):
+                if j1 < nbp:
+                    cond["PmC"][j1] += fold(P)
+                    cond["P2mC"][j1] += fold(P * P)
+        for names, a in ((("Um", "U2m", "Wm", "W2m", "UVm", "UWm"), su), (("Vm", "V2m", "wxm", "wx2m", "VWm"), sv),
+                         (("Pm", "P2m"), sp)):
+            for q, n in enumerate(names):
+                out[n] = a[q]
+        out.update(cond)
+        return out
+
+    def cfl(self):
+        g = self.g
+        um = max(np.abs(self.to_phys(self.u1[:, jj])).max() for jj in range(g.nyu))
+        wm = max(np.abs(self.to_phys(self.u3[:, jj])).max() for jj in range(g.nyu))
+        vm = max([1e-6] + [np.abs(self.to_phys(self.u2[:, jj])).max() * g.dthdyv[jj] for jj in range(1, g.nyv - 1)])
+        t = np.array([1.0 / (self.cfg.alp * (self.n1 // 2) * um), 1.0 / (self.cfg.bet * (self.n2 // 2) * wm), 1.0 / vm])
+        return min(t[0], t[1]), t
+
     def _ib(self, u, rhs, lst, j0, n):
         if lst is None:
             return

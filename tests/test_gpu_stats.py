@@ -1,0 +1,99 @@
+"""GPU statistics (cfd_stats_*) and CFL (cfd_cfl) against the FP64 oracle on the same state.
+
+The statistics pass is FP64 in both precisions, so both contexts must match the oracle to
+round-off (1e-10 of each sum's scale; zero-mean first moments on sqrt(points * second
+moment)), after one and after several accumulations.
+"""
+import numpy as np
+import pytest
+
+from cfd_b200 import build_channel, capi
+from cfd_b200.config import tiny
+from cfd_b200.geometry import lattice_params
+
+pytestmark = pytest.mark.gpu
+
+PLANE = capi.STATS_U + capi.STATS_V + capi.STATS_P
+COND = tuple(n + "C" for n in PLANE)
+SECOND = {"Um": "U2m", "Vm": "V2m", "Wm": "W2m", "Pm": "P2m", "wxm": "wx2m"}
+
+
+def close(got, ref, k, tol, npts):
+    a, b = got[k], ref[k]
+    base = k[:-1] if k.endswith("C") and k[:-1] in PLANE else k
+    floor = 0.0
+    if base in SECOND:
+        floor = tol * np.sqrt(npts * np.abs(ref[SECOND[base] + ("C" if base != k else "")]).max())
+    return np.abs(a - b).max() <= tol * np.abs(b).max() + floor + 1e-300
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def stepped(cfg, nsteps=2):
+    from oracle.oracle import OracleChannel
+    s = build_channel(cfg)
+    o = OracleChannel(s)
+    o.upload_state()
+    o.step(nsteps)
+    return s, o
+
+
+CASES = [tiny(24, 18, 17), tiny(96, 64, 21, cyl_diameter=0.3, cyl_spacing=1.0)]
+
+
+@pytest.mark.parametrize("cfg", CASES, ids=lambda c: c.name)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_stats_vs_oracle(torch_cuda, cfg, precision):
+    from cfd_b200.channel import Channel
+    s, o = stepped(cfg)
+    _, _, dnx, dnz, *_ = lattice_params(s.cfg)
+    jband = s.grid.jv0 + s.grid.nyv // 3
+    g = Channel(s, device=0, precision=precision)
+    g.upload_state(o.download_state())
+    npts = s.cfg.ngal1 * s.cfg.ngal2
+    for ch in (g, o):
+        ch.stats_configure(jband, dnx, dnz)
+    for n in (1, 3):
+        while o.stats_read()["istat"] < n:
+            g.stats_accumulate()
+            o.stats_accumulate()
+        got, ref = g.stats_read(), o.stats_read()
+        assert got["istat"] == ref["istat"] == n
+        for k in PLANE + COND:
+            assert got[k].shape == ref[k].shape, k
+            assert close(got, ref, k, 1e-10, npts), (n, k)
+    g.stats_reset()
+    z = g.stats_read()
+    assert z["istat"] == 0 and not any(np.any(z[k]) for k in PLANE + COND)
+    g.close()
+
+
+@pytest.mark.parametrize("cfg", CASES, ids=lambda c: c.name)
+def test_cfl_vs_oracle(torch_cuda, cfg):
+    from cfd_b200.channel import Channel
+    s, o = stepped(cfg)
+    g = Channel(s, device=0, precision="fp64")
+    g.upload_state(o.download_state())
+    dtc, t = g.cfl()
+    dto, to = o.cfl()
+    assert np.allclose(t, to, rtol=1e-11), (t, to)
+    assert dtc == min(t[0], t[1]) and abs(dtc - dto) <= 1e-11 * dto
+    g.close()
+
+
+def test_stats_bad_tile(torch_cuda):
+    from cfd_b200.channel import Channel
+    s = build_channel(tiny(24, 18, 17))
+    g = Channel(s, device=0)
+    g.upload_state()
+    with pytest.raises(RuntimeError, match="tile"):
+        g.stats_configure(s.grid.jv0 + 3, 5, 3)
+    with pytest.raises(RuntimeError, match="not configured"):
+        g.stats_accumulate()
+    g.close()
