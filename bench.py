@@ -85,6 +85,22 @@ def kernel_bytes(name, setup, mixed):
     return b.get(name[:-1]) if name.endswith("2") else None
 
 
+def ncu_traffic(config: str, kname: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a kernel from the
+    committed ncu summary profiles/dram_traffic_<config>.md, or None."""
+    p = os.path.join(ROOT, "profiles", f"dram_traffic_{config}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) >= 4 and cells[0].split("<")[0] == kname and "(" not in cells[0]:
+            try:
+                return int(cells[3])
+            except ValueError:
+                return None
+    return None
+
+
 # ------------------------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
@@ -132,7 +148,9 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------
-def dist_init():
+def dist_init(backend: str = "nccl"):
+    """One process per GPU (torchrun env); replicas only, so the process group carries just
+    the barrier and the max-over-ranks of the timings."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -140,10 +158,19 @@ def dist_init():
         import datetime
         import torch.distributed as dist
         import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return ws, rank, local
+
+
+def aggregate_rate(ws, units_per_rank, seconds_max):
+    """Whole-job throughput of independent replicas: every rank processed units_per_rank in
+    its own time; the job took the slowest rank's time."""
+    return ws * units_per_rank / seconds_max
 
 
 def barrier(ws):
@@ -293,7 +320,7 @@ def main():
         n0 = ch.launch_count()
         with ClockSampler(local) as cs:
             t = time_steps(torch, ch, stream, args.steps, ws, device)
-        results[prec] = {"seconds": t, "steps_per_s": ws * args.steps / t, "clocks": cs.summary(),
+        results[prec] = {"seconds": t, "steps_per_s": aggregate_rate(ws, args.steps, t), "clocks": cs.summary(),
                          "launches": ch.launch_count() - n0}
         chans[prec] = ch
 
@@ -350,7 +377,7 @@ def main():
     e.synchronize()
     barrier(ws)
     te2e = max_over_ranks(ws, s.elapsed_time(e) / 1e3, device)
-    e2e_val = ws * ne2e / te2e
+    e2e_val = aggregate_rate(ws, ne2e, te2e)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -385,7 +412,9 @@ def main():
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
-                     "traffic": None, "algorithmic_bytes_per_launch": kb,
+                     "traffic": ncu_traffic(args.config, kname), "traffic_source":
+                         f"profiles/dram_traffic_{args.config}.md (ncu, bytes per launch)",
+                     "algorithmic_bytes_per_launch": kb,
                      "avg_launch_ms": kms / kcalls, "share_of_step": kms / tot},
         "kernels_mixed": {k: {"calls": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
         "kernels_fp64": {k: {"calls": v[0], "ms": v[1]} for k, v in sorted(prof64.items(), key=lambda kv: -kv[1][1])},
