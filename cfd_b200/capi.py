@@ -142,6 +142,7 @@ SIGNATURES = {
     "cfd_stats_reset": (C.c_int, [_VP]),
     "cfd_stats_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, C.POINTER(C.c_int32)]),
     "cfd_cfl": (C.c_int, [_VP, _dp, _VP]),
+    "cfd_set_dt": (C.c_int, [_VP, C.c_double]),
     "cfd_launch_count": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "cfd_profile": (C.c_int, [_VP, C.c_int32]),
     "cfd_profile_read": (C.c_int, [_VP, C.c_char_p, C.c_int32]),

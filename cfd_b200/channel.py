@@ -201,6 +201,10 @@ class Channel:
         self._chk(self.lib.cfd_cfl(self.ctx, C.byref(dtc), t.ctypes.data), "cfl")
         return dtc.value, t
 
+    def set_dt(self, dt: float):
+        """New time step for the following stages and steps (the graph is captured again)."""
+        self._chk(self.lib.cfd_set_dt(self.ctx, float(dt)), "set_dt")
+
     def divergence_max(self) -> float:
         e = C.c_double()
         self._chk(self.lib.cfd_divergence_max(self.ctx, C.byref(e)), "divergence_max")

@@ -232,10 +232,11 @@ int ilog2(int b) {
         default: ok = false; break;                                          \
     }
 
-// shared memory of k_xline2 (elements): B*LX + N + RW*3*nk
+// shared memory of k_xline2 (elements): B*LX + N
 // Launch-shape overrides for tuning runs (unset: the built-in choice).
 //   CFD_XLINE_ROWS   rows per CTA of the two-step x-line kernel (power of two, 2..8)
 //   CFD_ZLINES_LOG2  log2 of the lines per CTA of the two-step z kernels (2..4)
+//   CFD_XLINE_STOCKHAM 1: nonlinear through the Stockham x-line kernel and per-slot z pass
 int env_int(const char* name, int dflt, int lo, int hi) {
     const char* v = std::getenv(name);
     if (!v || !*v) return dflt;
@@ -802,7 +803,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
-            int rw = env_int("CFD_XLINE_ROWS", 8, 2, 8);
+            int rw = env_int("CFD_XLINE_ROWS", mixed ? 8 : 4, 2, 8);
             while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
             if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
                 c->RW2 = rw;
@@ -811,7 +812,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
             }
         }
     }
-    if (!mixed) c->RW2 = 0;  // FP64: the Stockham x-line kernel is faster (register pressure)
+    if (env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)) c->RW2 = 0;
     {
         bool ok = true;
         int n1s = 0, n2s = 0;
@@ -1365,6 +1366,15 @@ int cfd_stats_read(cfd_ctx* c, double* u_sums, double* v_sums, double* p_sums, d
     if (!s) s = combine(cp, st.cp_, (size_t)2 * st.nbp * tsz);
     if (s) return s;
     if (istat) *istat = st.istat;
+    return CFD_OK;
+}
+
+int cfd_set_dt(cfd_ctx* c, double dt) {
+    if (!c) return CFD_ERR_ARG;
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(c, CFD_ERR_ARG, "dt must be positive and finite");
+    CK(cudaStreamSynchronize(c->stream));
+    c->dt = dt;
+    destroy_graph(c);
     return CFD_OK;
 }
 

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // elements of a subsequence are zero, direct or conjugated is resolved at compile time
 // except in the two blocks that straddle a boundary.
 template <typename T2, int N1, int N2>
-__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (N1 > N2 ? N1 : N2) <= 24 ? 2 : 1) k_xline2(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && (N1 > N2 ? N1 : N2) <= 24) ? 2 : 1) k_xline2(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
     using R = decltype(T2::x);
     constexpr int N = N1 * N2;

@@ -240,6 +240,12 @@ int cfd_stats_read(cfd_ctx *ctx, double *u_sums, double *v_sums, double *p_sums,
  * set, start.f90:684), so that term is 1/0 = +Inf and never limits the step. */
 int cfd_cfl(cfd_ctx *ctx, double *dtc, double *terms);
 
+/* Changes the time step used by every following stage and step (the reference's
+ * dt = min(2.5*dtv, CFL*dtc) update at kRK = 1, FOU3D.f90:177-183).  The captured RK3 graph
+ * holds dt in its kernel arguments, so it is dropped here and captured again by the next
+ * cfd_step. */
+int cfd_set_dt(cfd_ctx *ctx, double dt);
+
 /* ---- allocation-free solve ----------------------------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc/cudaFree: a

@@ -1082,6 +1082,11 @@ int orc_cfl(void* h, double* dtc, double* terms) {
     *dtc = std::min(t[0], t[1]);
     return 0;
 }
+int orc_set_dt(void* h, double dt) {
+    if (!(dt > 0)) return 1;
+    ((Oracle*)h)->dt = dt;
+    return 0;
+}
 int orc_set_quirk(void* h, int lastplane) { ((Oracle*)h)->quirk_lastplane = lastplane; return 0; }
 void orc_get_scalars(void* h, double* mpgx, double* qx, double* dgx) {
     Oracle& o = *(Oracle*)h;

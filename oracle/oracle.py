@@ -54,6 +54,7 @@ def lib():
         L.orc_stats_accumulate.argtypes = [C.c_void_p]
         L.orc_stats_read.argtypes = [C.c_void_p] + [C.c_void_p] * 6 + [C.POINTER(C.c_int)]
         L.orc_cfl.argtypes = [C.c_void_p, _dp, C.c_void_p]
+        L.orc_set_dt.argtypes = [C.c_void_p, C.c_double]
         _lib = L
     return _lib
 
@@ -166,6 +167,9 @@ class OracleChannel:
         ist = C.c_int()
         lib().orc_stats_read(self.h, *[b.ctypes.data for b in bufs], C.byref(ist))
         return capi.stats_dict(bufs, ist.value)
+
+    def set_dt(self, dt: float):
+        assert lib().orc_set_dt(self.h, float(dt)) == 0
 
     def cfl(self):
         dtc = C.c_double()

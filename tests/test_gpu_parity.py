@@ -225,3 +225,23 @@ def test_fixed_length_transforms(torch_cuda, ng1, ng2, ny):
     for k in ("u1", "u2", "u3"):
         assert rel(st[k], ref[k]) < 1e-5, (k, rel(st[k], ref[k]))
     m.close()
+
+
+@pytest.mark.parametrize("ng1,ng2,ny", [(96, 192, 13), (384, 768, 9)])
+def test_stockham_nonlinear_path(torch_cuda, monkeypatch, ng1, ng2, ny):
+    """The alternative nonlinear path (per-slot interpolating z pass + shared-memory Stockham
+    x-line kernel, selected with CFD_XLINE_STOCKHAM=1) on two-step lengths, both precisions."""
+    from cfd_b200.channel import build_channel
+    from cfd_b200.config import tiny
+    monkeypatch.setenv("CFD_XLINE_STOCKHAM", "1")
+    s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=ng1 + 2 * ng2))
+    o = oracle(s)
+    o.step(1)
+    ref = o.download_state()
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-5)):
+        g = make(s, prec)
+        g.step(1)
+        st = g.download_state()
+        for k in ("u1", "u2", "u3"):
+            assert rel(st[k], ref[k]) < tol, (prec, k, rel(st[k], ref[k]))
+        g.close()

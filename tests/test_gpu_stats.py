@@ -97,3 +97,27 @@ def test_stats_bad_tile(torch_cuda):
     with pytest.raises(RuntimeError, match="not configured"):
         g.stats_accumulate()
     g.close()
+
+
+def test_set_dt_recaptures_graph(torch_cuda):
+    """A CFL-driven dt change between graph replays: 1 step at dt, 2 steps at 0.8 dt,
+    against the oracle doing the same (FP64 path, 1e-10 relative L2)."""
+    from cfd_b200.channel import Channel
+    from oracle.oracle import OracleChannel
+    s = build_channel(tiny(24, 18, 17))
+    g = Channel(s, device=0, precision="fp64")
+    o = OracleChannel(s)
+    for ch in (g, o):
+        ch.upload_state()
+        ch.step(1)
+    dtc, _ = g.cfl()
+    new = min(0.8 * s.dt, 0.5 * dtc)
+    for ch in (g, o):
+        ch.set_dt(new)
+        ch.step(2)
+    a, b = g.download_state(), o.download_state()
+    for k in a:
+        assert np.linalg.norm(a[k] - b[k]) <= 1e-10 * np.linalg.norm(b[k]), k
+    with pytest.raises(RuntimeError, match="dt"):
+        g.set_dt(-1.0)
+    g.close()
