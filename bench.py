@@ -218,6 +218,40 @@ def profile_step(ch):
     return out
 
 
+def plane_profiles(st, npts):
+    """Mean and rms profiles of u, v, w from accumulated plane sums (stats.f90 quantities)."""
+    n = max(st["istat"], 1) * npts
+    out = {}
+    for f, m, m2 in (("u", "Um", "U2m"), ("v", "Vm", "V2m"), ("w", "Wm", "W2m")):
+        mean = st[m] / n
+        out["mean_" + f] = mean
+        out["rms_" + f] = np.sqrt(np.maximum(st[m2] / n - mean * mean, 0.0))
+    return out
+
+
+def profile_error(chans, setup, nsteps):
+    """Mean and rms velocity profiles of the mixed and FP64 paths from the same start, averaged
+    over nsteps steps with the on-device statistics: the largest difference over the planes
+    relative to the largest FP64 value of that profile."""
+    if nsteps <= 0:
+        return None
+    npts = setup.cfg.ngal1 * setup.cfg.ngal2
+    prof = {}
+    for prec, ch in chans.items():
+        ch.upload_state()
+        ch.stats_configure(setup.grid.jv0 - 1, 0, 0)
+        for _ in range(nsteps):
+            ch.step(1)
+            ch.stats_accumulate()
+        prof[prec] = plane_profiles(ch.stats_read(), npts)
+    out = {"steps": nsteps, "max_rel_diff": {}}
+    for k in ("mean_u", "rms_u", "rms_v", "rms_w"):  # mean v and w are zero up to round-off
+        ref = prof["fp64"][k]
+        scale = max(np.abs(ref).max(), 1e-300)
+        out["max_rel_diff"][k] = float(np.abs(prof["mixed"][k] - ref).max() / scale)
+    return out
+
+
 def rel_err(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
@@ -292,6 +326,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--error-steps", type=int, default=10)
+    ap.add_argument("--profile-steps", type=int, default=20,
+                    help="steps of the mean/rms profile comparison of mixed vs FP64 (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -334,6 +370,7 @@ def main():
     for k in ("u1", "u2", "u3", "p"):
         err[k] = rel_err(states["mixed"][k], states["fp64"][k])
     fp64_div = chans["fp64"].divergence_max()
+    prof_err = profile_error(chans, setup, args.profile_steps)
 
     # per-kernel timing (CUDA events on the launching stream) for the roofline
     hbm, peak_kind = peaks()
@@ -410,6 +447,7 @@ def main():
                  "max_divergence": fp64_div},
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
+        "profile_error_mixed_vs_fp64": prof_err,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
                      "traffic": ncu_traffic(args.config, kname), "traffic_source":

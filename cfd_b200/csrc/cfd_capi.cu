@@ -92,6 +92,9 @@ struct cfd_ctx {
     int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
     int RW2 = 0, NT2 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
     int LZ2 = -1, NTZ2 = 0; // two-step z kernels: log2(columns per CTA) (-1 = not used), threads
+    int SWM = 0, SWC = 8;   // warp-per-column solves: rows-per-lane bound (0 = not used), columns per CTA
+    double2* ed_uw = nullptr;  // LU factors {e, d} of the u/w and v systems, [RK substep][column][row]
+    double2* ed_v = nullptr;
     size_t SMZ2 = 0;
     int RWIX2 = 0, RWFX2 = 0;  // two-step IB x kernels: rows per CTA (0 = not used)
     int NTIX2 = 0, NTFX2 = 0;
@@ -237,6 +240,8 @@ int ilog2(int b) {
 //   CFD_XLINE_ROWS   rows per CTA of the two-step x-line kernel (power of two, 2..8)
 //   CFD_ZLINES_LOG2  log2 of the lines per CTA of the two-step z kernels (2..4)
 //   CFD_XLINE_STOCKHAM 1: nonlinear through the Stockham x-line kernel and per-slot z pass
+//   CFD_SOLVE_WARP   1: Helmholtz solves one warp per column on precomputed LU factors
+//   CFD_SOLVE_COLS   columns (warps) per CTA of the warp-per-column solve (1..8)
 int env_int(const char* name, int dflt, int lo, int hi) {
     const char* v = std::getenv(name);
     if (!v || !*v) return dflt;
@@ -517,9 +522,47 @@ int ib_all(cfd_ctx* c) {
     return ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr);
 }
 
+size_t solve_w_smem(const Dims& d, int swc) {
+    return (size_t)2 * swc * d.nyu * sizeof(double2) + (size_t)3 * d.nyu * sizeof(double);
+}
+
+// LU factors of the u/w and v systems for the three RK substeps at the current dt
+int factor_all(cfd_ctx* c) {
+    if (!c->SWM) return CFD_OK;
+    const Dims& d = c->d;
+    for (int k = 0; k < 3; ++k) {
+        const double beta = kRKb[k] * c->dt / c->re;
+        prof_mark(c);
+        k_factor_uv<<<dim3((d.ncol + 255) / 256, 2), 256, 0, c->stream>>>(
+            d, c->g, beta, c->ed_uw + (size_t)k * d.ncol * d.nyu, c->ed_v + (size_t)k * d.ncol * d.nyv);
+        LK("k_factor_uv");
+    }
+    return CFD_OK;
+}
+
 int solve_kernel(cfd_ctx* c, int krk) {
     const Dims& d = c->d;
     const double beta = kRKb[krk - 1] * c->dt / c->re;
+    if (c->SWM) {
+        const int lc = ilog2(c->SWC);
+        dim3 gw((d.ncol + c->SWC - 1) / c->SWC, 2);
+        const size_t sm = solve_w_smem(d, c->SWC);
+        const int nt = 32 * c->SWC;
+        const double2* eu = c->ed_uw + (size_t)(krk - 1) * d.ncol * d.nyu;
+        const double2* ev = c->ed_v + (size_t)(krk - 1) * d.ncol * d.nyv;
+        prof_mark(c);
+#define SOLVE_W(M) \
+    k_solve_uvw_w<M><<<gw, nt, sm, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, eu, ev, lc)
+        switch (c->SWM) {
+            case 4: SOLVE_W(4); break;
+            case 8: SOLVE_W(8); break;
+            case 12: SOLVE_W(12); break;
+            default: SOLVE_W(16); break;
+        }
+#undef SOLVE_W
+        LK("k_solve_uvw_w");
+        return CFD_OK;
+    }
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
     gb.y = 2;
@@ -826,6 +869,25 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     if (c->LZ2 < 0) c->RW2 = 0;  // the two-step x-line kernel reads the output of k_zinv2s
     {
+        // warp-per-column Helmholtz solves: up to 16 rows per lane (512 planes)
+        const int m = (d.nyu + 31) / 32;
+        c->SWM = m <= 4 ? 4 : (m <= 8 ? 8 : (m <= 12 ? 12 : (m <= 16 ? 16 : 0)));
+        // measured at re550: 482 us per launch against 400 us for the thread-per-column sweep
+        if (!env_int("CFD_SOLVE_WARP", 0, 0, 1)) c->SWM = 0;
+        c->SWC = 1 << ilog2(env_int("CFD_SOLVE_COLS", 8, 1, 8));
+        while (c->SWC > 1 && solve_w_smem(d, c->SWC) > 110 * 1024) c->SWC /= 2;
+        const int sm = (int)solve_w_smem(d, c->SWC);
+        cudaError_t e = cudaSuccess;
+        switch (c->SWM) {
+            case 4: e = cudaFuncSetAttribute(k_solve_uvw_w<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            case 8: e = cudaFuncSetAttribute(k_solve_uvw_w<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            case 12: e = cudaFuncSetAttribute(k_solve_uvw_w<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            case 16: e = cudaFuncSetAttribute(k_solve_uvw_w<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            default: break;
+        }
+        if (e != cudaSuccess) return fail(c, CFD_ERR_CUDA, "solve attributes: %s", cudaGetErrorString(e));
+    }
+    {
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
@@ -868,6 +930,10 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     AL(c->cs, double, nc * nyu);
     AL(c->cs_v, double, nc * nyv);
+    if (c->SWM) {
+        AL(c->ed_uw, double2, 3 * nc * nyu);
+        AL(c->ed_v, double2, 3 * nc * nyv);
+    }
     c->JC = 16;
     c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;
     AL(c->scal, double, 4);
@@ -898,6 +964,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
             AL(c->phys, double, nibp * d.ngal2 * d.ngal1);
         }
     }
+    if ((s = factor_all(c)) != CFD_OK) return s;
     CK(cudaDeviceSynchronize());
     return CFD_OK;
 }
@@ -1375,7 +1442,7 @@ int cfd_set_dt(cfd_ctx* c, double dt) {
     CK(cudaStreamSynchronize(c->stream));
     c->dt = dt;
     destroy_graph(c);
-    return CFD_OK;
+    return factor_all(c);
 }
 
 int cfd_cfl(cfd_ctx* c, double* dtc, double* terms) {

@@ -19,6 +19,7 @@
 
 #include "fft_smem.cuh"
 #include "fft_reg.cuh"
+#include "tridiag.cuh"
 
 namespace cfd {
 
@@ -1132,6 +1133,120 @@ __global__ void k_ib_zfwd2(Dims d, const T2* __restrict__ Hib, int npl, IBDst ds
         if (q >= 0 && live) out[(size_t)q * d.nkx] = to_d2(cscale(v, sc));
     };
     two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
+}
+
+// --------------------------------------------------------------------------------------
+// LU factors of the Helmholtz systems (LU_buildU/V + LU_dec, tridLU_3D_IB.f90:349-413,
+// 521-559) for one RK coefficient beta, one thread per column: ed[col][row] = {e_j, d_j},
+// e_j = a3_j d_j, d_j = 1/(a2_j - a1_j e_{j-1}).  u and w share rows (0, 1, gwb) /
+// interior / (gwt, 1, 0); v has identity wall rows.  grid: x = column block, y = system.
+// Column-major so that a warp lane reads its consecutive rows as one contiguous run.
+// --------------------------------------------------------------------------------------
+__device__ __forceinline__ void helm_row(const Dims& d, const Geo& g, bool uw, int n, int j, double beta,
+                                         double k2x, double k2z, double& a1, double& a2, double& a3) {
+    const double* D2 = uw ? g.dyu2i : g.dyv2i;
+    if (j == 0) { a1 = 0.0; a2 = 1.0; a3 = uw ? g.gwb : 0.0; }
+    else if (j == n - 1) { a1 = uw ? g.gwt : 0.0; a2 = 1.0; a3 = 0.0; }
+    else {
+        a1 = -beta * D2[3 * j + 0];
+        a2 = 1.0 - beta * (D2[3 * j + 1] + k2x + k2z);
+        a3 = -beta * D2[3 * j + 2];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_factor_uv(Dims d, Geo g, double beta, double2* __restrict__ ed_uw,
+                                                   double2* __restrict__ ed_v) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol) return;
+    const bool uw = blockIdx.y == 0;
+    const int n = uw ? d.nyu : d.nyv;
+    const int i = col % d.nkx, q = col / d.nkx;
+    const double k2x = -g.kx[i] * g.kx[i], k2z = -g.kz[q] * g.kz[q];
+    double2* ed = (uw ? ed_uw : ed_v) + (size_t)col * n;
+    double ep = 0.0;
+    for (int j = 0; j < n; ++j) {
+        double a1, a2, a3;
+        helm_row(d, g, uw, n, j, beta, k2x, k2z, a1, a2, a3);
+        const double dj = 1.0 / (a2 - a1 * ep);
+        ep = a3 * dj;
+        ed[j] = make_double2(ep, dj);
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// Implicit Helmholtz solves, one warp per (kx,kz) column (tridiag.cuh): LUsolU for u and w
+// with shared factors and LUsolV for v.  A CTA of 2^lc warps stages the right-hand sides of
+// 2^lc adjacent columns in shared memory with coalesced asynchronous copies ([field]
+// [column][plane]: planes contiguous, so the lanes' row blocks fall in distinct banks), reads
+// the precomputed factors of its columns as contiguous per-lane runs, substitutes in
+// registers and writes the solutions back coalesced.  grid: x = column block, y = 0 (u, w)
+// or 1 (v).
+// --------------------------------------------------------------------------------------
+template <int MAXM>
+__global__ void __launch_bounds__(256, MAXM <= 12 ? 2 : 1)
+    k_solve_uvw_w(Dims d, Geo g, double beta, double2* __restrict__ u1, double2* __restrict__ u2,
+                  double2* __restrict__ u3, const double2* __restrict__ r1, const double2* __restrict__ r2,
+                  const double2* __restrict__ r3, const double2* __restrict__ ed_uw,
+                  const double2* __restrict__ ed_v, int lc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ncpb = 1 << lc;
+    const bool uw = blockIdx.y == 0;
+    const int n = uw ? d.nyu : d.nyv;
+    const int nf = uw ? 2 : 1;
+    double2* sm = reinterpret_cast<double2*>(smem_raw);
+    double* D2 = reinterpret_cast<double*>(sm + (size_t)2 * ncpb * d.nyu);  // [n][3]
+    const int col0 = blockIdx.x * ncpb;
+    const size_t nc = d.ncol;
+    const int c = threadIdx.x & (ncpb - 1);
+    const bool cok = col0 + c < d.ncol;
+    for (int f = 0; f < nf; ++f) {
+        const double2* src = (f == 0 ? (uw ? r1 : r2) : r3) + col0 + c;
+        double2* dst = sm + ((size_t)f * ncpb + c) * n;
+        for (int j = threadIdx.x >> lc; j < n; j += blockDim.x >> lc)
+            if (cok) cp_async16(dst + j, src + (size_t)j * nc);
+    }
+    {
+        const double* g2 = uw ? g.dyu2i : g.dyv2i;
+        for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) D2[k] = g2[k];
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int col = col0 + w;
+    const bool act = w < ncpb && col < d.ncol;
+    const LaneRows lr = lane_rows(n, lane);
+    double2 ed[MAXM];
+    if (act) {
+        const double2* ec = (uw ? ed_uw : ed_v) + (size_t)col * n + lr.s;
+#pragma unroll
+        for (int t = 0; t < MAXM; ++t)
+            if (t < lr.mp) ed[t] = ec[t];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (act) {
+        const double gt = uw ? g.gwt : 0.0;
+        auto a1 = [&](int t) {
+            const int j = lr.s + t;
+            return j == 0 ? 0.0 : (j == n - 1 ? gt : -beta * D2[3 * j + 0]);
+        };
+        for (int f = 0; f < nf; ++f) {
+            double2* cs = sm + ((size_t)f * ncpb + w) * n + lr.s;
+            double2 y[MAXM];
+#pragma unroll
+            for (int t = 0; t < MAXM; ++t)
+                if (t < lr.mp) y[t] = cs[t];
+            warp_substitute<MAXM>(lr, lane, ed, a1, y);
+#pragma unroll
+            for (int t = 0; t < MAXM; ++t)
+                if (t < lr.mp) cs[t] = y[t];
+        }
+    }
+    __syncthreads();
+    for (int f = 0; f < nf; ++f) {
+        double2* dst = (f == 0 ? (uw ? u1 : u2) : u3) + col0 + c;
+        const double2* src = sm + ((size_t)f * ncpb + c) * n;
+        for (int j = threadIdx.x >> lc; j < n; j += blockDim.x >> lc)
+            if (cok) dst[(size_t)j * nc] = src[j];
+    }
 }
 
 // --------------------------------------------------------------------------------------
