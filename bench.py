@@ -252,6 +252,45 @@ def profile_error(chans, setup, nsteps):
     return out
 
 
+def run_ensemble(torch, device, nsteps, warmup):
+    """The 16-member batched ensemble (4 x 96x97x96, 8 x 128x129x128, 4 x 192x161x192, own
+    seeds and cylinder diameters) in both precisions: RK3 steps/s of the whole ensemble with
+    one graph launch per step (device time on the ensemble's stream), and the same members
+    stepped by their own graphs one after another (host wall time), for comparison."""
+    from cfd_b200 import Ensemble
+    from cfd_b200.config import ensemble_configs
+    out = {"members": 16, "workload": "4 x 96x97x96 Re_tau 180, 8 x 128x129x128 Re_tau 260, "
+                                      "4 x 192x161x192 Re_tau 395; D ~ U[0.03, 0.06] h, spacing 4 D"}
+    for prec in ("mixed", "fp64"):
+        cfgs = ensemble_configs(precision=prec)
+        ens = Ensemble.from_configs(cfgs, device=device.index or 0)
+        gp = sum(c.ngal1 * c.ngal2 * m.setup.grid.nyv for c, m in zip(cfgs, ens.members))
+        ens.step(warmup)
+        ens.synchronize()
+        st = torch.cuda.ExternalStream(ens.stream(), device=device)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(st)
+        ens.step(nsteps)
+        e.record(st)
+        e.synchronize()
+        t = s.elapsed_time(e) / 1e3
+        for m in ens.members:
+            m.step(1)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            for m in ens.members:
+                m.step(1)
+        for m in ens.members:
+            m.synchronize()
+        tsep = time.perf_counter() - t0
+        out[prec] = {"ensemble_steps_per_s": nsteps / t, "member_steps_per_s": 16 * nsteps / t,
+                     "grid_pt_updates_per_s": gp * nsteps / t,
+                     "separate_graphs_steps_per_s": nsteps / tsep}
+        ens.close(members=True)
+    return out
+
+
 def rel_err(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
@@ -326,6 +365,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--error-steps", type=int, default=10)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")
     ap.add_argument("--profile-steps", type=int, default=20,
                     help="steps of the mean/rms profile comparison of mixed vs FP64 (0: skip)")
     args = ap.parse_args()
@@ -371,6 +411,7 @@ def main():
         err[k] = rel_err(states["mixed"][k], states["fp64"][k])
     fp64_div = chans["fp64"].divergence_max()
     prof_err = profile_error(chans, setup, args.profile_steps)
+    ens = run_ensemble(torch, device, args.steps, args.warmup) if (ws == 1 and not args.no_ensemble) else None
 
     # per-kernel timing (CUDA events on the launching stream) for the roofline
     hbm, peak_kind = peaks()
@@ -448,6 +489,7 @@ def main():
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
         "profile_error_mixed_vs_fp64": prof_err,
+        "ensemble": ens,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
                      "traffic": ncu_traffic(args.config, kname), "traffic_source":

@@ -8,5 +8,6 @@ the host set-up of grids, IB lists and seeded initial fields.
 """
 from .config import ChannelConfig, PRESETS, preset, tiny  # noqa: F401
 from .channel import Channel, ChannelSetup, build_channel  # noqa: F401
+from .ensemble import Ensemble  # noqa: F401
 
 __version__ = "0.1.0"

@@ -143,6 +143,12 @@ SIGNATURES = {
     "cfd_stats_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, C.POINTER(C.c_int32)]),
     "cfd_cfl": (C.c_int, [_VP, _dp, _VP]),
     "cfd_set_dt": (C.c_int, [_VP, C.c_double]),
+    "cfd_ensemble_create": (C.c_int, [C.POINTER(_VP), C.c_int32, C.POINTER(_VP)]),
+    "cfd_ensemble_step": (C.c_int, [_VP, C.c_int32]),
+    "cfd_ensemble_synchronize": (C.c_int, [_VP]),
+    "cfd_ensemble_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "cfd_ensemble_last_error": (C.c_char_p, [_VP]),
+    "cfd_ensemble_destroy": (C.c_int, [_VP]),
     "cfd_launch_count": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "cfd_profile": (C.c_int, [_VP, C.c_int32]),
     "cfd_profile_read": (C.c_int, [_VP, C.c_char_p, C.c_int32]),

@@ -111,6 +111,26 @@ def preset(name: str, **overrides) -> ChannelConfig:
     return replace(PRESETS[name], **overrides)
 
 
+# Batched ensemble: 16 independent channels of uneven size (4 x 96x97x96 at Re_tau 180,
+# 8 x 128x129x128 at Re_tau 260, 4 x 192x161x192 at Re_tau 395), cylinder height 0.08 h,
+# diameter drawn uniformly from [0.03 h, 0.06 h] per member, spacing 4 diameters, own seeds.
+ENSEMBLE_GROUPS = ((4, 96, 97, 180.0), (8, 128, 129, 260.0), (4, 192, 161, 395.0))
+
+
+def ensemble_configs(seed: int = 2000, precision: str = "mixed", groups=ENSEMBLE_GROUPS):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for count, ng, ny, rt in groups:
+        for _ in range(count):
+            dia = float(rng.uniform(0.03, 0.06))
+            k = len(out)
+            out.append(ChannelConfig(ngal1=ng, ngal2=ng, ny=ny, re_tau=rt, posth=0.08, cyl_diameter=dia,
+                                     cyl_spacing=4.0 * dia, precision=precision, seed=seed + k,
+                                     name=f"ens{k}-{ng}x{ny}x{ng}"))
+    return out
+
+
 def tiny(ngal1: int = 24, ngal2: int = 18, ny: int = 17, **kw) -> ChannelConfig:
     """A small channel for parity tests (seconds on the oracle)."""
     base = dict(ngal1=ngal1, ngal2=ngal2, ny=ny, re_tau=180.0, posth=0.12,

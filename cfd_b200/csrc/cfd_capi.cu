@@ -107,6 +107,7 @@ struct cfd_ctx {
     int64_t graph_launches = 0;
     int64_t launches = 0;
     bool capturing = false;
+    int64_t epoch = 0;      // bumped when dt or the stream changes (ensembles capture again)
     bool profiling = false;
     cudaEvent_t prof_last = nullptr;
     std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> prof;
@@ -128,6 +129,19 @@ struct cfd_ctx {
         double* mx = nullptr;     // [3][nyu]: |u|, |w| per u plane, |v| dthdyv per v plane
         cfd::PlaneSrc* src = nullptr;  // [3*cp]
     } st;
+};
+
+struct cfd_ensemble {
+    std::vector<cfd_ctx*> m;
+    std::vector<cudaStream_t> streams;  // one branch stream per member (owned)
+    std::vector<cudaEvent_t> pre, join; // member stream -> master, branch -> master
+    std::vector<int64_t> epochs;        // member epochs the graph was captured with
+    cudaEvent_t fork = nullptr, done = nullptr;
+    cudaStream_t master = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int device = 0;
+    std::string err;
 };
 
 namespace {
@@ -1146,7 +1160,10 @@ int cfd_destroy(cfd_ctx* c) {
 int cfd_set_stream(cfd_ctx* c, void* stream) {
     if (!c) return CFD_ERR_ARG;
     cudaStream_t s = stream ? (cudaStream_t)stream : c->own_stream;
-    if (s != c->stream) destroy_graph(c);
+    if (s != c->stream) {
+        destroy_graph(c);
+        c->epoch++;
+    }
     c->stream = s;
     return CFD_OK;
 }
@@ -1436,11 +1453,161 @@ int cfd_stats_read(cfd_ctx* c, double* u_sums, double* v_sums, double* p_sums, d
     return CFD_OK;
 }
 
+namespace {
+int efail(cfd_ensemble* e, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (e) e->err = buf;
+    return code;
+}
+#define ECK(call)                                                                        \
+    do {                                                                                 \
+        cudaError_t _e = (call);                                                         \
+        if (_e != cudaSuccess) return efail(e, CFD_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e)); \
+    } while (0)
+
+void ens_release_graph(cfd_ensemble* e) {
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->gexec = nullptr;
+    e->graph = nullptr;
+}
+
+// One RK3 step of every member as parallel branches of one graph on the master stream.
+int ens_capture(cfd_ensemble* e) {
+    ens_release_graph(e);
+    ECK(cudaStreamBeginCapture(e->master, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = cudaEventRecord(e->fork, e->master);
+    int st = ce == cudaSuccess ? CFD_OK : efail(e, CFD_ERR_CUDA, "fork: %s", cudaGetErrorString(ce));
+    for (size_t i = 0; i < e->m.size() && st == CFD_OK; ++i) {
+        cfd_ctx* c = e->m[i];
+        cudaStream_t saved = c->stream;
+        c->stream = e->streams[i];
+        if ((ce = cudaStreamWaitEvent(c->stream, e->fork, 0)) != cudaSuccess) {
+            st = efail(e, CFD_ERR_CUDA, "branch %zu: %s", i, cudaGetErrorString(ce));
+        } else {
+            const int64_t before = c->launches;
+            c->capturing = true;
+            for (int k = 1; k <= 3 && st == CFD_OK; ++k) st = substep_any(c, k);
+            if (st == CFD_OK && c->ctpress == 1) st = meanflow_kernel(c, 1);
+            c->capturing = false;
+            c->launches = before;
+            if (st != CFD_OK) efail(e, st, "member %zu: %s", i, c->err.c_str());
+            else if ((ce = cudaEventRecord(e->join[i], c->stream)) != cudaSuccess ||
+                     (ce = cudaStreamWaitEvent(e->master, e->join[i], 0)) != cudaSuccess)
+                st = efail(e, CFD_ERR_CUDA, "join %zu: %s", i, cudaGetErrorString(ce));
+        }
+        c->stream = saved;
+        e->epochs[i] = c->epoch;
+    }
+    cudaGraph_t g = nullptr;
+    ce = cudaStreamEndCapture(e->master, &g);
+    if (st != CFD_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (ce != cudaSuccess) return efail(e, CFD_ERR_CUDA, "ensemble capture: %s", cudaGetErrorString(ce));
+    e->graph = g;
+    ECK(cudaGraphInstantiate(&e->gexec, e->graph, 0));
+    return CFD_OK;
+}
+}  // namespace
+
+int cfd_ensemble_create(cfd_ctx* const* members, int32_t n, cfd_ensemble** out) {
+    if (!out) return CFD_ERR_ARG;
+    *out = nullptr;
+    cfd_ensemble* e = new cfd_ensemble();
+    *out = e;  // returned even on failure so cfd_ensemble_last_error can report
+    if (!members || n <= 0) return efail(e, CFD_ERR_ARG, "need at least one member");
+    for (int i = 0; i < n; ++i) {
+        if (!members[i]) return efail(e, CFD_ERR_ARG, "member %d is NULL", i);
+        for (int k = 0; k < i; ++k)
+            if (members[k] == members[i]) return efail(e, CFD_ERR_ARG, "member %d repeated", i);
+        if (members[i]->device != members[0]->device)
+            return efail(e, CFD_ERR_ARG, "member %d is on device %d, member 0 on %d", i, members[i]->device,
+                         members[0]->device);
+        e->m.push_back(members[i]);
+    }
+    e->device = members[0]->device;
+    ECK(cudaSetDevice(e->device));
+    ECK(cudaStreamCreateWithFlags(&e->master, cudaStreamNonBlocking));
+    ECK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+    ECK(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
+    e->streams.assign(n, nullptr);
+    e->pre.assign(n, nullptr);
+    e->join.assign(n, nullptr);
+    e->epochs.assign(n, -1);
+    for (int i = 0; i < n; ++i) {
+        ECK(cudaStreamCreateWithFlags(&e->streams[i], cudaStreamNonBlocking));
+        ECK(cudaEventCreateWithFlags(&e->pre[i], cudaEventDisableTiming));
+        ECK(cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming));
+    }
+    return CFD_OK;
+}
+
+int cfd_ensemble_step(cfd_ensemble* e, int32_t nsteps) {
+    if (!e) return CFD_ERR_ARG;
+    if (nsteps < 0) return efail(e, CFD_ERR_ARG, "nsteps < 0");
+    ECK(cudaSetDevice(e->device));
+    bool stale = !e->gexec;
+    for (size_t i = 0; i < e->m.size(); ++i) {
+        if (!e->m[i]->state_loaded) return efail(e, CFD_ERR_STATE, "member %zu has no state", i);
+        if (e->m[i]->epoch != e->epochs[i]) stale = true;
+    }
+    // the members' pending work comes first
+    for (size_t i = 0; i < e->m.size(); ++i) {
+        ECK(cudaEventRecord(e->pre[i], e->m[i]->stream));
+        ECK(cudaStreamWaitEvent(e->master, e->pre[i], 0));
+    }
+    if (stale) {
+        int st = ens_capture(e);
+        if (st != CFD_OK) return st;
+    }
+    for (int k = 0; k < nsteps; ++k) ECK(cudaGraphLaunch(e->gexec, e->master));
+    // later work on a member's stream waits for the ensemble
+    ECK(cudaEventRecord(e->done, e->master));
+    for (cfd_ctx* c : e->m) ECK(cudaStreamWaitEvent(c->stream, e->done, 0));
+    return CFD_OK;
+}
+
+int cfd_ensemble_synchronize(cfd_ensemble* e) {
+    if (!e) return CFD_ERR_ARG;
+    ECK(cudaStreamSynchronize(e->master));
+    return CFD_OK;
+}
+
+int cfd_ensemble_stream(cfd_ensemble* e, void** stream) {
+    if (!e || !stream) return CFD_ERR_ARG;
+    *stream = (void*)e->master;
+    return CFD_OK;
+}
+
+const char* cfd_ensemble_last_error(const cfd_ensemble* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int cfd_ensemble_destroy(cfd_ensemble* e) {
+    if (!e) return CFD_OK;
+    cudaSetDevice(e->device);
+    if (e->master) cudaStreamSynchronize(e->master);
+    ens_release_graph(e);
+    for (cudaStream_t s : e->streams) if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t v : e->pre) if (v) cudaEventDestroy(v);
+    for (cudaEvent_t v : e->join) if (v) cudaEventDestroy(v);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->done) cudaEventDestroy(e->done);
+    if (e->master) cudaStreamDestroy(e->master);
+    delete e;
+    return CFD_OK;
+}
+
 int cfd_set_dt(cfd_ctx* c, double dt) {
     if (!c) return CFD_ERR_ARG;
     if (!(dt > 0) || !std::isfinite(dt)) return fail(c, CFD_ERR_ARG, "dt must be positive and finite");
     CK(cudaStreamSynchronize(c->stream));
     c->dt = dt;
+    c->epoch++;
     destroy_graph(c);
     return factor_all(c);
 }

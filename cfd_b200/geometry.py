@@ -142,13 +142,40 @@ def _nearest_divisor(n: int, target: float, even: bool) -> int:
     return min(divs, key=lambda d: (abs(d - target), d))
 
 
+def _fits(n: int, r: float, c: float) -> bool:
+    """The circle and its interpolation stencil (one point beyond it) stay in the tile."""
+    return math.floor(c - r - 1) >= 1 and math.ceil(c + r + 1) <= n
+
+
 def lattice_params(cfg):
-    """Tile counts and circle of the cylinder lattice of a ChannelConfig."""
-    ntilex = _nearest_divisor(cfg.ngal1, cfg.lx / cfg.cyl_spacing, even=True)
-    ntilez = _nearest_divisor(cfg.ngal2, cfg.lz / cfg.cyl_spacing, even=False)
-    dnx, dnz = cfg.ngal1 // ntilex, cfg.ngal2 // ntilez
+    """Tile counts and circle of the cylinder lattice of a ChannelConfig.  The counts are the
+    valid divisors nearest to Lx/spacing, Lz/spacing; where a tile that small cannot hold a
+    resolved circle with its stencil, the count drops to the next divisor that can (the
+    reference stops there instead, geom_circ_rough_mixed_forcing_24pt.f90:81-92, 132-140)."""
     dx, dz = cfg.lx / cfg.ngal1, cfg.lz / cfg.ngal2
     r = 0.5 * cfg.cyl_diameter / math.sqrt(dx * dz)
+    ntilex = _nearest_divisor(cfg.ngal1, cfg.lx / cfg.cyl_spacing, even=True)
+    ntilez = _nearest_divisor(cfg.ngal2, cfg.lz / cfg.cyl_spacing, even=False)
+
+    def resolved(dnx, dnz):
+        ci, ck = (dnx + 1) / 2.0, (dnz + 1) / 2.0
+        return any(_circ(i, k, r, ci, ck) < 0 for k in range(math.floor(ck - r), math.ceil(ck + r) + 1)
+                   for i in range(math.floor(ci - r), math.ceil(ci + r) + 1))
+
+    def smaller(n, cur, even):
+        divs = [d for d in range(1, cur) if n % d == 0 and (not even or d % 2 == 0)]
+        return max(divs) if divs else cur
+
+    while True:
+        dnx, dnz = cfg.ngal1 // ntilex, cfg.ngal2 // ntilez
+        ci, ck = (dnx + 1) / 2.0, (dnz + 1) / 2.0
+        if not resolved(dnx, dnz) or (_fits(dnx, r, ci) and _fits(dnz, r, ck)):
+            break
+        nx = ntilex if _fits(dnx, r, ci) else smaller(cfg.ngal1, ntilex, True)
+        nz = ntilez if _fits(dnz, r, ck) else smaller(cfg.ngal2, ntilez, False)
+        if (nx, nz) == (ntilex, ntilez):
+            break
+        ntilex, ntilez = nx, nz
     return ntilex, ntilez, dnx, dnz, r, (dnx + 1) / 2.0, (dnz + 1) / 2.0
 
 

@@ -246,6 +246,26 @@ int cfd_cfl(cfd_ctx *ctx, double *dtc, double *terms);
  * cfd_step. */
 int cfd_set_dt(cfd_ctx *ctx, double dt);
 
+/* ---- batched ensemble -------------------------------------------------------------- */
+
+/* No counterpart in the reference, which runs one channel per MPI job.  An ensemble
+ * advances several independent contexts of one device together: their RK3 steps (of any
+ * sizes, IB geometries and precisions) are captured as parallel branches of one CUDA graph,
+ * so one graph launch per step advances every member and small members share the GPU.
+ * Members stay owned by the caller (upload and download through their own entry points);
+ * each must hold a state before the first cfd_ensemble_step.  Work issued on a member's
+ * stream before cfd_ensemble_step completes before the ensemble step starts, and work
+ * issued after it waits for it.  A member whose dt or stream changes (cfd_set_dt,
+ * cfd_set_stream) is captured again at the next step. */
+typedef struct cfd_ensemble cfd_ensemble;
+int cfd_ensemble_create(cfd_ctx *const *members, int32_t nmembers, cfd_ensemble **out);
+int cfd_ensemble_step(cfd_ensemble *ens, int32_t nsteps);
+int cfd_ensemble_synchronize(cfd_ensemble *ens);
+/* The stream the ensemble's graph is launched on (to order or time work around it). */
+int cfd_ensemble_stream(cfd_ensemble *ens, void **stream);
+const char *cfd_ensemble_last_error(const cfd_ensemble *ens);
+int cfd_ensemble_destroy(cfd_ensemble *ens);
+
 /* ---- allocation-free solve ----------------------------------------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc/cudaFree: a
