@@ -252,7 +252,7 @@ def profile_error(chans, setup, nsteps):
     return out
 
 
-def run_ensemble(torch, device, nsteps, warmup):
+def run_ensemble(torch, device, nsteps, warmup, tuning):
     """The 16-member batched ensemble (4 x 96x97x96, 8 x 128x129x128, 4 x 192x161x192, own
     seeds and cylinder diameters) in both precisions: RK3 steps/s of the whole ensemble with
     one graph launch per step (device time on the ensemble's stream), and the same members
@@ -263,7 +263,7 @@ def run_ensemble(torch, device, nsteps, warmup):
                                       "4 x 192x161x192 Re_tau 395; D ~ U[0.03, 0.06] h, spacing 4 D"}
     for prec in ("mixed", "fp64"):
         cfgs = ensemble_configs(precision=prec)
-        ens = Ensemble.from_configs(cfgs, device=device.index or 0)
+        ens = Ensemble.from_configs(cfgs, device=device.index or 0, tuning=tuning)
         gp = sum(c.ngal1 * c.ngal2 * m.setup.grid.nyv for c, m in zip(cfgs, ens.members))
         ens.step(warmup)
         ens.synchronize()
@@ -366,6 +366,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--error-steps", type=int, default=10)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")
+    ap.add_argument("--no-autotune", action="store_true", help="library default launch shapes")
     ap.add_argument("--profile-steps", type=int, default=20,
                     help="steps of the mean/rms profile comparison of mixed vs FP64 (0: skip)")
     args = ap.parse_args()
@@ -388,8 +389,10 @@ def main():
     stream = torch.cuda.Stream(device)
     results = {}
     chans = {}
+    tuning = {}
     for prec in ("mixed", "fp64"):
-        ch = Channel(setup, device=local, precision=prec)
+        ch = Channel(setup, device=local, precision=prec, tuning=None if args.no_autotune else "auto")
+        tuning[prec] = ch.tuning()
         ch.set_stream(stream.cuda_stream)
         ch.upload_state()
         ch.step(args.warmup)
@@ -411,7 +414,8 @@ def main():
         err[k] = rel_err(states["mixed"][k], states["fp64"][k])
     fp64_div = chans["fp64"].divergence_max()
     prof_err = profile_error(chans, setup, args.profile_steps)
-    ens = run_ensemble(torch, device, args.steps, args.warmup) if (ws == 1 and not args.no_ensemble) else None
+    ens = run_ensemble(torch, device, args.steps, args.warmup, None if args.no_autotune else "auto") \
+        if (ws == 1 and not args.no_ensemble) else None
 
     # per-kernel timing (CUDA events on the launching stream) for the roofline
     hbm, peak_kind = peaks()
@@ -490,6 +494,8 @@ def main():
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
         "profile_error_mixed_vs_fp64": prof_err,
         "ensemble": ens,
+        "tuning": {"source": "defaults" if args.no_autotune else "cfd_b200.autotune (coordinate search, cached)",
+                   **tuning},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
                      "traffic": ncu_traffic(args.config, kname), "traffic_source":

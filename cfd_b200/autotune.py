@@ -1,0 +1,114 @@
+"""Autotuner of the launch shapes (cfd_tuning): for one grid, precision and GPU it builds a
+context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
+
+Candidates: the x-line path (register two-step or shared-memory Stockham), rows per CTA of
+the two-step x-line kernel, lines per CTA of the two-step z kernels, and the solve kind
+(thread-per-column sweeps or warp-per-column substitutions, with 4 or 8 columns per CTA).
+The search is coordinate-wise from the library default, one knob at a time, so it costs a
+dozen short timings.  Results are cached in a JSON file keyed by grid, precision and GPU
+name (CFD_TUNE_CACHE, default ~/.cache/cfd_b200/tuning.json).
+"""
+from __future__ import annotations
+
+import json
+import os
+
+KNOBS = (("xline_path", (1, 2)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
+         ("solve_kind", (1, 2)), ("solve_cols", (4, 8)))
+
+
+def _cache_path() -> str:
+    return os.environ.get("CFD_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "cfd_b200",
+                                                          "tuning.json"))
+
+
+def _key(setup, precision: str, gpu: str) -> str:
+    c, g = setup.cfg, setup.grid
+    return f"{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+
+
+def time_step(setup, precision, device, tuning, steps=5, warmup=2):
+    """Seconds per RK3 step of one context with the given launch shapes (CUDA events)."""
+    import torch
+    from .channel import Channel
+    ch = Channel(setup, device=device, precision=precision, tuning=tuning)
+    try:
+        ch.upload_state()
+        ch.step(warmup)
+        stream = torch.cuda.Stream(device)
+        ch.set_stream(stream.cuda_stream)
+        ch.step(1)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        ch.step(steps)
+        e.record(stream)
+        e.synchronize()
+        return s.elapsed_time(e) / 1e3 / steps, ch.tuning()
+    finally:
+        ch.close()
+
+
+def autotune(setup, precision: str, device: int = 0, steps: int = 5, log=None):
+    """Coordinate search over KNOBS from the default shapes; returns (best tuning, seconds)."""
+    best_t, best = time_step(setup, precision, device, None, steps)
+    tried = {json.dumps(best, sort_keys=True)}
+    for name, values in KNOBS:
+        for v in values:
+            cand = dict(best, **{name: v})
+            k = json.dumps(cand, sort_keys=True)
+            if k in tried:
+                continue
+            tried.add(k)
+            try:
+                t, eff = time_step(setup, precision, device, cand, steps)
+            except RuntimeError as err:  # a shape the grid cannot take
+                if log:
+                    log(f"skip {cand}: {err}")
+                continue
+            tried.add(json.dumps(eff, sort_keys=True))
+            if log:
+                log(f"{eff} {t * 1e3:.3f} ms/step")
+            if t < best_t:
+                best_t, best = t, eff
+    return best, best_t
+
+
+def tuned(setup, precision: str, device: int = 0):
+    """The cached tuning of this grid, precision and GPU, measured (and cached) if absent."""
+    import torch
+    gpu = torch.cuda.get_device_name(device)
+    key = _key(setup, precision, gpu)
+    path = _cache_path()
+    cache = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            cache = json.load(f)
+    if key not in cache:
+        best, t = autotune(setup, precision, device)
+        cache[key] = {"tuning": best, "ms_per_step": t * 1e3}
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = f"{path}.{os.getpid()}"
+        with open(tmp, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)  # atomic: concurrent processes never see a partial file
+    return cache[key]["tuning"]
+
+
+def main(argv=None):
+    import argparse
+    from .channel import build_channel
+    from .config import preset
+    ap = argparse.ArgumentParser(prog="python -m cfd_b200.autotune")
+    ap.add_argument("--config", default="re550")
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"])
+    ap.add_argument("--steps", type=int, default=5)
+    a = ap.parse_args(argv)
+    cfg = preset(a.config)
+    prec = a.precision or cfg.precision
+    setup = build_channel(cfg)
+    best, t = autotune(setup, prec, 0, a.steps, log=print)
+    print(json.dumps({"config": a.config, "precision": prec, "tuning": best, "ms_per_step": t * 1e3}))
+
+
+if __name__ == "__main__":
+    main()

@@ -38,6 +38,14 @@ class CfdIBList(C.Structure):
                 ("jlo", C.c_int32 * 2), ("jhi", C.c_int32 * 2)]
 
 
+class CfdTuning(C.Structure):
+    _fields_ = [("xline_path", C.c_int32), ("xline_rows", C.c_int32), ("zlines", C.c_int32),
+                ("solve_kind", C.c_int32), ("solve_cols", C.c_int32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class CfdStatsConfig(C.Structure):
     _fields_ = [("jband", C.c_int32), ("dnx", C.c_int32), ("dnz", C.c_int32)]
 
@@ -114,6 +122,9 @@ _VP = C.c_void_p
 SIGNATURES = {
     "cfd_create": (C.c_int, [C.POINTER(CfdConfig), C.POINTER(CfdIBList), C.POINTER(CfdIBList),
                              C.c_int32, C.POINTER(_VP)]),
+    "cfd_create_tuned": (C.c_int, [C.POINTER(CfdConfig), C.POINTER(CfdIBList), C.POINTER(CfdIBList),
+                                   C.c_int32, C.POINTER(CfdTuning), C.POINTER(_VP)]),
+    "cfd_get_tuning": (C.c_int, [_VP, C.POINTER(CfdTuning)]),
     "cfd_destroy": (C.c_int, [_VP]),
     "cfd_last_error": (C.c_char_p, [_VP]),
     "cfd_set_stream": (C.c_int, [_VP, _VP]),

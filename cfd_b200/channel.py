@@ -67,18 +67,26 @@ def field_planes(setup: ChannelSetup, name: str) -> int:
 class Channel:
     """One channel on one GPU, driven through the C ABI."""
 
-    def __init__(self, setup: ChannelSetup, device: int = 0, precision: Optional[str] = None):
+    def __init__(self, setup: ChannelSetup, device: int = 0, precision: Optional[str] = None,
+                 tuning=None):
+        """tuning: None (library defaults), a dict of cfd_tuning fields, or "auto" (the
+        cached or freshly measured choice of cfd_b200.autotune for this grid and GPU)."""
         self.setup = setup
         self.lib = capi.load()
         self._keep = []
         cfg = setup.cfg if precision is None else setup.cfg.with_(precision=precision)
         self.cfg = cfg
+        if tuning == "auto":
+            from .autotune import tuned
+            tuning = tuned(setup, cfg.precision, device)
         c = capi.make_config(cfg, setup.grid, setup.dt, self._keep)
         ibu = capi.make_iblist(setup.ibu, self._keep)
         ibv = capi.make_iblist(setup.ibv, self._keep)
         ctx = C.c_void_p()
-        st = self.lib.cfd_create(C.byref(c), C.byref(ibu) if ibu else None,
-                                 C.byref(ibv) if ibv else None, device, C.byref(ctx))
+        tun = capi.CfdTuning(**tuning) if tuning else None
+        st = self.lib.cfd_create_tuned(C.byref(c), C.byref(ibu) if ibu else None,
+                                       C.byref(ibv) if ibv else None, device,
+                                       C.byref(tun) if tun else None, C.byref(ctx))
         if st != capi.CFD_OK:
             msg = self.lib.cfd_last_error(ctx).decode() if ctx else ""
             if ctx:
@@ -200,6 +208,12 @@ class Channel:
         t = np.zeros(3)
         self._chk(self.lib.cfd_cfl(self.ctx, C.byref(dtc), t.ctypes.data), "cfl")
         return dtc.value, t
+
+    def tuning(self) -> dict:
+        """Launch shapes this context runs with (cfd_get_tuning)."""
+        t = capi.CfdTuning()
+        self._chk(self.lib.cfd_get_tuning(self.ctx, C.byref(t)), "get_tuning")
+        return t.as_dict()
 
     def set_dt(self, dt: float):
         """New time step for the following stages and steps (the graph is captured again)."""

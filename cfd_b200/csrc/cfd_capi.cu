@@ -250,7 +250,7 @@ int ilog2(int b) {
     }
 
 // shared memory of k_xline2 (elements): B*LX + N
-// Launch-shape overrides for tuning runs (unset: the built-in choice).
+// Launch-shape overrides (unset: the built-in choice; a cfd_tuning field takes precedence).
 //   CFD_XLINE_ROWS   rows per CTA of the two-step x-line kernel (power of two, 2..8)
 //   CFD_ZLINES_LOG2  log2 of the lines per CTA of the two-step z kernels (2..4)
 //   CFD_XLINE_STOCKHAM 1: nonlinear through the Stockham x-line kernel and per-slot z pass
@@ -261,6 +261,14 @@ int env_int(const char* name, int dflt, int lo, int hi) {
     if (!v || !*v) return dflt;
     const int x = std::atoi(v);
     return (x >= lo && x <= hi) ? x : dflt;
+}
+
+// explicit launch shapes of cfd_create_tuned (a zero field: environment, then default)
+thread_local const cfd_tuning* g_tuning = nullptr;
+int tune_int(int32_t cfd_tuning::*field, const char* env, int dflt, int lo, int hi) {
+    if (g_tuning && g_tuning->*field >= lo && g_tuning->*field <= hi && g_tuning->*field != 0)
+        return g_tuning->*field;
+    return env_int(env, dflt, lo, hi);
 }
 
 size_t xline2_smem(int n1s, int n2s, int rw, size_t esz) {
@@ -860,7 +868,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
-            int rw = env_int("CFD_XLINE_ROWS", mixed ? 8 : 4, 2, 8);
+            int rw = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", mixed ? 8 : 4, 2, 8);
+            rw = 1 << (31 - __builtin_clz(rw));  // a power of two
             while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
             if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
                 c->RW2 = rw;
@@ -869,13 +878,15 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
             }
         }
     }
-    if (env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)) c->RW2 = 0;
+    if ((g_tuning && g_tuning->xline_path == 2) || (!(g_tuning && g_tuning->xline_path == 1) && env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)))
+        c->RW2 = 0;
     {
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal2, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
-            const int lb = env_int("CFD_ZLINES_LOG2", mixed ? 4 : 3, 2, 4);
+            const int zl = g_tuning && (g_tuning->zlines == 4 || g_tuning->zlines == 8 || g_tuning->zlines == 16) ? g_tuning->zlines : 0;
+            const int lb = zl ? ilog2(zl) : env_int("CFD_ZLINES_LOG2", mixed ? 4 : 3, 2, 4);
             c->LZ2 = lb;
             c->NTZ2 = (1 << lb) * std::max(n1s, n2s);
             c->SMZ2 = ((size_t)(1 << lb) * ((n1s * (n2s + 1)) | 1) + (size_t)n1s * n2s) * esz;
@@ -887,8 +898,10 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         const int m = (d.nyu + 31) / 32;
         c->SWM = m <= 4 ? 4 : (m <= 8 ? 8 : (m <= 12 ? 12 : (m <= 16 ? 16 : 0)));
         // measured at re550: 482 us per launch against 400 us for the thread-per-column sweep
-        if (!env_int("CFD_SOLVE_WARP", 0, 0, 1)) c->SWM = 0;
-        c->SWC = 1 << ilog2(env_int("CFD_SOLVE_COLS", 8, 1, 8));
+        const int sk = g_tuning && (g_tuning->solve_kind == 1 || g_tuning->solve_kind == 2) ? g_tuning->solve_kind
+                                                                                        : (env_int("CFD_SOLVE_WARP", 0, 0, 1) ? 2 : 1);
+        if (sk != 2) c->SWM = 0;
+        c->SWC = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_COLS", 8, 1, 8));
         while (c->SWC > 1 && solve_w_smem(d, c->SWC) > 110 * 1024) c->SWC /= 2;
         const int sm = (int)solve_w_smem(d, c->SWC);
         cudaError_t e = cudaSuccess;
@@ -1144,6 +1157,24 @@ int cfd_create(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list*
     int s = create_impl(cfg, ibu, ibv, device, c);
     *out = c;  // returned even on failure so cfd_last_error can report; caller destroys
     return s;
+}
+
+int cfd_create_tuned(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list* ibv, int32_t device,
+                     const cfd_tuning* tuning, cfd_ctx** out) {
+    g_tuning = tuning;
+    const int s = cfd_create(cfg, ibu, ibv, device, out);
+    g_tuning = nullptr;
+    return s;
+}
+
+int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
+    if (!c || !t) return CFD_ERR_ARG;
+    t->xline_path = c->RW2 ? 1 : 2;
+    t->xline_rows = c->RW2 ? c->RW2 : 0;
+    t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
+    t->solve_kind = c->SWM ? 2 : 1;
+    t->solve_cols = c->SWM ? c->SWC : 0;
+    return CFD_OK;
 }
 
 int cfd_destroy(cfd_ctx* c) {

@@ -26,10 +26,11 @@ class Ensemble:
             raise capi.CfdError(f"ensemble_create: {capi.ERRORS.get(st, st)}: {msg.decode() if msg else ''}")
 
     @classmethod
-    def from_configs(cls, cfgs, device: int = 0):
+    def from_configs(cls, cfgs, device: int = 0, tuning=None):
+        """Members from ChannelConfigs (tuning as for Channel, e.g. "auto")."""
         chans = []
         for cfg in cfgs:
-            ch = Channel(build_channel(cfg), device=device, precision=cfg.precision)
+            ch = Channel(build_channel(cfg), device=device, precision=cfg.precision, tuning=tuning)
             ch.upload_state()
             chans.append(ch)
         return cls(chans)

@@ -120,6 +120,25 @@ int cfd_create(const cfd_config *cfg, const cfd_ib_list *ibu, const cfd_ib_list 
 int cfd_destroy(cfd_ctx *ctx);
 const char *cfd_last_error(const cfd_ctx *ctx);
 
+/* Launch shapes of the kernels (no counterpart in the reference).  A zero field keeps the
+ * library's choice (or the CFD_* environment override of the same name); cfd_b200/autotune.py
+ * picks them by timing the candidates on the device.
+ *   xline_path   1: register two-step x-line kernel with one z transform per field plane,
+ *                2: shared-memory Stockham x-line kernel with the per-slot z pass
+ *   xline_rows   rows per CTA of the two-step x-line kernel: 2, 4 or 8
+ *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
+ *   solve_kind   1: thread-per-column Thomas sweeps, 2: warp-per-column substitutions on
+ *                LU factors precomputed per time step
+ *   solve_cols   columns (warps) per CTA of the warp-per-column solve: 1, 2, 4 or 8 */
+typedef struct cfd_tuning {
+    int32_t xline_path, xline_rows, zlines, solve_kind, solve_cols;
+} cfd_tuning;
+/* cfd_create with explicit launch shapes (tuning may be NULL: as cfd_create). */
+int cfd_create_tuned(const cfd_config *cfg, const cfd_ib_list *ibu, const cfd_ib_list *ibv,
+                     int32_t device, const cfd_tuning *tuning, cfd_ctx **out);
+/* The launch shapes a context runs with (every field filled in). */
+int cfd_get_tuning(const cfd_ctx *ctx, cfd_tuning *tuning);
+
 /* Work on a caller-provided cudaStream_t (NULL = the context's own stream). */
 int cfd_set_stream(cfd_ctx *ctx, void *stream);
 int cfd_synchronize(cfd_ctx *ctx);
