@@ -921,7 +921,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         if (ok) {
             const int N = n1s * n2s, L1 = (n1s * (n2s + 1)) | 1, mx = std::max(n1s, n2s);
             for (int rw = 8; rw >= 1; rw /= 2) {
-                const size_t sm = ((size_t)N + 2 * rw * d.nkx + (size_t)rw * L1) * esz;
+                const size_t sm = ((size_t)N + (size_t)rw * L1) * esz;
                 if (d.ngal2 % rw == 0 && sm <= budget && rw * mx <= 1024) { c->RWIX2 = rw; c->SMIX2 = sm; c->NTIX2 = rw * mx; break; }
             }
             for (int rw = 16; rw >= 2; rw /= 2) {

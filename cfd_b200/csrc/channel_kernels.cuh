@@ -596,7 +596,7 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
 // planes gives the transform of the interpolated planes (FOU3D.f90:261-308).
 // grid: x = line chunk (line = plane * nkx + kx), y = field (u, w, v).
 template <typename T2, int TN1, int TN2>
-__global__ void k_zinv2s(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
+__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zinv2s(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
                          const double2* __restrict__ u3, T2* __restrict__ Hx, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
@@ -629,7 +629,7 @@ __global__ void k_zinv2s(Dims d, const double2* __restrict__ u1, const double2* 
 
 // Pass 3: grid x = line chunk, y = field 0..3, z = group (v-planes carry fields 0, 1 only).
 template <typename T2, int TN1, int TN2>
-__global__ void k_zfwd2(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
+__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zfwd2(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
                         const T2* __restrict__ H3, T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
                         T2* __restrict__ S3, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
@@ -1029,31 +1029,34 @@ __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype
                            const T2* __restrict__ twx, int RW) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
+    constexpr int HX = N / 3;   // highest retained kx (N1 = 2*(Ngal1/3))
+    constexpr int NK = HX + 1;  // kx columns per row (= d.nkx)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* twt = reinterpret_cast<T2*>(smem_raw);
-    T2* stg = twt + N;                       // [RW][2][nk]
-    T2* ex = stg + (size_t)RW * 2 * d.nkx;
+    T2* ex = twt + N;
     load_twiddles<T2, TN1, TN2>(twt, twx);
     const int z0 = blockIdx.x * RW, p = blockIdx.y, fb = blockIdx.z;
-    const int nk = d.nkx, h = d.n1 / 2;
-    const size_t pl = (size_t)d.ngal2 * nk;
-    const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl;
-    const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl;
-    for (int t = threadIdx.x; t < 2 * RW * nk; t += blockDim.x) {
-        const int rf = t / nk, k = t - rf * nk;
-        const int rr = rf >> 1, which = rf & 1;
-        stg[t] = (which == 0 ? Hr : Hu)[(size_t)(z0 + rr) * nk + k];
-    }
+    const size_t pl = (size_t)d.ngal2 * NK;
+    const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl + (size_t)z0 * NK;
+    const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl + (size_t)z0 * NK;
+    // this thread's offset within its stride-TN2 subsequence, computed as two_step_lines
+    // does, so that e - n2 is a compile-time constant in the unrolled element loop
+    const int tt = threadIdx.x;
+    const int n2me = tt - (tt / TN2) * TN2;
     __syncthreads();
+    // rows are read straight from global memory (consecutive threads, consecutive kx)
     auto load = [&](int e, int b) -> T2 {
-        const T2* A = stg + (size_t)(2 * b) * nk;
-        const T2* C = A + nk;
-        if (e <= h) {
+        const int e0 = e - n2me;
+        const bool lo = (e0 + TN2 - 1 <= HX) || (e0 <= HX && e <= HX);
+        const bool hi = (e0 >= N - HX) || (e0 + TN2 - 1 >= N - HX && e >= N - HX);
+        const T2* A = Hr + (size_t)b * NK;
+        const T2* C = Hu + (size_t)b * NK;
+        if (lo) {
             T2 a = A[e], c = C[e];
             if (e == 0) { a.y = 0; c.y = 0; }
             return cx<T2>(a.x - c.y, a.y + c.x);
         }
-        if (e >= N - h) {
+        if (hi) {
             const T2 a = A[N - e], c = C[N - e];
             return cx<T2>(a.x + c.y, -a.y + c.x);
         }
