@@ -994,7 +994,7 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
 
 // IB round trip with the two-step transform (same data flow as k_ib_zinv/xinv/xfwd/zfwd).
 template <typename T2, int TN1, int TN2>
-__global__ void k_ib_zinv2(Dims d, IBSrc src, int j0, const int* __restrict__ planes, int npl, T2* __restrict__ Hib,
+__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_ib_zinv2(Dims d, IBSrc src, int j0, const int* __restrict__ planes, int npl, T2* __restrict__ Hib,
                            const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
@@ -1093,24 +1093,22 @@ __global__ void k_ib_xfwd2(Dims d, T2* __restrict__ Hib, int npl, const decltype
     auto store = [&](int k, int b, T2 v) { ub[(size_t)b * LU + k] = v; };
     two_step_lines<T2, TN1, TN2, -1, false>(0, ex, twt, load, store, nl);
     const R hs = (R)0.5 / (R)N;
-    const int nk = d.nkx;
-    T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)d.ngal2 * nk;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int b = warp; b < nl; b += nwarp) {
+    constexpr int NK = N / 3 + 1;  // kx columns per row (= d.nkx)
+    T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * (size_t)d.ngal2 * NK;
+    // work items (line, k) flattened so that no lane idles on a partial last chunk
+    for (int it = threadIdx.x; it < nl * NK; it += blockDim.x) {
+        const int b = (unsigned)it / NK, k = it - b * NK;
         const T2* line = ub + (size_t)b * LU;
-        T2* o0 = Hr + (size_t)(z0 + 2 * b) * nk;
-        T2* o1 = o0 + nk;
-        for (int k = lane; k < nk; k += 32) {
-            const T2 Pk = line[k];
-            const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
-            o0[k] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
-            o1[k] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
-        }
+        T2* o0 = Hr + (size_t)(z0 + 2 * b) * NK + k;
+        const T2 Pk = line[k];
+        const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
+        o0[0] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+        o0[NK] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
     }
 }
 
 template <typename T2, int TN1, int TN2>
-__global__ void k_ib_zfwd2(Dims d, const T2* __restrict__ Hib, int npl, IBDst dst, int j0,
+__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_ib_zfwd2(Dims d, const T2* __restrict__ Hib, int npl, IBDst dst, int j0,
                            const int* __restrict__ planes, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
