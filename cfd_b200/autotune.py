@@ -3,7 +3,8 @@ context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
 
 Candidates: the x-line path (register two-step or shared-memory Stockham), rows per CTA of
 the two-step x-line kernel, lines per CTA of the two-step z kernels, and the solve kind
-(thread-per-column sweeps or warp-per-column substitutions, with 4 or 8 columns per CTA).
+(thread-per-column sweeps or warp-per-column substitutions, with 4 or 8 columns per CTA),
+and the y-planes per thread of the right-hand-side kernel.
 The search is coordinate-wise from the library default, one knob at a time, so it costs a
 dozen short timings.  Results are cached in a JSON file keyed by grid, precision and GPU
 name (CFD_TUNE_CACHE, default ~/.cache/cfd_b200/tuning.json).
@@ -14,7 +15,7 @@ import json
 import os
 
 KNOBS = (("xline_path", (1, 2)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
-         ("solve_kind", (1, 2)), ("solve_cols", (4, 8)))
+         ("solve_kind", (1, 2)), ("solve_cols", (4, 8)), ("rhs_chunk", (2, 4, 8, 16)))
 
 
 def _cache_path() -> str:
@@ -24,7 +25,7 @@ def _cache_path() -> str:
 
 def _key(setup, precision: str, gpu: str) -> str:
     c, g = setup.cfg, setup.grid
-    return f"{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+    return f"v2|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
 
 
 def time_step(setup, precision, device, tuning, steps=5, warmup=2):

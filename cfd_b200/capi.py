@@ -40,7 +40,7 @@ class CfdIBList(C.Structure):
 
 class CfdTuning(C.Structure):
     _fields_ = [("xline_path", C.c_int32), ("xline_rows", C.c_int32), ("zlines", C.c_int32),
-                ("solve_kind", C.c_int32), ("solve_cols", C.c_int32)]
+                ("solve_kind", C.c_int32), ("solve_cols", C.c_int32), ("rhs_chunk", C.c_int32)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

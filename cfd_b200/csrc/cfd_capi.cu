@@ -256,6 +256,7 @@ int ilog2(int b) {
 //   CFD_XLINE_STOCKHAM 1: nonlinear through the Stockham x-line kernel and per-slot z pass
 //   CFD_SOLVE_WARP   1: Helmholtz solves one warp per column on precomputed LU factors
 //   CFD_SOLVE_COLS   columns (warps) per CTA of the warp-per-column solve (1..8)
+//   CFD_RHS_CHUNK    y-planes per thread of the right-hand-side kernel (2..64)
 int env_int(const char* name, int dflt, int lo, int hi) {
     const char* v = std::getenv(name);
     if (!v || !*v) return dflt;
@@ -961,7 +962,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         AL(c->ed_uw, double2, 3 * nc * nyu);
         AL(c->ed_v, double2, 3 * nc * nyv);
     }
-    c->JC = 16;
+    c->JC = tune_int(&cfd_tuning::rhs_chunk, "CFD_RHS_CHUNK", 4, 2, 64);
     c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;
     AL(c->scal, double, 4);
     AL(c->mf_work, double, 4 * (size_t)(cfg->ny + 4));
@@ -1174,6 +1175,7 @@ int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
     t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
     t->solve_kind = c->SWM ? 2 : 1;
     t->solve_cols = c->SWM ? c->SWC : 0;
+    t->rhs_chunk = c->JC;
     return CFD_OK;
 }
 

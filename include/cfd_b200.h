@@ -129,9 +129,10 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
  *   solve_kind   1: thread-per-column Thomas sweeps, 2: warp-per-column substitutions on
  *                LU factors precomputed per time step
- *   solve_cols   columns (warps) per CTA of the warp-per-column solve: 1, 2, 4 or 8 */
+ *   solve_cols   columns (warps) per CTA of the warp-per-column solve: 1, 2, 4 or 8
+ *   rhs_chunk    y-planes per thread of the right-hand-side kernel: 2 .. 64 */
 typedef struct cfd_tuning {
-    int32_t xline_path, xline_rows, zlines, solve_kind, solve_cols;
+    int32_t xline_path, xline_rows, zlines, solve_kind, solve_cols, rhs_chunk;
 } cfd_tuning;
 /* cfd_create with explicit launch shapes (tuning may be NULL: as cfd_create). */
 int cfd_create_tuned(const cfd_config *cfg, const cfd_ib_list *ibu, const cfd_ib_list *ibv,
