@@ -1,7 +1,7 @@
 """Autotuner of the launch shapes (cfd_tuning): for one grid, precision and GPU it builds a
 context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
 
-Candidates: the x-line path (register two-step or shared-memory Stockham), rows per CTA of
+Candidates: the x-line path (register two-step, its packed form, or shared-memory Stockham), rows per CTA of
 the two-step x-line kernel, lines per CTA of the two-step z kernels, and the solve kind
 (thread-per-column sweeps or warp-per-column substitutions, with 4 or 8 columns per CTA),
 and the y-planes per thread of the right-hand-side kernel.
@@ -14,7 +14,7 @@ from __future__ import annotations
 import json
 import os
 
-KNOBS = (("xline_path", (1, 2)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
+KNOBS = (("xline_path", (1, 2, 3)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
          ("solve_kind", (1, 2)), ("solve_cols", (4, 8)), ("rhs_chunk", (2, 4, 8, 16)))
 
 

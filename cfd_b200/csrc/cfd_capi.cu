@@ -90,7 +90,9 @@ struct cfd_ctx {
     double2 *twx_d = nullptr, *twz_d = nullptr;
     float2 *twx_f = nullptr, *twz_f = nullptr;
     int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
-    int RW2 = 0, NT2 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
+    int RW2 = 0, NT2 = 0;
+    bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
+    size_t SM3 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
     int LZ2 = -1, NTZ2 = 0; // two-step z kernels: log2(columns per CTA) (-1 = not used), threads
     int SWM = 0, SWC = 8;   // warp-per-column solves: rows-per-lane bound (0 = not used), columns per CTA
     double2* ed_uw = nullptr;  // LU factors {e, d} of the u/w and v systems, [RK substep][column][row]
@@ -254,6 +256,7 @@ int ilog2(int b) {
 //   CFD_XLINE_ROWS   rows per CTA of the two-step x-line kernel (power of two, 2..8)
 //   CFD_ZLINES_LOG2  log2 of the lines per CTA of the two-step z kernels (2..4)
 //   CFD_XLINE_STOCKHAM 1: nonlinear through the Stockham x-line kernel and per-slot z pass
+//   CFD_XLINE_PATH   3: packed two-step x-line kernel (1.5 inverse lines per row)
 //   CFD_SOLVE_WARP   1: Helmholtz solves one warp per column on precomputed LU factors
 //   CFD_SOLVE_COLS   columns (warps) per CTA of the warp-per-column solve (1..8)
 //   CFD_RHS_CHUNK    y-planes per thread of the right-hand-side kernel (2..64)
@@ -334,6 +337,8 @@ int set_smem_attrs(cfd_ctx* c) {
         TWO_SWITCH(n1, ok, {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
+            if (e == cudaSuccess && c->XL3)
+                e = cudaFuncSetAttribute(k_xline3<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM3);
         });
     }
     CK(e);
@@ -395,7 +400,16 @@ int nl_transforms(cfd_ctx* c) {
         LK("k_zinv");
     }
     prof_mark(c);
-    if (c->RW2) {
+    if (c->RW2 && c->XL3) {
+        dim3 gx3(d.ngal2 / c->RW2, d.nslot);
+        bool ok = true;
+        TWO_SWITCH(d.ngal1, ok, {
+            k_xline3<T2, TN1, TN2><<<gx3, c->NT2, c->SM3, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0],
+                                                                    (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
+                                                                    twx<T2>(c), c->RW2);
+        });
+        LK("k_xline3");
+    } else if (c->RW2) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
         TWO_SWITCH(d.ngal1, ok, {
@@ -876,10 +890,18 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
                 c->RW2 = rw;
                 c->NT2 = 2 * rw * std::max(n1s, n2s);
                 c->SM2 = xline2_smem(n1s, n2s, rw, esz);
+                // packed lines (k_xline3): twiddles, exchange of 2*rw lines, physical rows /
+                // forward spectra
+                const size_t N = (size_t)n1s * n2s, LX = (size_t)((n1s * (n2s + 1)) | 1);
+                c->SM3 = (N + 2 * rw * LX + std::max((size_t)3 * (rw / 2) * N, (size_t)2 * rw * (N + 1))) * esz;
+                const int xp = g_tuning && g_tuning->xline_path ? g_tuning->xline_path
+                                                                : env_int("CFD_XLINE_PATH", 1, 1, 3);
+                c->XL3 = xp == 3 && c->SM3 <= 220 * 1024;
             }
         }
     }
-    if ((g_tuning && g_tuning->xline_path == 2) || (!(g_tuning && g_tuning->xline_path == 1) && env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)))
+    if ((g_tuning && g_tuning->xline_path == 2) ||
+        (!(g_tuning && (g_tuning->xline_path == 1 || g_tuning->xline_path == 3)) && env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)))
         c->RW2 = 0;
     {
         bool ok = true;
@@ -1170,7 +1192,7 @@ int cfd_create_tuned(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib
 
 int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
     if (!c || !t) return CFD_ERR_ARG;
-    t->xline_path = c->RW2 ? 1 : 2;
+    t->xline_path = c->RW2 ? (c->XL3 ? 3 : 1) : 2;
     t->xline_rows = c->RW2 ? c->RW2 : 0;
     t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
     t->solve_kind = c->SWM ? 2 : 1;

@@ -446,6 +446,154 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
     }
 }
 
+// Pass 2, packed form.  Three real inputs per row take 1.5 complex lines instead of 2: a
+// CTA holds RW rows as RW/2 row pairs (r0, r1) with three inverse lines each
+//   u-plane: u_r0 + i v_r0,  u_r1 + i v_r1,  w_r0 + i w_r1
+//   v-plane: u_r0 + i w_r0,  u_r1 + i w_r1,  v_r0 + i v_r1
+// (v on u-planes and u, w on v-planes y-interpolated as in k_xline2).  The inverse
+// transforms land in shared memory as physical rows; the forward lines are formed from them
+//   u-plane: uu + i vv per row, ww + i uw per row;   v-plane: uv + i vw per row
+// so v-planes run one forward line per row.  Both directions are two_step_lines
+// (element-fastest thread mapping, coalesced x-rows); the unpack writes the products to
+// H0..H3 as k_xline2 does.
+template <typename T2, int N1, int N2>
+__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && (N1 > N2 ? N1 : N2) <= 24) ? 2 : 1)
+    k_xline3(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1,
+             T2* __restrict__ H2, T2* __restrict__ H3, const T2* __restrict__ twx, int RW) {
+    using R = decltype(T2::x);
+    constexpr int N = N1 * N2;
+    constexpr int HX = N / 3, NK = HX + 1;
+    constexpr int LX = exch_row<N1, N2>();
+    constexpr int LU = N + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int NP = RW >> 1, NLI = 3 * NP;
+    T2* twt = reinterpret_cast<T2*>(smem_raw);
+    T2* ex = twt + N;                   // exchange of two_step_lines, 2*RW lines
+    T2* PU = ex + (size_t)2 * RW * LX;  // physical rows [NLI][N], then forward spectra [NLF][LU]
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const int b = i / N2, a = i - b * N2;
+        twt[i] = twx[(a * b) % N];
+    }
+    const int slot = (blockIdx.y & 1) ? d.nyu + (blockIdx.y >> 1) : (blockIdx.y >> 1);
+    const bool uplane = slot < d.nyu;
+    const int z0 = blockIdx.x * RW;
+    const int NLF = uplane ? 4 * NP : 2 * NP;
+    const size_t pls = (size_t)d.ngal2 * NK;
+    // field sources of this slot: value = ca * A[row] + cb * B[row]  (fields U = 0, V = 1, W = 2)
+    const T2* Hu = Hx;
+    const T2* Hw = Hx + (size_t)d.nyu * pls;
+    const T2* Hv = Hx + (size_t)(2 * d.nyu) * pls;
+    const T2 *fa0, *fb0, *fa1, *fb1, *fa2, *fb2;
+    R ca0 = 1, cb0 = 0, ca1 = 1, cb1 = 0, ca2 = 1, cb2 = 0;
+    if (uplane) {
+        const int sl = slot;
+        fa0 = fb0 = Hu + sl * pls;
+        fa2 = fb2 = Hw + sl * pls;
+        double ca, cb;
+        int pa;
+        if (sl == 0) {
+            pa = 1; ca = (1.0 - g.gwib) * g.vca[1]; cb = g.gwib + (1.0 - g.gwib) * g.vcb[1];
+        } else if (sl == d.nyu - 1) {
+            pa = sl - 1; ca = g.gwit + (1.0 - g.gwit) * g.vca[sl - 1]; cb = (1.0 - g.gwit) * g.vcb[sl - 1];
+        } else {
+            pa = sl; ca = g.vca[sl]; cb = g.vcb[sl];
+        }
+        fa1 = Hv + pa * pls; fb1 = fa1 - pls; ca1 = (R)ca; cb1 = (R)cb;
+    } else {
+        const int sl = slot - d.nyu;
+        fa1 = fb1 = Hv + sl * pls;
+        fa0 = Hu + (sl + 1) * pls; fb0 = fa0 - pls; ca0 = (R)g.ufa[sl]; cb0 = (R)g.ufb[sl];
+        fa2 = Hw + (sl + 1) * pls; fb2 = fa2 - pls; ca2 = (R)g.ufa[sl]; cb2 = (R)g.ufb[sl];
+    }
+    __syncthreads();
+
+    // ---- inverse: line b = 3p + t, thread (b, n2) of two_step_lines' step 1
+    const int tt = threadIdx.x;
+    const int bme = tt / N2, n2me = tt - bme * N2;
+    {
+        const int t = bme % 3, p = bme / 3;
+        const int r0 = z0 + 2 * p;
+        // A and C of this thread's line: (field, row)
+        const int fA = t < 2 ? 0 : (uplane ? 2 : 1);
+        const int fC = t < 2 ? (uplane ? 1 : 2) : fA;
+        const int rA = t == 1 ? r0 + 1 : r0;
+        const int rC = t == 0 ? r0 : r0 + 1;
+        const bool live = bme < NLI;
+        auto sel = [&](int f, const T2* x0, const T2* x1, const T2* x2) { return f == 0 ? x0 : (f == 1 ? x1 : x2); };
+        auto selr = [&](int f, R x0, R x1, R x2) { return f == 0 ? x0 : (f == 1 ? x1 : x2); };
+        const T2* A0 = sel(fA, fa0, fa1, fa2) + (size_t)(live ? rA : 0) * NK;
+        const T2* A1 = sel(fA, fb0, fb1, fb2) + (size_t)(live ? rA : 0) * NK;
+        const T2* C0 = sel(fC, fa0, fa1, fa2) + (size_t)(live ? rC : 0) * NK;
+        const T2* C1 = sel(fC, fb0, fb1, fb2) + (size_t)(live ? rC : 0) * NK;
+        const R cA = selr(fA, ca0, ca1, ca2), dA = selr(fA, cb0, cb1, cb2);
+        const R cC = selr(fC, ca0, ca1, ca2), dC = selr(fC, cb0, cb1, cb2);
+        const bool twoA = dA != (R)0, twoC = dC != (R)0;
+        auto fetch = [&](int k, T2& a, T2& c) {
+            const T2 z = cx<T2>((R)0, (R)0);
+            const T2 a0 = A0[k], a1 = twoA ? A1[k] : z, c0 = C0[k], c1 = twoC ? C1[k] : z;
+            a = cx<T2>(cA * a0.x + dA * a1.x, cA * a0.y + dA * a1.y);
+            c = cx<T2>(cC * c0.x + dC * c1.x, cC * c0.y + dC * c1.y);
+        };
+        auto load = [&](int e, int) -> T2 {
+            const int e0 = e - n2me;
+            const bool lo = (e0 + N2 - 1 <= HX) || (e0 <= HX && e <= HX);
+            const bool hi = (e0 >= N - HX) || (e0 + N2 - 1 >= N - HX && e >= N - HX);
+            T2 a, c;
+            if (lo) {  // A_e + i C_e; the rft inverse ignores Im of the kx = 0 entries
+                fetch(e, a, c);
+                if (e == 0) { a.y = 0; c.y = 0; }
+                return cx<T2>(a.x - c.y, a.y + c.x);
+            }
+            if (hi) {  // conj(A_k) + i conj(C_k), k = N - e
+                fetch(N - e, a, c);
+                return cx<T2>(a.x + c.y, -a.y + c.x);
+            }
+            return cx<T2>((R)0, (R)0);
+        };
+        auto store = [&](int x, int b, T2 v) { PU[(size_t)b * N + x] = v; };
+        two_step_lines<T2, N1, N2, +1, false>(0, ex, twt, load, store, NLI);
+    }
+
+    // ---- forward: line f, products from the physical rows
+    {
+        const int s = uplane ? (bme & 3) : (bme & 1), p = uplane ? (bme >> 2) : (bme >> 1);
+        const bool live = bme < NLF;
+        const int pp = live ? p : 0;
+        const T2* La = PU + (size_t)(3 * pp + (s & 1)) * N;  // u, v (u-plane) / u, w (v-plane) of the row
+        const T2* Lb = PU + (size_t)(3 * pp + 2) * N;        // w pair (u-plane) / v pair (v-plane)
+        const bool odd = (s & 1) != 0, sq = uplane && s < 2;
+        auto load = [&](int x, int) -> T2 {
+            const T2 a = La[x];
+            if (sq) return cx<T2>(a.x * a.x, a.y * a.y);  // uu + i vv
+            const T2 bb = Lb[x];
+            const R o = odd ? bb.y : bb.x;                // w (u-plane) or v (v-plane) of the row
+            return uplane ? cx<T2>(o * o, a.x * o)        // ww + i uw
+                          : cx<T2>(a.x * o, a.y * o);     // uv + i vw
+        };
+        auto store = [&](int k, int f, T2 v) { PU[(size_t)f * LU + k] = v; };
+        // the forward step 1 reads every physical row before any spectrum is stored: the
+        // stores of two_step_lines come after its internal barrier
+        two_step_lines<T2, N1, N2, -1, false>(0, ex, twt, load, store, NLF);
+    }
+
+    // ---- unpack A_k = (P_k + conj P_{N-k})/2, B_k = (P_k - conj P_{N-k})/(2i), x 1/N
+    const R hs = (R)0.5 / (R)N;
+    const size_t pbase = (size_t)slot * d.ngal2 * NK;
+    for (int it = threadIdx.x; it < NLF * NK; it += blockDim.x) {
+        const int f = (unsigned)it / NK, k = it - f * NK;
+        const int s = uplane ? (f & 3) : (f & 1), p = uplane ? (f >> 2) : (f >> 1);
+        const int row = z0 + 2 * p + (s & 1);
+        const T2* line = PU + (size_t)f * LU;
+        const T2 Pk = line[k];
+        const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
+        T2* da = uplane ? (s < 2 ? H0 : H3) : H0;  // uu / ww / uv
+        T2* db = uplane ? (s < 2 ? H2 : H1) : H1;  // vv / uw / vw
+        const size_t o = pbase + (size_t)row * NK + k;
+        da[o] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+        db[o] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
+    }
+}
+
 // --------------------------------------------------------------------------------------
 // Pass 3: forward z transform (cft forward of phys_to_four_du, x 1/Ngal2) and truncation
 // to the retained kz modes (planes_to_modes_UVP/NUVP picks rows k and k+Ngal2-N2).

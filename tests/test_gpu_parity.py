@@ -270,3 +270,28 @@ def test_warp_column_solves(torch_cuda, monkeypatch, ng1, ng2, ny):
     for k in a:
         assert rel(a[k], b[k]) < 1e-10, k
     g.close()
+
+
+@pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
+def test_packed_xline_path(torch_cuda, monkeypatch, ng1, ng2, ny):
+    """The packed x-line kernel (1.5 inverse lines per row, CFD_XLINE_PATH=3) on every
+    two-step length, FP64 (1e-10 after one RK3 step) and mixed (1e-5), against the oracle."""
+    from cfd_b200.channel import build_channel
+    from cfd_b200.config import tiny
+    monkeypatch.setenv("CFD_XLINE_PATH", "3")
+    s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=ng1 + ng2))
+    o = oracle(s)
+    o.step(1)
+    ref = o.download_state()
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-5)):
+        g = make(s, prec)
+        if g.tuning()["xline_path"] != 3:  # a length whose packed CTA does not fit
+            g.close()
+            continue
+        g.step(1)
+        st = g.download_state()
+        for k in ("u1", "u2", "u3", "p"):
+            if prec == "mixed" and k == "p":
+                continue
+            assert rel(st[k], ref[k]) < tol, (prec, k, rel(st[k], ref[k]))
+        g.close()

@@ -18,7 +18,8 @@ def torch_cuda():
     return torch
 
 
-SHAPES = [dict(xline_path=2), dict(xline_path=1, xline_rows=2, zlines=4),
+SHAPES = [dict(xline_path=2), dict(xline_path=1, xline_rows=2, zlines=4), dict(xline_path=3),
+          dict(xline_path=3, xline_rows=2, rhs_chunk=16),
           dict(xline_rows=4, zlines=8, solve_kind=2, solve_cols=4), dict(solve_kind=2, solve_cols=1)]
 
 
