@@ -50,6 +50,11 @@ struct IBDev {
     int* planes = nullptr;
     int* slot_of_j = nullptr;
     std::vector<int> h_planes;
+    // z rows (0-based) that hold a forcing point or one of its two stencil points: only
+    // these go through the x round trip; on the others it only zeroes Im of the kx = 0 entry
+    int nact = 0;
+    int* arow = nullptr;
+    unsigned char* rowflag = nullptr;
 };
 
 }  // namespace
@@ -493,13 +498,15 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     }
     prof_mark(c);
     if (c->RWIX2) {
-        dim3 g2(d.ngal2 / c->RWIX2, ib.npl, nb);
+        dim3 g2((ib.nact + c->RWIX2 - 1) / c->RWIX2, ib.npl, nb);
         bool ok = true;
-        TWO_SWITCH(d.ngal1, ok, {
-            k_ib_xinv2<T2, TN1, TN2><<<g2, c->NTIX2, c->SMIX2, c->stream>>>(d, (T2*)c->Hib, ib.npl, (R*)c->phys,
-                                                                          twx<T2>(c), c->RWIX2);
-        });
-        LK("k_ib_xinv2");
+        if (ib.nact > 0) {
+            TWO_SWITCH(d.ngal1, ok, {
+                k_ib_xinv2<T2, TN1, TN2><<<g2, c->NTIX2, c->SMIX2, c->stream>>>(d, (T2*)c->Hib, ib.npl, (R*)c->phys,
+                                                                              ib.arow, ib.nact, twx<T2>(c), c->RWIX2);
+            });
+            LK("k_ib_xinv2");
+        }
     } else {
         dim3 g2(d.ngal2 / c->RWib, ib.npl, nb);
         FFT_SWITCH(d.ngal1, {
@@ -516,13 +523,15 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     }
     prof_mark(c);
     if (c->RWIX2) {
-        dim3 g4(d.ngal2 / c->RWFX2, ib.npl, nb);
+        dim3 g4((ib.nact + c->RWFX2 - 1) / c->RWFX2, ib.npl, nb);
         bool ok = true;
-        TWO_SWITCH(d.ngal1, ok, {
-            k_ib_xfwd2<T2, TN1, TN2><<<g4, c->NTFX2, c->SMFX2, c->stream>>>(d, (T2*)c->Hib, ib.npl, (const R*)c->phys,
-                                                                          twx<T2>(c), c->RWFX2);
-        });
-        LK("k_ib_xfwd2");
+        if (ib.nact > 0) {
+            TWO_SWITCH(d.ngal1, ok, {
+                k_ib_xfwd2<T2, TN1, TN2><<<g4, c->NTFX2, c->SMFX2, c->stream>>>(
+                    d, (T2*)c->Hib, ib.npl, (const R*)c->phys, ib.arow, ib.nact, twx<T2>(c), c->RWFX2);
+            });
+            LK("k_ib_xfwd2");
+        }
     } else {
         dim3 g4(d.ngal2 / c->RWibf, ib.npl, nb);
         FFT_SWITCH(d.ngal1, {
@@ -538,7 +547,8 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
             k_ib_zfwd2<T2, TN1, TN2><<<g5, c->NTZ2, c->SMZ2, c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0,
-                                                                        ib.planes, twz<T2>(c), c->LZ2);
+                                                                        ib.planes, c->RWIX2 ? ib.rowflag : nullptr,
+                                                                        twz<T2>(c), c->LZ2);
         });
         LK("k_ib_zfwd2");
     } else {
@@ -775,6 +785,17 @@ int setup_ib(cfd_ctx* c, const cfd_ib_list* l, int j0, int j1, IBDev& ib, const 
     }
     if (ib.npl > 0) CK(cudaMemcpy(ib.planes, ib.h_planes.data(), sizeof(int) * ib.npl, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ib.slot_of_j, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice));
+    std::vector<unsigned char> flag(ng2, 0);
+    for (int p = 0; p < l->n; ++p)
+        for (int t = 0; t < 3; ++t) flag[l->idx[9 * (size_t)p + 3 * t + 1] - 1] = 1;
+    std::vector<int> rows;
+    for (int k = 0; k < ng2; ++k)
+        if (flag[k]) rows.push_back(k);
+    ib.nact = (int)rows.size();
+    AL(ib.arow, int, std::max(ib.nact, 1));
+    AL(ib.rowflag, unsigned char, ng2);
+    if (ib.nact > 0) CK(cudaMemcpy(ib.arow, rows.data(), sizeof(int) * ib.nact, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ib.rowflag, flag.data(), ng2, cudaMemcpyHostToDevice));
     return CFD_OK;
 }
 

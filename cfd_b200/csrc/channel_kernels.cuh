@@ -1174,7 +1174,7 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
 // inverse x: line (rhs + i u) of each of RW rows -> physical rhs, u (rows coalesced in x)
 template <typename T2, int TN1, int TN2>
 __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype(T2::x)* __restrict__ phys,
-                           const T2* __restrict__ twx, int RW) {
+                           const int* __restrict__ arow, int nact, const T2* __restrict__ twx, int RW) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     constexpr int HX = N / 3;   // highest retained kx (N1 = 2*(Ngal1/3))
@@ -1185,8 +1185,11 @@ __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype
     load_twiddles<T2, TN1, TN2>(twt, twx);
     const int z0 = blockIdx.x * RW, p = blockIdx.y, fb = blockIdx.z;
     const size_t pl = (size_t)d.ngal2 * NK;
-    const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl + (size_t)z0 * NK;
-    const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl + (size_t)z0 * NK;
+    // line b of the CTA is active row arow[z0 + b] (the last one repeated past the end: the
+    // repeated line writes the same values again)
+    const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl;
+    const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl;
+    auto row_of_line = [&](int b) { return arow[min(z0 + b, nact - 1)]; };
     // this thread's offset within its stride-TN2 subsequence, computed as two_step_lines
     // does, so that e - n2 is a compile-time constant in the unrolled element loop
     const int tt = threadIdx.x;
@@ -1197,8 +1200,9 @@ __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype
         const int e0 = e - n2me;
         const bool lo = (e0 + TN2 - 1 <= HX) || (e0 <= HX && e <= HX);
         const bool hi = (e0 >= N - HX) || (e0 + TN2 - 1 >= N - HX && e >= N - HX);
-        const T2* A = Hr + (size_t)b * NK;
-        const T2* C = Hu + (size_t)b * NK;
+        const size_t ro = (size_t)row_of_line(b) * NK;
+        const T2* A = Hr + ro;
+        const T2* C = Hu + ro;
         if (lo) {
             T2 a = A[e], c = C[e];
             if (e == 0) { a.y = 0; c.y = 0; }
@@ -1211,11 +1215,12 @@ __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype
         return cx<T2>((R)0, (R)0);
     };
     const size_t ppl = (size_t)d.ngal2 * N;
-    R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl + (size_t)z0 * N;
-    R* pu = phys + ((size_t)(2 * fb + 1) * npl + p) * ppl + (size_t)z0 * N;
+    R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl;
+    R* pu = phys + ((size_t)(2 * fb + 1) * npl + p) * ppl;
     auto store = [&](int x, int b, T2 v) {
-        pr[(size_t)b * N + x] = v.x;
-        pu[(size_t)b * N + x] = v.y;
+        const size_t o = (size_t)row_of_line(b) * N + x;
+        pr[o] = v.x;
+        pu[o] = v.y;
     };
     two_step_lines<T2, TN1, TN2, +1, false>(0, ex, twt, load, store, RW);
 }
@@ -1223,7 +1228,7 @@ __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype
 // forward x of physical rhs rows (two rows per complex line), unpack, truncate, x 1/Ngal1
 template <typename T2, int TN1, int TN2>
 __global__ void k_ib_xfwd2(Dims d, T2* __restrict__ Hib, int npl, const decltype(T2::x)* __restrict__ phys,
-                           const T2* __restrict__ twx, int RW) {
+                           const int* __restrict__ arow, int nact, const T2* __restrict__ twx, int RW) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     constexpr int LU = N + 1;
@@ -1235,9 +1240,13 @@ __global__ void k_ib_xfwd2(Dims d, T2* __restrict__ Hib, int npl, const decltype
     load_twiddles<T2, TN1, TN2>(twt, twx);
     const int z0 = blockIdx.x * RW, p = blockIdx.y, fb = blockIdx.z;
     const size_t ppl = (size_t)d.ngal2 * N;
-    const R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl + (size_t)z0 * N;
+    const R* pr = phys + ((size_t)(2 * fb) * npl + p) * ppl;
+    // line b packs active rows arow[z0 + 2b] and arow[z0 + 2b + 1] (the last repeated)
+    auto row_of = [&](int r) { return arow[min(z0 + r, nact - 1)]; };
     __syncthreads();
-    auto load = [&](int x, int b) -> T2 { return cx<T2>(pr[(size_t)(2 * b) * N + x], pr[(size_t)(2 * b + 1) * N + x]); };
+    auto load = [&](int x, int b) -> T2 {
+        return cx<T2>(pr[(size_t)row_of(2 * b) * N + x], pr[(size_t)row_of(2 * b + 1) * N + x]);
+    };
     auto store = [&](int k, int b, T2 v) { ub[(size_t)b * LU + k] = v; };
     two_step_lines<T2, TN1, TN2, -1, false>(0, ex, twt, load, store, nl);
     const R hs = (R)0.5 / (R)N;
@@ -1247,17 +1256,17 @@ __global__ void k_ib_xfwd2(Dims d, T2* __restrict__ Hib, int npl, const decltype
     for (int it = threadIdx.x; it < nl * NK; it += blockDim.x) {
         const int b = (unsigned)it / NK, k = it - b * NK;
         const T2* line = ub + (size_t)b * LU;
-        T2* o0 = Hr + (size_t)(z0 + 2 * b) * NK + k;
         const T2 Pk = line[k];
         const T2 Qc = cconj(line[k == 0 ? 0 : N - k]);
-        o0[0] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
-        o0[NK] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
+        Hr[(size_t)row_of(2 * b) * NK + k] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
+        Hr[(size_t)row_of(2 * b + 1) * NK + k] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
     }
 }
 
 template <typename T2, int TN1, int TN2>
 __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_ib_zfwd2(Dims d, const T2* __restrict__ Hib, int npl, IBDst dst, int j0,
-                           const int* __restrict__ planes, const T2* __restrict__ twz, int lb) {
+                           const int* __restrict__ planes, const unsigned char* __restrict__ rowflag,
+                           const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     const int nlines = npl * d.nkx;
@@ -1276,7 +1285,14 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
     const int r = threadIdx.x >> lb;
     const R sc = (R)1 / (R)N;
     __syncthreads();
-    auto load = [&](int z, int) -> T2 { return H[(size_t)z * d.nkx]; };
+    // rows left out of the x round trip still get its one effect: the inverse real transform
+    // ignores Im of the kx = 0 entry (rft_buff.f:78-80), so that entry leaves real
+    const bool zero_im = rowflag && i == 0;
+    auto load = [&](int z, int) -> T2 {
+        T2 v = H[(size_t)z * d.nkx];
+        if (zero_im && !rowflag[z]) v.y = (decltype(T2::x))0;
+        return v;
+    };
     auto store = [&](int e, int, T2 v) {
         const int q = zrow_q<N, TN1>(e, r);
         if (q >= 0 && live) out[(size_t)q * d.nkx] = to_d2(cscale(v, sc));
