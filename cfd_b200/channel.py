@@ -135,6 +135,19 @@ class Channel:
     def download_state(self):
         return {k: self.download(k) for k in ("u1", "u2", "u3", "p")}
 
+    def save_record_out(self, directory: str, tag: str, t: float = 0.0, it: int = 0, nband: int = 3):
+        """Write the state in the reference's record_out format (cfd_b200.checkpoint)."""
+        from .checkpoint import write_record_out
+        return write_record_out(directory, tag, self.download_state(), self.setup, t=t, it=it,
+                                mpgx=self.scalars()["mpgx"], nband=nband)
+
+    def load_record_out(self, directory: str, tag: str) -> dict:
+        """Upload a state from record_out files (read_in's role); returns their header."""
+        from .checkpoint import read_record_out
+        data = read_record_out(directory, tag, self.setup)
+        self.upload_state({k: data[k] for k in ("u1", "u2", "u3", "p")})
+        return data["header"]
+
     def synchronize(self):
         self._chk(self.lib.cfd_synchronize(self.ctx), "synchronize")
 
