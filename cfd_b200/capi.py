@@ -47,7 +47,7 @@ class CfdTuning(C.Structure):
 
 
 class CfdStatsConfig(C.Structure):
-    _fields_ = [("jband", C.c_int32), ("dnx", C.c_int32), ("dnz", C.c_int32)]
+    _fields_ = [("jband", C.c_int32), ("dnx", C.c_int32), ("dnz", C.c_int32), ("spectra", C.c_int32)]
 
 
 def dptr(a):
@@ -65,6 +65,16 @@ def stats_buffers(nyu, nyv, nyp, nbu, nbv, nbp, dnx, dnz):
     import numpy as np
     return (np.zeros((6, nyu)), np.zeros((5, nyv)), np.zeros((2, nyp)),
             np.zeros((6, nbu, dnz, dnx)), np.zeros((5, nbv, dnz, dnx)), np.zeros((2, nbp, dnz, dnx)))
+
+
+SPECTRA = ("spU", "spV", "spW", "spUV", "spP")
+
+
+def spectra_buffers(ncol, nyu, nyv, nyp):
+    """Host arrays for cfd_spectra_read / orc_spectra_read, sp(j,column): [column][plane]."""
+    import numpy as np
+    return {"spU": np.zeros((ncol, nyu)), "spV": np.zeros((ncol, nyv)), "spW": np.zeros((ncol, nyu)),
+            "spUV": np.zeros((ncol, nyu)), "spP": np.zeros((ncol, nyp))}
 
 
 def stats_dict(bufs, istat):
@@ -152,6 +162,7 @@ SIGNATURES = {
     "cfd_stats_accumulate": (C.c_int, [_VP]),
     "cfd_stats_reset": (C.c_int, [_VP]),
     "cfd_stats_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, C.POINTER(C.c_int32)]),
+    "cfd_spectra_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "cfd_cfl": (C.c_int, [_VP, _dp, _VP]),
     "cfd_set_dt": (C.c_int, [_VP, C.c_double]),
     "cfd_ensemble_create": (C.c_int, [C.POINTER(_VP), C.c_int32, C.POINTER(_VP)]),

@@ -191,10 +191,11 @@ class Channel:
         return {"mpgx": a.value, "qx": b.value, "dgx": c.value}
 
     # -- statistics and CFL (stats.f90, dtc_calc) ------------------------------------------
-    def stats_configure(self, jband: int, dnx: int, dnz: int):
+    def stats_configure(self, jband: int, dnx: int, dnz: int, spectra: bool = True):
         """Configure and zero the FP64 statistics accumulators (bottom band up to v plane
-        jband, tiles of dnx x dnz points; jband below the first v plane: plane sums only)."""
-        sc = capi.CfdStatsConfig(int(jband), int(dnx), int(dnz))
+        jband, tiles of dnx x dnz points; jband below the first v plane: plane sums only),
+        and with spectra the spectra of spectra.f90, which the reference always takes."""
+        sc = capi.CfdStatsConfig(int(jband), int(dnx), int(dnz), int(bool(spectra)))
         self._chk(self.lib.cfd_stats_configure(self.ctx, C.byref(sc)), "stats_configure")
         g = self.setup.grid
         self._stats_shape = capi.stats_band(g.nyu, g.nyv, g.nyp, int(jband), g.ju0, g.jv0, g.jp0) + \
@@ -214,6 +215,14 @@ class Channel:
         self._chk(self.lib.cfd_stats_read(self.ctx, *[b.ctypes.data for b in bufs], C.byref(ist)),
                   "stats_read")
         return capi.stats_dict(bufs, ist.value)
+
+    def spectra_read(self) -> dict:
+        """The accumulated spectra spU, spV, spW, spUV, spP as (columns, planes) arrays, the
+        reference's sp(j,column) layout."""
+        g = self.setup.grid
+        bufs = capi.spectra_buffers(self.setup.cfg.ncol, g.nyu, g.nyv, g.nyp)
+        self._chk(self.lib.cfd_spectra_read(self.ctx, *[b.ctypes.data for b in bufs.values()]), "spectra_read")
+        return bufs
 
     def cfl(self):
         """(dtc, [u term, w term, v term]) of dtc_calc on the current state."""

@@ -154,6 +154,12 @@ def read_record_out(directory: str, tag: str, setup=None) -> dict:
 STATS_ORDER = ("Um", "U2m", "Vm", "V2m", "Wm", "W2m", "Pm", "P2m", "UVm", "UWm", "VWm", "wxm", "wx2m")
 
 
+def _grid_bytes(y, dthdy) -> bytes:
+    """The y, dthetai, dthdy record; dthetai is never assigned by the reference
+    (declaration.f90:71) and is written as 0."""
+    return np.asarray(y, "<f8").tobytes() + struct.pack("<d", 0.0) + np.asarray(dthdy, "<f8").tobytes()
+
+
 def write_stats(path: str, stats: dict, setup, t: float = 0.0, it: int = 0, mpgx: float | None = None,
                 nband: int = 3, jband: int | None = None):
     """Write the dictionary of Channel.stats_read() as write_stats does."""
@@ -164,8 +170,8 @@ def write_stats(path: str, stats: dict, setup, t: float = 0.0, it: int = 0, mpgx
     with open(path, "wb") as f:
         _rec(f, struct.pack("<5d2i", t, cfg.re_b, cfg.alp, cfg.bet, mp, nband, it) + bytes(4 * 88))
         _rec(f, np.asarray(ngal, "<i4").T.tobytes())
-        _rec(f, np.asarray(g.yu, "<f8").tobytes() + struct.pack("<d", 1.0) + np.asarray(g.dthdyu, "<f8").tobytes())
-        _rec(f, np.asarray(g.yv, "<f8").tobytes() + struct.pack("<d", 1.0) + np.asarray(g.dthdyv, "<f8").tobytes())
+        _rec(f, _grid_bytes(g.yu, g.dthdyu))
+        _rec(f, _grid_bytes(g.yv, g.dthdyv))
         _rec(f, struct.pack("<i", int(stats["istat"])))
         for k in STATS_ORDER:
             _rec(f, np.asarray(stats[k], "<f8").tobytes())
@@ -198,3 +204,95 @@ def read_stats(path: str, setup, dnx: int = 0, dnz: int = 0) -> dict:
         if out[k].size != sizes[grid]:
             raise ValueError(f"{path}: {k} has {out[k].size} planes, expected {sizes[grid]}")
     return out
+
+
+# ----------------------------------------------------------------------------------------
+# Spectra files of write_spect / recvwrspec (spectra.f90:58-182): one file per spectrum,
+# header, N, both y-grids, istat and buffSP(0:N1/2, 1:N2/2+1, j) (float64, Fortran order).
+# ----------------------------------------------------------------------------------------
+SPECTRA_FILES = (("spU", "U"), ("spV", "V"), ("spW", "U"), ("spUV", "U"), ("spP", "P"))
+
+
+def column_owner(ncol: int, nranks: int) -> np.ndarray:
+    """Rank of every column of the long-column list: contiguous chunks, the remainder to the
+    first ranks (start.f90:1421-1444, 1500-1510)."""
+    cnt = np.full(nranks, ncol // nranks)
+    cnt[: ncol - cnt.sum()] += 1
+    return np.repeat(np.arange(nranks), cnt)
+
+
+def fold_spectrum(sp: np.ndarray, setup, nranks: int = 2) -> np.ndarray:
+    """buffSP of recvwrspec (spectra.f90:115-167) from sp(j,column) [column][plane]: the
+    column (i, k) goes to (i, kk) with kk = k for k <= N2/2, N2+2-k above (the -kz modes
+    onto +kz), then the i >= 1 entries are doubled.  The master's own columns are stored
+    (later columns replace earlier ones) and every other rank's are added, so the fold
+    depends on the rank count the run used: with one rank the -kz value replaces the +kz
+    one, with two or more every owner of a +kz column is rank 0 or below its mirror's and
+    the two are summed.  Returns [plane][N2/2+1][N1/2+1] (C order of buffSP(i,kk,j))."""
+    cfg = setup.cfg
+    nkx, n2 = cfg.nkx, cfg.n2
+    ncol, ny = sp.shape
+    col = np.arange(ncol)
+    i, k = col % nkx, col // nkx + 1
+    kk = np.where(k > n2 // 2, n2 + 2 - k, k)
+    out = np.zeros((ny, n2 // 2 + 1, nkx))
+    own = column_owner(ncol, nranks)
+    tgt = (kk - 1) * nkx + i
+    # the master's columns: the last column of each target is the one that stays
+    c0 = col[own == 0][::-1]
+    _, first = np.unique(tgt[c0], return_index=True)
+    keep = c0[first]
+    out.reshape(ny, -1)[:, tgt[keep]] = sp[keep].T
+    for r in range(1, nranks):
+        m = own == r
+        np.add.at(out, (slice(None), kk[m] - 1, i[m]), sp[m].T)
+    out[:, :, 1:] *= 2.0
+    return out
+
+
+def spectra_filename(name: str, setup, t: float) -> str:
+    """<name>_<N1>x<N2>x<ny>_<int(10t)>.dat, the names of write_spect (spectra.f90:86-95,
+    ext1..ext4 of start.f90:235-237 and FOU3D.f90:2238)."""
+    cfg = setup.cfg
+    return f"{name}_{cfg.n1:04d}x{cfg.n2:04d}x{cfg.ny:04d}_{int(10.0 * t):05d}.dat"
+
+
+def write_spect(directory: str, spectra: dict, setup, istat: int, t: float = 0.0, it: int = 0,
+                mpgx: float | None = None, nranks: int = 2, nband: int = 3) -> list:
+    """Write the five files of write_spect from the dictionary of Channel.spectra_read()."""
+    cfg, g = setup.cfg, setup.grid
+    mp = cfg.mpgx if mpgx is None else mpgx
+    N = band_array(setup, nband)
+    head = struct.pack("<5d2i", t, cfg.re_b, cfg.alp, cfg.bet, mp, N.shape[1] - 2, it) + bytes(4 * 88)
+    os.makedirs(directory, exist_ok=True)
+    paths = []
+    for name, _ in SPECTRA_FILES:
+        buff = fold_spectrum(np.asarray(spectra[name]), setup, nranks)
+        path = os.path.join(directory, spectra_filename(name, setup, t))
+        with open(path, "wb") as f:
+            _rec(f, head)
+            _rec(f, np.asarray(N, "<i4").T.tobytes())
+            _rec(f, _grid_bytes(g.yu, g.dthdyu))
+            _rec(f, _grid_bytes(g.yv, g.dthdyv))
+            _rec(f, struct.pack("<i", int(istat)))
+            _rec(f, buff.astype("<f8").tobytes())
+        paths.append(path)
+    return paths
+
+
+def read_spect(path: str) -> dict:
+    """Read one write_spect file: header values, N, istat and buffSP as
+    [plane][N2/2+1][N1/2+1]."""
+    with open(path, "rb") as f:
+        h = _read_rec(f)
+        t, re, alp, bet, mpgx, nband, it = struct.unpack("<5d2i", h[:48])
+        N = np.frombuffer(_read_rec(f), "<i4").reshape(nband + 2, 4).T.copy()
+        _read_rec(f)
+        _read_rec(f)
+        (istat,) = struct.unpack("<i", _read_rec(f))
+        raw = np.frombuffer(_read_rec(f), "<f8")
+    nkx, nkz = N[0, 1] // 2 + 1, N[1, 1] // 2 + 1
+    if raw.size % (nkx * nkz):
+        raise ValueError(f"{path}: spectrum of {raw.size} values is not a whole number of {nkx} x {nkz} planes")
+    return {"t": t, "re": re, "alp": alp, "bet": bet, "mpgx": mpgx, "nband": nband, "iter": it, "N": N,
+            "istat": istat, "buff": raw.reshape(-1, nkz, nkx).copy()}

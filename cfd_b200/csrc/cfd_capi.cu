@@ -135,6 +135,8 @@ struct cfd_ctx {
         double* planes = nullptr; // [3][cp] physical planes
         double* mx = nullptr;     // [3][nyu]: |u|, |w| per u plane, |v| dthdyv per v plane
         cfd::PlaneSrc* src = nullptr;  // [3*cp]
+        // spectra (spectra.f90): [plane][column] each; null when not configured
+        double *spu = nullptr, *spv = nullptr, *spw = nullptr, *spuv = nullptr, *spp = nullptr;
     } st;
 };
 
@@ -1453,8 +1455,9 @@ int cfd_stats_configure(cfd_ctx* c, const cfd_stats_config* sc) {
             return fail(c, CFD_ERR_ARG, "tile %d x %d must divide Ngal1 x Ngal2", sc->dnx, sc->dnz);
         if (sc->jband + 1 > d.ju1) return fail(c, CFD_ERR_ARG, "jband %d above the channel", sc->jband);
     }
-    for (double* p : {st.su, st.sv, st.sp, st.cu, st.cv, st.cp_}) dfree(c, p);
+    for (double* p : {st.su, st.sv, st.sp, st.cu, st.cv, st.cp_, st.spu, st.spv, st.spw, st.spuv, st.spp}) dfree(c, p);
     st.su = st.sv = st.sp = st.cu = st.cv = st.cp_ = nullptr;
+    st.spu = st.spv = st.spw = st.spuv = st.spp = nullptr;
     int s = stats_scratch(c);
     if (s) return s;
     st.jband = sc->jband;
@@ -1471,6 +1474,13 @@ int cfd_stats_configure(cfd_ctx* c, const cfd_stats_config* sc) {
     AL(st.cu, double, 2 * 6 * st.nbu * tsz);
     AL(st.cv, double, 2 * 5 * st.nbv * tsz);
     AL(st.cp_, double, 2 * 2 * st.nbp * tsz);
+    if (sc->spectra) {
+        AL(st.spu, double, (size_t)d.nyu * d.ncol);
+        AL(st.spv, double, (size_t)d.nyv * d.ncol);
+        AL(st.spw, double, (size_t)d.nyu * d.ncol);
+        AL(st.spuv, double, (size_t)d.nyu * d.ncol);
+        AL(st.spp, double, (size_t)d.nyp * d.ncol);
+    }
     st.on = true;
     return cfd_stats_reset(c);
 }
@@ -1489,6 +1499,14 @@ int cfd_stats_reset(cfd_ctx* c) {
         CK(cudaMemsetAsync(st.cv, 0, sizeof(double) * 2 * 5 * st.nbv * tsz, c->stream));
         CK(cudaMemsetAsync(st.cp_, 0, sizeof(double) * 2 * 2 * st.nbp * tsz, c->stream));
     }
+    if (st.spu) {
+        const size_t nc = d.ncol;
+        CK(cudaMemsetAsync(st.spu, 0, sizeof(double) * d.nyu * nc, c->stream));
+        CK(cudaMemsetAsync(st.spv, 0, sizeof(double) * d.nyv * nc, c->stream));
+        CK(cudaMemsetAsync(st.spw, 0, sizeof(double) * d.nyu * nc, c->stream));
+        CK(cudaMemsetAsync(st.spuv, 0, sizeof(double) * d.nyu * nc, c->stream));
+        CK(cudaMemsetAsync(st.spp, 0, sizeof(double) * d.nyp * nc, c->stream));
+    }
     st.istat = 0;
     return CFD_OK;
 }
@@ -1498,8 +1516,42 @@ int cfd_stats_accumulate(cfd_ctx* c) {
     if (!c->st.on) return fail(c, CFD_ERR_STATE, "statistics not configured");
     int s = stats_pass(c, true);
     if (s) return s;
-    c->st.istat += 1;
+    auto& st = c->st;
+    if (st.spu) {
+        const Dims& d = c->d;
+        dim3 grid((d.ncol + 255) / 256, d.nyu);
+        prof_mark(c);
+        k_spectra<<<grid, 256, 0, c->stream>>>(d, c->g, c->u1, c->u2, c->u3, c->p, st.spu, st.spv, st.spw, st.spuv,
+                                               st.spp);
+        LK("k_spectra");
+    }
+    st.istat += 1;
     return CFD_OK;
+}
+
+int cfd_spectra_read(cfd_ctx* c, double* spu, double* spv, double* spw, double* spuv, double* spp) {
+    if (!c) return CFD_ERR_ARG;
+    const Dims& d = c->d;
+    auto& st = c->st;
+    if (!st.on || !st.spu) return fail(c, CFD_ERR_STATE, "spectra not configured");
+    CK(cudaStreamSynchronize(c->stream));
+    // device [plane][column] -> the reference's sp(j,column), j fastest
+    std::vector<double> h;
+    auto get = [&](double* out, const double* dev, int ny) -> int {
+        if (!out) return CFD_OK;
+        const size_t nc = d.ncol;
+        h.resize((size_t)ny * nc);
+        CK(cudaMemcpy(h.data(), dev, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+        for (int j = 0; j < ny; ++j)
+            for (size_t col = 0; col < nc; ++col) out[col * ny + j] = h[(size_t)j * nc + col];
+        return CFD_OK;
+    };
+    int s = get(spu, st.spu, d.nyu);
+    if (!s) s = get(spv, st.spv, d.nyv);
+    if (!s) s = get(spw, st.spw, d.nyu);
+    if (!s) s = get(spuv, st.spuv, d.nyu);
+    if (!s) s = get(spp, st.spp, d.nyp);
+    return s;
 }
 
 int cfd_stats_read(cfd_ctx* c, double* u_sums, double* v_sums, double* p_sums, double* cu, double* cv, double* cp,

@@ -185,4 +185,47 @@ __global__ void __launch_bounds__(256) k_st_cond(Dims d, const double* __restric
     }
 }
 
+// Spectra (spectra.f90:1-56): buildsp / buildspUV on the spectral columns of every plane.
+// grid: x = column blocks, y = u plane (index j - ju0; v and p planes are the leading
+// nyv, nyp of them).  sp arrays are [plane][column] in FP64.  v_itp is interp_v
+// (FOU3D.f90:285-308): vca v(j) + vcb v(j-1) at the interior centres, the ghost centres
+// extrapolated with gridweighting_interp.  Each sum is added in the reference's order,
+// (sp + re^2) + im^2, with no fused multiply-adds.
+__device__ __forceinline__ double sp_add2(double s, double2 a) {
+    return __dadd_rn(__dadd_rn(s, __dmul_rn(a.x, a.x)), __dmul_rn(a.y, a.y));
+}
+
+__global__ void __launch_bounds__(256) k_spectra(Dims d, Geo g, const double2* __restrict__ u1,
+                                                 const double2* __restrict__ u2, const double2* __restrict__ u3,
+                                                 const double2* __restrict__ p, double* __restrict__ spu,
+                                                 double* __restrict__ spv, double* __restrict__ spw,
+                                                 double* __restrict__ spuv, double* __restrict__ spp) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jr = blockIdx.y;
+    if (col >= d.ncol) return;
+    const size_t nc = d.ncol, o = (size_t)jr * nc + col;
+    const double2 a = u1[o];
+    spu[o] = sp_add2(spu[o], a);
+    spw[o] = sp_add2(spw[o], u3[o]);
+    if (jr < d.nyv) spv[o] = sp_add2(spv[o], u2[o]);
+    if (jr < d.nyp) spp[o] = sp_add2(spp[o], p[o]);
+    // u and v planes share their first index (ju0 = jv0): face r is v index r
+    auto itp = [&](int r) {
+        const double2 va = u2[(size_t)r * nc + col], vb = u2[(size_t)(r - 1) * nc + col];
+        const double wa = g.vca[r], wb = g.vcb[r];
+        return make_double2(wa * va.x + wb * vb.x, wa * va.y + wb * vb.y);
+    };
+    double2 vi;
+    if (jr == 0) {
+        const double2 v1 = itp(1), vw = u2[col];
+        vi = make_double2(g.gwib * (vw.x - v1.x) + v1.x, g.gwib * (vw.y - v1.y) + v1.y);
+    } else if (jr == d.nyu - 1) {
+        const double2 v1 = itp(jr - 1), vw = u2[(size_t)(d.nyv - 1) * nc + col];
+        vi = make_double2(g.gwit * (vw.x - v1.x) + v1.x, g.gwit * (vw.y - v1.y) + v1.y);
+    } else {
+        vi = itp(jr);
+    }
+    spuv[o] = __dadd_rn(__dadd_rn(spuv[o], __dmul_rn(a.x, vi.x)), __dmul_rn(a.y, vi.y));
+}
+
 }  // namespace cfd

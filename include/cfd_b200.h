@@ -234,6 +234,7 @@ int cfd_cft(cfd_ctx *ctx, double *c_dev, int32_t ise, int32_t isa, int32_t m, in
 typedef struct cfd_stats_config {
     int32_t jband;      /* last v plane of the bottom band; < -dsty: no conditional sums */
     int32_t dnx, dnz;   /* tile size in points; must divide Ngal1, Ngal2 */
+    int32_t spectra;    /* nonzero: each accumulation also adds the spectra below */
 } cfd_stats_config;
 
 /* Sets the band and tile, allocates the accumulators (and the plane scratch) and zeroes
@@ -253,6 +254,19 @@ int cfd_stats_reset(cfd_ctx *ctx);
  *   istat: number of accumulated calls. */
 int cfd_stats_read(cfd_ctx *ctx, double *u_sums, double *v_sums, double *p_sums,
                    double *cu, double *cv, double *cp, int32_t *istat);
+/* Spectra of spectra.f90:1-56, accumulated by cfd_stats_accumulate when the configuration
+ * asks for them (the reference calls spectra at the same kRK = 1 steps as stats,
+ * FOU3D.f90:107-110): per plane j and column, in FP64,
+ *   spU += |u|^2, spV += |v|^2, spW += |w|^2, spP += |p|^2          (buildsp)
+ *   spUV += Re(u) Re(v_itp) + Im(u) Im(v_itp)                       (buildspUV)
+ * over every plane of the field's grid (the reference's midband holds the whole channel),
+ * v_itp being v interpolated to the u planes (interp_v, FOU3D.f90:285-308).  cfd_stats_reset
+ * zeroes them with the statistics (write_spect and write_stats run together,
+ * FOU3D.f90:222-225).  Copies them to host arrays in the reference's sp(j,column) layout,
+ * j fastest (any pointer may be NULL):
+ *   spu, spw, spuv [ncol][nyu], spv [ncol][nyv], spp [ncol][nyp] */
+int cfd_spectra_read(cfd_ctx *ctx, double *spu, double *spv, double *spw, double *spuv, double *spp);
+
 /* dtc_calc (FOU3D.f90:516-544) on the current state.  terms (may be NULL) receives
  *   [0] 1/(alp*(N1/2)*max|u|), [1] 1/(bet*(N2/2)*max|w|), [2] 1/max(1e-6, max|v|*dthdyv)
  * with the maxima over the physical u, w planes (all) and v planes (walls excluded).

@@ -200,6 +200,8 @@ struct Oracle {
         bool on = false;
         int jband = 0, dnx = 0, dnz = 0, nbu = 0, nbv = 0, nbp = 0, istat = 0;
         std::vector<double> su, sv, sp, cub, cut, cvb, cvt, cpb, cpt;
+        // spectra (spectra.f90:1-56), sp(j,column): [col][j - j0]; empty when not asked for
+        std::vector<double> spu, spv, spw, spuv, spp;
     } st;
 
     // RK coefficients, Le & Moin (start.f90:395-409)
@@ -733,8 +735,14 @@ static void rk_substep(Oracle& o, int krk) {
 // the same plane transforms as ops_in_planes: u, w, v_itp on u planes, v, w_itp, wx on v
 // planes (four_to_phys_u for velocities, four_to_phys_du for wx and p).
 // ------------------------------------------------------------------------------------
-static void stats_configure(Oracle& o, int jband, int dnx, int dnz) {
+static void stats_configure(Oracle& o, int jband, int dnx, int dnz, int spectra) {
     auto& st = o.st;
+    const size_t nc = o.ncol;
+    st.spu.assign(spectra ? nc * o.nyu : 0, 0.0);
+    st.spv.assign(spectra ? nc * o.nyv : 0, 0.0);
+    st.spw.assign(spectra ? nc * o.nyu : 0, 0.0);
+    st.spuv.assign(spectra ? nc * o.nyu : 0, 0.0);
+    st.spp.assign(spectra ? nc * o.nyp : 0, 0.0);
     const bool cond = jband >= o.jv0;
     st.jband = jband;
     st.dnx = cond ? dnx : 0;
@@ -896,6 +904,23 @@ static void stats_accumulate(Oracle& o) {
             }
         }
     }
+    // spectra (spectra.f90:1-56, called at FOU3D.f90:107-110 with u2_itp of interp_v):
+    // buildsp sp = sp + Re(u)^2 + Im(u)^2, buildspUV sp = sp + Re(u) Re(v) + Im(u) Im(v)
+    if (!st.spu.empty()) {
+#pragma omp parallel for schedule(static)
+        for (int col = 0; col < o.ncol; ++col) {
+            auto sq = [](double& sp, cplx a) { sp = sp + a.real() * a.real() + a.imag() * a.imag(); };
+            for (int j = o.ju0; j <= o.ju1; ++j) {
+                const size_t e = (size_t)col * o.nyu + (j - o.ju0);
+                sq(st.spu[e], o.U(o.u1, col, j));
+                sq(st.spw[e], o.U(o.u3, col, j));
+                const cplx a = o.U(o.u1, col, j), b = o.U(o.u2i, col, j);
+                st.spuv[e] = st.spuv[e] + a.real() * b.real() + a.imag() * b.imag();
+            }
+            for (int j = o.jv0; j <= o.jv1; ++j) sq(st.spv[(size_t)col * o.nyv + (j - o.jv0)], o.V(o.u2, col, j));
+            for (int j = o.jp0; j <= o.jp1; ++j) sq(st.spp[(size_t)col * o.nyp + (j - o.jp0)], o.P(o.p, col, j));
+        }
+    }
     st.istat += 1;
 }
 
@@ -1049,10 +1074,19 @@ int orc_step(void* h, int nsteps) {
     }
     return 0;
 }
-int orc_stats_configure(void* h, int jband, int dnx, int dnz) {
+int orc_stats_configure(void* h, int jband, int dnx, int dnz, int spectra) {
     Oracle& o = *(Oracle*)h;
     if (jband >= o.jv0 && (dnx <= 0 || dnz <= 0 || o.ngal1 % dnx || o.ngal2 % dnz)) return 1;
-    stats_configure(o, jband, dnx, dnz);
+    stats_configure(o, jband, dnx, dnz, spectra);
+    return 0;
+}
+// same layout as cfd_spectra_read: sp(j,column), j fastest
+int orc_spectra_read(void* h, double* spu, double* spv, double* spw, double* spuv, double* spp) {
+    Oracle& o = *(Oracle*)h;
+    auto& st = o.st;
+    if (!st.on || st.spu.empty()) return 5;
+    auto cp_ = [](double* dst, const std::vector<double>& a) { if (dst) std::copy(a.begin(), a.end(), dst); };
+    cp_(spu, st.spu); cp_(spv, st.spv); cp_(spw, st.spw); cp_(spuv, st.spuv); cp_(spp, st.spp);
     return 0;
 }
 int orc_stats_accumulate(void* h) {

@@ -50,7 +50,8 @@ def lib():
         L.orc_four_to_phys.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int]
         L.orc_phys_to_four.argtypes = [C.c_void_p, _dp, C.c_int]
         L.orc_set_num_threads.argtypes = [C.c_int]
-        L.orc_stats_configure.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.orc_stats_configure.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_spectra_read.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         L.orc_stats_accumulate.argtypes = [C.c_void_p]
         L.orc_stats_read.argtypes = [C.c_void_p] + [C.c_void_p] * 6 + [C.POINTER(C.c_int)]
         L.orc_cfl.argtypes = [C.c_void_p, _dp, C.c_void_p]
@@ -148,9 +149,9 @@ class OracleChannel:
         return {"mpgx": a.value, "qx": b.value, "dgx": c.value}
 
     # statistics (stats.f90) and dtc_calc, same interface as Channel
-    def stats_configure(self, jband: int, dnx: int, dnz: int):
+    def stats_configure(self, jband: int, dnx: int, dnz: int, spectra: bool = True):
         from cfd_b200 import capi
-        st = lib().orc_stats_configure(self.h, int(jband), int(dnx), int(dnz))
+        st = lib().orc_stats_configure(self.h, int(jband), int(dnx), int(dnz), int(bool(spectra)))
         assert st == 0, "bad statistics tile"
         g = self.setup.grid
         self._stats_shape = capi.stats_band(g.nyu, g.nyv, g.nyp, int(jband), g.ju0, g.jv0, g.jp0) + \
@@ -158,6 +159,13 @@ class OracleChannel:
 
     def stats_accumulate(self):
         assert lib().orc_stats_accumulate(self.h) == 0
+
+    def spectra_read(self) -> dict:
+        from cfd_b200 import capi
+        g = self.setup.grid
+        bufs = capi.spectra_buffers(self.setup.cfg.ncol, g.nyu, g.nyv, g.nyp)
+        assert lib().orc_spectra_read(self.h, *[b.ctypes.data for b in bufs.values()]) == 0, "spectra not configured"
+        return bufs
 
     def stats_read(self) -> dict:
         from cfd_b200 import capi

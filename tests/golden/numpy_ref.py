@@ -206,6 +206,13 @@ class NumpyChannel:
         out.update(cond)
         return out
 
+    def spectra(self):
+        """One spectra() call on zeroed accumulators (spectra.f90:1-56), sp(j,column)."""
+        u2i, _ = self._interp()
+        a = self.u1
+        return {"spU": np.abs(a) ** 2, "spV": np.abs(self.u2) ** 2, "spW": np.abs(self.u3) ** 2,
+                "spUV": a.real * u2i.real + a.imag * u2i.imag, "spP": np.abs(self.p) ** 2}
+
     def cfl(self):
         g = self.g
         um = max(np.abs(self.to_phys(self.u1[:, jj])).max() for jj in range(g.nyu))

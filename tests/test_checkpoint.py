@@ -85,3 +85,77 @@ def test_stats_file_round_trip(tmp_path):
         assert np.array_equal(back[k], st[k]), k
     for k in ("UmC", "V2mC", "PmC", "wx2mC"):
         assert np.array_equal(back[k], st[k]), k
+
+
+def _fold_loops(sp, nkx, n2, nranks):
+    """recvwrspec (spectra.f90:115-167) as the reference's loops: rank 0 stores, every
+    other rank adds, in column order; then the i >= 1 entries are doubled."""
+    from cfd_b200.checkpoint import column_owner
+    ncol, ny = sp.shape
+    own = column_owner(ncol, nranks)
+    buff = np.zeros((ny, n2 // 2 + 1, nkx))
+    for r in range(nranks):
+        for col in np.nonzero(own == r)[0]:
+            i, k = col % nkx, col // nkx + 1
+            kk = n2 + 2 - k if k > n2 // 2 else k
+            if r == 0:
+                buff[:, kk - 1, i] = sp[col]
+            else:
+                buff[:, kk - 1, i] += sp[col]
+    buff[:, :, 1:] *= 2.0
+    return buff
+
+
+@pytest.mark.parametrize("nranks", [1, 2, 3, 7])
+def test_spectrum_fold(setup, nranks):
+    from cfd_b200.checkpoint import column_owner, fold_spectrum
+    cfg = setup.cfg
+    rng = np.random.default_rng(5)
+    sp = rng.random((cfg.ncol, 6))
+    got = fold_spectrum(sp, setup, nranks)
+    assert np.array_equal(got, _fold_loops(sp, cfg.nkx, cfg.n2, nranks))
+    own = column_owner(cfg.ncol, nranks)
+    assert own.size == cfg.ncol and np.all(np.diff(own) >= 0) and own[-1] == nranks - 1
+    nkx, n2 = cfg.nkx, cfg.n2
+    kz = lambda k: sp[(k - 1) * nkx:(k - 1) * nkx + nkx].T  # [plane][i] of the column row k
+    # kz = 0 and the last row have no mirror
+    assert np.array_equal(got[:, 0, 0], kz(1)[:, 0]) and np.allclose(got[:, 0, 1:], 2 * kz(1)[:, 1:])
+    assert np.allclose(got[:, n2 // 2, 1:], 2 * kz(n2 // 2 + 1)[:, 1:])
+    if nranks == 1:  # one rank: the -kz column replaces the +kz one
+        assert np.allclose(got[:, 1, 1:], 2 * kz(n2)[:, 1:])
+    else:            # more: the two are summed
+        assert np.allclose(got[:, 1, 1:], 2 * (kz(2) + kz(n2))[:, 1:])
+
+
+def test_spect_file_round_trip(tmp_path):
+    """write_spect layout from the oracle's spectra (the GPU gives the same dictionary)."""
+    from cfd_b200.checkpoint import SPECTRA_FILES, fold_spectrum, read_spect, spectra_filename, write_spect
+    from oracle.oracle import OracleChannel
+    s = build_channel(tiny(24, 18, 17))
+    o = OracleChannel(s)
+    o.upload_state()
+    o.step(1)
+    o.stats_configure(s.grid.jv0 - 1, 0, 0)
+    o.stats_accumulate()
+    o.stats_accumulate()
+    sp = o.spectra_read()
+    paths = write_spect(str(tmp_path), sp, s, istat=2, t=1.25, it=9)
+    assert [p.split("/")[-1] for p in paths] == [spectra_filename(n, s, 1.25) for n, _ in SPECTRA_FILES]
+    assert paths[0].endswith(f"spU_{s.cfg.n1:04d}x{s.cfg.n2:04d}x{s.cfg.ny:04d}_00012.dat")
+    g = s.grid
+    for (name, grid), path in zip(SPECTRA_FILES, paths):
+        back = read_spect(path)
+        assert back["istat"] == 2 and back["iter"] == 9 and back["t"] == 1.25
+        ny = {"U": g.nyu, "V": g.nyv, "P": g.nyp}[grid]
+        assert back["buff"].shape == (ny, s.cfg.n2 // 2 + 1, s.cfg.nkx)
+        assert np.array_equal(back["buff"], fold_spectrum(sp[name], s, 2)), name
+    # the record holds buffSP(0:N1/2, 1:N2/2+1, j) with i fastest
+    with open(paths[0], "rb") as f:
+        for _ in range(5):
+            (n,) = struct.unpack("<i", f.read(4))
+            f.seek(n + 4, 1)
+        (n,) = struct.unpack("<i", f.read(4))
+        assert n == 8 * g.nyu * (s.cfg.n2 // 2 + 1) * s.cfg.nkx
+        first = struct.unpack("<2d", f.read(16))
+    b = read_spect(paths[0])["buff"]
+    assert first == (b[0, 0, 0], b[0, 0, 1])

@@ -121,3 +121,37 @@ def test_set_dt_recaptures_graph(torch_cuda):
     with pytest.raises(RuntimeError, match="dt"):
         g.set_dt(-1.0)
     g.close()
+
+
+@pytest.mark.parametrize("cfg", CASES, ids=lambda c: c.name)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_spectra_vs_oracle(torch_cuda, cfg, precision):
+    """spectra (spectra.f90:1-56) accumulated with the statistics: the |.|^2 spectra are
+    bit-exact against the oracle (same FP64 state, same order of additions), spUV within
+    1e-13 of its scale (interp_v weights rounded differently); reset zeroes them; the
+    write_spect files of both are the same to that tolerance."""
+    from cfd_b200.channel import Channel
+    from cfd_b200.checkpoint import fold_spectrum
+    s, o = stepped(cfg)
+    g = Channel(s, device=0, precision=precision)
+    g.upload_state(o.download_state())
+    for ch in (g, o):
+        ch.stats_configure(s.grid.jv0 - 1, 0, 0)
+        ch.stats_accumulate()
+        ch.stats_accumulate()
+    got, ref = g.spectra_read(), o.spectra_read()
+    for k in capi.SPECTRA:
+        assert got[k].shape == ref[k].shape, k
+        if k == "spUV":
+            assert np.abs(got[k] - ref[k]).max() <= 1e-13 * np.abs(ref[k]).max(), k
+        else:
+            assert np.array_equal(got[k], ref[k]), k
+        fg, fo = fold_spectrum(got[k], s), fold_spectrum(ref[k], s)
+        assert np.abs(fg - fo).max() <= 1e-13 * np.abs(fo).max(), k
+    g.stats_reset()
+    z = g.spectra_read()
+    assert not any(np.any(z[k]) for k in capi.SPECTRA)
+    g.stats_configure(s.grid.jv0 - 1, 0, 0, spectra=False)
+    with pytest.raises(RuntimeError, match="spectra not configured"):
+        g.spectra_read()
+    g.close()

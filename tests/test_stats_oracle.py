@@ -92,3 +92,27 @@ def test_cfl_oracle_vs_numpy(stepped):
     assert dtc == min(t[0], t[1]) and abs(dtc - dtn) <= 1e-12 * dtn
     # the step the setup chose is CFL-stable for this state
     assert s.dt < dtc
+
+
+def test_spectra_oracle_vs_numpy(stepped):
+    """spectra (spectra.f90:1-56) of the oracle: one call equals the numpy restatement,
+    two calls double it, a configuration without spectra holds none."""
+    s, o, n, jband, dnx, dnz = stepped
+    o.stats_configure(jband, dnx, dnz)
+    o.stats_accumulate()
+    one = o.spectra_read()
+    ref = n.spectra()
+    for k in capi.SPECTRA:
+        assert one[k].shape == ref[k].shape, k
+        scale = np.abs(ref[k]).max()
+        assert scale > 0 and np.abs(one[k] - ref[k]).max() <= 1e-13 * scale, k
+    # |.|^2 spectra are exact in the accumulation order of buildsp
+    assert np.array_equal(one["spU"], (o.download_state()["u1"].real ** 2) + o.download_state()["u1"].imag ** 2)
+    o.stats_accumulate()
+    two = o.spectra_read()
+    for k in capi.SPECTRA:
+        assert np.abs(two[k] - 2 * one[k]).max() <= 1e-15 * np.abs(one[k]).max(), k
+    o.stats_configure(jband, dnx, dnz, spectra=False)
+    o.stats_accumulate()
+    with pytest.raises(AssertionError):
+        o.spectra_read()
