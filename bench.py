@@ -59,6 +59,7 @@ def kernel_bytes(name, setup, mixed):
         "k_xline": (3 * nslot + 4 * nyu + 2 * nyv) * hpl * ct,
         # reads every transformed field plane once (y-neighbours of the interpolation from L2)
         "k_xline2": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,
+        "k_xline4": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,   # the same pass on packed line pairs
         "k_zfwd": (4 * nyu + 2 * nyv) * (hpl + ncol) * ct,
         "k_rhs": ncol * ((2 * nyu + nyv + nyp) * cs + (2 * nyu + nyv) * ct + (4 * nyu + 2 * nyv) * ct
                          + (2 * nyu + nyv) * cs + (2 * nyu + nyv) * ct),

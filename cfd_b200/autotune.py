@@ -14,7 +14,7 @@ from __future__ import annotations
 import json
 import os
 
-KNOBS = (("xline_path", (1, 2, 3)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
+KNOBS = (("xline_path", (1, 2, 3, 4)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
          ("solve_kind", (1, 2)), ("solve_cols", (4, 8)), ("rhs_chunk", (2, 4, 8, 16)))
 
 
@@ -25,7 +25,7 @@ def _cache_path() -> str:
 
 def _key(setup, precision: str, gpu: str) -> str:
     c, g = setup.cfg, setup.grid
-    return f"v2|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+    return f"v3|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
 
 
 def time_step(setup, precision, device, tuning, steps=5, warmup=2):

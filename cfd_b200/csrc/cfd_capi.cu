@@ -97,6 +97,8 @@ struct cfd_ctx {
     int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
     int RW2 = 0, NT2 = 0;
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
+    int RW4 = 0, NT4 = 0;   // line-pair x-line kernel (k_xline4, FP32): rows per CTA (0 = not used), threads
+    size_t SM4 = 0;
     size_t SM3 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
     int LZ2 = -1, NTZ2 = 0; // two-step z kernels: log2(columns per CTA) (-1 = not used), threads
     int SWM = 0, SWC = 8;   // warp-per-column solves: rows-per-lane bound (0 = not used), columns per CTA
@@ -346,6 +348,9 @@ int set_smem_attrs(cfd_ctx* c) {
                 e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
             if (e == cudaSuccess && c->XL3)
                 e = cudaFuncSetAttribute(k_xline3<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM3);
+            if constexpr (std::is_same<T2, float2>::value)
+                if (e == cudaSuccess && c->RW4)
+                    e = cudaFuncSetAttribute(k_xline4<TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM4);
         });
     }
     CK(e);
@@ -407,7 +412,22 @@ int nl_transforms(cfd_ctx* c) {
         LK("k_zinv");
     }
     prof_mark(c);
-    if (c->RW2 && c->XL3) {
+    bool xdone = false;
+    if constexpr (std::is_same<T2, float2>::value) {
+        if (c->RW4) {
+            dim3 gx4(d.ngal2 / c->RW4, d.nslot);
+            bool ok = true;
+            TWO_SWITCH(d.ngal1, ok, {
+                k_xline4<TN1, TN2><<<gx4, c->NT4, c->SM4, c->stream>>>(d, c->g, (const float2*)c->Hx, (float2*)c->H[0],
+                                                                     (float2*)c->H[1], (float2*)c->H[2],
+                                                                     (float2*)c->H[3], twx<float2>(c), c->RW4);
+            });
+            LK("k_xline4");
+            xdone = true;
+        }
+    }
+    if (xdone) {
+    } else if (c->RW2 && c->XL3) {
         dim3 gx3(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
         TWO_SWITCH(d.ngal1, ok, {
@@ -918,13 +938,29 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
                 const size_t N = (size_t)n1s * n2s, LX = (size_t)((n1s * (n2s + 1)) | 1);
                 c->SM3 = (N + 2 * rw * LX + std::max((size_t)3 * (rw / 2) * N, (size_t)2 * rw * (N + 1))) * esz;
                 const int xp = g_tuning && g_tuning->xline_path ? g_tuning->xline_path
-                                                                : env_int("CFD_XLINE_PATH", 1, 1, 3);
+                                                                : env_int("CFD_XLINE_PATH", 1, 1, 4);
                 c->XL3 = xp == 3 && c->SM3 <= 220 * 1024;
+                if (xp == 4 && mixed) {
+                    // line pairs: rows per CTA from the same tuning field, up to 8 (the
+                    // kernel's launch bound, 8*max(N1,N2) threads)
+                    int r4 = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", 8, 2, 8);
+                    r4 = 1 << (31 - __builtin_clz(r4));
+                    const size_t N4 = (size_t)n1s * n2s;
+                    const size_t LX4 = (size_t)std::max(n1s * (n2s + 1) + 1, std::max(n2s * (n1s + 1) + 1, n1s * n2s + 1));
+                    auto sm4 = [&](int r) { return ((size_t)r * LX4 + N4) * 2 * sizeof(float2); };
+                    while (r4 >= 2 && ((d.ngal2 % r4) || sm4(r4) > 220 * 1024)) r4 /= 2;
+                    if (r4 >= 2 && d.ngal2 % r4 == 0) {
+                        c->RW4 = r4;
+                        c->NT4 = r4 * std::max(n1s, n2s);
+                        c->SM4 = sm4(r4);
+                    }
+                }
             }
         }
     }
     if ((g_tuning && g_tuning->xline_path == 2) ||
-        (!(g_tuning && (g_tuning->xline_path == 1 || g_tuning->xline_path == 3)) && env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)))
+        (!(g_tuning && (g_tuning->xline_path == 1 || g_tuning->xline_path == 3 || g_tuning->xline_path == 4)) &&
+         env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)))
         c->RW2 = 0;
     {
         bool ok = true;
@@ -938,7 +974,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
             c->SMZ2 = ((size_t)(1 << lb) * ((n1s * (n2s + 1)) | 1) + (size_t)n1s * n2s) * esz;
         }
     }
-    if (c->LZ2 < 0) c->RW2 = 0;  // the two-step x-line kernel reads the output of k_zinv2s
+    if (c->LZ2 < 0) c->RW2 = 0;  // the two-step x-line kernels read the output of k_zinv2s
+    if (!c->RW2) c->RW4 = 0;
     {
         // warp-per-column Helmholtz solves: up to 16 rows per lane (512 planes)
         const int m = (d.nyu + 31) / 32;
@@ -1215,8 +1252,8 @@ int cfd_create_tuned(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib
 
 int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
     if (!c || !t) return CFD_ERR_ARG;
-    t->xline_path = c->RW2 ? (c->XL3 ? 3 : 1) : 2;
-    t->xline_rows = c->RW2 ? c->RW2 : 0;
+    t->xline_path = c->RW2 ? (c->RW4 ? 4 : (c->XL3 ? 3 : 1)) : 2;
+    t->xline_rows = c->RW4 ? c->RW4 : (c->RW2 ? c->RW2 : 0);
     t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
     t->solve_kind = c->SWM ? 2 : 1;
     t->solve_cols = c->SWM ? c->SWC : 0;

@@ -19,6 +19,7 @@
 
 #include "fft_smem.cuh"
 #include "fft_reg.cuh"
+#include "fft_pair.cuh"
 #include "tridiag.cuh"
 
 namespace cfd {
@@ -443,6 +444,184 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
         T2* db = which == 0 ? (uplane ? H2 : H1) : H1;
         da[o] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
         db[o] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
+    }
+}
+
+// Pass 2 on packed line pairs (FP32 only).  The two lines of a row (u + i v, w + i 0) travel
+// together, one cpair per element (fft_pair.cuh), so every DFT instruction of k_xline2
+// serves both lines through the .f32x2 instructions.  A CTA holds RW rows and runs with
+// RW*max(N1,N2) threads: the steps of k_xline2 with one thread per row where k_xline2 has
+// one per line, and the products formed inside the thread instead of across a lane pair.
+// On v-planes the second line of the forward transform is idle (one product line per row).
+template <int N1, int N2>
+__global__ void __launch_bounds__(8 * (N1 > N2 ? N1 : N2)) k_xline4(Dims d, Geo g, const float2* __restrict__ Hx,
+                                                                     float2* __restrict__ H0, float2* __restrict__ H1,
+                                                                     float2* __restrict__ H2, float2* __restrict__ H3,
+                                                                     const float2* __restrict__ twx, int RW) {
+    using T2 = float2;
+    using R = float;
+    constexpr int N = N1 * N2;
+    constexpr int HX = N / 3;
+    constexpr int NK = HX + 1;
+    constexpr int L1 = N1 * (N2 + 1) + 1;  // inverse exchange, per row: [k1][n2]
+    constexpr int L2 = N2 * (N1 + 1) + 1;  // forward exchange, per row: [kb][na]
+    constexpr int LU = N + 1;               // unpack buffer, per row
+    constexpr int LX = (L1 > L2 ? (L1 > LU ? L1 : LU) : (L2 > LU ? L2 : LU));
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpair* ex = reinterpret_cast<cpair*>(smem_raw);  // RW * LX
+    cpair* twt = ex + (size_t)RW * LX;               // N: twt[b*N2 + a] = w^(a*b) in both lanes
+    const int slot = (blockIdx.y & 1) ? d.nyu + (blockIdx.y >> 1) : (blockIdx.y >> 1);
+    const int z0 = blockIdx.x * RW;
+    const bool uplane = slot < d.nyu;
+    const int t = threadIdx.x;
+    for (int i = t; i < N; i += blockDim.x) {
+        const int b = i / N2, a = i - b * N2;
+        const T2 w = twx[(a * b) % N];
+        twt[i] = cpair{f2b(w.x), f2b(w.y)};
+    }
+    const size_t pbase = (size_t)slot * d.ngal2 * NK;
+    const size_t pls = (size_t)d.ngal2 * NK;
+    const T2* Hu = Hx;
+    const T2* Hw = Hx + (size_t)d.nyu * pls;
+    const T2* Hv = Hx + (size_t)(2 * d.nyu) * pls;
+    const T2 *ua, *ub, *va, *vb, *wa, *wb;
+    R uca = 1, ucb = 0, vca = 1, vcb = 0;
+    if (uplane) {
+        const int sl = slot;
+        ua = ub = Hu + sl * pls;
+        wa = wb = Hw + sl * pls;
+        double ca, cb;
+        int pa;
+        if (sl == 0) {
+            pa = 1; ca = (1.0 - g.gwib) * g.vca[1]; cb = g.gwib + (1.0 - g.gwib) * g.vcb[1];
+        } else if (sl == d.nyu - 1) {
+            pa = sl - 1; ca = g.gwit + (1.0 - g.gwit) * g.vca[sl - 1]; cb = (1.0 - g.gwit) * g.vcb[sl - 1];
+        } else {
+            pa = sl; ca = g.vca[sl]; cb = g.vcb[sl];
+        }
+        va = Hv + pa * pls; vb = va - pls; vca = (R)ca; vcb = (R)cb;
+    } else {
+        const int sl = slot - d.nyu;
+        va = vb = Hv + sl * pls;
+        ua = Hu + (sl + 1) * pls; ub = ua - pls;
+        wa = Hw + (sl + 1) * pls; wb = wa - pls;
+        uca = (R)g.ufa[sl]; ucb = (R)g.ufb[sl];
+    }
+    __syncthreads();
+
+    // ---- step 1: inverse, thread (row r, n2)
+    if (t < RW * N2) {
+        const int r = (unsigned)t / N2, n2 = t - r * N2;
+        const size_t ro = (size_t)(z0 + r) * NK;
+        const T2 *A0 = ua + ro, *A1 = ub + ro, *C0 = va + ro, *C1 = vb + ro, *W0 = wa + ro, *W1 = wb + ro;
+        cpair v[N1];
+        auto fill = [&](auto vplane) {
+            constexpr bool VP = decltype(vplane)::value;
+            auto fetch = [&](int k, T2& a, T2& c, T2& w) {
+                if (VP) {
+                    const T2 a0 = A0[k], a1 = A1[k], w0 = W0[k], w1 = W1[k];
+                    a = cx<T2>(uca * a0.x + ucb * a1.x, uca * a0.y + ucb * a1.y);
+                    w = cx<T2>(uca * w0.x + ucb * w1.x, uca * w0.y + ucb * w1.y);
+                    c = C0[k];
+                } else {
+                    a = A0[k];
+                    w = W0[k];
+                    const T2 c0 = C0[k], c1 = C1[k];
+                    c = cx<T2>(vca * c0.x + vcb * c1.x, vca * c0.y + vcb * c1.y);
+                }
+            };
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) {
+                const int e0 = n1 * N2, e = e0 + n2;
+                const bool lo = (e0 + N2 - 1 <= HX) || (e0 <= HX && e <= HX);
+                const bool hi = (e0 >= N - HX) || (e0 + N2 - 1 >= N - HX && e >= N - HX);
+                cpair val = cpair{f2b(0.0f), f2b(0.0f)};
+                T2 a, c, w;
+                if (lo) {  // (A_e + i C_e, W_e); the rft inverse ignores Im of the kx = 0 entries
+                    fetch(e, a, c, w);
+                    if (n1 == 0 && n2 == 0) { a.y = 0; c.y = 0; w.y = 0; }
+                    val = cpair{f2p(a.x - c.y, w.x), f2p(a.y + c.x, w.y)};
+                } else if (hi) {  // (conj A_k + i conj C_k, conj W_k), k = N - e
+                    fetch(N - e, a, c, w);
+                    val = cpair{f2p(a.x + c.y, w.x), f2p(c.x - a.y, -w.y)};
+                }
+                v[n1] = val;
+            }
+        };
+        if (uplane) fill(std::false_type{});
+        else fill(std::true_type{});
+        rdft<N1, +1>(v);
+        cpair* o = ex + (size_t)r * L1 + n2;
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) o[k1 * (N2 + 1)] = k1 == 0 ? v[0] : cmulc(v[k1], twt[k1 * N2 + n2]);
+    }
+    __syncthreads();
+
+    // ---- step 2: inverse N2-point DFT, products, forward N2-point DFT; thread (row, k1)
+    cpair y[N2];
+    const bool act2 = t < RW * N1;
+    const int k1 = t % N1, r2 = t / N1;
+    if (act2) {
+        const cpair* o = ex + (size_t)r2 * L1 + k1 * (N2 + 1);
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) y[n2] = o[n2];
+        rdft<N2, +1>(y);
+        // lanes (u, w) in x and (v, -) in y.  u-plane: (uu + i vv, ww + i uw); v-plane:
+        // (uv + i vw, idle)
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            const R u = y[k2].x.v.x, w = y[k2].x.v.y, vv = y[k2].y.v.x;
+            if (uplane) y[k2] = cpair{mul2(y[k2].x, y[k2].x), f2p(vv * vv, u * w)};
+            else y[k2] = cpair{f2p(u * vv, 0.0f), f2p(vv * w, 0.0f)};
+        }
+        rdft<N2, -1>(y);
+#pragma unroll
+        for (int kb = 1; kb < N2; ++kb) y[kb] = cmul(y[kb], twt[k1 * N2 + kb]);
+    }
+    __syncthreads();  // every thread has read the inverse exchange
+    if (act2) {
+        cpair* o = ex + (size_t)r2 * L2 + k1;
+#pragma unroll
+        for (int kb = 0; kb < N2; ++kb) o[kb * (N1 + 1)] = y[kb];
+    }
+    __syncthreads();
+
+    // ---- step 2': forward N1-point DFT, thread (row, kb) -> X[kb + N2*ka]
+    cpair z[N1];
+    const int kb = t % N2, r3 = t / N2;
+    const bool act3 = t < RW * N2;
+    if (act3) {
+        const cpair* o = ex + (size_t)r3 * L2 + kb * (N1 + 1);
+#pragma unroll
+        for (int na = 0; na < N1; ++na) z[na] = o[na];
+        rdft<N1, -1>(z);
+    }
+    __syncthreads();
+    if (act3) {
+        cpair* o = ex + (size_t)r3 * LU + kb;
+#pragma unroll
+        for (int ka = 0; ka < N1; ++ka) o[N2 * ka] = z[ka];
+    }
+    __syncthreads();
+
+    // ---- unpack both lines: A_k = (P_k + conj P_{N-k})/2, B_k = (P_k - conj P_{N-k})/(2i), x 1/N
+    const f2x hs = f2b((R)0.5 / (R)N);
+    for (int it = t; it < RW * NK; it += blockDim.x) {
+        const int r = (unsigned)it / NK, k = it - r * NK;
+        const size_t o = pbase + (size_t)(z0 + r) * NK + k;
+        const cpair* line = ex + (size_t)r * LU;
+        const cpair P = line[k], Q = line[k == 0 ? 0 : N - k];
+        const f2x ax = mul2(add2(P.x, Q.x), hs), ay = mul2(sub2(P.y, Q.y), hs);
+        const f2x bx = mul2(add2(P.y, Q.y), hs), by = mul2(sub2(Q.x, P.x), hs);
+        // lane 0: u-plane uu / vv, v-plane uv / vw; lane 1 (u-plane): ww / uw
+        H0[o] = cx<T2>(ax.v.x, ay.v.x);
+        if (uplane) {
+            H2[o] = cx<T2>(bx.v.x, by.v.x);
+            H3[o] = cx<T2>(ax.v.y, ay.v.y);
+            H1[o] = cx<T2>(bx.v.y, by.v.y);
+        } else {
+            H1[o] = cx<T2>(bx.v.x, by.v.x);
+        }
     }
 }
 

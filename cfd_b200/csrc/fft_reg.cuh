@@ -62,14 +62,19 @@ template <int M, int N, int SIGN> struct TwC {
     static constexpr bool one = (M % N) == 0;
 };
 
+// multiplication by the compile-time twiddle TW (overloaded for packed line pairs)
+template <typename TW, typename T2> __host__ __device__ __forceinline__ T2 cmul_k(T2 v) {
+    using R = decltype(T2::x);
+    constexpr R c = (R)TW::c, s = (R)TW::s;
+    return cx<T2>(v.x * c - v.y * s, v.x * s + v.y * c);
+}
+
 template <typename T2, int M, int N, int SIGN>
 __host__ __device__ __forceinline__ T2 twmul(T2 v) {
-    using R = decltype(T2::x);
     if constexpr (TwC<M, N, SIGN>::one) {
         return v;
     } else {
-        constexpr R c = (R)TwC<M, N, SIGN>::c, s = (R)TwC<M, N, SIGN>::s;
-        return cx<T2>(v.x * c - v.y * s, v.x * s + v.y * c);
+        return cmul_k<TwC<M, N, SIGN>>(v);
     }
 }
 

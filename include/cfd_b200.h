@@ -125,7 +125,9 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  * picks them by timing the candidates on the device.
  *   xline_path   1: register two-step x-line kernel with one z transform per field plane,
  *                2: shared-memory Stockham x-line kernel with the per-slot z pass,
- *                3: as 1 with three real inputs packed into 1.5 complex lines per row
+ *                3: as 1 with three real inputs packed into 1.5 complex lines per row,
+ *                4: as 1 with the two lines of a row in packed FP32 pairs (.f32x2
+ *                   instructions; FP32-mixed only, FP64 contexts run path 1)
  *   xline_rows   rows per CTA of the two-step x-line kernel: 2, 4 or 8
  *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
  *   solve_kind   1: thread-per-column Thomas sweeps, 2: warp-per-column substitutions on

@@ -295,3 +295,34 @@ def test_packed_xline_path(torch_cuda, monkeypatch, ng1, ng2, ny):
                 continue
             assert rel(st[k], ref[k]) < tol, (prec, k, rel(st[k], ref[k]))
         g.close()
+
+
+@pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
+def test_pair_xline_path(torch_cuda, monkeypatch, ng1, ng2, ny):
+    """The line-pair x-line kernel (packed .f32x2 DFTs, CFD_XLINE_PATH=4) on every two-step
+    length: mixed within 1e-5 of the oracle after one RK3 step and within 1e-6 of the scalar
+    FP32 kernel (k_xline2); an FP64 context asked for it runs the scalar path."""
+    from cfd_b200.channel import build_channel
+    from cfd_b200.config import tiny
+    s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=ng1 + 2 * ng2))
+    o = oracle(s)
+    o.step(1)
+    ref = o.download_state()
+    monkeypatch.setenv("CFD_XLINE_PATH", "1")
+    g1 = make(s, "mixed")
+    assert g1.tuning()["xline_path"] == 1
+    g1.step(1)
+    scalar = g1.download_state()
+    g1.close()
+    monkeypatch.setenv("CFD_XLINE_PATH", "4")
+    g = make(s, "mixed")
+    assert g.tuning()["xline_path"] == 4
+    g.step(1)
+    st = g.download_state()
+    for k in ("u1", "u2", "u3"):
+        assert rel(st[k], ref[k]) < 1e-5, (k, rel(st[k], ref[k]))
+        assert rel(st[k], scalar[k]) < 1e-6, (k, rel(st[k], scalar[k]))
+    g.close()
+    g = make(s, "fp64")
+    assert g.tuning()["xline_path"] == 1
+    g.close()

@@ -52,8 +52,29 @@ def test_autotune_small(torch_cuda, tmp_path, monkeypatch):
     monkeypatch.setenv("CFD_TUNE_CACHE", str(tmp_path / "tune.json"))
     s = build_channel(tiny(64, 96, 17, cyl_diameter=0.3, cyl_spacing=1.5, seed=3))
     best, t = autotune.autotune(s, "mixed", 0, steps=2)
-    assert t > 0 and best["xline_path"] in (1, 2, 3) and best["solve_kind"] in (1, 2)
+    assert t > 0 and best["xline_path"] in (1, 2, 3, 4) and best["solve_kind"] in (1, 2)
     assert autotune.tuned(s, "mixed", 0) in (best, autotune.tuned(s, "mixed", 0))
     ch = Channel(s, device=0, precision="mixed", tuning="auto")
     assert ch.tuning() == autotune.tuned(s, "mixed", 0)
     ch.close()
+
+
+def test_pair_xline_shapes(torch_cuda):
+    """Line-pair x-line kernel (xline_path 4) at every row count it takes: the same state as
+    the scalar FP32 path to 1e-6 after two RK3 steps."""
+    s = build_channel(tiny(96, 192, 13, cyl_diameter=0.3, cyl_spacing=1.5, seed=5))
+    ref = Channel(s, device=0, precision="mixed", tuning=dict(xline_path=1))
+    ref.upload_state()
+    ref.step(2)
+    base = ref.download_state()
+    ref.close()
+    for rows in (2, 4, 8):
+        ch = Channel(s, device=0, precision="mixed", tuning=dict(xline_path=4, xline_rows=rows))
+        got = ch.tuning()
+        assert got["xline_path"] == 4 and got["xline_rows"] == rows, got
+        ch.upload_state()
+        ch.step(2)
+        st = ch.download_state()
+        for k in ("u1", "u2", "u3"):
+            assert rel(st[k], base[k]) < 1e-6, (rows, k, rel(st[k], base[k]))
+        ch.close()
