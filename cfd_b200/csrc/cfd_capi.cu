@@ -87,7 +87,11 @@ struct cfd_ctx {
     double* part = nullptr;
     int npart = 0;
     IBDev ibu, ibv;
-    void* Hib = nullptr;
+    void* Hib = nullptr;    // IB round-trip planes of the u grid (u, w: 4 fields)
+    void* Hib_v = nullptr;  // and of the v grid (2 fields), so the two round trips can overlap
+    void* phys_v = nullptr;
+    cudaStream_t side = nullptr;                     // the v-grid IB branch
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void* Hx = nullptr;     // z-transformed u, w, v on their own planes (two-step x-line path)
     void* phys = nullptr;
     // FFT
@@ -490,7 +494,8 @@ int rhs_kernel(cfd_ctx* c, int krk) {
 
 // immersed_boundaries_U (u1,u3) and immersed_boundaries_V (u2)
 template <typename T2>
-int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2* u_a, double2* rhs_b, double2* u_b) {
+int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2* u_a, double2* rhs_b, double2* u_b,
+            void* Hib, void* phys) {
     if (ib.npl == 0) return CFD_OK;
     using R = decltype(T2::x);
     const Dims& d = c->d;
@@ -506,14 +511,14 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         dim3 g1((ib.npl * d.nkx + CH2 - 1) / CH2, 1, 2 * nb);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
-            k_ib_zinv2<T2, TN1, TN2><<<g1, c->NTZ2, c->SMZ2, c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib,
+            k_ib_zinv2<T2, TN1, TN2><<<g1, c->NTZ2, c->SMZ2, c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)Hib,
                                                                         twz<T2>(c), c->LZ2);
         });
         LK("k_ib_zinv2");
     } else {
         dim3 g1((d.nkx + CH - 1) / CH, ib.npl, 2 * nb);
         FFT_SWITCH(d.ngal2, {
-            k_ib_zinv<T2, NF><<<g1, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)c->Hib,
+            k_ib_zinv<T2, NF><<<g1, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)Hib,
                                                                             c->fz, twz<T2>(c), CH, ilog2(CH));
         });
         LK("k_ib_zinv");
@@ -524,7 +529,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         bool ok = true;
         if (ib.nact > 0) {
             TWO_SWITCH(d.ngal1, ok, {
-                k_ib_xinv2<T2, TN1, TN2><<<g2, c->NTIX2, c->SMIX2, c->stream>>>(d, (T2*)c->Hib, ib.npl, (R*)c->phys,
+                k_ib_xinv2<T2, TN1, TN2><<<g2, c->NTIX2, c->SMIX2, c->stream>>>(d, (T2*)Hib, ib.npl, (R*)phys,
                                                                               ib.arow, ib.nact, twx<T2>(c), c->RWIX2);
             });
             LK("k_ib_xinv2");
@@ -533,14 +538,14 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         dim3 g2(d.ngal2 / c->RWib, ib.npl, nb);
         FFT_SWITCH(d.ngal1, {
             k_ib_xinv<T2, NF><<<g2, 256, (size_t)(2 * c->RWib * d.ngal1 + d.ngal1) * e, c->stream>>>(
-                d, (T2*)c->Hib, ib.npl, (R*)c->phys, c->fx, twx<T2>(c), c->RWib, ilog2(c->RWib));
+                d, (T2*)Hib, ib.npl, (R*)phys, c->fx, twx<T2>(c), c->RWib, ilog2(c->RWib));
         });
         LK("k_ib_xinv");
     }
     if (ib.n > 0) {
         dim3 g3((ib.n + 255) / 256, nb);
         prof_mark(c);
-        k_ib_force<R><<<g3, 256, 0, c->stream>>>(d, ib.idx, ib.w, ib.n, ib.slot_of_j, j0, ib.npl, (R*)c->phys);
+        k_ib_force<R><<<g3, 256, 0, c->stream>>>(d, ib.idx, ib.w, ib.n, ib.slot_of_j, j0, ib.npl, (R*)phys);
         LK("k_ib_force");
     }
     prof_mark(c);
@@ -550,7 +555,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         if (ib.nact > 0) {
             TWO_SWITCH(d.ngal1, ok, {
                 k_ib_xfwd2<T2, TN1, TN2><<<g4, c->NTFX2, c->SMFX2, c->stream>>>(
-                    d, (T2*)c->Hib, ib.npl, (const R*)c->phys, ib.arow, ib.nact, twx<T2>(c), c->RWFX2);
+                    d, (T2*)Hib, ib.npl, (const R*)phys, ib.arow, ib.nact, twx<T2>(c), c->RWFX2);
             });
             LK("k_ib_xfwd2");
         }
@@ -558,7 +563,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         dim3 g4(d.ngal2 / c->RWibf, ib.npl, nb);
         FFT_SWITCH(d.ngal1, {
             k_ib_xfwd<T2, NF><<<g4, 256, (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * e, c->stream>>>(
-                d, (T2*)c->Hib, ib.npl, (const R*)c->phys, c->fx, twx<T2>(c), c->RWibf, ilog2(c->RWibf / 2));
+                d, (T2*)Hib, ib.npl, (const R*)phys, c->fx, twx<T2>(c), c->RWibf, ilog2(c->RWibf / 2));
         });
         LK("k_ib_xfwd");
     }
@@ -568,7 +573,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         dim3 g5((ib.npl * d.nkx + CH2 - 1) / CH2, 1, nb);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
-            k_ib_zfwd2<T2, TN1, TN2><<<g5, c->NTZ2, c->SMZ2, c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0,
+            k_ib_zfwd2<T2, TN1, TN2><<<g5, c->NTZ2, c->SMZ2, c->stream>>>(d, (const T2*)Hib, ib.npl, dst, j0,
                                                                         ib.planes, c->RWIX2 ? ib.rowflag : nullptr,
                                                                         twz<T2>(c), c->LZ2);
         });
@@ -576,7 +581,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     } else {
         dim3 g5((d.nkx + CH - 1) / CH, ib.npl, nb);
         FFT_SWITCH(d.ngal2, {
-            k_ib_zfwd<T2, NF><<<g5, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (const T2*)c->Hib, ib.npl, dst, j0,
+            k_ib_zfwd<T2, NF><<<g5, 256, zsmem(d.ngal2, CH, e), c->stream>>>(d, (const T2*)Hib, ib.npl, dst, j0,
                                                                             ib.planes, c->fz, twz<T2>(c), CH, ilog2(CH));
         });
         LK("k_ib_zfwd");
@@ -584,11 +589,29 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     return CFD_OK;
 }
 
+// immersed_boundaries_U on u and w, immersed_boundaries_V on v.  The two round trips touch
+// disjoint fields and buffers, so the v-grid one runs on a side stream forked from and joined
+// back into the context stream (two parallel branches when captured in a graph).  With the
+// per-kernel profiler on they run one after the other on the context stream.
 template <typename T2>
 int ib_all(cfd_ctx* c) {
-    int s = ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3);
+    const bool par = c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling;
+    if (!par) {
+        int s = ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys);
+        if (s != CFD_OK) return s;
+        return ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v);
+    }
+    CK(cudaEventRecord(c->ev_fork, c->stream));
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    cudaStream_t main = c->stream;
+    c->stream = c->side;
+    int s = ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v);
+    c->stream = main;
+    const cudaError_t ej = cudaEventRecord(c->ev_join, c->side);  // join even after a failure
+    if (ej == cudaSuccess) cudaStreamWaitEvent(c->stream, c->ev_join, 0);
     if (s != CFD_OK) return s;
-    return ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr);
+    CK(ej);
+    return ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys);
 }
 
 size_t solve_w_smem(const Dims& d, int swc) {
@@ -1064,15 +1087,19 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     // immersed boundaries
     if ((s = setup_ib(c, ibu, d.ju0, d.ju1, c->ibu, "ibu")) != CFD_OK) return s;
     if ((s = setup_ib(c, ibv, d.jv0, d.jv1, c->ibv, "ibv")) != CFD_OK) return s;
-    const size_t nibp = std::max((size_t)4 * c->ibu.npl, (size_t)2 * c->ibv.npl);
-    if (nibp > 0) {
-        if (mixed) {
-            AL(c->Hib, float2, nibp * d.ngal2 * d.nkx);
-            AL(c->phys, float, nibp * d.ngal2 * d.ngal1);
-        } else {
-            AL(c->Hib, double2, nibp * d.ngal2 * d.nkx);
-            AL(c->phys, double, nibp * d.ngal2 * d.ngal1);
-        }
+    const size_t nibu = (size_t)4 * c->ibu.npl, nibv = (size_t)2 * c->ibv.npl;
+    const size_t hz = (size_t)d.ngal2 * d.nkx, hx = (size_t)d.ngal2 * d.ngal1;
+    if (mixed) {
+        if (nibu) { AL(c->Hib, float2, nibu * hz); AL(c->phys, float, nibu * hx); }
+        if (nibv) { AL(c->Hib_v, float2, nibv * hz); AL(c->phys_v, float, nibv * hx); }
+    } else {
+        if (nibu) { AL(c->Hib, double2, nibu * hz); AL(c->phys, double, nibu * hx); }
+        if (nibv) { AL(c->Hib_v, double2, nibv * hz); AL(c->phys_v, double, nibv * hx); }
+    }
+    if (nibu && nibv) {
+        CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     }
     if ((s = factor_all(c)) != CFD_OK) return s;
     CK(cudaDeviceSynchronize());
@@ -1266,7 +1293,11 @@ int cfd_destroy(cfd_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     destroy_graph(c);
+    if (c->side) cudaStreamSynchronize(c->side);
     for (void* p : c->allocs) cudaFree(p);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return CFD_OK;
