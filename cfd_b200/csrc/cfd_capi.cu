@@ -100,6 +100,7 @@ struct cfd_ctx {
     float2 *twx_f = nullptr, *twz_f = nullptr;
     int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
     int RW2 = 0, NT2 = 0;
+    bool XSW = false;       // k_xline2 with the factors of its two-step split swapped
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
     int RW4 = 0, NT4 = 0;   // line-pair x-line kernel (k_xline4, FP32): rows per CTA (0 = not used), threads
     size_t SM4 = 0;
@@ -264,6 +265,24 @@ int ilog2(int b) {
         default: ok = false; break;                                          \
     }
 
+// The same lengths with the factors of the x-line kernel's split swapped (N1 > N2 becomes
+// the second, per-k1 step): the heaviest step (inverse DFT, products, forward DFT) then runs
+// on max(N1, N2) threads per line instead of the smaller factor.
+#define XL_SWITCH(n, swap, ok, ...)                                                    \
+    if (!(swap)) {                                                                     \
+        TWO_SWITCH(n, ok, __VA_ARGS__);                                                \
+    } else {                                                                           \
+        switch (n) {                                                                   \
+            case 64: { constexpr int TN1 = 8, TN2 = 8; __VA_ARGS__; } break;           \
+            case 96: { constexpr int TN1 = 12, TN2 = 8; __VA_ARGS__; } break;          \
+            case 128: { constexpr int TN1 = 16, TN2 = 8; __VA_ARGS__; } break;         \
+            case 192: { constexpr int TN1 = 12, TN2 = 16; __VA_ARGS__; } break;        \
+            case 384: { constexpr int TN1 = 24, TN2 = 16; __VA_ARGS__; } break;        \
+            case 768: { constexpr int TN1 = 24, TN2 = 32; __VA_ARGS__; } break;        \
+            default: ok = false; break;                                                \
+        }                                                                              \
+    }
+
 // shared memory of k_xline2 (elements): B*LX + N
 // Launch-shape overrides (unset: the built-in choice; a cfd_tuning field takes precedence).
 //   CFD_XLINE_ROWS   rows per CTA of the two-step x-line kernel (power of two, 2..8)
@@ -347,9 +366,11 @@ int set_smem_attrs(cfd_ctx* c) {
     }
     if (c->RW2) {
         bool ok = true;
-        TWO_SWITCH(n1, ok, {
+        XL_SWITCH(n1, c->XSW, ok, {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
+        });
+        TWO_SWITCH(n1, ok, {
             if (e == cudaSuccess && c->XL3)
                 e = cudaFuncSetAttribute(k_xline3<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM3);
             if constexpr (std::is_same<T2, float2>::value)
@@ -443,7 +464,7 @@ int nl_transforms(cfd_ctx* c) {
     } else if (c->RW2) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
-        TWO_SWITCH(d.ngal1, ok, {
+        XL_SWITCH(d.ngal1, c->XSW, ok, {
             k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2],
                                                                     (T2*)c->H[3], twx<T2>(c), c->RW2, ilog2(c->RW2));
         });
@@ -948,14 +969,18 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
+        // k_xline2's split: the production one, or swapped
+        c->XSW = env_int("CFD_XLINE_SWAP", 0, 0, 1) != 0;
+        int n1x = 0, n2x = 0;
+        XL_SWITCH(d.ngal1, c->XSW, ok, { n1x = TN1; n2x = TN2; });
         if (ok) {
             int rw = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", mixed ? 8 : 4, 2, 8);
             rw = 1 << (31 - __builtin_clz(rw));  // a power of two
-            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
-            if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
+            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1x, n2x, rw, esz) > budget)) rw /= 2;
+            if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1x) % 32 == 0) {
                 c->RW2 = rw;
-                c->NT2 = 2 * rw * std::max(n1s, n2s);
-                c->SM2 = xline2_smem(n1s, n2s, rw, esz);
+                c->NT2 = 2 * rw * std::max(n1x, n2x);
+                c->SM2 = xline2_smem(n1x, n2x, rw, esz);
                 // packed lines (k_xline3): twiddles, exchange of 2*rw lines, physical rows /
                 // forward spectra
                 const size_t N = (size_t)n1s * n2s, LX = (size_t)((n1s * (n2s + 1)) | 1);
@@ -1486,6 +1511,8 @@ int cfd_get_scalars(cfd_ctx* c, double* mpgx, double* qx, double* dgx) {
     if (mpgx) *mpgx = h[0];
     if (qx) *qx = h[1];
     if (dgx) *dgx = h[2];
+    if (!std::isfinite(h[0]) || !std::isfinite(h[1]) || !std::isfinite(h[2]))
+        return fail(c, CFD_ERR_NONFINITE, "non-finite mean-flow scalars (mpgx %g, Qx %g)", h[0], h[1]);
     return CFD_OK;
 }
 
@@ -1817,11 +1844,20 @@ int cfd_cfl(cfd_ctx* c, double* dtc, double* terms) {
     std::vector<double> h((size_t)3 * d.nyu);
     CK(cudaMemcpy(h.data(), c->st.mx, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
     double um = 0.0, wm = 0.0, vm = 1e-6;
-    for (int j = 0; j < d.nyu; ++j) { um = std::max(um, h[j]); wm = std::max(wm, h[d.nyu + j]); }
-    for (int j = 1; j < d.nyv - 1; ++j) vm = std::max(vm, h[2 * d.nyu + j]);
+    bool bad = false;
+    for (int j = 0; j < d.nyu; ++j) {
+        bad = bad || !std::isfinite(h[j]) || !std::isfinite(h[d.nyu + j]);
+        um = std::max(um, h[j]);
+        wm = std::max(wm, h[d.nyu + j]);
+    }
+    for (int j = 1; j < d.nyv - 1; ++j) {
+        bad = bad || !std::isfinite(h[2 * d.nyu + j]);
+        vm = std::max(vm, h[2 * d.nyu + j]);
+    }
     const double t0 = 1.0 / (c->alp * (d.n1 / 2) * um), t1 = 1.0 / (c->bet * (d.n2 / 2) * wm), t2 = 1.0 / vm;
-    if (terms) { terms[0] = t0; terms[1] = t1; terms[2] = t2; }
-    *dtc = std::min(t0, t1);
+    if (terms) { terms[0] = bad ? NAN : t0; terms[1] = bad ? NAN : t1; terms[2] = bad ? NAN : t2; }
+    *dtc = bad ? NAN : std::min(t0, t1);
+    if (bad) return fail(c, CFD_ERR_NONFINITE, "non-finite velocity in the physical planes");
     return CFD_OK;
 }
 

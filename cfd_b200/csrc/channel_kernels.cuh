@@ -63,6 +63,9 @@ __device__ __forceinline__ double2 dik(double k, double2 a) { return dc(-k * a.y
 template <typename T2> __device__ __forceinline__ T2 to_t2(double2 a);
 template <> __device__ __forceinline__ float2 to_t2<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
 template <> __device__ __forceinline__ double2 to_t2<double2>(double2 a) { return a; }
+// max that keeps a NaN (fmax drops it), so that the reductions of the diagnostics see a
+// non-finite field
+__device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
 __device__ __forceinline__ double2 to_d2(float2 a) { return dc((double)a.x, (double)a.y); }
 __device__ __forceinline__ double2 to_d2(double2 a) { return a; }
 
@@ -2021,12 +2024,12 @@ __global__ void k_absmax(const double2* __restrict__ a, size_t n, double* __rest
     double m = 0.0;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
         const double2 v = a[t];
-        m = fmax(m, sqrt(v.x * v.x + v.y * v.y));
+        m = nan_max(m, sqrt(v.x * v.x + v.y * v.y));
     }
     sm[threadIdx.x] = m;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + s]);
+        if (threadIdx.x < s) sm[threadIdx.x] = nan_max(sm[threadIdx.x], sm[threadIdx.x + s]);
         __syncthreads();
     }
     if (threadIdx.x == 0) part[blockIdx.x] = sm[0];

@@ -84,12 +84,12 @@ __global__ void __launch_bounds__(256) k_st_sums(Dims d, Geo g, const double* __
         if (KIND == 0) {
             const double x1 = f1[o], x2 = f2[o];
             s[0] += x0; s[1] += x0 * x0; s[2] += x1; s[3] += x1 * x1; s[4] += x0 * x2; s[5] += x0 * x1;
-            m0 = fmax(m0, fabs(x0)); m1 = fmax(m1, fabs(x1));
+            m0 = nan_max(m0, fabs(x0)); m1 = nan_max(m1, fabs(x1));
         } else if (KIND == 1) {
             const double x1 = f1[o];
             s[0] += x0; s[1] += x0 * x0; s[4] += x0 * x1;
             if (i < d.n1 && k < d.n2) { const double x2 = f2[o]; s[2] += x2; s[3] += x2 * x2; }
-            m0 = fmax(m0, fabs(x0));
+            m0 = nan_max(m0, fabs(x0));
         } else {
             s[0] += x0; s[1] += x0 * x0;
         }
@@ -104,9 +104,9 @@ __global__ void __launch_bounds__(256) k_st_sums(Dims d, Geo g, const double* __
         if (threadIdx.x < w) {
 #pragma unroll
             for (int k = 0; k < NQ; ++k) red[k * 256 + threadIdx.x] += red[k * 256 + threadIdx.x + w];
-            red[NQ * 256 + threadIdx.x] = fmax(red[NQ * 256 + threadIdx.x], red[NQ * 256 + threadIdx.x + w]);
+            red[NQ * 256 + threadIdx.x] = nan_max(red[NQ * 256 + threadIdx.x], red[NQ * 256 + threadIdx.x + w]);
             red[(NQ + 1) * 256 + threadIdx.x] =
-                fmax(red[(NQ + 1) * 256 + threadIdx.x], red[(NQ + 1) * 256 + threadIdx.x + w]);
+                nan_max(red[(NQ + 1) * 256 + threadIdx.x], red[(NQ + 1) * 256 + threadIdx.x + w]);
         }
         __syncthreads();
     }

@@ -189,7 +189,9 @@ int cfd_rk_substep(cfd_ctx *ctx, int32_t krk);
 int cfd_step(cfd_ctx *ctx, int32_t nsteps);
 
 /* Scalars of the mean mode: mpgx, Qx (flow rate between the crests), dgx (last
- * correction).  Synchronises the context stream. */
+ * correction).  Synchronises the context stream.  These are the cheap watchdog of a run: a
+ * NaN or Inf anywhere in the flow reaches the mean mode through the nonlinear term within
+ * one step, and the call then returns CFD_ERR_NONFINITE (the values are still written). */
 int cfd_get_scalars(cfd_ctx *ctx, double *mpgx, double *qx, double *dgx);
 
 /* Largest |div| over all columns and p-planes (error(), littleharsh.f90:322-351).
@@ -274,7 +276,8 @@ int cfd_spectra_read(cfd_ctx *ctx, double *spu, double *spv, double *spw, double
  * with the maxima over the physical u, w planes (all) and v planes (walls excluded).
  * *dtc is the reference's result min(terms[0], terms[1]): its v term divides by
  * dthetavi, a module variable that nothing assigns (declaration.f90:72; only ddthetavi is
- * set, start.f90:684), so that term is 1/0 = +Inf and never limits the step. */
+ * set, start.f90:684), so that term is 1/0 = +Inf and never limits the step.
+ * A NaN or Inf in the physical u, v, w planes gives CFD_ERR_NONFINITE with NaN results. */
 int cfd_cfl(cfd_ctx *ctx, double *dtc, double *terms);
 
 /* Changes the time step used by every following stage and step (the reference's

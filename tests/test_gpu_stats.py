@@ -155,3 +155,29 @@ def test_spectra_vs_oracle(torch_cuda, cfg, precision):
     with pytest.raises(RuntimeError, match="spectra not configured"):
         g.spectra_read()
     g.close()
+
+
+def test_nonfinite_watchdog(torch_cuda):
+    """A NaN planted in one interior spectral coefficient of u (host data, no GPU fault):
+    the CFL query reports CFD_ERR_NONFINITE at once, and after one RK3 step the mean-mode
+    scalars and the divergence do; a clean context is unaffected."""
+    from cfd_b200.channel import Channel
+    s = build_channel(tiny(24, 18, 17))
+    st = s.state()
+    bad = {k: v.copy() for k, v in st.items()}
+    bad["u1"][5, s.grid.nyu // 2] = complex(np.nan, 0.0)
+    for prec in ("fp64", "mixed"):
+        g = Channel(s, device=0, precision=prec)
+        g.upload_state(st)
+        g.step(1)
+        g.cfl()
+        g.scalars()
+        g.upload_state(bad)
+        with pytest.raises(RuntimeError, match="CFD_ERR_NONFINITE|non-finite"):
+            g.cfl()
+        g.step(1)
+        with pytest.raises(RuntimeError, match="CFD_ERR_NONFINITE|non-finite"):
+            g.scalars()
+        with pytest.raises(RuntimeError, match="CFD_ERR_NONFINITE|non-finite"):
+            g.divergence_max()
+        g.close()
