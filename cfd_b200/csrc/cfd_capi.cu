@@ -100,7 +100,6 @@ struct cfd_ctx {
     float2 *twx_f = nullptr, *twz_f = nullptr;
     int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
     int RW2 = 0, NT2 = 0;
-    bool XSW = false;       // k_xline2 with the factors of its two-step split swapped
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
     int RW4 = 0, NT4 = 0;   // line-pair x-line kernel (k_xline4, FP32): rows per CTA (0 = not used), threads
     size_t SM4 = 0;
@@ -265,24 +264,6 @@ int ilog2(int b) {
         default: ok = false; break;                                          \
     }
 
-// The same lengths with the factors of the x-line kernel's split swapped (N1 > N2 becomes
-// the second, per-k1 step): the heaviest step (inverse DFT, products, forward DFT) then runs
-// on max(N1, N2) threads per line instead of the smaller factor.
-#define XL_SWITCH(n, swap, ok, ...)                                                    \
-    if (!(swap)) {                                                                     \
-        TWO_SWITCH(n, ok, __VA_ARGS__);                                                \
-    } else {                                                                           \
-        switch (n) {                                                                   \
-            case 64: { constexpr int TN1 = 8, TN2 = 8; __VA_ARGS__; } break;           \
-            case 96: { constexpr int TN1 = 12, TN2 = 8; __VA_ARGS__; } break;          \
-            case 128: { constexpr int TN1 = 16, TN2 = 8; __VA_ARGS__; } break;         \
-            case 192: { constexpr int TN1 = 12, TN2 = 16; __VA_ARGS__; } break;        \
-            case 384: { constexpr int TN1 = 24, TN2 = 16; __VA_ARGS__; } break;        \
-            case 768: { constexpr int TN1 = 24, TN2 = 32; __VA_ARGS__; } break;        \
-            default: ok = false; break;                                                \
-        }                                                                              \
-    }
-
 // shared memory of k_xline2 (elements): B*LX + N
 // Launch-shape overrides (unset: the built-in choice; a cfd_tuning field takes precedence).
 //   CFD_XLINE_ROWS   rows per CTA of the two-step x-line kernel (power of two, 2..8)
@@ -366,11 +347,9 @@ int set_smem_attrs(cfd_ctx* c) {
     }
     if (c->RW2) {
         bool ok = true;
-        XL_SWITCH(n1, c->XSW, ok, {
+        TWO_SWITCH(n1, ok, {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
-        });
-        TWO_SWITCH(n1, ok, {
             if (e == cudaSuccess && c->XL3)
                 e = cudaFuncSetAttribute(k_xline3<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM3);
             if constexpr (std::is_same<T2, float2>::value)
@@ -464,7 +443,7 @@ int nl_transforms(cfd_ctx* c) {
     } else if (c->RW2) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
-        XL_SWITCH(d.ngal1, c->XSW, ok, {
+        TWO_SWITCH(d.ngal1, ok, {
             k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2],
                                                                     (T2*)c->H[3], twx<T2>(c), c->RW2, ilog2(c->RW2));
         });
@@ -969,18 +948,14 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
-        // k_xline2's split: the production one, or swapped
-        c->XSW = env_int("CFD_XLINE_SWAP", 0, 0, 1) != 0;
-        int n1x = 0, n2x = 0;
-        XL_SWITCH(d.ngal1, c->XSW, ok, { n1x = TN1; n2x = TN2; });
         if (ok) {
             int rw = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", mixed ? 8 : 4, 2, 8);
             rw = 1 << (31 - __builtin_clz(rw));  // a power of two
-            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1x, n2x, rw, esz) > budget)) rw /= 2;
-            if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1x) % 32 == 0) {
+            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
+            if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
                 c->RW2 = rw;
-                c->NT2 = 2 * rw * std::max(n1x, n2x);
-                c->SM2 = xline2_smem(n1x, n2x, rw, esz);
+                c->NT2 = 2 * rw * std::max(n1s, n2s);
+                c->SM2 = xline2_smem(n1s, n2s, rw, esz);
                 // packed lines (k_xline3): twiddles, exchange of 2*rw lines, physical rows /
                 // forward spectra
                 const size_t N = (size_t)n1s * n2s, LX = (size_t)((n1s * (n2s + 1)) | 1);
