@@ -92,6 +92,7 @@ struct cfd_ctx {
     void* phys_v = nullptr;
     cudaStream_t side = nullptr;                     // the v-grid IB branch
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool hx_valid = false;  // Hx holds the z transforms of the current u, w, v (nonlinear pass)
     void* Hx = nullptr;     // z-transformed u, w, v on their own planes (two-step x-line path)
     void* phys = nullptr;
     // FFT
@@ -397,6 +398,7 @@ int nl_transforms(cfd_ctx* c) {
                                                                       twz<T2>(c), c->LZ2);
         });
         LK("k_zinv2s");
+        c->hx_valid = true;
     } else if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
         dim3 gz2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 3, 2);
@@ -495,8 +497,11 @@ int rhs_kernel(cfd_ctx* c, int krk) {
 // immersed_boundaries_U (u1,u3) and immersed_boundaries_V (u2)
 template <typename T2>
 int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2* u_a, double2* rhs_b, double2* u_b,
-            void* Hib, void* phys) {
+            void* Hib, void* phys, int voff0, int voff1) {
     if (ib.npl == 0) return CFD_OK;
+    // the velocities' inverse z transforms are those of the nonlinear pass when it left them
+    IBVel vel{nullptr, {voff0, voff1}, ib.planes, j0};
+    if (c->hx_valid && c->RW2 && c->LZ2 >= 0 && c->RWIX2) vel.H = c->Hx;
     using R = decltype(T2::x);
     const Dims& d = c->d;
     const int CH = c->CHz;
@@ -508,11 +513,11 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     prof_mark(c);
     if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
-        dim3 g1((ib.npl * d.nkx + CH2 - 1) / CH2, 1, 2 * nb);
+        dim3 g1((ib.npl * d.nkx + CH2 - 1) / CH2, 1, vel.H ? nb : 2 * nb);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
             k_ib_zinv2<T2, TN1, TN2><<<g1, c->NTZ2, c->SMZ2, c->stream>>>(d, src, j0, ib.planes, ib.npl, (T2*)Hib,
-                                                                        twz<T2>(c), c->LZ2);
+                                                                        twz<T2>(c), c->LZ2, vel.H ? 2 : 1);
         });
         LK("k_ib_zinv2");
     } else {
@@ -530,7 +535,8 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         if (ib.nact > 0) {
             TWO_SWITCH(d.ngal1, ok, {
                 k_ib_xinv2<T2, TN1, TN2><<<g2, c->NTIX2, c->SMIX2, c->stream>>>(d, (T2*)Hib, ib.npl, (R*)phys,
-                                                                              ib.arow, ib.nact, twx<T2>(c), c->RWIX2);
+                                                                              ib.arow, ib.nact, twx<T2>(c), c->RWIX2,
+                                                                              vel);
             });
             LK("k_ib_xinv2");
         }
@@ -597,21 +603,22 @@ template <typename T2>
 int ib_all(cfd_ctx* c) {
     const bool par = c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling;
     if (!par) {
-        int s = ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys);
+        int s = ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys, 0, c->d.nyu);
         if (s != CFD_OK) return s;
-        return ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v);
+        return ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v,
+                           2 * c->d.nyu, 0);
     }
     CK(cudaEventRecord(c->ev_fork, c->stream));
     CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
     cudaStream_t main = c->stream;
     c->stream = c->side;
-    int s = ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v);
+    int s = ib_grid<T2>(c, c->ibv, c->d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v, 2 * c->d.nyu, 0);
     c->stream = main;
     const cudaError_t ej = cudaEventRecord(c->ev_join, c->side);  // join even after a failure
     if (ej == cudaSuccess) cudaStreamWaitEvent(c->stream, c->ev_join, 0);
     if (s != CFD_OK) return s;
     CK(ej);
-    return ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys);
+    return ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys, 0, c->d.nyu);
 }
 
 size_t solve_w_smem(const Dims& d, int swc) {
@@ -705,6 +712,7 @@ int substep(cfd_ctx* c, int krk) {
     if ((s = nl_transforms<T2>(c)) != CFD_OK) return s;
     if ((s = rhs_kernel<T2, 7>(c, krk)) != CFD_OK) return s;
     if ((s = ib_all<T2>(c)) != CFD_OK) return s;
+    c->hx_valid = false;  // the solve changes u, v, w
     if ((s = solve_kernel(c, krk)) != CFD_OK) return s;
     if (c->ctpress == 0 && (s = meanflow_kernel(c, krk)) != CFD_OK) return s;
     // solveP + v_corr in one column sweep (psi is not stored on this path)
@@ -1337,6 +1345,7 @@ int cfd_upload_field(cfd_ctx* c, int32_t field, const double* host, int32_t layo
     if (!field_info(c, field, fi)) return fail(c, CFD_ERR_ARG, "bad field %d", field);
     if (layout != CFD_LAYOUT_REF && layout != CFD_LAYOUT_PLANE) return fail(c, CFD_ERR_ARG, "bad layout %d", layout);
     CK(cudaSetDevice(c->device));
+    if (field <= CFD_FIELD_U3) c->hx_valid = false;  // the nonlinear pass's transforms are stale
     const size_t n = (size_t)fi.nplanes * c->d.ncol;
     double2* dst = fi.single ? c->stage1 : (double2*)fi.ptr;
     if (layout == CFD_LAYOUT_PLANE) {
@@ -1389,6 +1398,7 @@ int cfd_field_device_ptr(cfd_ctx* c, int32_t field, void** dev_ptr) {
     if (!field_info(c, field, fi)) return fail(c, CFD_ERR_ARG, "bad field %d", field);
     *dev_ptr = fi.ptr;
     if (field <= CFD_FIELD_P) c->state_loaded = true;
+    if (field <= CFD_FIELD_U3) c->hx_valid = false;  // the caller may write the field
     return CFD_OK;
 }
 
@@ -1419,6 +1429,7 @@ int cfd_solve_uvw(cfd_ctx* c, int32_t krk) {
         if ((s = rhs_kernel<double2, 4>(c, krk))) return s;
         if ((s = ib_all<double2>(c))) return s;
     }
+    c->hx_valid = false;  // the solve changes u, v, w
     return solve_kernel(c, krk);
 }
 

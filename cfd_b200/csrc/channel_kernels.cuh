@@ -1325,11 +1325,12 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
 // IB round trip with the two-step transform (same data flow as k_ib_zinv/xinv/xfwd/zfwd).
 template <typename T2, int TN1, int TN2>
 __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_ib_zinv2(Dims d, IBSrc src, int j0, const int* __restrict__ planes, int npl, T2* __restrict__ Hib,
-                           const T2* __restrict__ twz, int lb) {
+                           const T2* __restrict__ twz, int lb, int sstep) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     const int nlines = npl * d.nkx;
-    const int line0 = blockIdx.x << lb, sidx = blockIdx.z;
+    // sstep 2: the right-hand sides only (the velocities come from the nonlinear pass)
+    const int line0 = blockIdx.x << lb, sidx = blockIdx.z * sstep;
     if (line0 >= nlines) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* twt = reinterpret_cast<T2*>(smem_raw);
@@ -1354,9 +1355,19 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
 }
 
 // inverse x: line (rhs + i u) of each of RW rows -> physical rhs, u (rows coalesced in x)
+// With Hvel, the velocity of batch fb is read from the z-transformed field planes of the
+// nonlinear pass (k_zinv2s, the same transform of the same state): plane voff[fb] + (j - j0)
+// of Hvel for the IB plane j = planes[p].
+struct IBVel {
+    const void* H;
+    int voff[2];
+    const int* planes;
+    int j0;
+};
+
 template <typename T2, int TN1, int TN2>
 __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype(T2::x)* __restrict__ phys,
-                           const int* __restrict__ arow, int nact, const T2* __restrict__ twx, int RW) {
+                           const int* __restrict__ arow, int nact, const T2* __restrict__ twx, int RW, IBVel vel) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     constexpr int HX = N / 3;   // highest retained kx (N1 = 2*(Ngal1/3))
@@ -1370,7 +1381,8 @@ __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype
     // line b of the CTA is active row arow[z0 + b] (the last one repeated past the end: the
     // repeated line writes the same values again)
     const T2* Hr = Hib + ((size_t)(2 * fb) * npl + p) * pl;
-    const T2* Hu = Hib + ((size_t)(2 * fb + 1) * npl + p) * pl;
+    const T2* Hu = vel.H ? (const T2*)vel.H + (size_t)(vel.voff[fb] + vel.planes[p] - vel.j0) * pl
+                         : Hib + ((size_t)(2 * fb + 1) * npl + p) * pl;
     auto row_of_line = [&](int b) { return arow[min(z0 + b, nact - 1)]; };
     // this thread's offset within its stride-TN2 subsequence, computed as two_step_lines
     // does, so that e - n2 is a compile-time constant in the unrolled element loop
