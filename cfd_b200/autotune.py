@@ -1,10 +1,11 @@
 """Autotuner of the launch shapes (cfd_tuning): for one grid, precision and GPU it builds a
 context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
 
-Candidates: the x-line path (register two-step, its packed form, or shared-memory Stockham), rows per CTA of
-the two-step x-line kernel, lines per CTA of the two-step z kernels, and the solve kind
-(thread-per-column sweeps or warp-per-column substitutions, with 4 or 8 columns per CTA),
-and the y-planes per thread of the right-hand-side kernel.
+Candidates: the x-line path (register two-step; the same with 1.5 complex lines per row;
+the same on packed FP32 line pairs; or shared-memory Stockham), rows per CTA of the two-step
+x-line kernel, lines per CTA of the two-step z kernels, the solve kind (thread-per-column
+sweeps or warp-per-column substitutions, with 4 or 8 columns per CTA), and the y-planes per
+thread of the right-hand-side kernel.
 The search is coordinate-wise from the library default, one knob at a time, so it costs a
 dozen short timings.  Results are cached in a JSON file keyed by grid, precision and GPU
 name (CFD_TUNE_CACHE, default ~/.cache/cfd_b200/tuning.json).
@@ -16,6 +17,11 @@ import os
 
 KNOBS = (("xline_path", (1, 2, 3, 4)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
          ("solve_kind", (1, 2)), ("solve_cols", (4, 8)), ("rhs_chunk", (2, 4, 8, 16)))
+
+
+# knobs that only act with another setting (the library reports them as 0 otherwise)
+RELEVANT = {"solve_cols": lambda t: t.get("solve_kind") == 2,
+            "xline_rows": lambda t: t.get("xline_path") != 2}
 
 
 def _cache_path() -> str:
@@ -55,6 +61,8 @@ def autotune(setup, precision: str, device: int = 0, steps: int = 5, log=None):
     tried = {json.dumps(best, sort_keys=True)}
     for name, values in KNOBS:
         for v in values:
+            if name in RELEVANT and not RELEVANT[name](best):
+                continue
             cand = dict(best, **{name: v})
             k = json.dumps(cand, sort_keys=True)
             if k in tried:

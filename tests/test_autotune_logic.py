@@ -1,0 +1,81 @@
+"""The autotuner's coordinate search and cache (cfd_b200.autotune) with a fake timing model
+in place of the device (CPU)."""
+import json
+
+import pytest
+
+from cfd_b200 import autotune
+
+DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "solve_cols": 0, "rhs_chunk": 16}
+
+
+def fake_model(calls, bad=()):
+    """Seconds per step: a separable cost with its minimum at xline_rows 4, zlines 16,
+    rhs_chunk 4; path 2 is slow, warp solves are slow; shapes in `bad` raise."""
+    def time_step(setup, precision, device, tuning, steps=5, warmup=2):
+        eff = dict(DEFAULT, **(tuning or {}))
+        if eff["solve_kind"] == 1:
+            eff["solve_cols"] = 0          # the library reports no CTA width for the sweep
+        for k, v in bad:
+            if eff.get(k) == v:
+                raise RuntimeError(f"{k}={v} does not fit")
+        calls.append(json.dumps(eff, sort_keys=True))
+        t = 10.0
+        t += {1: 0.0, 2: 3.0, 3: 0.5, 4: 0.8}[eff["xline_path"]]
+        t += {2: 0.4, 4: 0.0, 8: 0.2}[eff["xline_rows"]]
+        t += {4: 0.5, 8: 0.3, 16: 0.0}[eff["zlines"]]
+        t += 0.0 if eff["solve_kind"] == 1 else 0.7
+        t += {2: 0.2, 4: 0.0, 8: 0.1, 16: 0.3}[eff["rhs_chunk"]]
+        return t * 1e-3, eff
+    return time_step
+
+
+def test_coordinate_search_finds_the_separable_minimum(monkeypatch):
+    calls = []
+    monkeypatch.setattr(autotune, "time_step", fake_model(calls))
+    best, t = autotune.autotune(None, "mixed")
+    assert best["xline_path"] == 1 and best["xline_rows"] == 4 and best["zlines"] == 16
+    assert best["solve_kind"] == 1 and best["rhs_chunk"] == 4
+    assert t == pytest.approx(10.0e-3)
+    assert len(calls) == len(set(calls)), "a shape was timed twice"
+
+
+def test_shapes_that_do_not_fit_are_skipped(monkeypatch):
+    calls = []
+    monkeypatch.setattr(autotune, "time_step", fake_model(calls, bad=(("xline_rows", 4),)))
+    logs = []
+    best, _ = autotune.autotune(None, "mixed", log=logs.append)
+    assert best["xline_rows"] == 8 and best["rhs_chunk"] == 4
+    assert any(m.startswith("skip") for m in logs)
+
+
+def test_cache_is_written_once_and_reused(monkeypatch, tmp_path):
+    torch = pytest.importorskip("torch")
+    calls = []
+    monkeypatch.setattr(autotune, "time_step", fake_model(calls))
+    monkeypatch.setattr(torch.cuda, "get_device_name", lambda device=None: "FAKE B200")
+    monkeypatch.setenv("CFD_TUNE_CACHE", str(tmp_path / "sub" / "tune.json"))
+
+    class G:
+        nyu = 33
+
+    class Cfg:
+        ngal1, ngal2 = 64, 96
+
+    class IB:
+        n = 5
+
+    class S:
+        cfg, grid, ibu = Cfg, G, IB
+
+    first = autotune.tuned(S, "mixed")
+    n = len(calls)
+    assert n > 0 and first["xline_rows"] == 4
+    again = autotune.tuned(S, "mixed")
+    assert again == first and len(calls) == n, "the cached tuning was measured again"
+    data = json.load(open(tmp_path / "sub" / "tune.json"))
+    (key,) = data
+    assert "FAKE B200" in key and "64x33x96" in key and key.endswith("ibTrue")
+    other = autotune.tuned(S, "fp64")
+    assert len(calls) > n and len(json.load(open(tmp_path / "sub" / "tune.json"))) == 2
+    assert other == first
