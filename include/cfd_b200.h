@@ -160,7 +160,10 @@ int cfd_field_shape(const cfd_ctx *ctx, int32_t field, int64_t *ncomplex,
 int cfd_upload_field(cfd_ctx *ctx, int32_t field, const double *host, int32_t layout);
 int cfd_download_field(cfd_ctx *ctx, int32_t field, double *host, int32_t layout);
 /* Device pointer of a field (FP64 [j][column] complex; NU* are FP32 complex in
- * CFD_PREC_MIXED).  Lets a caller fill state in place. */
+ * CFD_PREC_MIXED).  Lets a caller fill state in place.  The immersed-boundary forcing of
+ * cfd_solve_uvw reuses the z transforms of u, v, w made by the preceding cfd_nonlinear;
+ * uploads and this call mark them stale, so a caller that writes u, v or w through an
+ * earlier pointer between cfd_nonlinear and cfd_solve_uvw calls it again after writing. */
 int cfd_field_device_ptr(cfd_ctx *ctx, int32_t field, void **dev_ptr);
 
 /* ---- one RK substep, stage by stage (littleharsh.f90:163-189) -------------------- */
