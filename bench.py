@@ -70,20 +70,36 @@ def kernel_bytes(name, setup, mixed):
         "k_solve_p_vcorr": ncol * (3 * nfp * cs + nyp * (4 * cs + 2 * 8)),
         "k_vcorr": ncol * (2 * (2 * nyu + nyv) + nyp) * cs,
     }
-    # IB kernels: average over the u-grid (2 batches) and v-grid (1 batch) launches
+    # IB z kernels: average over the u-grid (2 batches) and v-grid (1 batch) launches; the
+    # inverse transforms the right-hand sides only (the velocities' transforms come from the
+    # nonlinear pass).  The IB x kernels work on the active rows only and are not modelled.
     ib = []
     for npl, nb in ((nplu, 2), (nplv, 1)):
         if npl:
-            ib.append({"k_ib_zinv": npl * 2 * nb * (ncol * cs + hpl * ct),
-                       "k_ib_xinv": npl * nb * (2 * hpl * ct + 2 * phys * rt),
-                       "k_ib_xfwd": npl * nb * (phys * rt + hpl * ct),
+            ib.append({"k_ib_zinv": npl * nb * (ncol * cs + hpl * ct),
                        "k_ib_zfwd": npl * nb * (hpl * ct + ncol * cs)})
-    for k in ("k_ib_zinv", "k_ib_xinv", "k_ib_xfwd", "k_ib_zfwd"):
+    for k in ("k_ib_zinv", "k_ib_zfwd"):
         if ib:
             b[k] = sum(x[k] for x in ib) / len(ib)
+    if name.startswith("k_ib_x"):
+        return None
     if name in b:
         return b[name]
     return b.get(name[:-1]) if name.endswith("2") else None
+
+
+def kernel_table(prof, setup, mixed, peak):
+    """Per kernel of one RK3 step: launches, ms, and where its algorithmic bytes are modelled
+    the achieved GB/s (bytes per launch / average launch time) and its fraction of `peak`."""
+    out = {}
+    for k, (calls, ms) in sorted(prof.items(), key=lambda kv: -kv[1][1]):
+        e = {"calls": calls, "ms": ms}
+        kb = kernel_bytes(k, setup, mixed)
+        if kb and calls and ms > 0:
+            gbs = kb / (ms / calls / 1e3) / 1e9
+            e.update(algorithmic_bytes_per_launch=kb, achieved_gbs=gbs, frac=gbs / peak)
+        out[k] = e
+    return out
 
 
 def ncu_traffic(config: str, kname: str):
@@ -516,8 +532,8 @@ def main():
                          f"profiles/dram_traffic_{args.config}.md (ncu, bytes per launch)",
                      "algorithmic_bytes_per_launch": kb,
                      "avg_launch_ms": kms / kcalls, "share_of_step": kms / tot},
-        "kernels_mixed": {k: {"calls": v[0], "ms": v[1]} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
-        "kernels_fp64": {k: {"calls": v[0], "ms": v[1]} for k, v in sorted(prof64.items(), key=lambda kv: -kv[1][1])},
+        "kernels_mixed": kernel_table(prof, setup, True, hbm),
+        "kernels_fp64": kernel_table(prof64, setup, False, hbm),
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": "RK3 steps/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                 "path": "cfd_upload_field x4 (pinned host, reference layout) + cfd_step + cfd_download_field x4"},
