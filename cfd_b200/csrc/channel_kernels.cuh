@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
         };
         if (uplane) fill(std::false_type{});
         else fill(std::true_type{});
-        rdft<N1, +1>(v);
+        rdft_z<N1, +1, gap_blocks<N1, N2, HX>()>(v);
         T2* o = ex + (size_t)b * L1 + n2;
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1) o[k1 * (N2 + 1)] = k1 == 0 ? v[0] : cmulc(v[k1], twt[k1 * N2 + n2]);
@@ -425,8 +425,11 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
     __syncthreads();
     if (act3) {
         T2* o = ex + (size_t)b3 * LU + kb;
+        // X[kb + N2*ka] is read by the unpack only for k <= HX or k >= N - HX; the blocks of
+        // ka that lie wholly between are not stored, so their last butterflies are dead code
 #pragma unroll
-        for (int ka = 0; ka < N1; ++ka) o[N2 * ka] = z[ka];
+        for (int ka = 0; ka < N1; ++ka)
+            if (!(N2 * ka > HX && N2 * ka + N2 - 1 < N - HX)) o[N2 * ka] = z[ka];
     }
     __syncthreads();
 

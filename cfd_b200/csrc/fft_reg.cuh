@@ -131,6 +131,78 @@ template <int N, int SIGN, typename T2> __host__ __device__ __forceinline__ void
     }
 }
 
+// ---- inputs known to be zero --------------------------------------------------------
+// The zero-padded inverse transforms get whole stride-N2 subsequences of zeros (the
+// dealiasing gap).  IEEE rules keep the compiler from dropping x + 0.0, so the first
+// radix-4 stage below skips the additions with inputs flagged in a compile-time mask; every
+// value it computes is the same as rdft's.
+template <int SIGN, int ZM, typename T2>
+__host__ __device__ __forceinline__ void dft4_z(T2& x0, T2& x1, T2& x2, T2& x3) {
+    if constexpr (ZM == 0) {
+        dft4<SIGN>(x0, x1, x2, x3);
+    } else {
+        auto neg = [](T2 a) { return cx<T2>(-a.x, -a.y); };
+        T2 a0, a1, b0, d;
+        if constexpr ((ZM & 4) != 0) { a0 = x0; a1 = x0; }
+        else if constexpr ((ZM & 1) != 0) { a0 = x2; a1 = neg(x2); }
+        else { a0 = cadd(x0, x2); a1 = csub(x0, x2); }
+        if constexpr ((ZM & 8) != 0) { b0 = x1; d = x1; }
+        else if constexpr ((ZM & 2) != 0) { b0 = x3; d = neg(x3); }
+        else { b0 = cadd(x1, x3); d = csub(x1, x3); }
+        const T2 b1 = mul_si<SIGN>(d);
+        x0 = cadd(a0, b0);
+        x2 = csub(a0, b0);
+        x1 = cadd(a1, b1);
+        x3 = csub(a1, b1);
+    }
+}
+
+template <int Q, int N2I, int SIGN, unsigned long long ZM, typename T2>
+__host__ __device__ __forceinline__ void rdft_cols_z(const T2* v, T2* y) {
+    if constexpr (N2I < Q) {
+        constexpr int m = (int)(((ZM >> N2I) & 1) | (((ZM >> (Q + N2I)) & 1) << 1) |
+                                (((ZM >> (2 * Q + N2I)) & 1) << 2) | (((ZM >> (3 * Q + N2I)) & 1) << 3));
+        T2 t0 = v[N2I], t1 = v[Q + N2I], t2 = v[2 * Q + N2I], t3 = v[3 * Q + N2I];
+        dft4_z<SIGN, m>(t0, t1, t2, t3);
+        y[N2I * 4 + 0] = t0;
+        y[N2I * 4 + 1] = twmul<T2, N2I * 1, 4 * Q, SIGN>(t1);
+        y[N2I * 4 + 2] = twmul<T2, N2I * 2, 4 * Q, SIGN>(t2);
+        y[N2I * 4 + 3] = twmul<T2, N2I * 3, 4 * Q, SIGN>(t3);
+        rdft_cols_z<Q, N2I + 1, SIGN, ZM>(v, y);
+    }
+}
+
+// rdft<N, SIGN> for inputs whose zeros are flagged in ZM (bit n: v[n] == 0)
+template <int N, int SIGN, unsigned long long ZM, typename T2>
+__host__ __device__ __forceinline__ void rdft_z(T2* v) {
+    if constexpr (ZM == 0 || N <= 4 || FirstFactor<N>::value != 4) {
+        rdft<N, SIGN>(v);
+    } else {
+        constexpr int P = 4, Q = N / 4;
+        T2 y[N];
+        rdft_cols_z<Q, 0, SIGN, ZM>(v, y);  // y[n2*P + k1], as rdft_cols
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) {
+            T2 t[Q];
+#pragma unroll
+            for (int n2 = 0; n2 < Q; ++n2) t[n2] = y[n2 * P + k1];
+            rdft<Q, SIGN>(t);
+#pragma unroll
+            for (int k2 = 0; k2 < Q; ++k2) v[k1 + P * k2] = t[k2];
+        }
+    }
+}
+
+// stride-N2 subsequences n1 (elements n1*N2 .. n1*N2+N2-1) wholly inside the gap between
+// the retained modes 0..HX and N-HX..N-1
+template <int N1, int N2, int HX>
+__host__ __device__ constexpr unsigned long long gap_blocks() {
+    unsigned long long m = 0;
+    for (int n1 = 0; n1 < N1; ++n1)
+        if (n1 * N2 > HX && n1 * N2 + N2 - 1 < N1 * N2 - HX) m |= 1ull << n1;
+    return m;
+}
+
 // (N1, N2) split of the production lengths
 template <int N> struct TwoStep { static constexpr int N1 = 0, N2 = 0; };
 template <> struct TwoStep<64> { static constexpr int N1 = 8, N2 = 8; };
