@@ -6,8 +6,8 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRCS = [os.path.join(HERE, "csrc", f) for f in ("cfd_capi.cu", "cfd_noalloc.cu")]
-DEPS = SRCS + [os.path.join(HERE, "csrc", f) for f in ("channel_kernels.cuh", "fft_smem.cuh")] + \
-    [os.path.join(os.path.dirname(HERE), "include", "cfd_b200.h")]
+DEPS = SRCS + [os.path.join(HERE, "csrc", f) for f in sorted(os.listdir(os.path.join(HERE, "csrc")))
+               if f.endswith(".cuh")] + [os.path.join(os.path.dirname(HERE), "include", "cfd_b200.h")]
 OUT = os.path.join(HERE, "_lib", "libcfdb200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]

@@ -134,8 +134,10 @@ template <int N, int SIGN, typename T2> __host__ __device__ __forceinline__ void
 // ---- inputs known to be zero --------------------------------------------------------
 // The zero-padded inverse transforms get whole stride-N2 subsequences of zeros (the
 // dealiasing gap).  IEEE rules keep the compiler from dropping x + 0.0, so the first
-// radix-4 stage below skips the additions with inputs flagged in a compile-time mask; every
-// value it computes is the same as rdft's.
+// radix-4 stage below skips the additions with inputs flagged in a compile-time mask.  Its
+// values equal rdft's, except that a zero may keep a negative sign that rdft's x + 0 would
+// have made positive (checked on the host for every production length by
+// tests/fft_prune_check.cu).
 template <int SIGN, int ZM, typename T2>
 __host__ __device__ __forceinline__ void dft4_z(T2& x0, T2& x1, T2& x2, T2& x3) {
     if constexpr (ZM == 0) {
