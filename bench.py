@@ -70,19 +70,25 @@ def kernel_bytes(name, setup, mixed):
         "k_solve_p_vcorr": ncol * (3 * nfp * cs + nyp * (4 * cs + 2 * 8)),
         "k_vcorr": ncol * (2 * (2 * nyu + nyv) + nyp) * cs,
     }
-    # IB z kernels: average over the u-grid (2 batches) and v-grid (1 batch) launches; the
-    # inverse transforms the right-hand sides only (the velocities' transforms come from the
-    # nonlinear pass).  The IB x kernels work on the active rows only and are not modelled.
+    # IB kernels: average over the u-grid (2 batches: u, w) and v-grid (1 batch) launches.
+    # z: the inverse transforms the right-hand sides only (the velocities' transforms come
+    # from the nonlinear pass).  x: only the z rows holding a forcing or stencil point
+    # (`nact` of them) make the round trip; the inverse reads the half-physical rows of the
+    # right-hand side and of the velocity and writes both physical rows, the forward reads
+    # the forced right-hand side row and writes its half-physical row.
     ib = []
-    for npl, nb in ((nplu, 2), (nplv, 1)):
+    for npl, nb, lst in ((nplu, 2, setup.ibu), (nplv, 1, setup.ibv)):
         if npl:
+            nact = int(np.unique(lst.idx[:, [1, 4, 7]]).size) if lst.n else 0
+            xi = lambda rows: npl * nb * rows * (2 * cfg.nkx * ct + 2 * cfg.ngal1 * (ct // 2))
+            xf = lambda rows: npl * nb * rows * (cfg.ngal1 * (ct // 2) + cfg.nkx * ct)
             ib.append({"k_ib_zinv": npl * nb * (ncol * cs + hpl * ct),
-                       "k_ib_zfwd": npl * nb * (hpl * ct + ncol * cs)})
-    for k in ("k_ib_zinv", "k_ib_zfwd"):
+                       "k_ib_zfwd": npl * nb * (hpl * ct + ncol * cs),
+                       "k_ib_xinv2": xi(nact), "k_ib_xfwd2": xf(nact),          # active rows
+                       "k_ib_xinv": xi(cfg.ngal2), "k_ib_xfwd": xf(cfg.ngal2)})  # every row
+    for k in ("k_ib_zinv", "k_ib_zfwd", "k_ib_xinv2", "k_ib_xfwd2", "k_ib_xinv", "k_ib_xfwd"):
         if ib:
             b[k] = sum(x[k] for x in ib) / len(ib)
-    if name.startswith("k_ib_x"):
-        return None
     if name in b:
         return b[name]
     return b.get(name[:-1]) if name.endswith("2") else None
@@ -118,19 +124,94 @@ def ncu_traffic(config: str, kname: str):
     return None
 
 
+def step_roofline(setup, mixed, seconds_per_step, peak):
+    """Whole RK3 step against the compulsory-traffic model of one substep: 608 S bytes in
+    FP32-mixed, 1040 S in FP64, S = columns x planes complex values per spectral field
+    (every pass reads its operands once and writes its results once)."""
+    S = setup.cfg.ncol * setup.grid.nyv
+    per_sub = (608 if mixed else 1040) * S
+    gbs = 3 * per_sub / seconds_per_step / 1e9
+    return {"model_bytes_per_substep": per_sub, "achieved_gbs": gbs, "frac": gbs / peak}
+
+
+def fp32_pipe(config, kname, launch_ms, clocks):
+    """FP32 operations per launch of a kernel (FADD + FMUL + 2 FFMA, counted by ncu on a
+    reduced-y launch and scaled to the full grid in profiles/fp32_ops_<config>.md) over its
+    CUDA-event launch time, against the FP32 peak at the measured SM clock (148 SMs x 128
+    lanes x 2 flops per FMA)."""
+    p = os.path.join(ROOT, "profiles", f"fp32_ops_{config}.md")
+    if not os.path.exists(p) or not clocks or not clocks.get("sm_mhz"):
+        return None
+    ops = None
+    for line in open(p):
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) >= 2 and cells[0] == kname:
+            try:
+                ops = float(cells[-1])
+            except ValueError:
+                ops = None
+    if not ops:
+        return None
+    peak = 148 * 128 * 2 * clocks["sm_mhz"] * 1e6
+    achieved = ops / (launch_ms * 1e-3)
+    return {"fp32_ops_per_launch": ops, "achieved_tflops": achieved / 1e12, "peak_tflops": peak / 1e12,
+            "frac": achieved / peak, "source": f"profiles/fp32_ops_{config}.md"}
+
+
 # ------------------------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled during the timed region: through NVML in a
+    thread every 10 ms (tens of samples even for a sub-second region), else nvidia-smi
+    every 200 ms.  Read-only queries; no GPU setting is touched."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.01):
         self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.period = period_s
+        self.rows = []          # (sm_mhz, sm_max_mhz, reason bits)
+        self.nv = None
         self.p = None
+        self.f = None
+        self.thread = None
+        self.stop = False
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:  # the CUDA device's PCI bus id: NVML numbers every GPU of the node
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _loop(self):
+        nv, h = self.nv
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(smax), int(rs)))
+            except Exception:
+                pass
+            time.sleep(self.period)
 
     def __enter__(self):
+        import threading
+        try:
+            self.nv = self._nvml_handle()
+            self.thread = threading.Thread(target=self._loop, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nv = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                        "-i", str(self.index), "-lms", "200"], stdout=self.f,
@@ -140,6 +221,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread:
+            self.stop = True
+            self.thread.join(timeout=5)
         if self.p:
             self.p.terminate()
             try:
@@ -148,20 +232,31 @@ class ClockSampler:
                 self.p.kill()
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
-            os.unlink(self.f.name)
-        except OSError:
-            return None
+        if self.nv is not None:
+            rows = self.rows
+            source = "nvml, 10 ms"
+        else:
+            source = "nvidia-smi, 200 ms"
+            try:
+                txt = open(self.f.name).read() if self.f else ""
+                if self.f:
+                    os.unlink(self.f.name)
+            except OSError:
+                return None
+            rows = []
+            for r in (x.split(",") for x in txt.strip().splitlines() if x.strip()):
+                try:
+                    bits = sum(b for (_, b), i in zip(self.REASONS, range(4))
+                               if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i])
+                    rows.append((float(r[1]), float(r[2]), bits))
+                except (ValueError, IndexError):
+                    continue
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
-                          and "Not" not in r[5 + i]})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(rows), "reasons": reasons}
+        reasons = sorted({n for _, _, bits in rows for n, b in self.REASONS if bits & b})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "sm_mhz_min": min(r[0] for r in rows), "samples": len(rows), "reasons": reasons,
+                "source": source}
 
 
 # ------------------------------------------------------------------------------------------
@@ -246,26 +341,34 @@ def plane_profiles(st, npts):
     return out
 
 
-def profile_error(chans, setup, nsteps):
-    """Mean and rms velocity profiles of the mixed and FP64 paths from the same start, averaged
-    over nsteps steps with the on-device statistics: the largest difference over the planes
-    relative to the largest FP64 value of that profile."""
+def profile_error(chans, setup, spinup, nsteps, nstat=20):
+    """Mean and rms velocity profiles of the mixed and FP64 paths from the same start: each
+    path spins up `spinup` RK3 steps, then accumulates the on-device statistics every
+    `nstat` steps over `nsteps` steps (the reference's cadence, nstat = min(20, nwrite),
+    start.f90:372).  Reported: the largest difference over the planes relative to the
+    largest FP64 value of that profile, against the 1 % bound."""
     if nsteps <= 0:
         return None
     npts = setup.cfg.ngal1 * setup.cfg.ngal2
     prof = {}
     for prec, ch in chans.items():
         ch.upload_state()
+        if spinup > 0:
+            ch.step(spinup)
         ch.stats_configure(setup.grid.jv0 - 1, 0, 0)
-        for _ in range(nsteps):
-            ch.step(1)
+        done = 0
+        while done < nsteps:
+            n = min(nstat, nsteps - done)
+            ch.step(n)
+            done += n
             ch.stats_accumulate()
         prof[prec] = plane_profiles(ch.stats_read(), npts)
-    out = {"steps": nsteps, "max_rel_diff": {}}
+    out = {"spinup_steps": spinup, "steps": nsteps, "nstat": nstat, "bound": 0.01, "max_rel_diff": {}}
     for k in ("mean_u", "rms_u", "rms_v", "rms_w"):  # mean v and w are zero up to round-off
         ref = prof["fp64"][k]
         scale = max(np.abs(ref).max(), 1e-300)
         out["max_rel_diff"][k] = float(np.abs(prof["mixed"][k] - ref).max() / scale)
+    out["within_bound"] = all(v < out["bound"] for v in out["max_rel_diff"].values())
     return out
 
 
@@ -306,6 +409,44 @@ def run_ensemble(torch, device, nsteps, warmup, tuning):
                      "separate_graphs_steps_per_s": nsteps / tsep}
         ens.close(members=True)
     return out
+
+
+def run_e2e(torch, ch, setup, stream, steps, warmup, ws, device):
+    """The step through the reference-facing C ABI with host data: every step uploads u, v,
+    w, p from pinned host memory in the reference's f(j,column) layout, advances one RK3
+    step and downloads them again (synchronising)."""
+    host = {}
+    nbytes = 0
+    for k in ("u1", "u2", "u3", "p"):
+        a = torch.from_numpy(np.ascontiguousarray(setup.state()[k]).view(np.float64).copy()).pin_memory()
+        host[k] = a
+        nbytes += a.numel() * 8
+    lib = ch.lib
+    fid = {"u1": 0, "u2": 1, "u3": 2, "p": 3}
+
+    def e2e_step():
+        for k in host:
+            lib.cfd_upload_field(ch.ctx, fid[k], C.cast(host[k].data_ptr(), C.POINTER(C.c_double)), 0)
+        ch.step(1)
+        for k in host:
+            lib.cfd_download_field(ch.ctx, fid[k], C.cast(host[k].data_ptr(), C.POINTER(C.c_double)), 0)
+        ch.synchronize()
+
+    for _ in range(warmup):
+        e2e_step()
+    n = max(3, min(steps, 10))
+    barrier(ws)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(n):
+        e2e_step()
+    e.record(stream)
+    e.synchronize()
+    barrier(ws)
+    t = max_over_ranks(ws, s.elapsed_time(e) / 1e3, device)
+    return {"value": aggregate_rate(ws, n, t), "unit": "RK3 steps/s", "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes, "steps": n,
+            "path": "cfd_upload_field x4 (pinned host, reference layout) + cfd_step + cfd_download_field x4"}
 
 
 def rel_err(a, b):
@@ -402,8 +543,12 @@ def main():
     ap.add_argument("--error-steps", type=int, default=10)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 16-member ensemble measurement")
     ap.add_argument("--no-autotune", action="store_true", help="library default launch shapes")
-    ap.add_argument("--profile-steps", type=int, default=20,
-                    help="steps of the mean/rms profile comparison of mixed vs FP64 (0: skip)")
+    ap.add_argument("--profile-steps", type=int, default=2000,
+                    help="averaging steps of the mean/rms profile comparison of mixed vs FP64 (0: skip)")
+    ap.add_argument("--spinup-steps", type=int, default=2000,
+                    help="spin-up steps before the profile averaging window")
+    ap.add_argument("--sustained-steps", type=int, default=200,
+                    help="steps of the longer second timing window per precision (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -448,7 +593,7 @@ def main():
     for k in ("u1", "u2", "u3", "p"):
         err[k] = rel_err(states["mixed"][k], states["fp64"][k])
     fp64_div = chans["fp64"].divergence_max()
-    prof_err = profile_error(chans, setup, args.profile_steps)
+    prof_err = profile_error(chans, setup, args.spinup_steps, args.profile_steps)
     ens = run_ensemble(torch, device, args.steps, args.warmup, None if args.no_autotune else "auto") \
         if (ws == 1 and not args.no_ensemble) else None
 
@@ -463,38 +608,22 @@ def main():
     achieved = kb / per_launch_s / 1e9 if kb else None
     prof64 = profile_step(chans["fp64"])
 
-    # end-to-end through the C ABI with pinned host buffers: H2D state, step, D2H state
-    ch = chans["mixed"]
-    host = {}
-    nbytes = 0
-    for k in ("u1", "u2", "u3", "p"):
-        a = torch.from_numpy(np.ascontiguousarray(setup.state()[k]).view(np.float64).copy()).pin_memory()
-        host[k] = a
-        nbytes += a.numel() * 8
-    lib = ch.lib
-    fid = {"u1": 0, "u2": 1, "u3": 2, "p": 3}
+    # end-to-end through the C ABI with pinned host buffers: H2D state, step, D2H state,
+    # for both precisions (FP64 is the reference's arithmetic)
+    e2e = {prec: run_e2e(torch, chans[prec], setup, stream, args.steps, args.warmup, ws, device)
+           for prec in ("mixed", "fp64")}
 
-    def e2e_step():
-        for k in host:
-            lib.cfd_upload_field(ch.ctx, fid[k], C.cast(host[k].data_ptr(), C.POINTER(C.c_double)), 0)
-        ch.step(1)
-        for k in host:
-            lib.cfd_download_field(ch.ctx, fid[k], C.cast(host[k].data_ptr(), C.POINTER(C.c_double)), 0)
-        ch.synchronize()
-
-    for _ in range(args.warmup):
-        e2e_step()
-    ne2e = max(3, min(args.steps, 10))
-    barrier(ws)
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record(stream)
-    for _ in range(ne2e):
-        e2e_step()
-    e.record(stream)
-    e.synchronize()
-    barrier(ws)
-    te2e = max_over_ranks(ws, s.elapsed_time(e) / 1e3, device)
-    e2e_val = aggregate_rate(ws, ne2e, te2e)
+    # the step seen over a longer window (clock record with many samples); the timed region
+    # above stays exactly --steps steps
+    sustained = {}
+    if args.sustained_steps > 0:
+        for prec, ch in chans.items():
+            ch.upload_state()
+            ch.step(args.warmup)
+            with ClockSampler(local) as cs2:
+                t2 = time_steps(torch, ch, stream, args.sustained_steps, ws, device)
+            sustained[prec] = {"steps": args.sustained_steps, "steps_per_s": aggregate_rate(ws, args.sustained_steps, t2),
+                               "clocks": cs2.summary()}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -519,7 +648,10 @@ def main():
         "grid_pt_updates_per_s": mixed["steps_per_s"] * gp,
         "fp64": {"steps_per_s": fp64["steps_per_s"], "grid_pt_updates_per_s": fp64["steps_per_s"] * gp,
                  "ms_per_step": 1e3 * fp64["seconds"] / args.steps, "clocks": fp64["clocks"],
-                 "max_divergence": fp64_div},
+                 "max_divergence": fp64_div, "e2e": e2e["fp64"],
+                 "step_roofline": step_roofline(setup, False, fp64["seconds"] / args.steps, hbm)},
+        "step_roofline": step_roofline(setup, True, mixed["seconds"] / args.steps, hbm),
+        "sustained": sustained or None,
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
         "profile_error_mixed_vs_fp64": prof_err,
@@ -531,12 +663,12 @@ def main():
                      "traffic": ncu_traffic(args.config, kname), "traffic_source":
                          f"profiles/dram_traffic_{args.config}.md (ncu, bytes per launch)",
                      "algorithmic_bytes_per_launch": kb,
-                     "avg_launch_ms": kms / kcalls, "share_of_step": kms / tot},
+                     "avg_launch_ms": kms / kcalls, "share_of_step": kms / tot,
+                     "fp32_pipe": fp32_pipe(args.config, kname, kms / kcalls, mixed["clocks"])},
         "kernels_mixed": kernel_table(prof, setup, True, hbm),
         "kernels_fp64": kernel_table(prof64, setup, False, hbm),
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_val, "unit": "RK3 steps/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                "path": "cfd_upload_field x4 (pinned host, reference layout) + cfd_step + cfd_download_field x4"},
+        "e2e": e2e["mixed"],
         "gpu_launches": mixed["launches"],
         "launches_per_step": mixed["launches"] // max(args.steps, 1),
         "clocks": mixed["clocks"],
