@@ -40,7 +40,8 @@ class CfdIBList(C.Structure):
 
 class CfdTuning(C.Structure):
     _fields_ = [("xline_path", C.c_int32), ("xline_rows", C.c_int32), ("zlines", C.c_int32),
-                ("solve_kind", C.c_int32), ("solve_cols", C.c_int32), ("rhs_chunk", C.c_int32)]
+                ("solve_kind", C.c_int32), ("solve_cols", C.c_int32), ("rhs_chunk", C.c_int32),
+                ("xsplit", C.c_int32), ("zsplit", C.c_int32)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -165,6 +166,7 @@ SIGNATURES = {
     "cfd_spectra_read": (C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "cfd_cfl": (C.c_int, [_VP, _dp, _VP]),
     "cfd_set_dt": (C.c_int, [_VP, C.c_double]),
+    "cfd_set_lastplane": (C.c_int, [_VP, C.c_int32]),
     "cfd_ensemble_create": (C.c_int, [C.POINTER(_VP), C.c_int32, C.POINTER(_VP)]),
     "cfd_ensemble_step": (C.c_int, [_VP, C.c_int32]),
     "cfd_ensemble_synchronize": (C.c_int, [_VP]),

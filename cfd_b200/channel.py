@@ -241,6 +241,11 @@ class Channel:
         """New time step for the following stages and steps (the graph is captured again)."""
         self._chk(self.lib.cfd_set_dt(self.ctx, float(dt)), "set_dt")
 
+    def set_lastplane(self, on: bool):
+        """Single-slab (bug-compatible) x/z advective term of the reference's ops_in_planes
+        (on) or the per-plane term (off, the default)."""
+        self._chk(self.lib.cfd_set_lastplane(self.ctx, int(bool(on))), "set_lastplane")
+
     def divergence_max(self) -> float:
         e = C.c_double()
         self._chk(self.lib.cfd_divergence_max(self.ctx, C.byref(e)), "divergence_max")

@@ -47,11 +47,13 @@ int scratch_for_current_device(double** out) {
 
 // Same sweep as the u/w part of k_solve_uvw (LUsolU with LU_buildU + LU_dec computed on
 // the fly, tridLU_3D_IB.f90:50-103, 349-380, 521-559) for one right-hand side; the scaled
-// upper diagonal of the forward sweep goes to `cs` (the file-scope scratch).
+// upper diagonal of the forward sweep goes to `cs` (the file-scope scratch).  r and u may
+// be the same array: plane jj of r is read before plane jj of u is written, and the back
+// sweep reads u only, so they carry no __restrict__.
 __global__ void __launch_bounds__(256) k_lusol_u_noalloc(int nkx, int n2, int n, double beta, double gwb, double gwt,
                                                          const double* __restrict__ kx, const double* __restrict__ kz,
                                                          const double* __restrict__ dyu2i,
-                                                         const double2* __restrict__ r, double2* __restrict__ u,
+                                                         const double2* r, double2* u,
                                                          double* __restrict__ cs) {
     const int ncol = nkx * n2;
     const int col = blockIdx.x * blockDim.x + threadIdx.x;

@@ -133,9 +133,14 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *   solve_kind   1: thread-per-column Thomas sweeps, 2: warp-per-column substitutions on
  *                LU factors precomputed per time step
  *   solve_cols   columns (warps) per CTA of the warp-per-column solve: 1, 2, 4 or 8
- *   rhs_chunk    y-planes per thread of the right-hand-side kernel: 2 .. 64 */
+ *   rhs_chunk    y-planes per thread of the right-hand-side kernel: 2 .. 64
+ *   xsplit       radix order of the x-line transforms (x-line path 1): 1 = the split
+ *                N = N1*N2 of 64 = 8*8, 96 = 8*12, 128 = 8*16, 192 = 16*12, 384 = 16*24,
+ *                768 = 32*24 (first step N1 points); 2 = the transposed split (16*4, 12*8,
+ *                16*8, 12*16, 24*16, 24*32)
+ *   zsplit       the same for the z transforms of the nonlinear pass (x-line path 1) */
 typedef struct cfd_tuning {
-    int32_t xline_path, xline_rows, zlines, solve_kind, solve_cols, rhs_chunk;
+    int32_t xline_path, xline_rows, zlines, solve_kind, solve_cols, rhs_chunk, xsplit, zsplit;
 } cfd_tuning;
 /* cfd_create with explicit launch shapes (tuning may be NULL: as cfd_create). */
 int cfd_create_tuned(const cfd_config *cfg, const cfd_ib_list *ibu, const cfd_ib_list *ibv,
@@ -289,6 +294,16 @@ int cfd_cfl(cfd_ctx *ctx, double *dtc, double *terms);
  * cfd_step. */
 int cfd_set_dt(cfd_ctx *ctx, double dt);
 
+/* Bug-compatible x/z advective term of a single-slab run (on = 1) or the per-plane term
+ * (on = 0, the default).  ops_in_planes (FOU3D.f90:1529-1617) forms der_x/der_z of each
+ * plane's products into 2-D scratch inside its plane loop and adds the scratch into
+ * Nu1PL/Nu3PL/Nu2PL after the loop (FOU3D.f90:1541, 1571-1585, 1602-1613), so every interior
+ * plane of a rank receives the term of the rank's last plane.  With on = 1 the whole channel
+ * behaves as one rank's slab: every interior plane takes the term of the top ghost centre
+ * (u, w) and of the top wall face (v, where it is zero), for comparisons with an unpatched
+ * reference run on one rank.  Drops the captured RK3 graph like cfd_set_dt. */
+int cfd_set_lastplane(cfd_ctx *ctx, int32_t on);
+
 /* ---- batched ensemble -------------------------------------------------------------- */
 
 /* No counterpart in the reference, which runs one channel per MPI job.  An ensemble
@@ -313,17 +328,20 @@ int cfd_ensemble_destroy(cfd_ensemble *ens);
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc/cudaFree: a
  * driver whose device memory belongs to another allocator or sits under a hard cap, or a
- * loop that must not take cudaFree's implicit device synchronisation.  Solves the u/w
- * Helmholtz system of LUsolU (ghost rows (0,1,gw_bot) and (gw_top,1,0), interior rows
- * -beta*dyu2i(1), 1-beta*(dyu2i(2)+k2x+k2z), -beta*dyu2i(3)) for one complex right-hand
- * side on caller-owned device memory, with no context and no allocation.
- *   rhs_dev, u_dev : [nplanes][nkx*n2] complex (interleaved doubles, CFD_LAYOUT_PLANE order)
+ * loop that must not take cudaFree's implicit device synchronisation.  Solves, per
+ * (kx,kz) column, the tridiagonal u/w Helmholtz system with the ghost rows (0,1,gw_bot)
+ * and (gw_top,1,0) and the interior rows -beta*dyu2i(1), 1-beta*(dyu2i(2)+k2x+k2z),
+ * -beta*dyu2i(3), for one complex right-hand side on caller-owned device memory, with no
+ * context and no allocation.
+ *   rhs_dev, u_dev : [nplanes][nkx*n2] complex (interleaved doubles, CFD_LAYOUT_PLANE order);
+ *                    they may be the same buffer (an in-place solve)
  *   kx_dev [nkx], kz_dev [n2], dyu2i_dev [nplanes][3] : device arrays
  * Its Thomas scratch is one file-scope device array of CFD_NOALLOC_MAX_SCRATCH doubles
  * (128 MiB) that every GPU loading the library holds until exit; (nplanes-1)*nkx*n2 above
  * that returns CFD_ERR_SIZE before any GPU work.  The first call on a device looks up that
- * device's copy of the array (with the device current), so make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other streams, other
+ * device's copy of the array (with the device current) and keeps its address for the life
+ * of the process, so make it before any stream capture; after a cudaDeviceReset the
+ * library must be unloaded and loaded again before the next call.  All calls share the array: calls that overlap on the GPU (other streams, other
  * host threads) race on it and give wrong results.  Nothing in it needs to start at zero.
  * Enqueued on `stream` (NULL = legacy default stream); returns CFD_ERR_CUDA on a launch
  * failure. */

@@ -34,7 +34,7 @@ module cfd_b200_mod
   end type
 
   type, bind(c) :: cfd_tuning
-    integer(c_int32_t) :: xline_path, xline_rows, zlines, solve_kind, solve_cols, rhs_chunk
+    integer(c_int32_t) :: xline_path, xline_rows, zlines, solve_kind, solve_cols, rhs_chunk, xsplit, zsplit
   end type
 
   type, bind(c) :: cfd_stats_config
@@ -156,6 +156,9 @@ module cfd_b200_mod
     end function
     integer(c_int) function cfd_set_dt(ctx, dt) bind(c, name='cfd_set_dt')
       import; type(c_ptr), value :: ctx; real(c_double), value :: dt
+    end function
+    integer(c_int) function cfd_set_lastplane(ctx, on) bind(c, name='cfd_set_lastplane')
+      import; type(c_ptr), value :: ctx; integer(c_int32_t), value :: on
     end function
 
     ! ---- ensembles ----------------------------------------------------------------------------

@@ -6,16 +6,20 @@ import pytest
 
 from cfd_b200 import autotune
 
-DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "solve_cols": 0, "rhs_chunk": 16}
+DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "solve_cols": 0, "rhs_chunk": 16,
+           "xsplit": 1, "zsplit": 1}
 
 
 def fake_model(calls, bad=()):
     """Seconds per step: a separable cost with its minimum at xline_rows 4, zlines 16,
-    rhs_chunk 4; path 2 is slow, warp solves are slow; shapes in `bad` raise."""
+    rhs_chunk 4, the transposed x split and the default z split; path 2 is slow, warp solves
+    are slow; shapes in `bad` raise."""
     def time_step(setup, precision, device, tuning, steps=5, warmup=2):
         eff = dict(DEFAULT, **(tuning or {}))
         if eff["solve_kind"] == 1:
             eff["solve_cols"] = 0          # the library reports no CTA width for the sweep
+        if eff["xline_path"] != 1:
+            eff["xsplit"] = eff["zsplit"] = 1  # the splits act on path 1 only
         for k, v in bad:
             if eff.get(k) == v:
                 raise RuntimeError(f"{k}={v} does not fit")
@@ -26,6 +30,7 @@ def fake_model(calls, bad=()):
         t += {4: 0.5, 8: 0.3, 16: 0.0}[eff["zlines"]]
         t += 0.0 if eff["solve_kind"] == 1 else 0.7
         t += {2: 0.2, 4: 0.0, 8: 0.1, 16: 0.3}[eff["rhs_chunk"]]
+        t += {1: 0.1, 2: 0.0}[eff["xsplit"]] + {1: 0.0, 2: 0.2}[eff["zsplit"]]
         return t * 1e-3, eff
     return time_step
 
@@ -36,6 +41,7 @@ def test_coordinate_search_finds_the_separable_minimum(monkeypatch):
     best, t = autotune.autotune(None, "mixed")
     assert best["xline_path"] == 1 and best["xline_rows"] == 4 and best["zlines"] == 16
     assert best["solve_kind"] == 1 and best["rhs_chunk"] == 4
+    assert best["xsplit"] == 2 and best["zsplit"] == 1
     assert t == pytest.approx(10.0e-3)
     assert len(calls) == len(set(calls)), "a shape was timed twice"
 

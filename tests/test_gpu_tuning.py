@@ -75,6 +75,6 @@ def test_pair_xline_shapes(torch_cuda):
         ch.upload_state()
         ch.step(2)
         st = ch.download_state()
-        for k in ("u1", "u2", "u3"):
+        for k in ("u1", "u2", "u3", "p"):
             assert rel(st[k], base[k]) < 1e-6, (rows, k, rel(st[k], base[k]))
         ch.close()

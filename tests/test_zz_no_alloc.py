@@ -60,6 +60,12 @@ def test_noalloc_solve_matches_context_path():
         got = x_d.cpu().numpy().view(np.complex128).reshape(expect[a].shape)
         err = np.linalg.norm(got - expect[a]) / np.linalg.norm(expect[a])
         assert err < TOL, (a, err)
+        # in place: the right-hand side buffer receives the solution
+        st = lib.cfd_lusol_u_noalloc(cfg.nkx, cfg.n2, g.nyu, beta, gwb, gwt, kx_d.data_ptr(), kz_d.data_ptr(),
+                                     dy_d.data_ptr(), r_d.data_ptr(), r_d.data_ptr(), None)
+        assert st == capi.CFD_OK
+        torch.cuda.synchronize()
+        assert torch.equal(r_d, x_d), a
 
     # sizes above the fixed scratch are refused before any GPU work
     too_many = capi.CFD_OK
