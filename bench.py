@@ -61,6 +61,9 @@ def kernel_bytes(name, setup, mixed):
         "k_xline2": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,
         "k_xline4": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,   # the same pass on packed line pairs
         "k_zfwd": (4 * nyu + 2 * nyv) * (hpl + ncol) * ct,
+        # packed x-line output: P of every slot (+ the second line of the u-slots), 2N/3 + 1
+        # entries per z row, read once; the four (u) or two (v) product spectra written
+        "k_zfwd2p": (nslot + nyu) * cfg.ngal2 * (2 * cfg.nkx - 1) * ct + (4 * nyu + 2 * nyv) * ncol * ct,
         "k_rhs": ncol * ((2 * nyu + nyv + nyp) * cs + (2 * nyu + nyv) * ct + (4 * nyu + 2 * nyv) * ct
                          + (2 * nyu + nyv) * cs + (2 * nyu + nyv) * ct),
         "k_solve_uvw": ncol * 2 * (2 * nyu + nyv) * cs,
@@ -69,6 +72,9 @@ def kernel_bytes(name, setup, mixed):
         # written; psi and the scaled upper diagonal (FP64 real) written and read once
         "k_solve_p_vcorr": ncol * (3 * nfp * cs + nyp * (4 * cs + 2 * 8)),
         "k_vcorr": ncol * (2 * (2 * nyu + nyv) + nyp) * cs,
+        # mean mode, one thread: the flow-rate integral reads yv and u(kx=kz=0) per plane
+        # (constant pressure gradient; the constant-flow-rate solve adds a one-column sweep)
+        "k_meanflow": nyu * (8 + cs),
     }
     # IB kernels: average over the u-grid (2 batches: u, w) and v-grid (1 batch) launches.
     # z: the inverse transforms the right-hand sides only (the velocities' transforms come
@@ -82,11 +88,14 @@ def kernel_bytes(name, setup, mixed):
             nact = int(np.unique(lst.idx[:, [1, 4, 7]]).size) if lst.n else 0
             xi = lambda rows: npl * nb * rows * (2 * cfg.nkx * ct + 2 * cfg.ngal1 * (ct // 2))
             xf = lambda rows: npl * nb * rows * (cfg.ngal1 * (ct // 2) + cfg.nkx * ct)
-            ib.append({"k_ib_zinv": npl * nb * (ncol * cs + hpl * ct),
+            # force: per point its 9 indices and 3 weights, the target's rhs and u, the two
+            # stencil values of u, and the target's rhs written back (physical, real)
+            ib.append({"k_ib_force": nb * lst.n * (9 * 4 + 3 * 8 + 5 * (ct // 2)),
+                       "k_ib_zinv": npl * nb * (ncol * cs + hpl * ct),
                        "k_ib_zfwd": npl * nb * (hpl * ct + ncol * cs),
                        "k_ib_xinv2": xi(nact), "k_ib_xfwd2": xf(nact),          # active rows
                        "k_ib_xinv": xi(cfg.ngal2), "k_ib_xfwd": xf(cfg.ngal2)})  # every row
-    for k in ("k_ib_zinv", "k_ib_zfwd", "k_ib_xinv2", "k_ib_xfwd2", "k_ib_xinv", "k_ib_xfwd"):
+    for k in ("k_ib_force", "k_ib_zinv", "k_ib_zfwd", "k_ib_xinv2", "k_ib_xfwd2", "k_ib_xinv", "k_ib_xfwd"):
         if ib:
             b[k] = sum(x[k] for x in ib) / len(ib)
     if name in b:
