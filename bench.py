@@ -61,9 +61,6 @@ def kernel_bytes(name, setup, mixed):
         "k_xline2": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,
         "k_xline4": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,   # the same pass on packed line pairs
         "k_zfwd": (4 * nyu + 2 * nyv) * (hpl + ncol) * ct,
-        # packed x-line output: P of every slot (+ the second line of the u-slots), 2N/3 + 1
-        # entries per z row, read once; the four (u) or two (v) product spectra written
-        "k_zfwd2p": (nslot + nyu) * cfg.ngal2 * (2 * cfg.nkx - 1) * ct + (4 * nyu + 2 * nyv) * ncol * ct,
         "k_rhs": ncol * ((2 * nyu + nyv + nyp) * cs + (2 * nyu + nyv) * ct + (4 * nyu + 2 * nyv) * ct
                          + (2 * nyu + nyv) * cs + (2 * nyu + nyv) * ct),
         "k_solve_uvw": ncol * 2 * (2 * nyu + nyv) * cs,

@@ -102,12 +102,9 @@ struct cfd_ctx {
     int CHz = 8, RWx = 4, RWib = 4, RWibf = 4;
     int RW2 = 0, NT2 = 0;
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
-    bool PK = false;        // k_xline2 stores packed spectra (Hp) and k_zfwd2p unpacks them
     bool XALT = false, ZALT = false;  // transposed two-step splits (x-line; nonlinear z kernels)
     int NTZN = 0;           // threads and shared memory of the nonlinear pass's z kernels
     size_t SMZN = 0;
-    int NPP = 0;            // row pitch of the packed spectra (2*Ngal1/3 + 1, padded to 4)
-    void* Hp[2] = {nullptr, nullptr};  // packed x-line output: PA [slot][z][NPP], PB [u-slot][z][NPP]
     int RW4 = 0, NT4 = 0;   // line-pair x-line kernel (k_xline4, FP32): rows per CTA (0 = not used), threads
     size_t SM4 = 0;
     size_t SM3 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
@@ -317,11 +314,11 @@ int tune_int(int32_t cfd_tuning::*field, const char* env, int dflt, int lo, int 
     return env_int(env, dflt, lo, hi);
 }
 
-size_t xline2_smem(int n1s, int n2s, int rw, size_t esz, bool pk) {
+size_t xline2_smem(int n1s, int n2s, int rw, size_t esz) {
     const int N = n1s * n2s;
     const int L1 = n1s * (n2s + 1) + 1, L2 = n2s * (n1s + 1) + 1, LU = N + 1;
     const int LX = std::max(L1, std::max(L2, LU));
-    return pk ? ((size_t)2 * rw * (L1 + L2) + N) * esz : ((size_t)2 * rw * LX + N) * esz;
+    return ((size_t)2 * rw * LX + N) * esz;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -350,14 +347,12 @@ int set_smem_attrs(cfd_ctx* c) {
         TWO_SWITCH(n2, ok, {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_zinv2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(k_zfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZ2);
         });
         TWO_SWITCH_SEL(c->ZALT, n2, ok, {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_zinv2s<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZN);
-            if (e == cudaSuccess && c->PK)
-                e = cudaFuncSetAttribute(k_zfwd2p<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZN);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_zfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZN);
         });
     }
     if (c->LZ2 >= 0) {
@@ -378,18 +373,13 @@ int set_smem_attrs(cfd_ctx* c) {
                 e = cudaFuncSetAttribute(k_ib_xfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMFX2);
         });
     }
-    if (c->RW2 && c->PK) {
+    if (c->RW2) {
         bool ok = true;
         TWO_SWITCH_SEL(c->XALT, n1, ok, {
             if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
+                e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
         });
-    }
-    if (c->RW2) {
-        bool ok = true;
         TWO_SWITCH(n1, ok, {
-            if (e == cudaSuccess && !c->PK)
-                e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
             if (e == cudaSuccess && c->XL3)
                 e = cudaFuncSetAttribute(k_xline3<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM3);
             if constexpr (std::is_same<T2, float2>::value)
@@ -485,19 +475,11 @@ int nl_transforms(cfd_ctx* c) {
     } else if (c->RW2) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
-        if (c->PK) {
-            TWO_SWITCH_SEL(c->XALT, d.ngal1, ok, {
-                k_xline2<T2, TN1, TN2, true><<<gx2, c->NT2, c->SM2, c->stream>>>(
-                    d, c->g, (const T2*)c->Hx, (T2*)c->Hp[0], (T2*)c->Hp[1], nullptr, nullptr, twx<T2>(c), c->RW2,
-                    ilog2(c->RW2), c->NPP);
-            });
-        } else {
-            TWO_SWITCH(d.ngal1, ok, {
-                k_xline2<T2, TN1, TN2, false><<<gx2, c->NT2, c->SM2, c->stream>>>(
-                    d, c->g, (const T2*)c->Hx, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], twx<T2>(c),
-                    c->RW2, ilog2(c->RW2), 0);
-            });
-        }
+        TWO_SWITCH_SEL(c->XALT, d.ngal1, ok, {
+            k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0],
+                                                                    (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
+                                                                    twx<T2>(c), c->RW2, ilog2(c->RW2));
+        });
         LK("k_xline2");
     } else {
         dim3 gx(d.ngal2 / c->RWx, d.nslot);
@@ -508,22 +490,12 @@ int nl_transforms(cfd_ctx* c) {
         LK("k_xline");
     }
     prof_mark(c);
-    if (c->PK) {
-        const int CP = 1 << (c->LZ2 - 1);  // (slot, kx) pairs per CTA, two lines each
-        dim3 gf2((std::max(d.nyu, d.nyv) * d.nkx + CP - 1) / CP, 2, 2);
-        bool ok = true;
-        TWO_SWITCH_SEL(c->ZALT, d.ngal2, ok, {
-            k_zfwd2p<T2, TN1, TN2><<<gf2, c->NTZN, c->SMZN, c->stream>>>(
-                d, (const T2*)c->Hp[0], (const T2*)c->Hp[1], c->NPP, (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
-                (T2*)c->S[3], twz<T2>(c), c->LZ2);
-        });
-        LK("k_zfwd2p");
-    } else if (c->LZ2 >= 0) {
+    if (c->LZ2 >= 0) {
         const int CH2 = 1 << c->LZ2;
         dim3 gf2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 4, 2);
         bool ok = true;
-        TWO_SWITCH(d.ngal2, ok, {
-            k_zfwd2<T2, TN1, TN2><<<gf2, c->NTZ2, c->SMZ2, c->stream>>>(
+        TWO_SWITCH_SEL(c->ZALT, d.ngal2, ok, {
+            k_zfwd2<T2, TN1, TN2><<<gf2, c->NTZN, c->SMZN, c->stream>>>(
                 d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
                 (T2*)c->S[3], twz<T2>(c), c->LZ2);
         });
@@ -1011,25 +983,21 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     while (c->RWibf > 2 && ((d.ngal2 % c->RWibf) || (size_t)(2 * (c->RWibf / 2) * d.ngal1 + d.ngal1) * esz > budget))
         c->RWibf /= 2;
     if (d.ngal2 % c->RWibf) return fail(c, CFD_ERR_SIZE, "Ngal2 must be even");
-    // k_xline2 with packed output (see k_zfwd2p) unless CFD_XLINE_UNPACKED=1
+    // the transposed split of the x-line transform (tuning xsplit = 2) is for path 1 only
     const int xpath = g_tuning && g_tuning->xline_path ? g_tuning->xline_path : env_int("CFD_XLINE_PATH", 1, 1, 4);
-    const bool pk_want = xpath == 1 && !env_int("CFD_XLINE_UNPACKED", 0, 0, 1);
-    const bool xalt = pk_want && tune_int(&cfd_tuning::xsplit, "CFD_XSPLIT", 1, 1, 2) == 2;
-    int xn1 = 0, xn2 = 0;
+    const bool xalt = xpath == 1 && tune_int(&cfd_tuning::xsplit, "CFD_XSPLIT", 1, 1, 2) == 2;
     {
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH_SEL(xalt, d.ngal1, ok, { n1s = TN1; n2s = TN2; });
-        xn1 = n1s;
-        xn2 = n2s;
         if (ok) {
             int rw = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", mixed ? 8 : 4, 2, 8);
             rw = 1 << (31 - __builtin_clz(rw));  // a power of two
-            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz, pk_want) > budget)) rw /= 2;
+            while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
             if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {
                 c->RW2 = rw;
                 c->NT2 = 2 * rw * std::max(n1s, n2s);
-                c->SM2 = xline2_smem(n1s, n2s, rw, esz, pk_want);
+                c->SM2 = xline2_smem(n1s, n2s, rw, esz);
                 // packed lines (k_xline3): twiddles, exchange of 2*rw lines, physical rows /
                 // forward spectra
                 const size_t N = (size_t)n1s * n2s, LX = (size_t)((n1s * (n2s + 1)) | 1);
@@ -1074,10 +1042,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     if (c->LZ2 < 0) c->RW2 = 0;  // the two-step x-line kernels read the output of k_zinv2s
     if (!c->RW2) c->RW4 = 0;
-    c->PK = c->RW2 && !c->XL3 && !c->RW4 && pk_want;
-    if (c->RW2 && !c->PK) c->SM2 = xline2_smem(xn1, xn2, c->RW2, esz, false);
-    c->XALT = c->PK && xalt;  // (xalt implies path 1, so PK unless the two-step path is off)
-    if (c->PK && c->LZ2 >= 0 && tune_int(&cfd_tuning::zsplit, "CFD_ZSPLIT", 1, 1, 2) == 2) {
+    c->XALT = c->RW2 && xalt;  // (xalt implies path 1: neither k_xline3 nor k_xline4)
+    if (c->RW2 && c->LZ2 >= 0 && tune_int(&cfd_tuning::zsplit, "CFD_ZSPLIT", 1, 1, 2) == 2) {
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH_ALT(d.ngal2, ok, { n1s = TN1; n2s = TN2; });
@@ -1087,7 +1053,6 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
             c->SMZN = ((size_t)(1 << c->LZ2) * ((n1s * (n2s + 1)) | 1) + (size_t)n1s * n2s) * esz;
         }
     }
-    c->NPP = (2 * (d.nkx - 1) + 1 + 3) & ~3;
     {
         // warp-per-column Helmholtz solves: up to 16 rows per lane (512 planes)
         const int m = (d.nyu + 31) / 32;
@@ -1143,17 +1108,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     const size_t hsz = (size_t)d.nslot * d.ngal2 * d.nkx;
     for (int k = 0; k < 4; ++k) {
-        if (!c->PK) {
-            if (mixed) AL(c->H[k], float2, hsz);
-            else AL(c->H[k], double2, hsz);
-        }
-        if (mixed) AL(c->S[k], float2, (size_t)d.nslot * nc);
-        else AL(c->S[k], double2, (size_t)d.nslot * nc);
-    }
-    if (c->PK) {
-        const size_t pa = (size_t)d.nslot * d.ngal2 * c->NPP, pb = (size_t)nyu * d.ngal2 * c->NPP;
-        if (mixed) { AL(c->Hp[0], float2, pa); AL(c->Hp[1], float2, pb); }
-        else { AL(c->Hp[0], double2, pa); AL(c->Hp[1], double2, pb); }
+        if (mixed) { AL(c->H[k], float2, hsz); AL(c->S[k], float2, (size_t)d.nslot * nc); }
+        else { AL(c->H[k], double2, hsz); AL(c->S[k], double2, (size_t)d.nslot * nc); }
     }
     if (c->RW2) {
         const size_t hxs = (size_t)(2 * nyu + nyv) * d.ngal2 * d.nkx;

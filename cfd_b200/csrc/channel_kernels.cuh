@@ -265,19 +265,9 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // The retained modes are kx = 0..N/3 (N1 = 2*(Ngal1/3)), a compile-time bound, so which
 // elements of a subsequence are zero, direct or conjugated is resolved at compile time
 // except in the two blocks that straddle a boundary.
-//
-// PK = true (the default path): the inverse and forward exchanges have buffers of their own
-// and step 2' stores the packed forward spectra P (line 2r: A + iB of the row's first two
-// products, line 2r+1 on u-planes: the other two) straight from registers, retained modes
-// only (k <= N/3 at k, k >= N - N/3 at k - (N - 2N/3 - 1)), unscaled, in rows of `npp`
-// elements: PA = H0 [slot][z][npp] for the even lines, PB = H1 [u-slot][z][npp] for the odd
-// ones.  The unpack into the two real spectra and the 1/Ngal1 scale move to the forward z
-// pass (k_zfwd2p), which reads both P_k and P_{N-k} anyway, so the kernel ends after step 2'
-// with three barriers instead of six.  PK = false writes the four unpacked product spectra
-// H0..H3 [slot][z][kx], as the other x-line paths do.
-template <typename T2, int N1, int N2, bool PK>
+template <typename T2, int N1, int N2>
 __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && (N1 > N2 ? N1 : N2) <= 24) ? 2 : 1) k_xline2(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
-                         T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw, int npp) {
+                         T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
     using R = decltype(T2::x);
     constexpr int N = N1 * N2;
     constexpr int HX = N / 3;               // highest retained kx
@@ -288,9 +278,8 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
     constexpr int LX = (L1 > L2 ? (L1 > LU ? L1 : LU) : (L2 > LU ? L2 : LU));
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = 2 * RW;
-    T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX (PK: B * L1, inverse exchange)
-    T2* exf = PK ? ex + (size_t)B * L1 : ex;         // forward exchange (PK: B * L2 of its own)
-    T2* twt = PK ? exf + (size_t)B * L2 : ex + (size_t)B * LX;  // N1 * N2: twt[b*N2 + a] = w^(a*b), a < N2, b < N1
+    T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX
+    T2* twt = ex + (size_t)B * LX;                   // N1 * N2: twt[b*N2 + a] = w^(a*b), a < N2, b < N1
     // u- and v-slots interleaved in y (nyu = nyv + 1), so that the y-neighbour planes read
     // by the interpolation are still in L2 from the adjacent slots
     const int slot = (blockIdx.y & 1) ? d.nyu + (blockIdx.y >> 1) : (blockIdx.y >> 1);
@@ -413,9 +402,9 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
 #pragma unroll
         for (int kb = 1; kb < N2; ++kb) y[kb] = cmul(y[kb], twt[k1 * N2 + kb]);
     }
-    if (!PK) __syncthreads();  // every lane has read the inverse exchange (shared buffer)
+    __syncthreads();  // every lane has read the inverse exchange
     if (act2) {
-        T2* o = exf + (size_t)b2 * L2 + k1;
+        T2* o = ex + (size_t)b2 * L2 + k1;
 #pragma unroll
         for (int kb = 0; kb < N2; ++kb) o[kb * (N1 + 1)] = y[kb];
     }
@@ -428,32 +417,10 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
     const int b3 = i3 < RW ? 2 * i3 : 2 * (i3 - RW) + 1;
     const bool act3 = t < B * N2 && (uplane || i3 < RW);
     if (act3) {
-        const T2* o = exf + (size_t)b3 * L2 + kb * (N1 + 1);
+        const T2* o = ex + (size_t)b3 * L2 + kb * (N1 + 1);
 #pragma unroll
         for (int na = 0; na < N1; ++na) z[na] = o[na];
         rdft<N1, -1>(z);
-    }
-    if constexpr (PK) {
-        // packed spectra straight to HBM: X[kb + N2*ka] of line b3, retained modes only;
-        // blocks of ka wholly inside the gap are neither stored nor computed
-        constexpr int GAPX = N - 2 * HX - 1;
-        if (act3) {
-            const int rr = b3 >> 1;
-            T2* dst = ((b3 & 1) ? H1 : H0) + ((size_t)slot * d.ngal2 + z0 + rr) * npp;
-#pragma unroll
-            for (int ka = 0; ka < N1; ++ka) {
-                const int k0 = N2 * ka, k = k0 + kb;
-                if (k0 + N2 - 1 <= HX) {
-                    dst[k] = z[ka];
-                } else if (k0 >= N - HX) {
-                    dst[k - GAPX] = z[ka];
-                } else if (!(k0 > HX && k0 + N2 - 1 < N - HX)) {
-                    if (k <= HX) dst[k] = z[ka];
-                    else if (k >= N - HX) dst[k - GAPX] = z[ka];
-                }
-            }
-        }
-        return;
     }
     __syncthreads();
     if (act3) {
@@ -1021,56 +988,6 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
     const R sc = (R)1 / (R)N;
     __syncthreads();
     auto load = [&](int z, int) -> T2 { return H[(size_t)z * d.nkx]; };
-    auto store = [&](int e, int, T2 v) {
-        const int q = zrow_q<N, TN1>(e, r);
-        if (q >= 0 && live) S[(size_t)q * d.nkx] = cscale(v, sc);
-    };
-    two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
-}
-
-// Pass 3 on the packed x-line output (k_xline2 with PK): the two real spectra of a packed
-// line P = A + iB are A_k = (P_k + conj P_{N-k})/2 and B_k = (P_k - conj P_{N-k})/(2i) (the
-// unpack that ends rfft of two real rows, rft_buff.f:60-70), formed here while loading, so
-// that a CTA transforms CH/2 kx values of one packed line as CH lines: line 2m = A at kx
-// i0 + m, line 2m+1 = B at the same kx.  Both lanes read P_i and P_{N-i} (the partner's loads
-// hit L1).  The 1/2, 1/Ngal1 and 1/Ngal2 scales are applied together at the store.
-// grid: x = chunk of CH/2 (slot-in-group, kx) pairs, y = packed line (0: PA, 1: PB),
-// z = group (u-planes, v-planes; v-planes have PA only).
-//   u-plane PA = uu + i vv -> S0, S2;  PB = ww + i uw -> S3, S1;  v-plane PA = uv + i vw -> S0, S1
-template <typename T2, int TN1, int TN2>
-__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zfwd2p(Dims d, const T2* __restrict__ PA, const T2* __restrict__ PB, int npp,
-                        T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2, T2* __restrict__ S3,
-                        const T2* __restrict__ twz, int lb) {
-    using R = decltype(T2::x);
-    constexpr int N = TN1 * TN2;
-    const int grp = blockIdx.z, pl = blockIdx.y;
-    if (grp == 1 && pl == 1) return;
-    const int nsl = grp ? d.nyv : d.nyu;
-    const int npairs = nsl * d.nkx;
-    const int pair0 = blockIdx.x << (lb - 1);
-    if (pair0 >= npairs) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T2* twt = reinterpret_cast<T2*>(smem_raw);
-    T2* ex = twt + N;
-    load_twiddles<T2, TN1, TN2>(twt, twz);
-    const int b = threadIdx.x & ((1 << lb) - 1);
-    const int half = b & 1;
-    const bool live = pair0 + (b >> 1) < npairs;
-    const int pair = live ? pair0 + (b >> 1) : npairs - 1;
-    const int sl = pair / d.nkx, i = pair - sl * d.nkx;
-    const int slot = grp ? d.nyu + sl : sl;
-    const int hx = d.nkx - 1;
-    const int im = i == 0 ? 0 : 2 * hx + 1 - i;     // packed position of P_{Ngal1 - i}
-    const T2* P = (pl ? PB : PA) + (size_t)slot * d.ngal2 * npp;
-    T2* S = pl ? (half ? S1 : S3) : (half ? (grp ? S1 : S2) : S0);
-    S += (size_t)slot * d.ncol + i;
-    const int r = threadIdx.x >> lb;
-    const R sc = (R)(0.5 / ((double)d.ngal1 * (double)N));
-    __syncthreads();
-    auto load = [&](int z, int) -> T2 {
-        const T2 pk = P[(size_t)z * npp + i], pm = P[(size_t)z * npp + im];
-        return half ? cx<T2>(pk.y + pm.y, pm.x - pk.x) : cx<T2>(pk.x + pm.x, pk.y - pm.y);
-    };
     auto store = [&](int e, int, T2 v) {
         const int q = zrow_q<N, TN1>(e, r);
         if (q >= 0 && live) S[(size_t)q * d.nkx] = cscale(v, sc);
