@@ -30,7 +30,8 @@ class CfdConfig(C.Structure):
                 ("bet", C.c_double), ("dt", C.c_double), ("mpgx", C.c_double),
                 ("qxt", C.c_double), ("flag_ctpress", C.c_int32), ("precision", C.c_int32),
                 ("yu", _dp), ("yv", _dp), ("dthdyu", _dp), ("dthdyv", _dp),
-                ("dyu2i", _dp), ("dyv2i", _dp)]
+                ("dyu2i", _dp), ("dyv2i", _dp),
+                ("ngal1_mid", C.c_int32), ("ngal2_mid", C.c_int32), ("band_vface", C.c_int32)]
 
 
 class CfdIBList(C.Structure):
@@ -109,6 +110,9 @@ def make_config(cfg, grid, dt, keep: list) -> CfdConfig:
     c.mpgx, c.qxt, c.flag_ctpress = cfg.mpgx, cfg.qxt, cfg.flag_ctpress
     c.precision = PREC[cfg.precision]
     c.yu, c.yv, c.dthdyu, c.dthdyv, c.dyu2i, c.dyv2i = [dptr(a) for a in arrs]
+    c.ngal1_mid = getattr(cfg, "ngal1_mid", 0) or cfg.ngal1
+    c.ngal2_mid = getattr(cfg, "ngal2_mid", 0) or cfg.ngal2
+    c.band_vface = getattr(cfg, "band_vface", 0)
     return c
 
 

@@ -49,6 +49,10 @@ def build_channel(cfg: ChannelConfig, with_fields: bool = True) -> ChannelSetup:
     ibu, ibv = ib_lists(cfg, grid)
     if with_fields:
         u1, u2, u3, p = initial_state(cfg, grid)
+        # three bands: the short columns start from zero outside their segments
+        from .bands import restrict
+        u1, u3 = restrict(cfg, grid, u1, "u"), restrict(cfg, grid, u3, "u")
+        u2, p = restrict(cfg, grid, u2, "v"), restrict(cfg, grid, p, "p")
         dt = cfg.dt if cfg.dt is not None else cfl_dt(cfg, grid, u1, u2, u3)
     else:
         u1 = u2 = u3 = p = None

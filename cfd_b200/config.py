@@ -58,6 +58,11 @@ class ChannelConfig:
     perturbation: float = 0.1
     kmax: int = 8
     name: str = ""
+    # three y-bands (start.f90:76-111): band_vface = N(3,1), the last v face of the bottom
+    # band; the middle band runs at ngal1_mid x ngal2_mid (0: the wall bands' size)
+    band_vface: int = 0
+    ngal1_mid: int = 0
+    ngal2_mid: int = 0
 
     def __post_init__(self):
         if self.re_b is None:

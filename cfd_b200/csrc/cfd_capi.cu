@@ -914,6 +914,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     d.nyu = d.ju1 - d.ju0 + 1; d.nyv = d.jv1 - d.jv0 + 1; d.nyp = d.jp1 - d.jp0 + 1;
     d.nslot = d.nyu + d.nyv;
     c->precision = cfg->precision;
+    if (cfg->band_vface > 0 && (cfg->ngal1_mid != cfg->ngal1 || cfg->ngal2_mid != cfg->ngal2))
+        return fail(c, CFD_ERR_SIZE, "a middle band of another x/z size than the wall bands");
     c->re = cfg->re; c->alp = cfg->alp; c->bet = cfg->bet; c->dt = cfg->dt; c->qxt = cfg->qxt;
     c->mpgx0 = cfg->mpgx; c->ctpress = cfg->flag_ctpress;
 

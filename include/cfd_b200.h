@@ -89,6 +89,16 @@ typedef struct cfd_config {
     const double *dthdyv;   /* [ny+2*dsty]                                         */
     const double *dyu2i;    /* [ny+2*dsty+1][3]  (Fortran dyu2i(3,j))              */
     const double *dyv2i;    /* [ny+2*dsty][3]                                      */
+    /* Three y-bands (start.f90:76-111) when band_vface > 0: band_vface is the reference's
+     * N(3,1), the last v face of the bottom band.  The wall bands (u/w centres up to
+     * band_vface+1 and from ny-1-band_vface, v faces up to band_vface and from
+     * ny-1-band_vface) run at ngal1 x ngal2, the middle band at ngal1_mid x ngal2_mid
+     * (2^a*3^b, at most the wall bands' size); the modes of the wall bands that the middle
+     * band lacks are "short" columns, solved in each wall band separately with the band
+     * interface rows of LU_buildU/V/P (tridLU_3D_IB.f90:349-413, 417-491).  band_vface = 0:
+     * one band, ngal*_mid ignored.  The column list and the field layout are those of the
+     * wall bands; a short column is zero outside its two segments. */
+    int32_t ngal1_mid, ngal2_mid, band_vface;
 } cfd_config;
 
 /* Immersed-boundary forcing list of one grid (start.f90:1133-1145 f_list_ib_u/w_list_ib_u).

@@ -25,6 +25,7 @@ module cfd_b200_mod
     real(c_double)     :: re, alp, bet, dt, mpgx, qxt
     integer(c_int32_t) :: flag_ctpress, precision
     type(c_ptr)        :: yu, yv, dthdyu, dthdyv, dyu2i, dyv2i
+    integer(c_int32_t) :: ngal1_mid, ngal2_mid, band_vface
   end type
 
   type, bind(c) :: cfd_ib_list

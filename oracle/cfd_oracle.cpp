@@ -8,9 +8,18 @@
 // transforms, scipy banded solves for the Thomas sweeps, an independent numpy
 // restatement of the substep (tests/golden), and discrete invariants.
 //
-// Single y-band (uniform x/z resolution), one process: the reference's MPI transposes
-// become per-plane gathers/scatters and its ranks become OpenMP threads over planes or
-// columns.  Every function cites the reference routine it restates.
+// One process: the reference's MPI transposes become per-plane gathers/scatters and its
+// ranks become OpenMP threads over planes or columns.  Every function cites the reference
+// routine it restates.
+//
+// y-bands (start.f90:76-111, 1382-1651): with one band every (kx,kz) column spans the whole
+// channel.  With three (cfd_config.band_vface > 0) the two wall bands keep the x/z
+// resolution Ngal1 x Ngal2 and the middle band runs at ngal1_mid x ngal2_mid: the modes of
+// the middle band ("long" columns) span the channel, the others ("short" columns) exist in
+// the wall bands only, as two independent segments with their own boundary rows at the
+// band interfaces (jlim, start.f90:1538-1557; gridweighting(band,:), start.f90:494-508).
+// Every plane is transformed at its band's resolution and carries the columns that exist
+// there (modes_to_planes_UVP/planes_to_modes_UVP, FOU3D.f90:808-906, 1662-1758).
 //
 // Data layout mirrors the reference: a spectral field is f[column][j-j0] (Fortran
 // f(j,column)), a physical plane is xPL[k][i] with row length Ngal1+2.
@@ -174,9 +183,29 @@ struct IBData {
     int jlo[2] = {0, 0}, jhi[2] = {-1, -1};
 };
 
+// one column segment: the y rows of a column in one band (jlim(:,grid,band)) and the
+// gridweighting / gridweighting_interp of its two ends
+struct Seg {
+    int u0, u1, v0, v1, p0, p1;
+    double gwb, gwt, gwib, gwit;
+};
+
+// x/z size of a plane's band and its transforms
+struct PlaneGeom {
+    int ngal1, ngal2, n1, n2, rowlen;
+    bool mid;  // the middle band of a three-band run
+    const struct RFFTPlan* px;
+    const struct FFTPlan* pz;
+};
+
 struct Oracle {
-    // sizes
+    // sizes (the wall bands' with three bands)
     int ngal1, ngal2, n1, n2, nkx, ncol, ny, dny;
+    // three bands: middle band size and the last v face of the bottom band (N(3,1));
+    // mb = 0 for one band
+    int mb = 0, jb = 0, ngal1m = 0, ngal2m = 0, n1m = 0, n2m = 0;
+    std::vector<unsigned char> islong;  // column exists in the middle band
+    Seg segL{}, segS[2]{};              // long columns; bottom and top segments of short ones
     int ju0, ju1, jv0, jv1, jp0, jp1, nyu, nyv, nyp;
     int rowlen;  // Ngal1 + 2
     // parameters
@@ -190,8 +219,8 @@ struct Oracle {
     // spectral fields [col*ny + (j - j0)]
     std::vector<cplx> u1, u2, u3, p, psi, div, Nu1, Nu2, Nu3, du1, du2, du3;
     std::vector<cplx> u1i, u2i, u3i, uvf, vvc, vwf;
-    RFFTPlan px;
-    FFTPlan pz;
+    RFFTPlan px, pxm;
+    FFTPlan pz, pzm;
     int quirk_lastplane = 0;
     // statistics accumulators (stats.f90:1-253, allocated as start.f90:2705-2793):
     // plane sums [q][j - j0]; conditional sums of the bottom (b) and top (t) band
@@ -227,6 +256,23 @@ struct Oracle {
     int col_q(int col) const { return col / nkx; }
     // physical row (0-based) of spectral kz index q (0-based): start.f90:1561-1573
     int row_of(int q) const { return q < n2 / 2 ? q : q + (ngal2 - n2); }
+    // segments of a column
+    bool is_long(int col) const { return !mb || islong[col]; }
+    int nseg(int col) const { return is_long(col) ? 1 : 2; }
+    const Seg& seg(int col, int s) const { return is_long(col) ? segL : segS[s]; }
+    // band of a u/w plane and of a v plane (planelim, start.f90:1778-1800): 2 = middle
+    bool u_mid(int j) const { return mb && j > jb + 1 && j <= ny - 2 - jb; }
+    bool v_mid(int j) const { return mb && j > jb && j <= ny - 2 - jb; }
+    PlaneGeom geom(bool mid) const {
+        return mid ? PlaneGeom{ngal1m, ngal2m, n1m, n2m, ngal1m + 2, true, &pxm, &pzm}
+                   : PlaneGeom{ngal1, ngal2, n1, n2, ngal1 + 2, false, &px, &pz};
+    }
+    // a column is carried by a plane of the middle band only if it is long
+    bool on_plane(int col, bool mid) const { return !mid || is_long(col); }
+    // physical row of column q in a plane of geometry g (dk shift, start.f90:1625-1637)
+    int row_in(const PlaneGeom& g, int q) const { return q < g.n2 / 2 ? q : q + (g.ngal2 - n2); }
+    // spectral kz index of the plane's dealiasing row kz = -N2(band)/2 (der_x/der_z zero it)
+    int zrow_q(const PlaneGeom& g) const { return n2 - g.n2 / 2; }
 };
 
 // ------------------------------------------------------------------------------------
@@ -242,49 +288,58 @@ struct PlaneWork {
     }
 };
 
-static void cft_plane(const Oracle& o, double* pl, int iopt, PlaneWork& w) {
+static void cft_plane(const PlaneGeom& g, double* pl, int iopt, PlaneWork& w) {
     // cft(pl, ise=Ngal1+2, isa=2, m=(N1+2)/2, iopt): z-transform of kx-modes 0..N1/2
-    const int L = o.rowlen;
-    for (int i = 0; i <= o.n1 / 2; ++i) {
-        for (int k = 0; k < o.ngal2; ++k) w.zl[k] = cplx(pl[k * L + 2 * i], pl[k * L + 2 * i + 1]);
-        o.pz.exec(w.zl.data(), w.t.data(), iopt < 0 ? -1 : +1);
-        const double s = iopt < 0 ? 1.0 / o.ngal2 : 1.0;
-        for (int k = 0; k < o.ngal2; ++k) {
+    const int L = g.rowlen;
+    for (int i = 0; i <= g.n1 / 2; ++i) {
+        for (int k = 0; k < g.ngal2; ++k) w.zl[k] = cplx(pl[k * L + 2 * i], pl[k * L + 2 * i + 1]);
+        g.pz->exec(w.zl.data(), w.t.data(), iopt < 0 ? -1 : +1);
+        const double s = iopt < 0 ? 1.0 / g.ngal2 : 1.0;
+        for (int k = 0; k < g.ngal2; ++k) {
             pl[k * L + 2 * i] = s * w.zl[k].real();
             pl[k * L + 2 * i + 1] = s * w.zl[k].imag();
         }
     }
 }
 
-static void rft_plane(const Oracle& o, double* pl, int iopt, PlaneWork& w) {
-    const int L = o.rowlen;
-    for (int k = 0; k < o.ngal2; ++k) {
-        if (iopt < 0) o.px.forward(pl + (size_t)k * L, w.z.data(), w.t.data());
-        else o.px.inverse(pl + (size_t)k * L, w.z.data(), w.t.data());
+static void rft_plane(const PlaneGeom& g, double* pl, int iopt, PlaneWork& w) {
+    const int L = g.rowlen;
+    for (int k = 0; k < g.ngal2; ++k) {
+        if (iopt < 0) g.px->forward(pl + (size_t)k * L, w.z.data(), w.t.data());
+        else g.px->inverse(pl + (size_t)k * L, w.z.data(), w.t.data());
     }
 }
 
-static void four_to_phys(const Oracle& o, double* pl, bool zero_oddball, PlaneWork& w) {
+static void four_to_phys(const PlaneGeom& g, double* pl, bool zero_oddball, PlaneWork& w) {
     if (zero_oddball)
-        for (int i = 0; i < o.rowlen; ++i) pl[(o.ngal2 / 2) * o.rowlen + i] = 0.0;
-    cft_plane(o, pl, +1, w);
-    rft_plane(o, pl, +1, w);
+        for (int i = 0; i < g.rowlen; ++i) pl[(g.ngal2 / 2) * g.rowlen + i] = 0.0;
+    cft_plane(g, pl, +1, w);
+    rft_plane(g, pl, +1, w);
 }
 
-static void phys_to_four(const Oracle& o, double* pl, PlaneWork& w) {
-    rft_plane(o, pl, -1, w);
-    cft_plane(o, pl, -1, w);
+static void phys_to_four(const PlaneGeom& g, double* pl, PlaneWork& w) {
+    rft_plane(g, pl, -1, w);
+    cft_plane(g, pl, -1, w);
 }
+static void four_to_phys(const Oracle& o, double* pl, bool zero_oddball, PlaneWork& w) {
+    four_to_phys(o.geom(false), pl, zero_oddball, w);
+}
+static void phys_to_four(const Oracle& o, double* pl, PlaneWork& w) { phys_to_four(o.geom(false), pl, w); }
 
-// modes_to_planes for one plane (FOU3D.f90:842-848): zero, then scatter spectral columns
-static void gather_plane(Oracle& o, std::vector<cplx>& f, int nyf, int j0, int j, double* pl) {
-    std::memset(pl, 0, sizeof(double) * (size_t)o.rowlen * o.ngal2);
+// modes_to_planes for one plane (FOU3D.f90:842-848): zero, then scatter the spectral
+// columns the plane's band carries
+static void gather_plane(Oracle& o, const PlaneGeom& g, std::vector<cplx>& f, int nyf, int j0, int j, double* pl) {
+    std::memset(pl, 0, sizeof(double) * (size_t)g.rowlen * g.ngal2);
     for (int col = 0; col < o.ncol; ++col) {
-        int i = o.col_i(col), row = o.row_of(o.col_q(col));
+        if (!o.on_plane(col, g.mid)) continue;
+        int i = o.col_i(col), row = o.row_in(g, o.col_q(col));
         cplx v = f[(size_t)col * nyf + (j - j0)];
-        pl[(size_t)row * o.rowlen + 2 * i] = v.real();
-        pl[(size_t)row * o.rowlen + 2 * i + 1] = v.imag();
+        pl[(size_t)row * g.rowlen + 2 * i] = v.real();
+        pl[(size_t)row * g.rowlen + 2 * i + 1] = v.imag();
     }
+}
+static void gather_plane(Oracle& o, std::vector<cplx>& f, int nyf, int j0, int j, double* pl) {
+    gather_plane(o, o.geom(false), f, nyf, j0, j, pl);
 }
 
 // ------------------------------------------------------------------------------------
@@ -300,7 +355,9 @@ static void rhs0(Oracle& o, int krk) {
         const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
         const cplx C3x = -Oracle::dRK[r] * cplx(0.0, o.kx[i]);
         const cplx C3z = -Oracle::dRK[r] * cplx(0.0, o.kz[q]);
-        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
+        for (int sg = 0; sg < o.nseg(col); ++sg) {
+        const Seg& S = o.seg(col, sg);
+        for (int j = S.u0 + 1; j <= S.u1 - 1; ++j) {
             cplx Lu = o.DU2(0, j) * o.U(o.u1, col, j - 1) + (k2x + k2z + o.DU2(1, j)) * o.U(o.u1, col, j) +
                       o.DU2(2, j) * o.U(o.u1, col, j + 1);
             o.U(o.du1, col, j) = C1 * Lu + C2 * o.U(o.Nu1, col, j) + C3x * o.P(o.p, col, j);
@@ -308,11 +365,12 @@ static void rhs0(Oracle& o, int krk) {
                       o.DU2(2, j) * o.U(o.u3, col, j + 1);
             o.U(o.du3, col, j) = C1 * Lw + C2 * o.U(o.Nu3, col, j) + C3z * o.P(o.p, col, j);
         }
-        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) {
+        for (int j = S.v0 + 1; j <= S.v1 - 1; ++j) {
             const double C3 = -Oracle::dRK[r] * o.DTHV(j);
             cplx Lv = o.DV2(0, j) * o.V(o.u2, col, j - 1) + (k2x + k2z + o.DV2(1, j)) * o.V(o.u2, col, j) +
                       o.DV2(2, j) * o.V(o.u2, col, j + 1);
             o.V(o.du2, col, j) = C1 * Lv + C2 * o.V(o.Nu2, col, j) + C3 * (o.P(o.p, col, j + 1) - o.P(o.p, col, j));
+        }
         }
     }
     // mean pressure gradient on mode (0,0), j = N(4,0)+1..N(4,nband) (littleharsh.f90:650-656)
@@ -330,29 +388,31 @@ static void rhs0(Oracle& o, int krk) {
 static void interp(Oracle& o) {
 #pragma omp parallel for schedule(static)
     for (int col = 0; col < o.ncol; ++col) {
-        for (int j = o.jv0; j <= o.jv1; ++j) {
+        for (int sg = 0; sg < o.nseg(col); ++sg) {
+        const Seg& S = o.seg(col, sg);
+        for (int j = S.v0; j <= S.v1; ++j) {
             const double den = o.YU(j + 1) - o.YU(j);
             o.V(o.u1i, col, j) = ((o.YV(j) - o.YU(j)) * o.U(o.u1, col, j + 1) + (o.YU(j + 1) - o.YV(j)) * o.U(o.u1, col, j)) / den;
             o.V(o.u3i, col, j) = ((o.YV(j) - o.YU(j)) * o.U(o.u3, col, j + 1) + (o.YU(j + 1) - o.YV(j)) * o.U(o.u3, col, j)) / den;
         }
-        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j)
+        for (int j = S.u0 + 1; j <= S.u1 - 1; ++j)
             o.U(o.u2i, col, j) = ((o.YU(j) - o.YV(j - 1)) * o.V(o.u2, col, j) + (o.YV(j) - o.YU(j)) * o.V(o.u2, col, j - 1)) /
                                  (o.YV(j) - o.YV(j - 1));
-        o.U(o.u2i, col, o.ju0) = o.gwib * (o.V(o.u2, col, o.jv0) - o.U(o.u2i, col, o.ju0 + 1)) + o.U(o.u2i, col, o.ju0 + 1);
-        o.U(o.u2i, col, o.ju1) = o.gwit * (o.V(o.u2, col, o.jv1) - o.U(o.u2i, col, o.ju1 - 1)) + o.U(o.u2i, col, o.ju1 - 1);
+        o.U(o.u2i, col, S.u0) = S.gwib * (o.V(o.u2, col, S.v0) - o.U(o.u2i, col, S.u0 + 1)) + o.U(o.u2i, col, S.u0 + 1);
+        o.U(o.u2i, col, S.u1) = S.gwit * (o.V(o.u2, col, S.v1) - o.U(o.u2i, col, S.u1 - 1)) + o.U(o.u2i, col, S.u1 - 1);
+        }
     }
 }
 
-// derivative value of one spectral entry with the dealiasing zero of der_x/der_z:
-// the kz = -N2/2 mode (physical row Ngal2-N2/2) is zeroed (FOU3D.f90:334-338)
-static inline cplx dxdz(const Oracle& o, int i, int q, cplx a, cplx b) {
-    if (q == o.n2 / 2) return cplx(0.0, 0.0);
+// derivative value of one spectral entry with the dealiasing zero of der_x/der_z: the
+// kz = -N2/2 mode of the plane's band (physical row Ngal2-N2/2) is zeroed (FOU3D.f90:334-338)
+static inline cplx dxdz(const Oracle& o, int i, int q, int qzero, cplx a, cplx b) {
+    if (q == qzero) return cplx(0.0, 0.0);
     return cplx(0.0, o.kx[i]) * a + cplx(0.0, o.kz[q]) * b;
 }
 
 static void ops_in_planes(Oracle& o) {
-    const size_t psz = (size_t)o.rowlen * o.ngal2;
-    const int nphys = o.ngal1;
+    const size_t psz = (size_t)o.rowlen * o.ngal2;  // the largest plane
     // u planes (ugrid, incl. ghosts): uu, uw, vv, ww
 #pragma omp parallel
     {
@@ -361,67 +421,75 @@ static void ops_in_planes(Oracle& o) {
         std::vector<double> a(psz), b(psz), c(psz), uu(psz), uw(psz), vv(psz), ww(psz);
 #pragma omp for schedule(dynamic)
         for (int j = o.ju0; j <= o.ju1; ++j) {
-            gather_plane(o, o.u1, o.nyu, o.ju0, j, a.data());
-            gather_plane(o, o.u2i, o.nyu, o.ju0, j, b.data());
-            gather_plane(o, o.u3, o.nyu, o.ju0, j, c.data());
-            four_to_phys(o, a.data(), true, w);
-            four_to_phys(o, b.data(), true, w);
-            four_to_phys(o, c.data(), true, w);
-            std::fill(uu.begin(), uu.end(), 0.0);
-            std::fill(uw.begin(), uw.end(), 0.0);
-            std::fill(vv.begin(), vv.end(), 0.0);
-            std::fill(ww.begin(), ww.end(), 0.0);
-            for (int k = 0; k < o.ngal2; ++k)
-                for (int i = 0; i < nphys; ++i) {
-                    size_t e = (size_t)k * o.rowlen + i;
+            const PlaneGeom g = o.geom(o.u_mid(j));
+            const size_t gsz = (size_t)g.rowlen * g.ngal2;
+            gather_plane(o, g, o.u1, o.nyu, o.ju0, j, a.data());
+            gather_plane(o, g, o.u2i, o.nyu, o.ju0, j, b.data());
+            gather_plane(o, g, o.u3, o.nyu, o.ju0, j, c.data());
+            four_to_phys(g, a.data(), true, w);
+            four_to_phys(g, b.data(), true, w);
+            four_to_phys(g, c.data(), true, w);
+            std::fill(uu.begin(), uu.begin() + gsz, 0.0);
+            std::fill(uw.begin(), uw.begin() + gsz, 0.0);
+            std::fill(vv.begin(), vv.begin() + gsz, 0.0);
+            std::fill(ww.begin(), ww.begin() + gsz, 0.0);
+            for (int k = 0; k < g.ngal2; ++k)
+                for (int i = 0; i < g.ngal1; ++i) {
+                    size_t e = (size_t)k * g.rowlen + i;
                     uu[e] = a[e] * a[e];
                     uw[e] = a[e] * c[e];
                     vv[e] = b[e] * b[e];
                     ww[e] = c[e] * c[e];
                 }
-            phys_to_four(o, uu.data(), w);
-            phys_to_four(o, uw.data(), w);
-            phys_to_four(o, vv.data(), w);
-            phys_to_four(o, ww.data(), w);
+            phys_to_four(g, uu.data(), w);
+            phys_to_four(g, uw.data(), w);
+            phys_to_four(g, vv.data(), w);
+            phys_to_four(g, ww.data(), w);
             const bool interior = (j > o.ju0 && j < o.ju1);
+            const int qz = o.zrow_q(g);
             for (int col = 0; col < o.ncol; ++col) {
+                if (!o.on_plane(col, g.mid)) continue;
                 const int i = o.col_i(col), q = o.col_q(col);
-                const size_t e = (size_t)o.row_of(q) * o.rowlen + 2 * i;
+                const size_t e = (size_t)o.row_in(g, q) * g.rowlen + 2 * i;
                 cplx UU(uu[e], uu[e + 1]), UW(uw[e], uw[e + 1]), VV(vv[e], vv[e + 1]), WW(ww[e], ww[e + 1]);
                 o.U(o.vvc, col, j) = VV;
                 if (interior || o.quirk_lastplane) {
-                    o.U(o.Nu1, col, j) = dxdz(o, i, q, UU, UW);
-                    o.U(o.Nu3, col, j) = dxdz(o, i, q, UW, WW);
+                    o.U(o.Nu1, col, j) = dxdz(o, i, q, qz, UU, UW);
+                    o.U(o.Nu3, col, j) = dxdz(o, i, q, qz, UW, WW);
                 }
             }
         }
         // v planes (vgrid, incl. walls): uv, vw
 #pragma omp for schedule(dynamic)
         for (int j = o.jv0; j <= o.jv1; ++j) {
-            gather_plane(o, o.u1i, o.nyv, o.jv0, j, a.data());
-            gather_plane(o, o.u2, o.nyv, o.jv0, j, b.data());
-            gather_plane(o, o.u3i, o.nyv, o.jv0, j, c.data());
-            four_to_phys(o, a.data(), true, w);
-            four_to_phys(o, b.data(), true, w);
-            four_to_phys(o, c.data(), true, w);
-            std::fill(uu.begin(), uu.end(), 0.0);
-            std::fill(uw.begin(), uw.end(), 0.0);
-            for (int k = 0; k < o.ngal2; ++k)
-                for (int i = 0; i < nphys; ++i) {
-                    size_t e = (size_t)k * o.rowlen + i;
+            const PlaneGeom g = o.geom(o.v_mid(j));
+            const size_t gsz = (size_t)g.rowlen * g.ngal2;
+            gather_plane(o, g, o.u1i, o.nyv, o.jv0, j, a.data());
+            gather_plane(o, g, o.u2, o.nyv, o.jv0, j, b.data());
+            gather_plane(o, g, o.u3i, o.nyv, o.jv0, j, c.data());
+            four_to_phys(g, a.data(), true, w);
+            four_to_phys(g, b.data(), true, w);
+            four_to_phys(g, c.data(), true, w);
+            std::fill(uu.begin(), uu.begin() + gsz, 0.0);
+            std::fill(uw.begin(), uw.begin() + gsz, 0.0);
+            for (int k = 0; k < g.ngal2; ++k)
+                for (int i = 0; i < g.ngal1; ++i) {
+                    size_t e = (size_t)k * g.rowlen + i;
                     uu[e] = a[e] * b[e];  // uv
                     uw[e] = c[e] * b[e];  // vw
                 }
-            phys_to_four(o, uu.data(), w);
-            phys_to_four(o, uw.data(), w);
+            phys_to_four(g, uu.data(), w);
+            phys_to_four(g, uw.data(), w);
             const bool interior = (j > o.jv0 && j < o.jv1);
+            const int qz = o.zrow_q(g);
             for (int col = 0; col < o.ncol; ++col) {
+                if (!o.on_plane(col, g.mid)) continue;
                 const int i = o.col_i(col), q = o.col_q(col);
-                const size_t e = (size_t)o.row_of(q) * o.rowlen + 2 * i;
+                const size_t e = (size_t)o.row_in(g, q) * g.rowlen + 2 * i;
                 cplx UV(uu[e], uu[e + 1]), VW(uw[e], uw[e + 1]);
                 o.V(o.uvf, col, j) = UV;
                 o.V(o.vwf, col, j) = VW;
-                if (interior || o.quirk_lastplane) o.V(o.Nu2, col, j) = dxdz(o, i, q, UV, VW);
+                if (interior || o.quirk_lastplane) o.V(o.Nu2, col, j) = dxdz(o, i, q, qz, UV, VW);
             }
         }
     }
@@ -444,19 +512,26 @@ static void nonlinear(Oracle& o, int krk) {
     interp(o);
     ops_in_planes(o);
     const double C1 = -Oracle::gRK[krk - 1];
+    // der_yu_h / der_yv_h over each column segment (FOU3D.f90:158-173); a short column reads
+    // the products of the interface plane it is not carried on as the zero they were
+    // allocated with (start.f90:613), as the reference does
 #pragma omp parallel for schedule(static)
     for (int col = 0; col < o.ncol; ++col) {
-        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
-            o.U(o.Nu1, col, j) = o.U(o.Nu1, col, j) + (o.V(o.uvf, col, j) - o.V(o.uvf, col, j - 1)) * o.DTHU(j);
-            o.U(o.Nu3, col, j) = o.U(o.Nu3, col, j) + (o.V(o.vwf, col, j) - o.V(o.vwf, col, j - 1)) * o.DTHU(j);
+        for (int sg = 0; sg < o.nseg(col); ++sg) {
+            const Seg& S = o.seg(col, sg);
+            for (int j = S.u0 + 1; j <= S.u1 - 1; ++j) {
+                o.U(o.Nu1, col, j) = o.U(o.Nu1, col, j) + (o.V(o.uvf, col, j) - o.V(o.uvf, col, j - 1)) * o.DTHU(j);
+                o.U(o.Nu3, col, j) = o.U(o.Nu3, col, j) + (o.V(o.vwf, col, j) - o.V(o.vwf, col, j - 1)) * o.DTHU(j);
+            }
+            for (int j = S.v0 + 1; j <= S.v1 - 1; ++j)
+                o.V(o.Nu2, col, j) = o.V(o.Nu2, col, j) + (o.U(o.vvc, col, j + 1) - o.U(o.vvc, col, j)) * o.DTHV(j);
+            for (int j = S.u0 + 1; j <= S.u1 - 1; ++j) {
+                o.U(o.du1, col, j) = o.U(o.du1, col, j) + C1 * o.U(o.Nu1, col, j);
+                o.U(o.du3, col, j) = o.U(o.du3, col, j) + C1 * o.U(o.Nu3, col, j);
+            }
+            for (int j = S.v0 + 1; j <= S.v1 - 1; ++j)
+                o.V(o.du2, col, j) = o.V(o.du2, col, j) + C1 * o.V(o.Nu2, col, j);
         }
-        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j)
-            o.V(o.Nu2, col, j) = o.V(o.Nu2, col, j) + (o.U(o.vvc, col, j + 1) - o.U(o.vvc, col, j)) * o.DTHV(j);
-        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
-            o.U(o.du1, col, j) = o.U(o.du1, col, j) + C1 * o.U(o.Nu1, col, j);
-            o.U(o.du3, col, j) = o.U(o.du3, col, j) + C1 * o.U(o.Nu3, col, j);
-        }
-        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) o.V(o.du2, col, j) = o.V(o.du2, col, j) + C1 * o.V(o.Nu2, col, j);
     }
 }
 
@@ -533,15 +608,20 @@ static void thomas(int n, double* a1, double* a2, double* a3, const cplx* rhs, c
 }
 
 static void solve_u(Oracle& o, std::vector<cplx>& u, std::vector<cplx>& du, int krk) {
-    // solveU prologue (littleharsh.f90:744-755)
+    // solveU prologue (littleharsh.f90:744-755), per column segment
 #pragma omp parallel for schedule(static)
     for (int col = 0; col < o.ncol; ++col) {
-        o.U(du, col, o.ju0) = 0.0;
-        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) o.U(du, col, j) = o.U(u, col, j) + o.dt * o.U(du, col, j);
-        o.U(du, col, o.ju1) = 0.0;
+        for (int sg = 0; sg < o.nseg(col); ++sg) {
+            const Seg& S = o.seg(col, sg);
+            o.U(du, col, S.u0) = 0.0;
+            for (int j = S.u0 + 1; j <= S.u1 - 1; ++j) o.U(du, col, j) = o.U(u, col, j) + o.dt * o.U(du, col, j);
+            o.U(du, col, S.u1) = 0.0;
+        }
     }
     immersed_boundaries(o, u, du, o.nyu, o.ju0, o.ju1, o.ibu);
     const double beta = Oracle::bRK[krk - 1] * o.dt / o.Re;
+    // LUsolU per band: LU_buildU over jlim with the band's gridweighting rows (tridLU_3D_IB.f90:
+    // 50-103, 349-380)
 #pragma omp parallel
     {
         std::vector<double> a1(o.nyu), a2(o.nyu), a3(o.nyu);
@@ -549,15 +629,20 @@ static void solve_u(Oracle& o, std::vector<cplx>& u, std::vector<cplx>& du, int 
         for (int col = 0; col < o.ncol; ++col) {
             const int i = o.col_i(col), q = o.col_q(col);
             const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
-            a1[0] = 0.0; a2[0] = 1.0; a3[0] = o.gwb;
-            for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
-                int jj = j - o.ju0;
-                a1[jj] = -beta * o.DU2(0, j);
-                a2[jj] = 1.0 - beta * (o.DU2(1, j) + k2x + k2z);
-                a3[jj] = -beta * o.DU2(2, j);
+            for (int sg = 0; sg < o.nseg(col); ++sg) {
+                const Seg& S = o.seg(col, sg);
+                const int n = S.u1 - S.u0 + 1;
+                a1[0] = 0.0; a2[0] = 1.0; a3[0] = S.gwb;
+                for (int j = S.u0 + 1; j <= S.u1 - 1; ++j) {
+                    int jj = j - S.u0;
+                    a1[jj] = -beta * o.DU2(0, j);
+                    a2[jj] = 1.0 - beta * (o.DU2(1, j) + k2x + k2z);
+                    a3[jj] = -beta * o.DU2(2, j);
+                }
+                a1[n - 1] = S.gwt; a2[n - 1] = 1.0; a3[n - 1] = 0.0;
+                const size_t off = (size_t)col * o.nyu + (S.u0 - o.ju0);
+                thomas(n, a1.data(), a2.data(), a3.data(), &du[off], &u[off]);
             }
-            a1[o.nyu - 1] = o.gwt; a2[o.nyu - 1] = 1.0; a3[o.nyu - 1] = 0.0;
-            thomas(o.nyu, a1.data(), a2.data(), a3.data(), &du[(size_t)col * o.nyu], &u[(size_t)col * o.nyu]);
         }
     }
 }
@@ -565,9 +650,12 @@ static void solve_u(Oracle& o, std::vector<cplx>& u, std::vector<cplx>& du, int 
 static void solve_v(Oracle& o, int krk) {
 #pragma omp parallel for schedule(static)
     for (int col = 0; col < o.ncol; ++col) {
-        o.V(o.du2, col, o.jv0) = 0.0;
-        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) o.V(o.du2, col, j) = o.V(o.u2, col, j) + o.dt * o.V(o.du2, col, j);
-        o.V(o.du2, col, o.jv1) = 0.0;
+        for (int sg = 0; sg < o.nseg(col); ++sg) {
+            const Seg& S = o.seg(col, sg);
+            o.V(o.du2, col, S.v0) = 0.0;
+            for (int j = S.v0 + 1; j <= S.v1 - 1; ++j) o.V(o.du2, col, j) = o.V(o.u2, col, j) + o.dt * o.V(o.du2, col, j);
+            o.V(o.du2, col, S.v1) = 0.0;
+        }
     }
     immersed_boundaries(o, o.u2, o.du2, o.nyv, o.jv0, o.jv1, o.ibv);
     const double beta = Oracle::bRK[krk - 1] * o.dt / o.Re;
@@ -578,15 +666,20 @@ static void solve_v(Oracle& o, int krk) {
         for (int col = 0; col < o.ncol; ++col) {
             const int i = o.col_i(col), q = o.col_q(col);
             const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
-            a1[0] = 0.0; a2[0] = 1.0; a3[0] = 0.0;
-            for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) {
-                int jj = j - o.jv0;
-                a1[jj] = -beta * o.DV2(0, j);
-                a2[jj] = 1.0 - beta * (o.DV2(1, j) + k2x + k2z);
-                a3[jj] = -beta * o.DV2(2, j);
+            for (int sg = 0; sg < o.nseg(col); ++sg) {
+                const Seg& S = o.seg(col, sg);
+                const int n = S.v1 - S.v0 + 1;
+                a1[0] = 0.0; a2[0] = 1.0; a3[0] = 0.0;
+                for (int j = S.v0 + 1; j <= S.v1 - 1; ++j) {
+                    int jj = j - S.v0;
+                    a1[jj] = -beta * o.DV2(0, j);
+                    a2[jj] = 1.0 - beta * (o.DV2(1, j) + k2x + k2z);
+                    a3[jj] = -beta * o.DV2(2, j);
+                }
+                a1[n - 1] = 0.0; a2[n - 1] = 1.0; a3[n - 1] = 0.0;
+                const size_t off = (size_t)col * o.nyv + (S.v0 - o.jv0);
+                thomas(n, a1.data(), a2.data(), a3.data(), &o.du2[off], &o.u2[off]);
             }
-            a1[o.nyv - 1] = 0.0; a2[o.nyv - 1] = 1.0; a3[o.nyv - 1] = 0.0;
-            thomas(o.nyv, a1.data(), a2.data(), a3.data(), &o.du2[(size_t)col * o.nyv], &o.u2[(size_t)col * o.nyv]);
         }
     }
 }
@@ -642,23 +735,26 @@ static void divergence(Oracle& o) {
 #pragma omp parallel for schedule(static)
     for (int col = 0; col < o.ncol; ++col) {
         const cplx kx(0.0, o.kx[o.col_i(col)]), kz(0.0, o.kz[o.col_q(col)]);
-        for (int j = o.jp0; j <= o.jp1; ++j)
-            o.P(o.div, col, j) = kx * o.U(o.u1, col, j) + kz * o.U(o.u3, col, j) +
-                                 o.DTHU(j) * (o.V(o.u2, col, j) - o.V(o.u2, col, j - 1));
+        for (int sg = 0; sg < o.nseg(col); ++sg) {
+            const Seg& S = o.seg(col, sg);
+            for (int j = S.p0; j <= S.p1; ++j)
+                o.P(o.div, col, j) = kx * o.U(o.u1, col, j) + kz * o.U(o.u3, col, j) +
+                                     o.DTHU(j) * (o.V(o.u2, col, j) - o.V(o.u2, col, j - 1));
+        }
     }
 }
 
 static void solve_p(Oracle& o, int krk) {
     const double dtirk = (1.0 / o.dt) / (Oracle::aRK[krk - 1] + Oracle::bRK[krk - 1]);
     divergence(o);
+    // per band (solveP, littleharsh.f90:569-609): LU_buildP over jlim(:,pgrid,band), the mean
+    // mode's bottom row replaced in the middle band only (tridLU_3D_IB.f90:468-474)
 #pragma omp parallel
     {
         std::vector<double> a1(o.nyp), a2(o.nyp), a3(o.nyp);
         std::vector<cplx> x(o.nyp), r(o.nyp);
 #pragma omp for schedule(static)
         for (int col = 0; col < o.ncol; ++col) {
-            for (int j = o.jp0; j <= o.jp1; ++j) r[j - o.jp0] = dtirk * o.P(o.div, col, j);
-            if (col == 0) r[0] = 0.0;
             const int i = o.col_i(col), q = o.col_q(col);
             const double k2x = -o.kx[i] * o.kx[i], k2z = -o.kz[q] * o.kz[q];
             // D_vec/G_vec (tridLU_3D_IB.f90:434-439)
@@ -666,28 +762,33 @@ static void solve_p(Oracle& o, int krk) {
             auto Gb = [&](int m) { return -o.DTHV(m); };
             auto Dt = [&](int m) { return o.DTHU(m); };
             auto Gt = [&](int m) { return o.DTHV(m - 1); };
-            const int n = o.nyp;
-            a2[0] = (Dt(o.jp0) * Gb(o.jp0)) + k2x + k2z;
-            a3[0] = (Dt(o.jp0) * Gt(o.jp0 + 1));
-            a1[0] = 0.0;
-            a2[n - 1] = (Db(o.jp1 - 1) * Gt(o.jp1)) + k2x + k2z;
-            a1[n - 1] = (Db(o.jp1 - 1) * Gb(o.jp1 - 1));
-            a3[n - 1] = 0.0;
-            for (int j = o.jp0 + 1; j <= o.jp1 - 1; ++j) {
-                int jj = j - o.jp0;
-                a2[jj] = (Db(j - 1) * Gt(j)) + (Dt(j) * Gb(j)) + k2x + k2z;
-                a1[jj] = (Db(j - 1) * Gb(j - 1));
-                a3[jj] = (Dt(j) * Gt(j + 1));
-            }
-            if (col == 0) {
+            for (int sg = 0; sg < o.nseg(col); ++sg) {
+                const Seg& S = o.seg(col, sg);
+                const int n = S.p1 - S.p0 + 1;
+                for (int j = S.p0; j <= S.p1; ++j) r[j - S.p0] = dtirk * o.P(o.div, col, j);
+                if (col == 0) r[0] = 0.0;
+                a2[0] = (Dt(S.p0) * Gb(S.p0)) + k2x + k2z;
+                a3[0] = (Dt(S.p0) * Gt(S.p0 + 1));
                 a1[0] = 0.0;
-                a2[0] = 1.0 / ((o.YU(2) - o.YU(1)) * (o.YU(2) - o.YU(1)));
-                a3[0] = 0.0;
-            }
-            thomas(n, a1.data(), a2.data(), a3.data(), r.data(), x.data());
-            for (int j = o.jp0; j <= o.jp1; ++j) {
-                o.P(o.psi, col, j) = x[j - o.jp0];
-                o.P(o.p, col, j) = o.P(o.p, col, j) + x[j - o.jp0];
+                a2[n - 1] = (Db(S.p1 - 1) * Gt(S.p1)) + k2x + k2z;
+                a1[n - 1] = (Db(S.p1 - 1) * Gb(S.p1 - 1));
+                a3[n - 1] = 0.0;
+                for (int j = S.p0 + 1; j <= S.p1 - 1; ++j) {
+                    int jj = j - S.p0;
+                    a2[jj] = (Db(j - 1) * Gt(j)) + (Dt(j) * Gb(j)) + k2x + k2z;
+                    a1[jj] = (Db(j - 1) * Gb(j - 1));
+                    a3[jj] = (Dt(j) * Gt(j + 1));
+                }
+                if (col == 0) {
+                    a1[0] = 0.0;
+                    a2[0] = 1.0 / ((o.YU(2) - o.YU(1)) * (o.YU(2) - o.YU(1)));
+                    a3[0] = 0.0;
+                }
+                thomas(n, a1.data(), a2.data(), a3.data(), r.data(), x.data());
+                for (int j = S.p0; j <= S.p1; ++j) {
+                    o.P(o.psi, col, j) = x[j - S.p0];
+                    o.P(o.p, col, j) = o.P(o.p, col, j) + x[j - S.p0];
+                }
             }
         }
     }
@@ -695,22 +796,32 @@ static void solve_p(Oracle& o, int krk) {
 
 static void v_corr(Oracle& o, int krk) {
     const double dtrk = o.dt * (Oracle::aRK[krk - 1] + Oracle::bRK[krk - 1]);
+    // per band (littleharsh.f90:816-899): the ghost rows are set from the channel's own
+    // gridweighting at the bottom of bands 1-2 and the top of bands 2-3 only; the ghost
+    // rows of the short segments at the band interfaces keep what the solve left there
 #pragma omp parallel for schedule(static)
     for (int col = 0; col < o.ncol; ++col) {
         const cplx kx = dtrk * cplx(0.0, o.kx[o.col_i(col)]);
         const cplx kz = dtrk * cplx(0.0, o.kz[o.col_q(col)]);
-        for (int j = o.ju0 + 1; j <= o.ju1 - 1; ++j) {
-            o.U(o.u1, col, j) = o.U(o.u1, col, j) - kx * o.P(o.psi, col, j);
-            o.U(o.u3, col, j) = o.U(o.u3, col, j) - kz * o.P(o.psi, col, j);
+        for (int sg = 0; sg < o.nseg(col); ++sg) {
+            const Seg& S = o.seg(col, sg);
+            for (int j = S.u0 + 1; j <= S.u1 - 1; ++j) {
+                o.U(o.u1, col, j) = o.U(o.u1, col, j) - kx * o.P(o.psi, col, j);
+                o.U(o.u3, col, j) = o.U(o.u3, col, j) - kz * o.P(o.psi, col, j);
+            }
+            if (S.u0 == o.ju0) {
+                o.U(o.u1, col, o.ju0) = -o.gwb * o.U(o.u1, col, o.ju0 + 1);
+                o.U(o.u3, col, o.ju0) = -o.gwb * o.U(o.u3, col, o.ju0 + 1);
+            }
+            if (S.u1 == o.ju1) {
+                o.U(o.u1, col, o.ju1) = -o.gwt * o.U(o.u1, col, o.ju1 - 1);
+                o.U(o.u3, col, o.ju1) = -o.gwt * o.U(o.u3, col, o.ju1 - 1);
+            }
+            for (int j = S.v0 + 1; j <= S.v1 - 1; ++j)
+                o.V(o.u2, col, j) = o.V(o.u2, col, j) - dtrk * o.DTHV(j) * (o.P(o.psi, col, j + 1) - o.P(o.psi, col, j));
+            o.V(o.u2, col, S.v0) = 0.0;
+            o.V(o.u2, col, S.v1) = 0.0;
         }
-        o.U(o.u1, col, o.ju0) = -o.gwb * o.U(o.u1, col, o.ju0 + 1);
-        o.U(o.u1, col, o.ju1) = -o.gwt * o.U(o.u1, col, o.ju1 - 1);
-        o.U(o.u3, col, o.ju0) = -o.gwb * o.U(o.u3, col, o.ju0 + 1);
-        o.U(o.u3, col, o.ju1) = -o.gwt * o.U(o.u3, col, o.ju1 - 1);
-        for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j)
-            o.V(o.u2, col, j) = o.V(o.u2, col, j) - dtrk * o.DTHV(j) * (o.P(o.psi, col, j + 1) - o.P(o.psi, col, j));
-        o.V(o.u2, col, o.jv0) = 0.0;
-        o.V(o.u2, col, o.jv1) = 0.0;
     }
     divergence(o);
 }
@@ -925,40 +1036,52 @@ static void stats_accumulate(Oracle& o) {
 }
 
 static void dtc_calc(Oracle& o, double* terms) {
-    double um = 0.0, wm = 0.0, vm = 1e-6;
+    // maxima per band (index 0: wall bands, 1: middle band); each band's x/z terms use its
+    // own N (dtc_calc runs per rank with bandPL, the MPI MIN combines them, FOU3D.f90:177-180)
+    double um[2] = {0.0, 0.0}, wm[2] = {0.0, 0.0}, vm = 1e-6;
 #pragma omp parallel
     {
         PlaneWork w;
         w.init(o);
         const size_t psz = (size_t)o.rowlen * o.ngal2;
         std::vector<double> a(psz);
-        double lu = 0.0, lw = 0.0, lv = 0.0;
+        double lu[2] = {0.0, 0.0}, lw[2] = {0.0, 0.0}, lv = 0.0;
 #pragma omp for schedule(dynamic) nowait
         for (int j = o.ju0; j <= o.ju1; ++j) {
-            gather_plane(o, o.u1, o.nyu, o.ju0, j, a.data());
-            four_to_phys(o, a.data(), true, w);
-            for (size_t e = 0; e < psz; ++e) lu = std::max(lu, std::fabs(a[e]));
-            gather_plane(o, o.u3, o.nyu, o.ju0, j, a.data());
-            four_to_phys(o, a.data(), true, w);
-            for (size_t e = 0; e < psz; ++e) lw = std::max(lw, std::fabs(a[e]));
+            const bool mid = o.u_mid(j);
+            const PlaneGeom g = o.geom(mid);
+            const size_t gsz = (size_t)g.rowlen * g.ngal2;
+            gather_plane(o, g, o.u1, o.nyu, o.ju0, j, a.data());
+            four_to_phys(g, a.data(), true, w);
+            for (size_t e = 0; e < gsz; ++e) lu[mid] = std::max(lu[mid], std::fabs(a[e]));
+            gather_plane(o, g, o.u3, o.nyu, o.ju0, j, a.data());
+            four_to_phys(g, a.data(), true, w);
+            for (size_t e = 0; e < gsz; ++e) lw[mid] = std::max(lw[mid], std::fabs(a[e]));
         }
 #pragma omp for schedule(dynamic) nowait
         for (int j = o.jv0 + 1; j <= o.jv1 - 1; ++j) {
-            gather_plane(o, o.u2, o.nyv, o.jv0, j, a.data());
-            four_to_phys(o, a.data(), true, w);
-            for (int k = 0; k < o.ngal2; ++k)
-                for (int i = 0; i < o.ngal1; ++i)
-                    lv = std::max(lv, std::fabs(a[(size_t)k * o.rowlen + i]) * o.DTHV(j));
+            const PlaneGeom g = o.geom(o.v_mid(j));
+            gather_plane(o, g, o.u2, o.nyv, o.jv0, j, a.data());
+            four_to_phys(g, a.data(), true, w);
+            for (int k = 0; k < g.ngal2; ++k)
+                for (int i = 0; i < g.ngal1; ++i)
+                    lv = std::max(lv, std::fabs(a[(size_t)k * g.rowlen + i]) * o.DTHV(j));
         }
 #pragma omp critical
         {
-            um = std::max(um, lu);
-            wm = std::max(wm, lw);
+            for (int b = 0; b < 2; ++b) {
+                um[b] = std::max(um[b], lu[b]);
+                wm[b] = std::max(wm[b], lw[b]);
+            }
             vm = std::max(vm, lv);
         }
     }
-    terms[0] = 1.0 / (o.alp * (o.n1 / 2) * um);
-    terms[1] = 1.0 / (o.bet * (o.n2 / 2) * wm);
+    terms[0] = 1.0 / (o.alp * (o.n1 / 2) * um[0]);
+    terms[1] = 1.0 / (o.bet * (o.n2 / 2) * wm[0]);
+    if (o.mb) {
+        terms[0] = std::min(terms[0], 1.0 / (o.alp * (o.n1m / 2) * um[1]));
+        terms[1] = std::min(terms[1], 1.0 / (o.bet * (o.n2m / 2) * wm[1]));
+    }
     terms[2] = 1.0 / vm;
 }
 
@@ -993,6 +1116,37 @@ void* orc_create(const cfd_config* c, const cfd_ib_list* ibu, const cfd_ib_list*
         o->gwt = (o->YU(o->ju1) - o->YV(o->jv1)) / (o->YV(o->jv1) - o->YU(o->ju1 - 1));
         o->gwib = (o->YU(o->ju0) - o->YU(o->ju0 + 1)) / (o->YV(o->jv0) - o->YU(o->ju0 + 1));
         o->gwit = (o->YU(o->ju1) - o->YU(o->ju1 - 1)) / (o->YV(o->jv1) - o->YU(o->ju1 - 1));
+        // column segments: the channel (long columns) and, with three bands, the bottom and
+        // top segments of the short columns (jlim, start.f90:1538-1557) with their
+        // gridweighting / gridweighting_interp (start.f90:494-508)
+        o->segL = Seg{o->ju0, o->ju1, o->jv0, o->jv1, o->jp0, o->jp1, o->gwb, o->gwt, o->gwib, o->gwit};
+        if (c->band_vface > 0) {
+            const int jb = c->band_vface, m = o->ny - 2 - jb;  // N(3,1), N(3,2) = N(4,2)
+            if (jb + 2 >= m || jb + 1 <= o->jv0 + 1)
+                throw std::runtime_error("band_vface leaves no middle band of two planes");
+            if (c->ngal1_mid > c->ngal1 || c->ngal2_mid > c->ngal2 || c->ngal1_mid < 6 || c->ngal2_mid < 6)
+                throw std::runtime_error("middle-band sizes must lie between 6 and the wall bands' sizes");
+            o->mb = 1;
+            o->jb = jb;
+            o->ngal1m = c->ngal1_mid; o->ngal2m = c->ngal2_mid;
+            o->n1m = 2 * (o->ngal1m / 3); o->n2m = 2 * (o->ngal2m / 3);
+            const double gw1t = (o->YU(jb + 2) - o->YV(jb + 1)) / (o->YV(jb + 1) - o->YU(jb + 1));
+            const double gwi1t = (o->YU(jb + 2) - o->YU(jb + 1)) / (o->YV(jb + 1) - o->YU(jb + 1));
+            const double gw3b = -(o->YV(m) - o->YU(m)) / (o->YV(m) - o->YU(m + 1));
+            const double gwi3b = (o->YU(m) - o->YU(m + 1)) / (o->YV(m) - o->YU(m + 1));
+            o->segS[0] = Seg{o->ju0, jb + 2, o->jv0, jb + 1, o->ju0 + 1, jb + 1, o->gwb, gw1t, o->gwib, gwi1t};
+            o->segS[1] = Seg{m, o->ju1, m, o->jv1, m + 1, o->jp1, gw3b, o->gwt, gwi3b, o->gwit};
+            o->islong.assign(o->ncol, 0);
+            for (int col = 0; col < o->ncol; ++col) {
+                const int i = col % o->nkx, q = col / o->nkx;
+                o->islong[col] = i <= o->n1m / 2 && (q < o->n2m / 2 || q >= o->n2 - o->n2m / 2);
+            }
+            for (const cfd_ib_list* l : {ibu, ibv})
+                if (l)
+                    for (int s = 0; s < 2; ++s)
+                        if (l->jhi[s] >= l->jlo[s] && !(l->jhi[s] <= jb || l->jlo[s] > m))
+                            throw std::runtime_error("immersed-boundary planes must lie in the wall bands");
+        }
         o->kx.resize(o->nkx);
         for (int i = 0; i < o->nkx; ++i) o->kx[i] = o->alp * i;
         o->kz.resize(o->n2);
@@ -1012,6 +1166,10 @@ void* orc_create(const cfd_config* c, const cfd_ib_list* ibu, const cfd_ib_list*
         for (auto* f : {&o->p, &o->psi, &o->div}) f->assign(sp, 0.0);
         o->px.init(o->ngal1);
         o->pz.init(o->ngal2);
+        if (o->mb) {
+            o->pxm.init(o->ngal1m);
+            o->pzm.init(o->ngal2m);
+        }
         return o;
     } catch (std::exception& e) {
         g_err = e.what();
@@ -1075,6 +1233,7 @@ int orc_step(void* h, int nsteps) {
     return 0;
 }
 int orc_stats_configure(void* h, int jband, int dnx, int dnz, int spectra) {
+    if (((Oracle*)h)->mb) return CFD_ERR_ARG;  // statistics of one band only
     Oracle& o = *(Oracle*)h;
     if (jband >= o.jv0 && (dnx <= 0 || dnz <= 0 || o.ngal1 % dnx || o.ngal2 % dnz)) return 1;
     stats_configure(o, jband, dnx, dnz, spectra);
@@ -1121,7 +1280,11 @@ int orc_set_dt(void* h, double dt) {
     ((Oracle*)h)->dt = dt;
     return 0;
 }
-int orc_set_quirk(void* h, int lastplane) { ((Oracle*)h)->quirk_lastplane = lastplane; return 0; }
+int orc_set_quirk(void* h, int lastplane) {
+    if (((Oracle*)h)->mb && lastplane) return CFD_ERR_ARG;  // a single slab has one band
+    ((Oracle*)h)->quirk_lastplane = lastplane;
+    return 0;
+}
 void orc_get_scalars(void* h, double* mpgx, double* qx, double* dgx) {
     Oracle& o = *(Oracle*)h;
     *mpgx = o.mpgx; *qx = o.Qx; *dgx = o.dgx;

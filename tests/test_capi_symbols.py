@@ -34,5 +34,7 @@ def test_version_string():
 
 def test_struct_layout_matches_header():
     # 4 int32 + 6 double + 2 int32 + 6 pointers on LP64
-    assert ctypes.sizeof(capi.CfdConfig) == 16 + 48 + 8 + 48
+    # 4 ints, 6 doubles, 2 ints, 6 pointers, 3 ints (the band fields) + 4 bytes of tail padding
+    assert ctypes.sizeof(capi.CfdConfig) == 16 + 48 + 8 + 48 + 12 + 4
+    assert capi.CfdConfig.band_vface.offset == 16 + 48 + 8 + 48 + 8
     assert ctypes.sizeof(capi.CfdIBList) == 8 + 8 + 8 + 16
