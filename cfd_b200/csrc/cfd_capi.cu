@@ -18,6 +18,7 @@
 
 #include "../../include/cfd_b200.h"
 #include "channel_kernels.cuh"
+#include "bands_kernels.cuh"
 #include "stats_kernels.cuh"
 
 using namespace cfd;
@@ -103,6 +104,15 @@ struct cfd_ctx {
     int RW2 = 0, NT2 = 0;
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
     bool XALT = false, ZALT = false;  // transposed two-step splits (x-line; nonlinear z kernels)
+    // three bands: the launch dimensions of the nonlinear pass over the bottom wall band,
+    // the middle band and the top wall band; the middle band's transforms
+    bool mb = false;
+    Dims dB{}, dM{}, dT{};
+    FFTDesc fxm{};
+    double2 *twxm_d = nullptr, *twzm_d = nullptr;
+    float2 *twxm_f = nullptr, *twzm_f = nullptr;
+    int NTZm = 0;
+    size_t SMZm = 0;
     int NTZN = 0;           // threads and shared memory of the nonlinear pass's z kernels
     size_t SMZN = 0;
     int RW4 = 0, NT4 = 0;   // line-pair x-line kernel (k_xline4, FP32): rows per CTA (0 = not used), threads
@@ -387,6 +397,17 @@ int set_smem_attrs(cfd_ctx* c) {
                     e = cudaFuncSetAttribute(k_xline4<TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM4);
         });
     }
+    if (c->mb && c->LZ2 >= 0) {
+        bool ok = true;
+        const int smz = (int)std::max(c->SMZ2, c->SMZm);
+        TWO_SWITCH(c->dM.ngal2, ok, {
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k_zinv2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz);
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k_zfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smz);
+        });
+        FFT_SWITCH(c->dM.ngal1, {
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xline<T2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sx);
+        });
+    }
     CK(e);
     return CFD_OK;
 }
@@ -412,8 +433,65 @@ RKCoef coef(cfd_ctx* c, int krk) {
 }
 
 // nonlinear passes 1-3 (FOU3D.f90:79-155)
+// the nonlinear passes of a three-band channel: each kernel launched over the bottom wall
+// band, the middle band and the top wall band with that band's sizes and transforms
+template <typename T2>
+int nl_transforms_mb(cfd_ctx* c) {
+    const size_t e = sizeof(T2);
+    const Dims* bands[3] = {&c->dB, &c->dM, &c->dT};
+    const int CH2 = 1 << c->LZ2;
+    auto twx_b = [&](bool mid) -> const T2* {
+        if constexpr (std::is_same<T2, float2>::value) return mid ? c->twxm_f : c->twx_f;
+        else return mid ? c->twxm_d : c->twx_d;
+    };
+    auto twz_b = [&](bool mid) -> const T2* {
+        if constexpr (std::is_same<T2, float2>::value) return mid ? c->twzm_f : c->twz_f;
+        else return mid ? c->twzm_d : c->twz_d;
+    };
+    prof_mark(c);
+    for (const Dims* bp : bands) {
+        const Dims& d = *bp;
+        const bool mid = bp == &c->dM;
+        dim3 gz2((std::max(d.nsu, d.nsv) * d.nkx + CH2 - 1) / CH2, 3, 2);
+        bool ok = true;
+        TWO_SWITCH(d.ngal2, ok, {
+            k_zinv2<T2, TN1, TN2><<<gz2, mid ? c->NTZm : c->NTZ2, mid ? c->SMZm : c->SMZ2, c->stream>>>(
+                d, c->g, c->u1, c->u2, c->u3, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], twz_b(mid), c->LZ2);
+        });
+        if (!ok) return fail(c, CFD_ERR_SIZE, "no two-step split for Ngal2=%d", d.ngal2);
+    }
+    LK("k_zinv2");
+    prof_mark(c);
+    for (const Dims* bp : bands) {
+        const Dims& d = *bp;
+        const bool mid = bp == &c->dM;
+        dim3 gx(d.ngal2 / c->RWx, d.nsu + d.nsv);
+        FFT_SWITCH(d.ngal1, {
+            k_xline<T2, NF><<<gx, 256, (size_t)(2 * (2 * c->RWx) * d.ngal1 + d.ngal1) * e, c->stream>>>(
+                d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], mid ? c->fxm : c->fx, twx_b(mid), c->RWx,
+                ilog2(2 * c->RWx));
+        });
+    }
+    LK("k_xline");
+    prof_mark(c);
+    for (const Dims* bp : bands) {
+        const Dims& d = *bp;
+        const bool mid = bp == &c->dM;
+        dim3 gf2((std::max(d.nsu, d.nsv) * d.nkx + CH2 - 1) / CH2, 4, 2);
+        bool ok = true;
+        TWO_SWITCH(d.ngal2, ok, {
+            k_zfwd2<T2, TN1, TN2><<<gf2, mid ? c->NTZm : c->NTZ2, mid ? c->SMZm : c->SMZ2, c->stream>>>(
+                d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
+                (T2*)c->S[3], twz_b(mid), c->LZ2);
+        });
+    }
+    LK("k_zfwd2");
+    return CFD_OK;
+}
+
 template <typename T2>
 int nl_transforms(cfd_ctx* c) {
+    if (c->mb) return nl_transforms_mb<T2>(c);
     const Dims& d = c->d;
     const int CH = c->CHz;
     const size_t e = sizeof(T2);
@@ -517,6 +595,14 @@ int rhs_kernel(cfd_ctx* c, int krk) {
     const Dims& d = c->d;
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
+    if (c->mb) {
+        k_mb_rhs<T2, MODE><<<gb, 256, 0, c->stream>>>(d, c->g, coef(c, krk), c->scal, c->u1, c->u2, c->u3, c->p,
+                                                      (T2*)c->Nu1, (T2*)c->Nu2, (T2*)c->Nu3, c->du1, c->du2, c->du3,
+                                                      (const T2*)c->S[0], (const T2*)c->S[1], (const T2*)c->S[2],
+                                                      (const T2*)c->S[3]);
+        LK("k_mb_rhs");
+        return CFD_OK;
+    }
     gb.y = c->nch;
     k_rhs<T2, MODE><<<gb, 256, 0, c->stream>>>(d, c->g, coef(c, krk), c->scal, c->u1, c->u2, c->u3, c->p, (T2*)c->Nu1,
                                                (T2*)c->Nu2, (T2*)c->Nu3, c->du1, c->du2, c->du3, (const T2*)c->S[0],
@@ -695,6 +781,12 @@ int solve_kernel(cfd_ctx* c, int krk) {
     }
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
+    if (c->mb) {
+        k_mb_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs,
+                                                 c->cs_v);
+        LK("k_mb_solve_uvw");
+        return CFD_OK;
+    }
     gb.y = 2;
     k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v);
     LK("k_solve_uvw");
@@ -715,6 +807,12 @@ int solvep_kernel(cfd_ctx* c, int krk, bool with_div) {
     const double dtirk = (1.0 / c->dt) / (kRKa[krk - 1] + kRKb[krk - 1]);
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
+    if (c->mb) {
+        k_mb_solve_p<false><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi,
+                                                       with_div ? c->div : nullptr, c->cs, c->mean_diag, 0.0);
+        LK("k_mb_solve_p");
+        return CFD_OK;
+    }
     k_solve_p<false><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi,
                                                 with_div ? c->div : nullptr, c->cs, c->mean_diag, 0.0);
     LK("k_solve_p");
@@ -726,6 +824,11 @@ int vcorr_kernel(cfd_ctx* c, int krk, bool with_div) {
     const double dtrk = c->dt * (kRKa[krk - 1] + kRKb[krk - 1]);
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
+    if (c->mb) {
+        k_mb_vcorr<<<gb, 256, 0, c->stream>>>(d, c->g, dtrk, c->u1, c->u2, c->u3, c->psi, with_div ? c->div : nullptr);
+        LK("k_mb_vcorr");
+        return CFD_OK;
+    }
     if (with_div) {
         k_vcorr<<<gb, 256, 0, c->stream>>>(d, c->g, dtrk, c->u1, c->u2, c->u3, c->psi, c->div);
         LK("k_vcorr");
@@ -752,6 +855,12 @@ int substep(cfd_ctx* c, int krk) {
     const double dtrk = c->dt * (kRKa[krk - 1] + kRKb[krk - 1]);
     dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
+    if (c->mb) {
+        k_mb_solve_p<true><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, nullptr,
+                                                      c->cs, c->mean_diag, dtrk);
+        LK("k_mb_solve_p_vcorr");
+        return CFD_OK;
+    }
     k_solve_p<true><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, nullptr, c->cs,
                                                c->mean_diag, dtrk);
     LK("k_solve_p_vcorr");
@@ -913,9 +1022,38 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     d.jp0 = -cfg->dsty + 1; d.jp1 = cfg->ny + cfg->dsty - 1;
     d.nyu = d.ju1 - d.ju0 + 1; d.nyv = d.jv1 - d.jv0 + 1; d.nyp = d.jp1 - d.jp0 + 1;
     d.nslot = d.nyu + d.nyv;
+    // stored layout and slot range of a launch over the whole channel (one band)
+    d.pstride = d.ncol; d.kstride = d.nkx; d.qshift = 0; d.hstride = (long long)d.ngal2 * d.nkx;
+    d.su0 = 0; d.nsu = d.nyu; d.sv0 = 0; d.nsv = d.nyv;
+    d.mb = 0; d.jb = 0; d.n1m = d.n1; d.n2m = d.n2;
     c->precision = cfg->precision;
-    if (cfg->band_vface > 0 && (cfg->ngal1_mid != cfg->ngal1 || cfg->ngal2_mid != cfg->ngal2))
-        return fail(c, CFD_ERR_SIZE, "a middle band of another x/z size than the wall bands");
+    if (cfg->band_vface > 0 && (cfg->ngal1_mid != cfg->ngal1 || cfg->ngal2_mid != cfg->ngal2)) {
+        // three bands (start.f90:76-111): middle band ngal1_mid x ngal2_mid between the
+        // v faces band_vface+1 .. ny-2-band_vface
+        const int jb = cfg->band_vface, m = cfg->ny - 2 - jb;
+        FFTDesc fxm, fzm;
+        if (jb + 2 >= m || jb + 1 <= d.jv0 + 1)
+            return fail(c, CFD_ERR_SIZE, "band_vface=%d leaves no middle band of two planes", jb);
+        if (!fft_plan(cfg->ngal1_mid, fxm) || !fft_plan(cfg->ngal2_mid, fzm) || cfg->ngal1_mid < 6 ||
+            cfg->ngal2_mid < 6 || (cfg->ngal1_mid & 1) || (cfg->ngal2_mid & 1) || cfg->ngal1_mid > cfg->ngal1 ||
+            cfg->ngal2_mid > cfg->ngal2)
+            return fail(c, CFD_ERR_SIZE, "middle band %d x %d: even 2^a*3^b >= 6, at most the wall bands' size",
+                        cfg->ngal1_mid, cfg->ngal2_mid);
+        c->mb = true;
+        c->fxm = fxm;
+        d.mb = 1; d.jb = jb;
+        d.n1m = 2 * (cfg->ngal1_mid / 3); d.n2m = 2 * (cfg->ngal2_mid / 3);
+        // launches of the nonlinear pass: the bottom wall band (u centres up to jb+1, v faces
+        // up to jb), the middle band, the top wall band (planelim, start.f90:1778-1800)
+        c->dB = d; c->dM = d; c->dT = d;
+        c->dB.nsu = jb + 2 - d.ju0; c->dB.nsv = jb + 1 - d.jv0;
+        c->dT.su0 = m + 1 - d.ju0; c->dT.nsu = d.ju1 - m; c->dT.sv0 = m + 1 - d.jv0; c->dT.nsv = d.jv1 - m;
+        Dims& dm = c->dM;
+        dm.su0 = jb + 2 - d.ju0; dm.nsu = m - jb - 1; dm.sv0 = jb + 1 - d.jv0; dm.nsv = m - jb;
+        dm.ngal1 = cfg->ngal1_mid; dm.ngal2 = cfg->ngal2_mid; dm.n1 = d.n1m; dm.n2 = d.n2m;
+        dm.nkx = dm.n1 / 2 + 1; dm.ncol = dm.nkx * dm.n2;
+        dm.qshift = d.n2 - d.n2m;
+    }
     c->re = cfg->re; c->alp = cfg->alp; c->bet = cfg->bet; c->dt = cfg->dt; c->qxt = cfg->qxt;
     c->mpgx0 = cfg->mpgx; c->ctpress = cfg->flag_ctpress;
 
@@ -967,6 +1105,11 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     g.gwt = (YU(d.ju1) - YV(d.jv1)) / (YV(d.jv1) - YU(d.ju1 - 1));
     g.gwib = (YU(d.ju0) - YU(d.ju0 + 1)) / (YV(d.jv0) - YU(d.ju0 + 1));
     g.gwit = (YU(d.ju1) - YU(d.ju1 - 1)) / (YV(d.jv1) - YU(d.ju1 - 1));
+    if (c->mb) {  // gridweighting(1,2) and gridweighting(3,1) (start.f90:496, 499)
+        const int jb = d.jb, m = d.ny - 2 - d.jb;
+        g.gw1t = (YU(jb + 2) - YV(jb + 1)) / (YV(jb + 1) - YU(jb + 1));
+        g.gw3b = -(YV(m) - YU(m)) / (YV(m) - YU(m + 1));
+    }
     // mean-mode Poisson row (tridLU_3D_IB.f90:468-474): 1/(yu(2)-yu(1))^2
     if (d.ju0 > 1 || d.ju1 < 2) return fail(c, CFD_ERR_SIZE, "grid too small");
     c->mean_diag = 1.0 / ((YU(2) - YU(1)) * (YU(2) - YU(1)));
@@ -1093,10 +1236,27 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
             if (!c->RWIX2 || !c->RWFX2) c->RWIX2 = c->RWFX2 = 0;
         }
     }
+    if (c->mb) {
+        // three bands: the per-slot interpolating z pass, the Stockham x-line kernel and the
+        // two-step forward z pass, launched once per band; thread-per-column solves
+        c->RW2 = 0; c->XL3 = false; c->RW4 = 0; c->XALT = c->ZALT = false; c->SWM = 0;
+        bool ok = true;
+        int n1s = 0, n2s = 0;
+        TWO_SWITCH(cfg->ngal2_mid, ok, { n1s = TN1; n2s = TN2; });
+        if (c->LZ2 < 0 || !ok)
+            return fail(c, CFD_ERR_SIZE, "three bands need two-step z lengths (64, 96, 128, 192, 384, 768) in both");
+        c->NTZm = (1 << c->LZ2) * std::max(n1s, n2s);
+        c->SMZm = ((size_t)(1 << c->LZ2) * ((n1s * (n2s + 1)) | 1) + (size_t)n1s * n2s) * esz;
+        while (c->RWx > 1 && (cfg->ngal2_mid % c->RWx)) c->RWx /= 2;
+    }
     int s = mixed ? set_smem_attrs<float2>(c) : set_smem_attrs<double2>(c);
     if (s != CFD_OK) return s;
     if ((s = fill_tw(c, d.ngal1, &c->twx_d, &c->twx_f)) != CFD_OK) return s;
     if ((s = fill_tw(c, d.ngal2, &c->twz_d, &c->twz_f)) != CFD_OK) return s;
+    if (c->mb) {
+        if ((s = fill_tw(c, cfg->ngal1_mid, &c->twxm_d, &c->twxm_f)) != CFD_OK) return s;
+        if ((s = fill_tw(c, cfg->ngal2_mid, &c->twzm_d, &c->twzm_f)) != CFD_OK) return s;
+    }
 
     // fields
     const size_t nc = d.ncol;
@@ -1112,6 +1272,9 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     for (int k = 0; k < 4; ++k) {
         if (mixed) { AL(c->H[k], float2, hsz); AL(c->S[k], float2, (size_t)d.nslot * nc); }
         else { AL(c->H[k], double2, hsz); AL(c->S[k], double2, (size_t)d.nslot * nc); }
+        // three bands: the products of a short column on a middle-band plane are never
+        // written and must read as zero
+        if (c->mb) CK(cudaMemset(c->S[k], 0, (size_t)d.nslot * nc * esz));
     }
     if (c->RW2) {
         const size_t hxs = (size_t)(2 * nyu + nyv) * d.ngal2 * d.nkx;
@@ -1557,7 +1720,10 @@ int cfd_divergence_max(cfd_ctx* c, double* errmax) {
     const Dims& d = c->d;
     // recompute div from the current state (divergence, littleharsh.f90:209-244)
     prof_mark(c);
-    k_divergence<<<(d.ncol + 255) / 256, 256, 0, c->stream>>>(d, c->g, c->u1, c->u2, c->u3, c->div);
+    if (c->mb)
+        k_mb_divergence<<<(d.ncol + 255) / 256, 256, 0, c->stream>>>(d, c->g, c->u1, c->u2, c->u3, c->div);
+    else
+        k_divergence<<<(d.ncol + 255) / 256, 256, 0, c->stream>>>(d, c->g, c->u1, c->u2, c->u3, c->div);
     LK("k_divergence");
     prof_mark(c);
     k_absmax<<<c->npart, 256, 0, c->stream>>>(c->div, (size_t)d.ncol * d.nyp, c->part);
@@ -1577,6 +1743,7 @@ int cfd_divergence_max(cfd_ctx* c, double* errmax) {
 }
 
 int cfd_stats_configure(cfd_ctx* c, const cfd_stats_config* sc) {
+    if (c && c->mb) return fail(c, CFD_ERR_ARG, "statistics of a three-band channel are not supported");
     if (!c || !sc) return fail(c, CFD_ERR_ARG, "bad arguments");
     const Dims& d = c->d;
     auto& st = c->st;
@@ -1874,6 +2041,7 @@ int cfd_set_dt(cfd_ctx* c, double dt) {
 int cfd_set_lastplane(cfd_ctx* c, int32_t on) {
     if (!c) return CFD_ERR_ARG;
     if (on != 0 && on != 1) return fail(c, CFD_ERR_ARG, "lastplane must be 0 or 1");
+    if (on && c->mb) return fail(c, CFD_ERR_ARG, "the single-slab term needs one band");
     CK(cudaStreamSynchronize(c->stream));
     c->lastplane = on;
     c->epoch++;
@@ -1882,6 +2050,7 @@ int cfd_set_lastplane(cfd_ctx* c, int32_t on) {
 }
 
 int cfd_cfl(cfd_ctx* c, double* dtc, double* terms) {
+    if (c && c->mb) return fail(c, CFD_ERR_ARG, "cfd_cfl of a three-band channel is not supported");
     if (!c || !dtc) return fail(c, CFD_ERR_ARG, "bad arguments");
     const Dims& d = c->d;
     int s = stats_scratch(c);

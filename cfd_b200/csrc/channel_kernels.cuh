@@ -29,7 +29,23 @@ struct Dims {
     int ju0, ju1, jv0, jv1, jp0, jp1, nyu, nyv, nyp;
     int nslot;  // nyu + nyv
     int ny;     // faces from y=-1 to y=1 (input.in ny)
+    // Stored layout of the spectral fields (the wall bands' column list) as seen by a launch
+    // over one band (the transform kernels of the nonlinear pass): columns per plane, per kz
+    // row, and the stored kz index q + qshift of the negative modes q >= n2/2; the elements
+    // per slot of the half-physical buffers; the u-slots su0..su0+nsu-1 and v-slots
+    // sv0..sv0+nsv-1 (0-based within their grid) of the launch.  With one band: ncol, nkx,
+    // 0, ngal2*nkx, and every slot.
+    int pstride, kstride, qshift;
+    long long hstride;
+    int su0, nsu, sv0, nsv;
+    // three bands: 1, the last v face of the bottom band (N(3,1)) and the middle band's N1, N2
+    int mb, jb, n1m, n2m;
 };
+
+// stored column of spectral entry (kx i, kz q) in a launch over one band
+__device__ __forceinline__ size_t scol(const Dims& d, int i, int q) {
+    return (size_t)(q < d.n2 / 2 ? q : q + d.qshift) * d.kstride + i;
+}
 
 // Grid and wavenumber tables on the device (array index = j - j0 of the grid).
 struct Geo {
@@ -49,6 +65,7 @@ struct Geo {
     const double* ufa;
     const double* ufb;
     double gwb, gwt, gwib, gwit;
+    double gw1t, gw3b;  // three bands: gridweighting(1,2) and gridweighting(3,1)
 };
 
 __device__ __forceinline__ int row_of(const Dims& d, int q) { return q < d.n2 / 2 ? q : q + (d.ngal2 - d.n2); }
@@ -188,7 +205,9 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
     T2* buf0 = reinterpret_cast<T2*>(smem_raw);
     T2* buf1 = buf0 + (size_t)n * B;
     T2* tw = buf1 + (size_t)n * B;
-    const int slot = blockIdx.y;
+    // the launch's u-slots, then its v-slots
+    const int by = blockIdx.y;
+    const int slot = by < d.nsu ? d.su0 + by : d.nyu + d.sv0 + (by - d.nsu);
     const int z0 = blockIdx.x * RW;
     const bool uplane = slot < d.nyu;
     const int h = d.n1 / 2;  // retained kx modes 0..h
@@ -201,7 +220,7 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
     }
     // Hermitian lines from the kx spectra, k fastest across threads (coalesced rows);
     // the rft inverse ignores Im of the kx = 0 entry (rft_buff.f:78-80)
-    const size_t pbase = (size_t)slot * d.ngal2 * d.nkx;
+    const size_t pbase = (size_t)slot * d.hstride;
     const int nk = d.nkx;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int b = warp; b < B; b += nwarp) {
@@ -850,7 +869,7 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     const int grp = blockIdx.z, f = blockIdx.y;
-    const int nsl = grp ? d.nyv : d.nyu;
+    const int nsl = grp ? d.nsv : d.nsu;
     const int nlines = nsl * d.nkx;
     const int line0 = blockIdx.x << lb;
     if (line0 >= nlines) return;
@@ -861,8 +880,8 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
     const int b = threadIdx.x & ((1 << lb) - 1);
     const bool live = line0 + b < nlines;
     const int line = live ? line0 + b : nlines - 1;
-    const int sl = line / d.nkx, i = line - sl * d.nkx;
-    const size_t nc = d.ncol;
+    const int sl = (line / d.nkx) + (grp ? d.sv0 : d.su0), i = line - (line / d.nkx) * d.nkx;
+    const size_t nc = d.pstride;
     const double2* pa;
     const double2* pb;
     double ca = 1.0, cb = 0.0;
@@ -875,7 +894,7 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
             pa = u2 + nc;
             ca = (1.0 - g.gwib) * g.vca[1];
             cb = g.gwib + (1.0 - g.gwib) * g.vcb[1];
-        } else if (sl == nsl - 1) {
+        } else if (sl == d.nyu - 1) {
             pa = u2 + (size_t)(sl - 1) * nc;
             ca = g.gwit + (1.0 - g.gwit) * g.vca[sl - 1];
             cb = (1.0 - g.gwit) * g.vcb[sl - 1];
@@ -897,7 +916,7 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
     pa += i;
     pb = two ? pa - nc : pa;
     const int r = threadIdx.x >> lb;
-    T2* H = (f == 0 ? H0 : (f == 1 ? H1 : H2)) + (size_t)(grp ? d.nyu + sl : sl) * N * d.nkx + i;
+    T2* H = (f == 0 ? H0 : (f == 1 ? H1 : H2)) + (size_t)(grp ? d.nyu + sl : sl) * d.hstride + i;
     __syncthreads();
     auto qof = [&](int e) { return zrow_q<N, TN2>(e, r); };
     auto store = [&](int z, int, T2 v) {
@@ -908,8 +927,8 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
             const int q = qof(e);
             double2 va = dc(0.0, 0.0), vb = dc(0.0, 0.0);
             if (q >= 0) {
-                va = pa[(size_t)q * d.nkx];
-                vb = pb[(size_t)q * d.nkx];
+                va = pa[scol(d, 0, q)];
+                vb = pb[scol(d, 0, q)];
             }
             return to_t2<T2>(dc(ca * va.x + cb * vb.x, ca * va.y + cb * vb.y));
         };
@@ -917,7 +936,7 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
     } else {
         auto load = [&](int e, int) -> T2 {
             const int q = qof(e);
-            return q >= 0 ? to_t2<T2>(pa[(size_t)q * d.nkx]) : cx<T2>((R)0, (R)0);
+            return q >= 0 ? to_t2<T2>(pa[scol(d, 0, q)]) : cx<T2>((R)0, (R)0);
         };
         two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
     }
@@ -969,7 +988,7 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
     constexpr int N = TN1 * TN2;
     const int grp = blockIdx.z, f = blockIdx.y;
     if (grp == 1 && f >= 2) return;
-    const int nsl = grp ? d.nyv : d.nyu;
+    const int nsl = grp ? d.nsv : d.nsu;
     const int nlines = nsl * d.nkx;
     const int line0 = blockIdx.x << lb;
     if (line0 >= nlines) return;
@@ -981,16 +1000,16 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
     const bool live = line0 + b < nlines;
     const int line = live ? line0 + b : nlines - 1;
     const int sl = line / d.nkx, i = line - sl * d.nkx;
-    const int slot = grp ? d.nyu + sl : sl;
-    const T2* H = (f == 0 ? H0 : (f == 1 ? H1 : (f == 2 ? H2 : H3))) + (size_t)slot * N * d.nkx + i;
-    T2* S = (f == 0 ? S0 : (f == 1 ? S1 : (f == 2 ? S2 : S3))) + (size_t)slot * d.ncol + i;
+    const int slot = grp ? d.nyu + d.sv0 + sl : d.su0 + sl;
+    const T2* H = (f == 0 ? H0 : (f == 1 ? H1 : (f == 2 ? H2 : H3))) + (size_t)slot * d.hstride + i;
+    T2* S = (f == 0 ? S0 : (f == 1 ? S1 : (f == 2 ? S2 : S3))) + (size_t)slot * d.pstride + i;
     const int r = threadIdx.x >> lb;
     const R sc = (R)1 / (R)N;
     __syncthreads();
     auto load = [&](int z, int) -> T2 { return H[(size_t)z * d.nkx]; };
     auto store = [&](int e, int, T2 v) {
         const int q = zrow_q<N, TN1>(e, r);
-        if (q >= 0 && live) S[(size_t)q * d.nkx] = cscale(v, sc);
+        if (q >= 0 && live) S[scol(d, 0, q)] = cscale(v, sc);
     };
     two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
 }
