@@ -75,6 +75,9 @@ def write_record_out(directory: str, tag: str, state: dict, setup, t: float = 0.
     """Write u1_<tag>.dat, u2_<tag>.dat, u3_<tag>.dat, p_<tag>.dat; state holds the spectral
     fields as (columns, planes) complex arrays (the reference's f(j,column) layout)."""
     cfg, g = setup.cfg, setup.grid
+    from .bands import multiband
+    if multiband(cfg):
+        raise ValueError("record_out files of a three-band channel (planes of two sizes) are not written")
     if N is None:
         N = band_array(setup, nband)
     nband = N.shape[1] - 2
