@@ -738,6 +738,47 @@ int ib_all(cfd_ctx* c) {
     return ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys, 0, c->d.nyu);
 }
 
+// The IB round trips and the Helmholtz solves of one substep as two graph branches: the
+// v grid's round trip and v solve on the side stream while the u/w grid's round trip and
+// u/w solve run on the context stream (the thread-per-column sweep; its two systems are
+// independent).  Otherwise the round trips, then one solve launch.
+int solve_kernel(cfd_ctx* c, int krk);
+
+template <typename T2>
+int ib_solve_all(cfd_ctx* c, int krk) {
+    const bool par = c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling && !c->SWM && !c->mb;
+    if (!par) {
+        int s = ib_all<T2>(c);
+        if (s != CFD_OK) return s;
+        c->hx_valid = false;  // the solve changes u, v, w
+        return solve_kernel(c, krk);
+    }
+    const Dims& d = c->d;
+    const double beta = kRKb[krk - 1] * c->dt / c->re;
+    const dim3 gb((d.ncol + 255) / 256, 1);
+    CK(cudaEventRecord(c->ev_fork, c->stream));
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    cudaStream_t main = c->stream;
+    c->stream = c->side;
+    int s = ib_grid<T2>(c, c->ibv, d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v, 2 * d.nyu, 0);
+    if (s == CFD_OK) {
+        k_solve_uvw<<<gb, 256, 0, c->side>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs,
+                                             c->cs_v, 1);
+        s = launched(c, "k_solve_uvw");
+    }
+    c->stream = main;
+    const cudaError_t ej = cudaEventRecord(c->ev_join, c->side);  // join even after a failure
+    if (ej == cudaSuccess) cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    if (s != CFD_OK) return s;
+    CK(ej);
+    s = ib_grid<T2>(c, c->ibu, d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys, 0, d.nyu);
+    if (s != CFD_OK) return s;
+    c->hx_valid = false;
+    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v, 0);
+    LK("k_solve_uvw");
+    return CFD_OK;
+}
+
 size_t solve_w_smem(const Dims& d, int swc) {
     return (size_t)2 * swc * d.nyu * sizeof(double2) + (size_t)3 * d.nyu * sizeof(double);
 }
@@ -788,7 +829,8 @@ int solve_kernel(cfd_ctx* c, int krk) {
         return CFD_OK;
     }
     gb.y = 2;
-    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v);
+    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v,
+                                           0);
     LK("k_solve_uvw");
     return CFD_OK;
 }
@@ -845,9 +887,7 @@ int substep(cfd_ctx* c, int krk) {
     int s;
     if ((s = nl_transforms<T2>(c)) != CFD_OK) return s;
     if ((s = rhs_kernel<T2, 7>(c, krk)) != CFD_OK) return s;
-    if ((s = ib_all<T2>(c)) != CFD_OK) return s;
-    c->hx_valid = false;  // the solve changes u, v, w
-    if ((s = solve_kernel(c, krk)) != CFD_OK) return s;
+    if ((s = ib_solve_all<T2>(c, krk)) != CFD_OK) return s;
     if (c->ctpress == 0 && (s = meanflow_kernel(c, krk)) != CFD_OK) return s;
     // solveP + v_corr in one column sweep (psi is not stored on this path)
     const Dims& d = c->d;

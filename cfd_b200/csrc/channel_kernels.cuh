@@ -1650,13 +1650,14 @@ __global__ void __launch_bounds__(256) k_solve_uvw(Dims d, Geo g, double beta, d
                                                    double2* __restrict__ u2, double2* __restrict__ u3,
                                                    const double2* __restrict__ r1, const double2* __restrict__ r2,
                                                    const double2* __restrict__ r3, double* __restrict__ cs_uw,
-                                                   double* __restrict__ cs_v) {
+                                                   double* __restrict__ cs_v, int part0) {
+    // blockIdx.y + part0: 0 = the u/w systems, 1 = the v system
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
     const int i = col % d.nkx, q = col / d.nkx;
     const double k2x = -g.kx[i] * g.kx[i], k2z = -g.kz[q] * g.kz[q];
     const size_t nc = d.ncol;
-    if (blockIdx.y == 0) {
+    if (blockIdx.y + part0 == 0) {
         // u and w share the matrix: rows (0,1,gwb), interior, (gwt,1,0)
         const int n = d.nyu;
         double dprev = 1.0, a3prev = g.gwb;
