@@ -661,7 +661,9 @@ def main():
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
         "profile_error_mixed_vs_fp64": prof_err,
-        "ensemble": ens,
+        "ensemble": dict(ens, grid_pt_rate_vs_single={
+            prec: ens[prec]["grid_pt_updates_per_s"] / (results[prec]["steps_per_s"] * gp)
+            for prec in ("mixed", "fp64")}) if ens else None,
         "tuning": {"source": "defaults" if args.no_autotune else "cfd_b200.autotune (coordinate search, cached)",
                    **tuning},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
