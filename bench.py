@@ -351,25 +351,50 @@ def profile_error(chans, setup, spinup, nsteps, nstat=20):
     """Mean and rms velocity profiles of the mixed and FP64 paths from the same start: each
     path spins up `spinup` RK3 steps, then accumulates the on-device statistics every
     `nstat` steps over `nsteps` steps (the reference's cadence, nstat = min(20, nwrite),
-    start.f90:372).  Reported: the largest difference over the planes relative to the
-    largest FP64 value of that profile, against the 1 % bound."""
+    start.f90:372).  The time step follows the reference's rule dt = min(2.5 dtv, CFL dtc)
+    (FOU3D.f90:178-181), re-chosen from the FP64 state every `nstat` steps (the reference
+    re-chooses it every step); the mixed path replays the FP64 path's dt sequence so both
+    integrate with the same steps.  Reported: the largest difference over the planes
+    relative to the largest FP64 value of that profile, against the 1 % bound."""
     if nsteps <= 0:
         return None
     npts = setup.cfg.ngal1 * setup.cfg.ngal2
-    prof = {}
-    for prec, ch in chans.items():
+    prof, dts = {}, []
+    out = {"spinup_steps": spinup, "steps": nsteps, "nstat": nstat, "bound": 0.01,
+           "dt_rule": "min(2.5 dtv, CFL dtc) from the FP64 state every nstat steps", "max_rel_diff": {}}
+    for prec in ("fp64", "mixed"):
+        ch = chans[prec]
         ch.upload_state()
-        if spinup > 0:
-            ch.step(spinup)
-        ch.stats_configure(setup.grid.jv0 - 1, 0, 0)
-        done = 0
-        while done < nsteps:
-            n = min(nstat, nsteps - done)
-            ch.step(n)
-            done += n
-            ch.stats_accumulate()
-        prof[prec] = plane_profiles(ch.stats_read(), npts)
-    out = {"spinup_steps": spinup, "steps": nsteps, "nstat": nstat, "bound": 0.01, "max_rel_diff": {}}
+        blk = 0
+        try:
+            def advance(n):
+                nonlocal blk
+                if prec == "fp64":
+                    dts.append(ch.adapt_dt())
+                else:
+                    ch.set_dt(dts[blk])
+                blk += 1
+                ch.step(n)
+            done = 0
+            while done < spinup:
+                n = min(nstat, spinup - done)
+                advance(n)
+                done += n
+            ch.stats_configure(setup.grid.jv0 - 1, 0, 0)
+            done = 0
+            while done < nsteps:
+                n = min(nstat, nsteps - done)
+                advance(n)
+                done += n
+                ch.stats_accumulate()
+            ch.cfl()   # raises on a non-finite state
+            prof[prec] = plane_profiles(ch.stats_read(), npts)
+        except RuntimeError as e:
+            out["error"] = f"{prec}: {str(e)[:160]} (after {blk} blocks of {nstat} steps)"
+            return out
+        finally:
+            ch.set_dt(setup.dt)
+    out["dt_first_last_min_max"] = [dts[0], dts[-1], min(dts), max(dts)]
     for k in ("mean_u", "rms_u", "rms_v", "rms_w"):  # mean v and w are zero up to round-off
         ref = prof["fp64"][k]
         scale = max(np.abs(ref).max(), 1e-300)

@@ -20,7 +20,7 @@ from . import capi
 from .config import ChannelConfig
 from .geometry import IBList, ib_lists
 from .grid import YGrid, y_grid_rough
-from .initial import cfl_dt, initial_state
+from .initial import cfl_dt, initial_state, viscous_dt
 
 
 @dataclass
@@ -240,6 +240,18 @@ class Channel:
         t = capi.CfdTuning()
         self._chk(self.lib.cfd_get_tuning(self.ctx, C.byref(t)), "get_tuning")
         return t.as_dict()
+
+    def adapt_dt(self) -> float:
+        """The reference's time-step rule (FOU3D.f90:178-181), dt = min(2.5 dtv, CFL dtc)
+        with dtc from dtc_calc on the current state and dtv of start.f90:432; the new dt is
+        set (the step graph is captured again) and returned.  The reference applies it at
+        the start of every step; a caller that re-captures less often applies it every few
+        steps."""
+        dtc, _ = self.cfl()
+        cfg = self.setup.cfg
+        dt = min(2.5 * viscous_dt(cfg, self.setup.grid), cfg.cfl * dtc)
+        self.set_dt(dt)
+        return dt
 
     def set_dt(self, dt: float):
         """New time step for the following stages and steps (the graph is captured again)."""

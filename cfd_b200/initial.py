@@ -141,7 +141,6 @@ def to_physical_plane(f_col: np.ndarray, cfg) -> np.ndarray:
 
 
 def cfl_dt(cfg, grid: YGrid, u, v, w) -> float:
-    kx, kz = wavenumbers(cfg.n1, cfg.n2, cfg.alp, cfg.bet)
     umax = max(np.abs(to_physical_plane(u[:, j], cfg)).max() for j in range(grid.nyu))
     wmax = max(np.abs(to_physical_plane(w[:, j], cfg)).max() for j in range(grid.nyu))
     vmax = 1e-6
@@ -149,7 +148,13 @@ def cfl_dt(cfg, grid: YGrid, u, v, w) -> float:
         vmax = max(vmax, np.abs(to_physical_plane(v[:, jj], cfg)).max() * grid.dthdyv[jj])
     dtc = min(1.0 / (cfg.alp * (cfg.n1 // 2) * umax), 1.0 / (cfg.bet * (cfg.n2 // 2) * wmax),
               1.0 / vmax)
+    return float(min(2.5 * viscous_dt(cfg, grid), cfg.cfl * dtc))
+
+
+def viscous_dt(cfg, grid: YGrid) -> float:
+    """dtv of start.f90:432: Re / (kx_max^2 + kz_max^2 + 4 / (yv(1) - yv(0))^2), with the
+    reference's kx = alp N1/2 and kz = bet (N2/2 - 1) extremes."""
+    kx, _ = wavenumbers(cfg.n1, cfg.n2, cfg.alp, cfg.bet)
     k2x = -(kx[cfg.n1 // 2] ** 2)
     k2z = -(cfg.bet * (cfg.n2 // 2 - 1)) ** 2
-    dtv = cfg.re_b / (-k2x - k2z + 4.0 / (grid.yv[1] - grid.yv[0]) ** 2)
-    return float(min(2.5 * dtv, cfg.cfl * dtc))
+    return float(cfg.re_b / (-k2x - k2z + 4.0 / (grid.yv[1] - grid.yv[0]) ** 2))

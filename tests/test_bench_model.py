@@ -33,3 +33,75 @@ def test_step_roofline_model(setup):
     S = setup.cfg.ncol * setup.grid.nyv
     assert r["model_bytes_per_substep"] == 608 * S
     assert r["achieved_gbs"] == pytest.approx(3 * 608 * S / 1e-3 / 1e9)
+
+
+class _FakeChannel:
+    """Host stand-in for a Channel: records the dt of every block of steps and returns
+    plane sums whose values depend on the dt sequence it was given."""
+
+    def __init__(self, setup, dt_seq=None, fail_after=None):
+        self.setup, self.dt, self.log, self.fail_after = setup, setup.dt, [], fail_after
+        self.dt_seq = list(dt_seq or [])
+        self.acc = None
+
+    def upload_state(self):
+        self.log.clear()
+
+    def adapt_dt(self):
+        self.dt = self.dt_seq[len(self.log)]
+        return self.dt
+
+    def set_dt(self, dt):
+        self.dt = dt
+
+    def step(self, n):
+        self.log.append((self.dt, n))
+        if self.fail_after is not None and len(self.log) > self.fail_after:
+            self.nonfinite = True
+
+    def cfl(self):
+        if getattr(self, "nonfinite", False):
+            raise RuntimeError("cfl: CFD_ERR_NONFINITE: non-finite velocity in the physical planes")
+        return 1.0, [1.0, 1.0, 1.0]
+
+    def stats_configure(self, *a):
+        self.acc = 0
+
+    def stats_accumulate(self):
+        self.acc += 1
+
+    def stats_read(self):
+        import numpy as np
+        ny = 4
+        s = float(sum(d for d, _ in self.log))
+        st = {"istat": self.acc}
+        for m in ("Um", "Vm", "Wm"):
+            st[m] = np.full(ny, s * self.acc)
+        for m in ("U2m", "V2m", "W2m"):
+            st[m] = np.full(ny, 2 * s * s * self.acc)
+        return st
+
+
+def test_profile_error_replays_the_fp64_dt_sequence(setup):
+    """The statistics window re-chooses dt from the FP64 state every nstat steps and the
+    mixed path integrates with the same sequence; the caller's dt is restored after."""
+    import bench
+    seq = [1e-3 * (1 + 0.01 * k) for k in range(10)]
+    f64, mix = _FakeChannel(setup, seq), _FakeChannel(setup)
+    out = bench.profile_error({"fp64": f64, "mixed": mix}, setup, spinup=40, nsteps=60, nstat=20)
+    assert [n for _, n in f64.log] == [20] * 5 and f64.log == mix.log
+    assert [d for d, _ in f64.log] == seq[:5]
+    assert f64.dt == setup.dt and mix.dt == setup.dt
+    assert out["steps"] == 60 and out["within_bound"] and max(out["max_rel_diff"].values()) == 0.0
+    assert out["dt_first_last_min_max"] == [seq[0], seq[4], seq[0], seq[4]]
+
+
+def test_profile_error_reports_a_blow_up(setup):
+    """A state that goes non-finite ends the window with the error and the block it
+    happened in, instead of NaN profiles."""
+    import bench
+    seq = [1e-3] * 10
+    f64 = _FakeChannel(setup, seq, fail_after=3)
+    out = bench.profile_error({"fp64": f64, "mixed": _FakeChannel(setup)}, setup, spinup=40, nsteps=60, nstat=20)
+    assert "error" in out and "NONFINITE" in out["error"] and "within_bound" not in out
+    assert f64.dt == setup.dt
