@@ -64,6 +64,7 @@ def kernel_bytes(name, setup, mixed):
         "k_rhs": ncol * ((2 * nyu + nyv + nyp) * cs + (2 * nyu + nyv) * ct + (4 * nyu + 2 * nyv) * ct
                          + (2 * nyu + nyv) * cs + (2 * nyu + nyv) * ct),
         "k_solve_uvw": ncol * 2 * (2 * nyu + nyv) * cs,
+        "k_solve_uvw_r": ncol * 2 * (2 * nyu + nyv) * cs,   # the warp-per-column form, same bytes
         "k_solve_p": ncol * (2 * nyu + nyv + nyp + 2 * nyp) * cs,
         # fused pressure solve + correction: u, v, w read twice and written once; p read and
         # written; psi and the scaled upper diagonal (FP64 real) written and read once

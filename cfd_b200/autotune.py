@@ -35,7 +35,7 @@ def _cache_path() -> str:
 
 def _key(setup, precision: str, gpu: str) -> str:
     c, g = setup.cfg, setup.grid
-    return f"v4|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+    return f"v5|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
 
 
 def time_step(setup, precision, device, tuning, steps=5, warmup=2):

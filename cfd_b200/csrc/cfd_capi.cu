@@ -120,8 +120,6 @@ struct cfd_ctx {
     size_t SM3 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
     int LZ2 = -1, NTZ2 = 0; // two-step z kernels: log2(columns per CTA) (-1 = not used), threads
     int SWM = 0, SWC = 8;   // warp-per-column solves: rows-per-lane bound (0 = not used), columns per CTA
-    double2* ed_uw = nullptr;  // LU factors {e, d} of the u/w and v systems, [RK substep][column][row]
-    double2* ed_v = nullptr;
     size_t SMZ2 = 0;
     int RWIX2 = 0, RWFX2 = 0;  // two-step IB x kernels: rows per CTA (0 = not used)
     int NTIX2 = 0, NTFX2 = 0;
@@ -738,15 +736,41 @@ int ib_all(cfd_ctx* c) {
     return ib_grid<T2>(c, c->ibu, c->d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys, 0, c->d.nyu);
 }
 
+// One launch of the Helmholtz solves on stream st: the systems part0 .. part0 + nsys - 1
+// (0 = u/w, 1 = v), by the thread-per-column sweep or the warp-per-column solve.
+int launch_solve(cfd_ctx* c, cudaStream_t st, double beta, int part0, int nsys) {
+    const Dims& d = c->d;
+    if (c->SWM) {
+        const int lc = ilog2(c->SWC);
+        const dim3 gw((d.ncol + c->SWC - 1) / c->SWC, nsys);
+        const size_t sm = solve_r_smem(std::max(d.nyu, d.nyv), c->SWC);
+        const int nt = 32 * c->SWC;
+#define SOLVE_R(M) \
+    k_solve_uvw_r<M><<<gw, nt, sm, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, lc, part0)
+        switch (c->SWM) {
+            case 4: SOLVE_R(4); break;
+            case 8: SOLVE_R(8); break;
+            case 12: SOLVE_R(12); break;
+            default: SOLVE_R(16); break;
+        }
+#undef SOLVE_R
+        return launched(c, "k_solve_uvw_r");
+    }
+    const dim3 gb((d.ncol + 255) / 256, nsys);
+    k_solve_uvw<<<gb, 256, 0, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v,
+                                    part0);
+    return launched(c, "k_solve_uvw");
+}
+
 // The IB round trips and the Helmholtz solves of one substep as two graph branches: the
 // v grid's round trip and v solve on the side stream while the u/w grid's round trip and
-// u/w solve run on the context stream (the thread-per-column sweep; its two systems are
-// independent).  Otherwise the round trips, then one solve launch.
+// u/w solve run on the context stream (the two systems are independent).  Otherwise the
+// round trips, then one solve launch.
 int solve_kernel(cfd_ctx* c, int krk);
 
 template <typename T2>
 int ib_solve_all(cfd_ctx* c, int krk) {
-    const bool par = c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling && !c->SWM && !c->mb;
+    const bool par = c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling && !c->mb;
     if (!par) {
         int s = ib_all<T2>(c);
         if (s != CFD_OK) return s;
@@ -755,17 +779,12 @@ int ib_solve_all(cfd_ctx* c, int krk) {
     }
     const Dims& d = c->d;
     const double beta = kRKb[krk - 1] * c->dt / c->re;
-    const dim3 gb((d.ncol + 255) / 256, 1);
     CK(cudaEventRecord(c->ev_fork, c->stream));
     CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
     cudaStream_t main = c->stream;
     c->stream = c->side;
     int s = ib_grid<T2>(c, c->ibv, d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v, 2 * d.nyu, 0);
-    if (s == CFD_OK) {
-        k_solve_uvw<<<gb, 256, 0, c->side>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs,
-                                             c->cs_v, 1);
-        s = launched(c, "k_solve_uvw");
-    }
+    if (s == CFD_OK) s = launch_solve(c, c->side, beta, 1, 1);
     c->stream = main;
     const cudaError_t ej = cudaEventRecord(c->ev_join, c->side);  // join even after a failure
     if (ej == cudaSuccess) cudaStreamWaitEvent(c->stream, c->ev_join, 0);
@@ -774,65 +793,21 @@ int ib_solve_all(cfd_ctx* c, int krk) {
     s = ib_grid<T2>(c, c->ibu, d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys, 0, d.nyu);
     if (s != CFD_OK) return s;
     c->hx_valid = false;
-    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v, 0);
-    LK("k_solve_uvw");
-    return CFD_OK;
-}
-
-size_t solve_w_smem(const Dims& d, int swc) {
-    return (size_t)2 * swc * d.nyu * sizeof(double2) + (size_t)3 * d.nyu * sizeof(double);
-}
-
-// LU factors of the u/w and v systems for the three RK substeps at the current dt
-int factor_all(cfd_ctx* c) {
-    if (!c->SWM) return CFD_OK;
-    const Dims& d = c->d;
-    for (int k = 0; k < 3; ++k) {
-        const double beta = kRKb[k] * c->dt / c->re;
-        prof_mark(c);
-        k_factor_uv<<<dim3((d.ncol + 255) / 256, 2), 256, 0, c->stream>>>(
-            d, c->g, beta, c->ed_uw + (size_t)k * d.ncol * d.nyu, c->ed_v + (size_t)k * d.ncol * d.nyv);
-        LK("k_factor_uv");
-    }
-    return CFD_OK;
+    return launch_solve(c, c->stream, beta, 0, 1);
 }
 
 int solve_kernel(cfd_ctx* c, int krk) {
     const Dims& d = c->d;
     const double beta = kRKb[krk - 1] * c->dt / c->re;
-    if (c->SWM) {
-        const int lc = ilog2(c->SWC);
-        dim3 gw((d.ncol + c->SWC - 1) / c->SWC, 2);
-        const size_t sm = solve_w_smem(d, c->SWC);
-        const int nt = 32 * c->SWC;
-        const double2* eu = c->ed_uw + (size_t)(krk - 1) * d.ncol * d.nyu;
-        const double2* ev = c->ed_v + (size_t)(krk - 1) * d.ncol * d.nyv;
-        prof_mark(c);
-#define SOLVE_W(M) \
-    k_solve_uvw_w<M><<<gw, nt, sm, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, eu, ev, lc)
-        switch (c->SWM) {
-            case 4: SOLVE_W(4); break;
-            case 8: SOLVE_W(8); break;
-            case 12: SOLVE_W(12); break;
-            default: SOLVE_W(16); break;
-        }
-#undef SOLVE_W
-        LK("k_solve_uvw_w");
-        return CFD_OK;
-    }
-    dim3 gb((d.ncol + 255) / 256);
     prof_mark(c);
     if (c->mb) {
+        dim3 gb((d.ncol + 255) / 256);
         k_mb_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs,
                                                  c->cs_v);
         LK("k_mb_solve_uvw");
         return CFD_OK;
     }
-    gb.y = 2;
-    k_solve_uvw<<<gb, 256, 0, c->stream>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v,
-                                           0);
-    LK("k_solve_uvw");
-    return CFD_OK;
+    return launch_solve(c, c->stream, beta, 0, 2);
 }
 
 int meanflow_kernel(cfd_ctx* c, int krk) {
@@ -1240,21 +1215,21 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     {
         // warp-per-column Helmholtz solves: up to 16 rows per lane (512 planes)
-        const int m = (d.nyu + 31) / 32;
+        const int m = (std::max(d.nyu, d.nyv) + 31) / 32;
         c->SWM = m <= 4 ? 4 : (m <= 8 ? 8 : (m <= 12 ? 12 : (m <= 16 ? 16 : 0)));
-        // measured at re550: 482 us per launch against 400 us for the thread-per-column sweep
         const int sk = g_tuning && (g_tuning->solve_kind == 1 || g_tuning->solve_kind == 2) ? g_tuning->solve_kind
                                                                                         : (env_int("CFD_SOLVE_WARP", 0, 0, 1) ? 2 : 1);
         if (sk != 2) c->SWM = 0;
         c->SWC = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_COLS", 8, 1, 8));
-        while (c->SWC > 1 && solve_w_smem(d, c->SWC) > 110 * 1024) c->SWC /= 2;
-        const int sm = (int)solve_w_smem(d, c->SWC);
+        const int nmax = std::max(d.nyu, d.nyv);
+        while (c->SWC > 1 && solve_r_smem(nmax, c->SWC) > 110 * 1024) c->SWC /= 2;
+        const int sm = (int)solve_r_smem(nmax, c->SWC);
         cudaError_t e = cudaSuccess;
         switch (c->SWM) {
-            case 4: e = cudaFuncSetAttribute(k_solve_uvw_w<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-            case 8: e = cudaFuncSetAttribute(k_solve_uvw_w<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-            case 12: e = cudaFuncSetAttribute(k_solve_uvw_w<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-            case 16: e = cudaFuncSetAttribute(k_solve_uvw_w<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            case 4: e = cudaFuncSetAttribute(k_solve_uvw_r<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            case 8: e = cudaFuncSetAttribute(k_solve_uvw_r<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            case 12: e = cudaFuncSetAttribute(k_solve_uvw_r<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+            case 16: e = cudaFuncSetAttribute(k_solve_uvw_r<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
             default: break;
         }
         if (e != cudaSuccess) return fail(c, CFD_ERR_CUDA, "solve attributes: %s", cudaGetErrorString(e));
@@ -1322,10 +1297,6 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     AL(c->cs, double, nc * nyu);
     AL(c->cs_v, double, nc * nyv);
-    if (c->SWM) {
-        AL(c->ed_uw, double2, 3 * nc * nyu);
-        AL(c->ed_v, double2, 3 * nc * nyv);
-    }
     c->JC = tune_int(&cfd_tuning::rhs_chunk, "CFD_RHS_CHUNK", 4, 2, 64);
     c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;
     AL(c->scal, double, 4);
@@ -1360,7 +1331,6 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     }
-    if ((s = factor_all(c)) != CFD_OK) return s;
     CK(cudaDeviceSynchronize());
     return CFD_OK;
 }
@@ -2075,7 +2045,7 @@ int cfd_set_dt(cfd_ctx* c, double dt) {
     c->dt = dt;
     c->epoch++;
     destroy_graph(c);
-    return factor_all(c);
+    return CFD_OK;
 }
 
 int cfd_set_lastplane(cfd_ctx* c, int32_t on) {

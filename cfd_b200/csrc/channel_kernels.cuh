@@ -1523,116 +1523,117 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
 }
 
 // --------------------------------------------------------------------------------------
-// LU factors of the Helmholtz systems (LU_buildU/V + LU_dec, tridLU_3D_IB.f90:349-413,
-// 521-559) for one RK coefficient beta, one thread per column: ed[col][row] = {e_j, d_j},
-// e_j = a3_j d_j, d_j = 1/(a2_j - a1_j e_{j-1}).  u and w share rows (0, 1, gwb) /
-// interior / (gwt, 1, 0); v has identity wall rows.  grid: x = column block, y = system.
-// Column-major so that a warp lane reads its consecutive rows as one contiguous run.
+// Implicit Helmholtz solves, one warp per (kx,kz) column (tridiag.cuh): LUsolU for u and w
+// with shared factors and LUsolV for v (tridLU_3D_IB.f90:50-160), the factors of
+// LU_buildU/V + LU_dec (:349-413, 521-559) computed in the warp, so that the right-hand
+// side is read once and the solution written once.  Lane p owns the rows
+// [p m, p m + m); the pivot recurrence e_j = a3_j / (a2_j - a1_j e_{j-1}) is a linear
+// fractional map of e_{j-1}, so the lanes compose their rows' maps as 2x2 matrices, a warp
+// scan hands every lane its incoming e, and each lane replays its rows with the reference's
+// formula d_j = 1 / (a2_j - a1_j e_{j-1}).  The right-hand sides of the lane's rows are
+// copied to shared memory asynchronously while the pivots are computed (u/w: the w copies
+// complete behind the u substitution).  A CTA of 2^lc warps covers 2^lc adjacent columns,
+// so each plane row segment it reads or writes is contiguous.  grid: x = column block,
+// y + part0 = 0 (u, w) or 1 (v).
 // --------------------------------------------------------------------------------------
-__device__ __forceinline__ void helm_row(const Dims& d, const Geo& g, bool uw, int n, int j, double beta,
-                                         double k2x, double k2z, double& a1, double& a2, double& a3) {
-    const double* D2 = uw ? g.dyu2i : g.dyv2i;
+__device__ __forceinline__ void helm_coef(const double* D2, bool uw, const Geo& g, int n, int j, double beta,
+                                          double k2, double& a1, double& a2, double& a3) {
     if (j == 0) { a1 = 0.0; a2 = 1.0; a3 = uw ? g.gwb : 0.0; }
     else if (j == n - 1) { a1 = uw ? g.gwt : 0.0; a2 = 1.0; a3 = 0.0; }
     else {
         a1 = -beta * D2[3 * j + 0];
-        a2 = 1.0 - beta * (D2[3 * j + 1] + k2x + k2z);
+        a2 = 1.0 - beta * (D2[3 * j + 1] + k2);
         a3 = -beta * D2[3 * j + 2];
     }
 }
 
-__global__ void __launch_bounds__(256) k_factor_uv(Dims d, Geo g, double beta, double2* __restrict__ ed_uw,
-                                                   double2* __restrict__ ed_v) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= d.ncol) return;
-    const bool uw = blockIdx.y == 0;
-    const int n = uw ? d.nyu : d.nyv;
-    const int i = col % d.nkx, q = col / d.nkx;
-    const double k2x = -g.kx[i] * g.kx[i], k2z = -g.kz[q] * g.kz[q];
-    double2* ed = (uw ? ed_uw : ed_v) + (size_t)col * n;
-    double ep = 0.0;
-    for (int j = 0; j < n; ++j) {
-        double a1, a2, a3;
-        helm_row(d, g, uw, n, j, beta, k2x, k2z, a1, a2, a3);
-        const double dj = 1.0 / (a2 - a1 * ep);
-        ep = a3 * dj;
-        ed[j] = make_double2(ep, dj);
-    }
+// shared memory of k_solve_uvw_r: the y-metric table of one system and, per warp and
+// field, 32 lanes x (m | 1) rows (an odd row pitch keeps the lanes' 16-byte accesses in
+// distinct banks)
+__host__ __device__ __forceinline__ int solve_r_pitch(int n) { return ((n + 31) >> 5) | 1; }
+// bytes of the metric table, rounded up to 16 so that the rows after it are 16-byte aligned
+__host__ __device__ __forceinline__ size_t solve_r_table(int nmax) { return ((size_t)3 * nmax * sizeof(double) + 15) & ~(size_t)15; }
+__host__ __device__ __forceinline__ size_t solve_r_smem(int nmax, int nwarps) {
+    return solve_r_table(nmax) + (size_t)nwarps * 2 * 32 * solve_r_pitch(nmax) * sizeof(double2);
 }
 
-// --------------------------------------------------------------------------------------
-// Implicit Helmholtz solves, one warp per (kx,kz) column (tridiag.cuh): LUsolU for u and w
-// with shared factors and LUsolV for v.  A CTA of 2^lc warps stages the right-hand sides of
-// 2^lc adjacent columns in shared memory with coalesced asynchronous copies ([field]
-// [column][plane]: planes contiguous, so the lanes' row blocks fall in distinct banks), reads
-// the precomputed factors of its columns as contiguous per-lane runs, substitutes in
-// registers and writes the solutions back coalesced.  grid: x = column block, y = 0 (u, w)
-// or 1 (v).
-// --------------------------------------------------------------------------------------
 template <int MAXM>
-__global__ void __launch_bounds__(256, MAXM <= 12 ? 2 : 1)
-    k_solve_uvw_w(Dims d, Geo g, double beta, double2* __restrict__ u1, double2* __restrict__ u2,
+__global__ void __launch_bounds__(256, 2)
+    k_solve_uvw_r(Dims d, Geo g, double beta, double2* __restrict__ u1, double2* __restrict__ u2,
                   double2* __restrict__ u3, const double2* __restrict__ r1, const double2* __restrict__ r2,
-                  const double2* __restrict__ r3, const double2* __restrict__ ed_uw,
-                  const double2* __restrict__ ed_v, int lc) {
+                  const double2* __restrict__ r3, int lc, int part0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int ncpb = 1 << lc;
-    const bool uw = blockIdx.y == 0;
+    const bool uw = blockIdx.y + part0 == 0;
     const int n = uw ? d.nyu : d.nyv;
     const int nf = uw ? 2 : 1;
-    double2* sm = reinterpret_cast<double2*>(smem_raw);
-    double* D2 = reinterpret_cast<double*>(sm + (size_t)2 * ncpb * d.nyu);  // [n][3]
-    const int col0 = blockIdx.x * ncpb;
-    const size_t nc = d.ncol;
-    const int c = threadIdx.x & (ncpb - 1);
-    const bool cok = col0 + c < d.ncol;
-    for (int f = 0; f < nf; ++f) {
-        const double2* src = (f == 0 ? (uw ? r1 : r2) : r3) + col0 + c;
-        double2* dst = sm + ((size_t)f * ncpb + c) * n;
-        for (int j = threadIdx.x >> lc; j < n; j += blockDim.x >> lc)
-            if (cok) cp_async16(dst + j, src + (size_t)j * nc);
-    }
+    const int nmax = d.nyu > d.nyv ? d.nyu : d.nyv;
+    double* D2 = reinterpret_cast<double*>(smem_raw);
     {
         const double* g2 = uw ? g.dyu2i : g.dyv2i;
         for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) D2[k] = g2[k];
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int col = col0 + w;
-    const bool act = w < ncpb && col < d.ncol;
+    const int col = (blockIdx.x << lc) + w;
+    const bool act = col < d.ncol;  // uniform over the warp
+    const int mo = solve_r_pitch(nmax);
+    double2* rows = reinterpret_cast<double2*>(smem_raw + solve_r_table(nmax)) +
+                    ((size_t)w * 2 * 32 + lane) * mo;  // field f at rows + f * 32 * mo
     const LaneRows lr = lane_rows(n, lane);
-    double2 ed[MAXM];
+    const size_t nc = d.ncol;
     if (act) {
-        const double2* ec = (uw ? ed_uw : ed_v) + (size_t)col * n + lr.s;
-#pragma unroll
-        for (int t = 0; t < MAXM; ++t)
-            if (t < lr.mp) ed[t] = ec[t];
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    if (act) {
-        const double gt = uw ? g.gwt : 0.0;
-        auto a1 = [&](int t) {
-            const int j = lr.s + t;
-            return j == 0 ? 0.0 : (j == n - 1 ? gt : -beta * D2[3 * j + 0]);
-        };
         for (int f = 0; f < nf; ++f) {
-            double2* cs = sm + ((size_t)f * ncpb + w) * n + lr.s;
-            double2 y[MAXM];
+            const double2* src = (f == 0 ? (uw ? r1 : r2) : r3) + (size_t)lr.s * nc + col;
 #pragma unroll
             for (int t = 0; t < MAXM; ++t)
-                if (t < lr.mp) y[t] = cs[t];
-            warp_substitute<MAXM>(lr, lane, ed, a1, y);
-#pragma unroll
-            for (int t = 0; t < MAXM; ++t)
-                if (t < lr.mp) cs[t] = y[t];
+                if (t < lr.mp) cp_async16(rows + (size_t)f * 32 * mo + t, src + (size_t)t * nc);
+            cp_async_commit();
         }
     }
-    __syncthreads();
+    __syncthreads();  // the metric table
+    if (!act) return;
+    const int i = col % d.nkx, q = col / d.nkx;
+    const double k2 = -g.kx[i] * g.kx[i] - g.kz[q] * g.kz[q];
+    // pivots: compose the rows' maps e -> a3 / (a2 - a1 e) as [[0, a3], [-a1, a2]]
+    Mob P = mob_identity();
+#pragma unroll
+    for (int t = 0; t < MAXM; ++t)
+        if (t < lr.mp) {
+            double a1, a2, a3;
+            helm_coef(D2, uw, g, n, lr.s + t, beta, k2, a1, a2, a3);
+            P = mob_norm(mob_mul(Mob{0.0, a3, -a1, a2}, P));
+        }
+    P = mob_scan_exclusive(P, lane);
+    double e = lane == 0 ? 0.0 : P.b / P.d;
+    double dd[MAXM];
+#pragma unroll
+    for (int t = 0; t < MAXM; ++t)
+        if (t < lr.mp) {
+            double a1, a2, a3;
+            helm_coef(D2, uw, g, n, lr.s + t, beta, k2, a1, a2, a3);
+            dd[t] = 1.0 / (a2 - a1 * e);
+            e = a3 * dd[t];
+        }
+    auto a1f = [&](int t) {
+        const int j = lr.s + t;
+        return j == 0 ? 0.0 : (j == n - 1 ? (uw ? g.gwt : 0.0) : -beta * D2[3 * j + 0]);
+    };
+    auto ef = [&](int t) {
+        const int j = lr.s + t;
+        return (j == 0 ? (uw ? g.gwb : 0.0) : (j == n - 1 ? 0.0 : -beta * D2[3 * j + 2])) * dd[t];
+    };
     for (int f = 0; f < nf; ++f) {
-        double2* dst = (f == 0 ? (uw ? u1 : u2) : u3) + col0 + c;
-        const double2* src = sm + ((size_t)f * ncpb + c) * n;
-        for (int j = threadIdx.x >> lc; j < n; j += blockDim.x >> lc)
-            if (cok) dst[(size_t)j * nc] = src[j];
+        if (f == 0 && nf == 2) cp_async_wait_group<1>();
+        else cp_async_wait_group<0>();
+        const double2* cs = rows + (size_t)f * 32 * mo;
+        double2 y[MAXM];
+#pragma unroll
+        for (int t = 0; t < MAXM; ++t)
+            if (t < lr.mp) y[t] = cs[t];
+        warp_substitute<MAXM>(lr, lane, dd, a1f, ef, y);
+        double2* dst = (f == 0 ? (uw ? u1 : u2) : u3) + (size_t)lr.s * nc + col;
+#pragma unroll
+        for (int t = 0; t < MAXM; ++t)
+            if (t < lr.mp) dst[(size_t)t * nc] = y[t];
     }
 }
 

@@ -5,13 +5,14 @@
 // row, LUsolU/V/P (:50-160, :284-318) run the substitutions
 //   y_j = d_j (r_j - a1_j y_{j-1})      forward, affine in y_{j-1}
 //   x_j = y_j - e_j x_{j+1}             backward, affine in x_{j+1}
-// Here the factors are computed once per time step size (they depend on kx, kz, the y-grid
-// and the RK coefficient only) and stored column-major, and one warp substitutes one column:
-// lane p owns the m consecutive rows [p*m, p*m + m), composes the affine maps of its rows,
-// a warp scan hands every lane its incoming value, and the lane replays its rows with the
-// reference's formulas.  The column stays in registers, so the right-hand side is read once
-// and the solution written once; only the grouping of the chained maps differs from the
-// sequential sweep, so results agree to round-off.
+// Here one warp solves one column: lane p owns the m consecutive rows [p*m, p*m + m).  The
+// pivot recurrence e_j = a3_j / (a2_j - a1_j e_{j-1}) is a linear fractional map of e_{j-1}:
+// the lanes compose their rows' maps, a warp scan hands every lane its incoming e, and each
+// lane replays its rows with d_j = 1 / (a2_j - a1_j e_{j-1}).  The two substitutions are
+// affine maps, composed and scanned the same way, then replayed with the reference's
+// formulas.  The column stays in the warp, so the right-hand side is read once and the
+// solution written once; only the grouping of the chained maps differs from the sequential
+// sweep, so results agree to round-off.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -32,16 +33,17 @@ __device__ __forceinline__ LaneRows lane_rows(int n, int lane) {
 }
 
 // Substitutions of one column: y[t] holds the lane's right-hand side on entry and the
-// solution on exit; ed[t] = {e, d} of the lane's rows, a1(t) their sub-diagonal.
-template <int MAXM, typename A1F>
-__device__ __forceinline__ void warp_substitute(const LaneRows& lr, int lane, const double2 (&ed)[MAXM], A1F a1,
-                                                double2 (&y)[MAXM]) {
+// solution on exit; dd[t] are the pivots d of the lane's rows, a1(t) their sub-diagonal and
+// e(t) their scaled upper diagonal.
+template <int MAXM, typename A1F, typename EF>
+__device__ __forceinline__ void warp_substitute(const LaneRows& lr, int lane, const double (&dd)[MAXM], A1F a1,
+                                                EF e, double2 (&y)[MAXM]) {
     double A = 1.0;  // y_last = A * y_in + B over the lane's rows
     double2 B = make_double2(0.0, 0.0);
 #pragma unroll
     for (int t = 0; t < MAXM; ++t)
         if (t < lr.mp) {
-            const double dj = ed[t].y, al = -a1(t) * dj;
+            const double dj = dd[t], al = -a1(t) * dj;
             B = make_double2(al * B.x + dj * y[t].x, al * B.y + dj * y[t].y);
             A *= al;
         }
@@ -58,7 +60,7 @@ __device__ __forceinline__ void warp_substitute(const LaneRows& lr, int lane, co
 #pragma unroll
     for (int t = 0; t < MAXM; ++t)
         if (t < lr.mp) {
-            const double dj = ed[t].y;
+            const double dj = dd[t];
             const double a = a1(t);
             y[t] = make_double2(dj * (y[t].x - a * yp.x), dj * (y[t].y - a * yp.y));
             yp = y[t];
@@ -68,8 +70,9 @@ __device__ __forceinline__ void warp_substitute(const LaneRows& lr, int lane, co
 #pragma unroll
     for (int t = MAXM - 1; t >= 0; --t)
         if (t < lr.mp) {
-            H = make_double2(y[t].x - ed[t].x * H.x, y[t].y - ed[t].x * H.y);
-            G *= -ed[t].x;
+            const double et = e(t);
+            H = make_double2(y[t].x - et * H.x, y[t].y - et * H.y);
+            G *= -et;
         }
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -84,9 +87,38 @@ __device__ __forceinline__ void warp_substitute(const LaneRows& lr, int lane, co
 #pragma unroll
     for (int t = MAXM - 1; t >= 0; --t)
         if (t < lr.mp) {
-            y[t] = make_double2(y[t].x - ed[t].x * xn.x, y[t].y - ed[t].x * xn.y);
+            const double et = e(t);
+            y[t] = make_double2(y[t].x - et * xn.x, y[t].y - et * xn.y);
             xn = y[t];
         }
+}
+
+// Linear fractional maps x -> (a x + b) / (c x + d) as 2x2 matrices.  Only the ratios
+// matter, so products are rescaled by a power of two (exact) to keep the entries near 1.
+struct Mob {
+    double a, b, c, d;
+};
+__device__ __forceinline__ Mob mob_identity() { return Mob{1.0, 0.0, 0.0, 1.0}; }
+// x after y
+__device__ __forceinline__ Mob mob_mul(const Mob& x, const Mob& y) {
+    return Mob{x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c, x.c * y.b + x.d * y.d};
+}
+__device__ __forceinline__ Mob mob_norm(const Mob& m) {
+    const double mx = fmax(fmax(fabs(m.a), fabs(m.b)), fmax(fabs(m.c), fabs(m.d)));
+    int ex;
+    frexp(mx, &ex);
+    const double s = ldexp(1.0, -ex);
+    return Mob{m.a * s, m.b * s, m.c * s, m.d * s};
+}
+// composition of the maps of all lanes below this one (lane 0: identity)
+__device__ __forceinline__ Mob mob_scan_exclusive(Mob P, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const Mob O{shfl_up_d(P.a, off), shfl_up_d(P.b, off), shfl_up_d(P.c, off), shfl_up_d(P.d, off)};
+        if (lane >= off) P = mob_norm(mob_mul(P, O));
+    }
+    Mob E{shfl_up_d(P.a, 1), shfl_up_d(P.b, 1), shfl_up_d(P.c, 1), shfl_up_d(P.d, 1)};
+    return lane == 0 ? mob_identity() : E;
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -94,5 +126,8 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 }  // namespace cfd

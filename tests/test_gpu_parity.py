@@ -254,10 +254,11 @@ def test_stockham_nonlinear_path(torch_cuda, monkeypatch, ng1, ng2, ny):
         g.close()
 
 
-@pytest.mark.parametrize("ng1,ng2,ny", [(24, 18, 17), (96, 192, 13)])
+@pytest.mark.parametrize("ng1,ng2,ny", [(24, 18, 17), (96, 192, 13), (24, 18, 129), (24, 18, 257), (24, 18, 385)])
 def test_warp_column_solves(torch_cuda, monkeypatch, ng1, ng2, ny):
-    """The warp-per-column Helmholtz solves on precomputed LU factors (CFD_SOLVE_WARP=1),
-    stage by stage and over a dt change, against the oracle (FP64, 1e-11 / 1e-10)."""
+    """The warp-per-column Helmholtz solves, LU factors composed by warp scans
+    (CFD_SOLVE_WARP=1), stage by stage and over a dt change, against the oracle (FP64,
+    1e-11 / 1e-10); the sizes put 1, 6, 11 and 16 rows on a lane (every row bound)."""
     from cfd_b200.channel import build_channel
     from cfd_b200.config import tiny
     monkeypatch.setenv("CFD_SOLVE_WARP", "1")
