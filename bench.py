@@ -348,29 +348,36 @@ def plane_profiles(st, npts):
     return out
 
 
-def profile_error(chans, setup, spinup, nsteps, nstat=20):
+def profile_error(chans, setup, spinup, nsteps, nstat=20, floor=True):
     """Mean and rms velocity profiles of the mixed and FP64 paths from the same start: each
     path spins up `spinup` RK3 steps, then accumulates the on-device statistics every
     `nstat` steps over `nsteps` steps (the reference's cadence, nstat = min(20, nwrite),
     start.f90:372).  The time step follows the reference's rule dt = min(2.5 dtv, CFL dtc)
     (FOU3D.f90:178-181), re-chosen from the FP64 state every `nstat` steps (the reference
-    re-chooses it every step); the mixed path replays the FP64 path's dt sequence so both
+    re-chooses it every step); the other runs replay the FP64 run's dt sequence so all
     integrate with the same steps.  Reported: the largest difference over the planes
-    relative to the largest FP64 value of that profile, against the 1 % bound."""
+    relative to the largest FP64 value of that profile, against the 1 % bound.  With
+    `floor`, a second FP64 run from the initial state rounded to FP32 measures how far two
+    FP64 trajectories that start one rounding apart drift in the same window (the flow is
+    chaotic, so the profiles of any two runs differ by at least this much)."""
     if nsteps <= 0:
         return None
     npts = setup.cfg.ngal1 * setup.cfg.ngal2
     prof, dts = {}, []
     out = {"spinup_steps": spinup, "steps": nsteps, "nstat": nstat, "bound": 0.01,
            "dt_rule": "min(2.5 dtv, CFL dtc) from the FP64 state every nstat steps", "max_rel_diff": {}}
-    for prec in ("fp64", "mixed"):
-        ch = chans[prec]
-        ch.upload_state()
+    runs = [("fp64", chans["fp64"], None), ("mixed", chans["mixed"], None)]
+    if floor:
+        st = setup.state()
+        rounded = {k: v.astype(np.complex64).astype(np.complex128) for k, v in st.items()}
+        runs.append(("fp64_from_fp32_rounded_start", chans["fp64"], rounded))
+    for name, ch, start in runs:
+        ch.upload_state(start)
         blk = 0
         try:
             def advance(n):
                 nonlocal blk
-                if prec == "fp64":
+                if name == "fp64":
                     dts.append(ch.adapt_dt())
                 else:
                     ch.set_dt(dts[blk])
@@ -389,18 +396,25 @@ def profile_error(chans, setup, spinup, nsteps, nstat=20):
                 done += n
                 ch.stats_accumulate()
             ch.cfl()   # raises on a non-finite state
-            prof[prec] = plane_profiles(ch.stats_read(), npts)
+            prof[name] = plane_profiles(ch.stats_read(), npts)
         except RuntimeError as e:
-            out["error"] = f"{prec}: {str(e)[:160]} (after {blk} blocks of {nstat} steps)"
+            out["error"] = f"{name}: {str(e)[:160]} (after {blk} blocks of {nstat} steps)"
             return out
         finally:
             ch.set_dt(setup.dt)
     out["dt_first_last_min_max"] = [dts[0], dts[-1], min(dts), max(dts)]
-    for k in ("mean_u", "rms_u", "rms_v", "rms_w"):  # mean v and w are zero up to round-off
-        ref = prof["fp64"][k]
-        scale = max(np.abs(ref).max(), 1e-300)
-        out["max_rel_diff"][k] = float(np.abs(prof["mixed"][k] - ref).max() / scale)
+
+    def diffs(other):
+        r = {}
+        for k in ("mean_u", "rms_u", "rms_v", "rms_w"):  # mean v and w are zero up to round-off
+            ref = prof["fp64"][k]
+            scale = max(np.abs(ref).max(), 1e-300)
+            r[k] = float(np.abs(prof[other][k] - ref).max() / scale)
+        return r
+    out["max_rel_diff"] = diffs("mixed")
     out["within_bound"] = all(v < out["bound"] for v in out["max_rel_diff"].values())
+    if floor:
+        out["chaos_floor_max_rel_diff"] = diffs("fp64_from_fp32_rounded_start")
     return out
 
 

@@ -1215,7 +1215,9 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     {
         // warp-per-column Helmholtz solves: up to 16 rows per lane (512 planes)
-        const int m = (std::max(d.nyu, d.nyv) + 31) / 32;
+        // (odd rows per lane where the bound allows: solve_r_rows)
+        const int m0 = (std::max(d.nyu, d.nyv) + 31) / 32;
+        const int m = m0 > 16 ? m0 : std::min(m0 | 1, 16);
         c->SWM = m <= 4 ? 4 : (m <= 8 ? 8 : (m <= 12 ? 12 : (m <= 16 ? 16 : 0)));
         const int sk = g_tuning && (g_tuning->solve_kind == 1 || g_tuning->solve_kind == 2) ? g_tuning->solve_kind
                                                                                         : (env_int("CFD_SOLVE_WARP", 0, 0, 1) ? 2 : 1);

@@ -105,9 +105,9 @@ __device__ __forceinline__ Mob mob_mul(const Mob& x, const Mob& y) {
 }
 __device__ __forceinline__ Mob mob_norm(const Mob& m) {
     const double mx = fmax(fmax(fabs(m.a), fabs(m.b)), fmax(fabs(m.c), fabs(m.d)));
-    int ex;
-    frexp(mx, &ex);
-    const double s = ldexp(1.0, -ex);
+    // 2^-(E - 1023) for the biased exponent E of mx (a normal number): biased 2046 - E
+    const long long eb = (__double_as_longlong(mx) >> 52) & 0x7ff;
+    const double s = __longlong_as_double((2046 - eb) << 52);
     return Mob{m.a * s, m.b * s, m.c * s, m.d * s};
 }
 // composition of the maps of all lanes below this one (lane 0: identity)

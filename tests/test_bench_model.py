@@ -44,8 +44,9 @@ class _FakeChannel:
         self.dt_seq = list(dt_seq or [])
         self.acc = None
 
-    def upload_state(self):
+    def upload_state(self, state=None):
         self.log.clear()
+        self.started_from = state
 
     def adapt_dt(self):
         self.dt = self.dt_seq[len(self.log)]
@@ -90,6 +91,10 @@ def test_profile_error_replays_the_fp64_dt_sequence(setup):
     f64, mix = _FakeChannel(setup, seq), _FakeChannel(setup)
     out = bench.profile_error({"fp64": f64, "mixed": mix}, setup, spinup=40, nsteps=60, nstat=20)
     assert [n for _, n in f64.log] == [20] * 5 and f64.log == mix.log
+    # the chaos-floor run: FP64 again, from the FP32-rounded start, with the same dt sequence
+    assert f64.started_from is not None and mix.started_from is None
+    assert f64.started_from["u1"].dtype == "complex128"
+    assert max(out["chaos_floor_max_rel_diff"].values()) == 0.0
     assert [d for d, _ in f64.log] == seq[:5]
     assert f64.dt == setup.dt and mix.dt == setup.dt
     assert out["steps"] == 60 and out["within_bound"] and max(out["max_rel_diff"].values()) == 0.0
