@@ -4,9 +4,8 @@ context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
 Candidates: the x-line path (register two-step; the same with 1.5 complex lines per row;
 the same on packed FP32 line pairs; or shared-memory Stockham), rows per CTA of the two-step
 x-line kernel, lines per CTA of the two-step z kernels, the radix order of the x and z
-two-step transforms (N = N1*N2 or N2*N1: which register DFT runs first), the solve kind (thread-per-column
-sweeps or warp-per-column substitutions, with 4 or 8 columns per CTA), and the y-planes per
-thread of the right-hand-side kernel.
+two-step transforms (N = N1*N2 or N2*N1: which register DFT runs first), and the y-planes
+per thread of the right-hand-side kernel.
 The search is coordinate-wise from the library default, one knob at a time, so it costs a
 dozen short timings.  Results are cached in a JSON file keyed by grid, precision and GPU
 name (CFD_TUNE_CACHE, default ~/.cache/cfd_b200/tuning.json).
@@ -17,13 +16,11 @@ import json
 import os
 
 KNOBS = (("xline_path", (1, 2, 3, 4)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
-         ("xsplit", (1, 2)), ("zsplit", (1, 2)),
-         ("solve_kind", (1, 2)), ("solve_cols", (4, 8)), ("rhs_chunk", (2, 4, 8, 16)))
+         ("xsplit", (1, 2)), ("zsplit", (1, 2)), ("rhs_chunk", (2, 4, 8, 16)))
 
 
 # knobs that only act with another setting (the library reports them as 0 or 1 otherwise)
-RELEVANT = {"solve_cols": lambda t: t.get("solve_kind") == 2,
-            "xline_rows": lambda t: t.get("xline_path") != 2,
+RELEVANT = {"xline_rows": lambda t: t.get("xline_path") != 2,
             "xsplit": lambda t: t.get("xline_path") == 1,
             "zsplit": lambda t: t.get("xline_path") == 1}
 
@@ -35,7 +32,7 @@ def _cache_path() -> str:
 
 def _key(setup, precision: str, gpu: str) -> str:
     c, g = setup.cfg, setup.grid
-    return f"v5|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+    return f"v6|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
 
 
 def time_step(setup, precision, device, tuning, steps=5, warmup=2):

@@ -119,7 +119,6 @@ struct cfd_ctx {
     size_t SM4 = 0;
     size_t SM3 = 0;   // two-step x-line kernel: rows per CTA (0 = not used), threads
     int LZ2 = -1, NTZ2 = 0; // two-step z kernels: log2(columns per CTA) (-1 = not used), threads
-    int SWM = 0, SWC = 8;   // warp-per-column solves: rows-per-lane bound (0 = not used), columns per CTA
     size_t SMZ2 = 0;
     int RWIX2 = 0, RWFX2 = 0;  // two-step IB x kernels: rows per CTA (0 = not used)
     int NTIX2 = 0, NTFX2 = 0;
@@ -737,25 +736,9 @@ int ib_all(cfd_ctx* c) {
 }
 
 // One launch of the Helmholtz solves on stream st: the systems part0 .. part0 + nsys - 1
-// (0 = u/w, 1 = v), by the thread-per-column sweep or the warp-per-column solve.
+// (0 = u/w, 1 = v).
 int launch_solve(cfd_ctx* c, cudaStream_t st, double beta, int part0, int nsys) {
     const Dims& d = c->d;
-    if (c->SWM) {
-        const int lc = ilog2(c->SWC);
-        const dim3 gw((d.ncol + c->SWC - 1) / c->SWC, nsys);
-        const size_t sm = solve_r_smem(std::max(d.nyu, d.nyv), c->SWC);
-        const int nt = 32 * c->SWC;
-#define SOLVE_R(M) \
-    k_solve_uvw_r<M><<<gw, nt, sm, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, lc, part0)
-        switch (c->SWM) {
-            case 4: SOLVE_R(4); break;
-            case 8: SOLVE_R(8); break;
-            case 12: SOLVE_R(12); break;
-            default: SOLVE_R(16); break;
-        }
-#undef SOLVE_R
-        return launched(c, "k_solve_uvw_r");
-    }
     const dim3 gb((d.ncol + 255) / 256, nsys);
     k_solve_uvw<<<gb, 256, 0, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v,
                                     part0);
@@ -1214,29 +1197,6 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         }
     }
     {
-        // warp-per-column Helmholtz solves: up to 16 rows per lane (512 planes)
-        // (odd rows per lane where the bound allows: solve_r_rows)
-        const int m0 = (std::max(d.nyu, d.nyv) + 31) / 32;
-        const int m = m0 > 16 ? m0 : std::min(m0 | 1, 16);
-        c->SWM = m <= 4 ? 4 : (m <= 8 ? 8 : (m <= 12 ? 12 : (m <= 16 ? 16 : 0)));
-        const int sk = g_tuning && (g_tuning->solve_kind == 1 || g_tuning->solve_kind == 2) ? g_tuning->solve_kind
-                                                                                        : (env_int("CFD_SOLVE_WARP", 0, 0, 1) ? 2 : 1);
-        if (sk != 2) c->SWM = 0;
-        c->SWC = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_COLS", 8, 1, 8));
-        const int nmax = std::max(d.nyu, d.nyv);
-        while (c->SWC > 1 && solve_r_smem(nmax, c->SWC) > 110 * 1024) c->SWC /= 2;
-        const int sm = (int)solve_r_smem(nmax, c->SWC);
-        cudaError_t e = cudaSuccess;
-        switch (c->SWM) {
-            case 4: e = cudaFuncSetAttribute(k_solve_uvw_r<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-            case 8: e = cudaFuncSetAttribute(k_solve_uvw_r<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-            case 12: e = cudaFuncSetAttribute(k_solve_uvw_r<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-            case 16: e = cudaFuncSetAttribute(k_solve_uvw_r<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
-            default: break;
-        }
-        if (e != cudaSuccess) return fail(c, CFD_ERR_CUDA, "solve attributes: %s", cudaGetErrorString(e));
-    }
-    {
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
@@ -1256,7 +1216,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (c->mb) {
         // three bands: the per-slot interpolating z pass, the Stockham x-line kernel and the
         // two-step forward z pass, launched once per band; thread-per-column solves
-        c->RW2 = 0; c->XL3 = false; c->RW4 = 0; c->XALT = c->ZALT = false; c->SWM = 0;
+        c->RW2 = 0; c->XL3 = false; c->RW4 = 0; c->XALT = c->ZALT = false;
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(cfg->ngal2_mid, ok, { n1s = TN1; n2s = TN2; });
@@ -1513,8 +1473,8 @@ int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
     t->xline_path = c->RW2 ? (c->RW4 ? 4 : (c->XL3 ? 3 : 1)) : 2;
     t->xline_rows = c->RW4 ? c->RW4 : (c->RW2 ? c->RW2 : 0);
     t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
-    t->solve_kind = c->SWM ? 2 : 1;
-    t->solve_cols = c->SWM ? c->SWC : 0;
+    t->solve_kind = 1;
+    t->solve_cols = 0;
     t->rhs_chunk = c->JC;
     t->xsplit = c->XALT ? 2 : 1;
     t->zsplit = c->ZALT ? 2 : 1;

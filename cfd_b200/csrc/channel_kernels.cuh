@@ -20,7 +20,6 @@
 #include "fft_smem.cuh"
 #include "fft_reg.cuh"
 #include "fft_pair.cuh"
-#include "tridiag.cuh"
 
 namespace cfd {
 
@@ -1520,138 +1519,6 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
         if (q >= 0 && live) out[(size_t)q * d.nkx] = to_d2(cscale(v, sc));
     };
     two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
-}
-
-// --------------------------------------------------------------------------------------
-// Implicit Helmholtz solves, one warp per (kx,kz) column (tridiag.cuh): LUsolU for u and w
-// with shared factors and LUsolV for v (tridLU_3D_IB.f90:50-160), the factors of
-// LU_buildU/V + LU_dec (:349-413, 521-559) computed in the warp, so that the right-hand
-// side is read once and the solution written once.  Lane p owns the rows [p m, p m + m)
-// (m odd, so that the lanes' rows fall in distinct shared-memory banks); the pivot
-// recurrence e_j = a3_j / (a2_j - a1_j e_{j-1}) is a linear fractional map of e_{j-1}, so
-// the lanes compose their rows' maps as 2x2 matrices, a warp scan hands every lane its
-// incoming e, and each lane replays its rows with d_j = 1 / (a2_j - a1_j e_{j-1}).
-// A CTA of 2^lc warps covers 2^lc adjacent columns and moves their right-hand sides and
-// solutions as [plane][column] tiles through shared memory, so every global access is a
-// contiguous run of 2^lc columns: the tiles are requested with cp.async before the pivots
-// are computed (u/w: the w tile arrives behind the u substitution), each warp substitutes
-// its column in place, and the CTA writes the tile back.  grid: x = column block,
-// y + part0 = 0 (u, w) or 1 (v).
-// --------------------------------------------------------------------------------------
-__device__ __forceinline__ void helm_coef(const double* D2, bool uw, const Geo& g, int n, int j, double beta,
-                                          double k2, double& a1, double& a2, double& a3) {
-    if (j == 0) { a1 = 0.0; a2 = 1.0; a3 = uw ? g.gwb : 0.0; }
-    else if (j == n - 1) { a1 = uw ? g.gwt : 0.0; a2 = 1.0; a3 = 0.0; }
-    else {
-        a1 = -beta * D2[3 * j + 0];
-        a2 = 1.0 - beta * (D2[3 * j + 1] + k2);
-        a3 = -beta * D2[3 * j + 2];
-    }
-}
-
-// rows per lane of an n-row system: odd, at least ceil(n / 32), at most MAXM
-__host__ __device__ __forceinline__ int solve_r_rows(int n, int maxm) {
-    const int m = ((n + 31) >> 5) | 1;
-    return m < maxm ? m : maxm;
-}
-// shared memory of k_solve_uvw_r: the y-metric table of one system (rounded up to 16 bytes)
-// and the tiles [field][column][plane] with an odd plane pitch, so that the tile copies'
-// column-fastest accesses fall in distinct banks
-__host__ __device__ __forceinline__ int solve_r_pitch(int nmax) { return nmax | 1; }
-__host__ __device__ __forceinline__ size_t solve_r_table(int nmax) { return ((size_t)3 * nmax * sizeof(double) + 15) & ~(size_t)15; }
-__host__ __device__ __forceinline__ size_t solve_r_smem(int nmax, int ncols) {
-    return solve_r_table(nmax) + (size_t)2 * ncols * solve_r_pitch(nmax) * sizeof(double2);
-}
-
-template <int MAXM>
-__global__ void __launch_bounds__(256, 2)
-    k_solve_uvw_r(Dims d, Geo g, double beta, double2* __restrict__ u1, double2* __restrict__ u2,
-                  double2* __restrict__ u3, const double2* __restrict__ r1, const double2* __restrict__ r2,
-                  const double2* __restrict__ r3, int lc, int part0) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const bool uw = blockIdx.y + part0 == 0;
-    const int n = uw ? d.nyu : d.nyv;
-    const int nf = uw ? 2 : 1;
-    const int nmax = d.nyu > d.nyv ? d.nyu : d.nyv;
-    const int pitch = solve_r_pitch(nmax);
-    const int ncpb = 1 << lc;
-    double* D2 = reinterpret_cast<double*>(smem_raw);
-    double2* tile = reinterpret_cast<double2*>(smem_raw + solve_r_table(nmax));  // [f][c][pitch]
-    const int col0 = blockIdx.x << lc;
-    const size_t nc = d.ncol;
-    const int c = threadIdx.x & (ncpb - 1);
-    const bool cok = col0 + c < d.ncol;
-    for (int f = 0; f < nf; ++f) {
-        const double2* src = (f == 0 ? (uw ? r1 : r2) : r3) + col0 + c;
-        double2* dst = tile + ((size_t)f * ncpb + c) * pitch;
-        if (cok)
-            for (int j = threadIdx.x >> lc; j < n; j += blockDim.x >> lc) cp_async16(dst + j, src + (size_t)j * nc);
-        cp_async_commit();
-    }
-    {
-        const double* g2 = uw ? g.dyu2i : g.dyv2i;
-        for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) D2[k] = g2[k];
-    }
-    __syncthreads();  // the metric table
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int col = col0 + w;
-    const bool act = col < d.ncol;  // uniform over the warp
-    const int m = solve_r_rows(n, MAXM);
-    const LaneRows lr{lane * m, max(0, min(m, n - lane * m))};
-    double dd[MAXM];
-    if (act) {
-        const int i = col % d.nkx, q = col / d.nkx;
-        const double k2 = -g.kx[i] * g.kx[i] - g.kz[q] * g.kz[q];
-        // pivots: compose the rows' maps e -> a3 / (a2 - a1 e) as [[0, a3], [-a1, a2]]
-        Mob P = mob_identity();
-#pragma unroll
-        for (int t = 0; t < MAXM; ++t)
-            if (t < lr.mp) {
-                double a1, a2, a3;
-                helm_coef(D2, uw, g, n, lr.s + t, beta, k2, a1, a2, a3);
-                P = mob_mul(Mob{0.0, a3, -a1, a2}, P);
-                if ((t & 3) == 3) P = mob_norm(P);
-            }
-        P = mob_scan_exclusive(mob_norm(P), lane);
-        double e = lane == 0 ? 0.0 : P.b / P.d;
-#pragma unroll
-        for (int t = 0; t < MAXM; ++t)
-            if (t < lr.mp) {
-                double a1, a2, a3;
-                helm_coef(D2, uw, g, n, lr.s + t, beta, k2, a1, a2, a3);
-                dd[t] = 1.0 / (a2 - a1 * e);
-                e = a3 * dd[t];
-            }
-    }
-    auto a1f = [&](int t) {
-        const int j = lr.s + t;
-        return j == 0 ? 0.0 : (j == n - 1 ? (uw ? g.gwt : 0.0) : -beta * D2[3 * j + 0]);
-    };
-    auto ef = [&](int t) {
-        const int j = lr.s + t;
-        return (j == 0 ? (uw ? g.gwb : 0.0) : (j == n - 1 ? 0.0 : -beta * D2[3 * j + 2])) * dd[t];
-    };
-    for (int f = 0; f < nf; ++f) {
-        if (f == 0 && nf == 2) cp_async_wait_group<1>();
-        else cp_async_wait_group<0>();
-        __syncthreads();  // tile f complete
-        if (act) {
-            double2* cs = tile + ((size_t)f * ncpb + w) * pitch + lr.s;
-            double2 y[MAXM];
-#pragma unroll
-            for (int t = 0; t < MAXM; ++t)
-                if (t < lr.mp) y[t] = cs[t];
-            warp_substitute<MAXM>(lr, lane, dd, a1f, ef, y);
-#pragma unroll
-            for (int t = 0; t < MAXM; ++t)
-                if (t < lr.mp) cs[t] = y[t];
-        }
-        __syncthreads();  // solutions of tile f in place
-        double2* dst = (f == 0 ? (uw ? u1 : u2) : u3) + col0 + c;
-        const double2* src = tile + ((size_t)f * ncpb + c) * pitch;
-        if (cok)
-            for (int j = threadIdx.x >> lc; j < n; j += blockDim.x >> lc) dst[(size_t)j * nc] = src[j];
-    }
 }
 
 // --------------------------------------------------------------------------------------

@@ -140,9 +140,9 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *                   instructions; FP32-mixed only, FP64 contexts run path 1)
  *   xline_rows   rows per CTA of the two-step x-line kernel: 2, 4 or 8
  *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
- *   solve_kind   1: thread-per-column Thomas sweeps, 2: warp-per-column substitutions on
- *                LU factors precomputed per time step
- *   solve_cols   columns (warps) per CTA of the warp-per-column solve: 1, 2, 4 or 8
+ *   solve_kind   1: thread-per-column Thomas sweeps (the only kind; other values fall back
+ *                to it)
+ *   solve_cols   reported as 0 (kept so that the structure's layout stays fixed)
  *   rhs_chunk    y-planes per thread of the right-hand-side kernel: 2 .. 64
  *   xsplit       radix order of the x-line transforms (x-line path 1): 1 = the split
  *                N = N1*N2 of 64 = 8*8, 96 = 8*12, 128 = 8*16, 192 = 16*12, 384 = 16*24,

@@ -12,12 +12,10 @@ DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "sol
 
 def fake_model(calls, bad=()):
     """Seconds per step: a separable cost with its minimum at xline_rows 4, zlines 16,
-    rhs_chunk 4, the transposed x split and the default z split; path 2 is slow, warp solves
-    are slow; shapes in `bad` raise."""
+    rhs_chunk 4, the transposed x split and the default z split; path 2 is slow; shapes in
+    `bad` raise."""
     def time_step(setup, precision, device, tuning, steps=5, warmup=2):
         eff = dict(DEFAULT, **(tuning or {}))
-        if eff["solve_kind"] == 1:
-            eff["solve_cols"] = 0          # the library reports no CTA width for the sweep
         if eff["xline_path"] != 1:
             eff["xsplit"] = eff["zsplit"] = 1  # the splits act on path 1 only
         for k, v in bad:
@@ -28,7 +26,6 @@ def fake_model(calls, bad=()):
         t += {1: 0.0, 2: 3.0, 3: 0.5, 4: 0.8}[eff["xline_path"]]
         t += {2: 0.4, 4: 0.0, 8: 0.2}[eff["xline_rows"]]
         t += {4: 0.5, 8: 0.3, 16: 0.0}[eff["zlines"]]
-        t += 0.0 if eff["solve_kind"] == 1 else 0.7
         t += {2: 0.2, 4: 0.0, 8: 0.1, 16: 0.3}[eff["rhs_chunk"]]
         t += {1: 0.1, 2: 0.0}[eff["xsplit"]] + {1: 0.0, 2: 0.2}[eff["zsplit"]]
         return t * 1e-3, eff

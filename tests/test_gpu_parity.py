@@ -254,32 +254,6 @@ def test_stockham_nonlinear_path(torch_cuda, monkeypatch, ng1, ng2, ny):
         g.close()
 
 
-@pytest.mark.parametrize("ng1,ng2,ny", [(24, 18, 17), (96, 192, 13), (24, 18, 129), (24, 18, 257), (24, 18, 385)])
-def test_warp_column_solves(torch_cuda, monkeypatch, ng1, ng2, ny):
-    """The warp-per-column Helmholtz solves, LU factors composed by warp scans
-    (CFD_SOLVE_WARP=1), stage by stage and over a dt change, against the oracle (FP64,
-    1e-11 / 1e-10); the sizes put 1, 6, 11 and 16 rows on a lane (every row bound)."""
-    from cfd_b200.channel import build_channel
-    from cfd_b200.config import tiny
-    monkeypatch.setenv("CFD_SOLVE_WARP", "1")
-    s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=7 * ng1 + ng2))
-    g, o = make(s), oracle(s)
-    for krk in (1, 2, 3):
-        for stage in STAGES:
-            getattr(g, stage)(krk)
-            getattr(o, stage)(krk)
-        for k in ("u1", "u2", "u3", "p"):
-            e = rel(g.download(k), o.download(k))
-            assert e < 1e-11, (krk, k, e)
-    for ch in (g, o):
-        ch.set_dt(0.7 * s.dt)
-        ch.step(2)
-    a, b = g.download_state(), o.download_state()
-    for k in a:
-        assert rel(a[k], b[k]) < 1e-10, k
-    g.close()
-
-
 @pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
 def test_packed_xline_path(torch_cuda, monkeypatch, ng1, ng2, ny):
     """The packed x-line kernel (1.5 inverse lines per row, CFD_XLINE_PATH=3) on every
