@@ -4,8 +4,8 @@ context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
 Candidates: the x-line path (register two-step; the same with 1.5 complex lines per row;
 the same on packed FP32 line pairs; or shared-memory Stockham), rows per CTA of the two-step
 x-line kernel, lines per CTA of the two-step z kernels, the radix order of the x and z
-two-step transforms (N = N1*N2 or N2*N1: which register DFT runs first), and the y-planes
-per thread of the right-hand-side kernel.
+two-step transforms (N = N1*N2 or N2*N1: which register DFT runs first), the y-planes
+per thread of the right-hand-side kernel, and the threads per CTA of the column sweeps.
 The search is coordinate-wise from the library default, one knob at a time, so it costs a
 dozen short timings.  Results are cached in a JSON file keyed by grid, precision and GPU
 name (CFD_TUNE_CACHE, default ~/.cache/cfd_b200/tuning.json).
@@ -16,7 +16,7 @@ import json
 import os
 
 KNOBS = (("xline_path", (1, 2, 3, 4)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
-         ("xsplit", (1, 2)), ("zsplit", (1, 2)), ("rhs_chunk", (2, 4, 8, 16)))
+         ("xsplit", (1, 2)), ("zsplit", (1, 2)), ("rhs_chunk", (2, 4, 8, 16)), ("solve_cols", (64, 128, 256)))
 
 
 # knobs that only act with another setting (the library reports them as 0 or 1 otherwise)
@@ -32,7 +32,7 @@ def _cache_path() -> str:
 
 def _key(setup, precision: str, gpu: str) -> str:
     c, g = setup.cfg, setup.grid
-    return f"v6|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+    return f"v7|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
 
 
 def time_step(setup, precision, device, tuning, steps=5, warmup=2):

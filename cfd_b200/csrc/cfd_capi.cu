@@ -80,6 +80,8 @@ struct cfd_ctx {
     double* cs = nullptr;
     double* cs_v = nullptr;
     int JC = 16;
+    int SNT = 256;          // threads per CTA of the column sweeps (k_solve_uvw, k_solve_p)
+    bool PAIR = true;       // IB round trip + solve of the u/w and v grids as two graph branches
     int nch = 1;
     double* scal = nullptr;
     double* mf_work = nullptr;
@@ -739,8 +741,8 @@ int ib_all(cfd_ctx* c) {
 // (0 = u/w, 1 = v).
 int launch_solve(cfd_ctx* c, cudaStream_t st, double beta, int part0, int nsys) {
     const Dims& d = c->d;
-    const dim3 gb((d.ncol + 255) / 256, nsys);
-    k_solve_uvw<<<gb, 256, 0, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v,
+    const dim3 gb((d.ncol + c->SNT - 1) / c->SNT, nsys);
+    k_solve_uvw<<<gb, c->SNT, 0, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v,
                                     part0);
     return launched(c, "k_solve_uvw");
 }
@@ -753,7 +755,7 @@ int solve_kernel(cfd_ctx* c, int krk);
 
 template <typename T2>
 int ib_solve_all(cfd_ctx* c, int krk) {
-    const bool par = c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling && !c->mb;
+    const bool par = c->PAIR && c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling && !c->mb;
     if (!par) {
         int s = ib_all<T2>(c);
         if (s != CFD_OK) return s;
@@ -813,8 +815,9 @@ int solvep_kernel(cfd_ctx* c, int krk, bool with_div) {
         LK("k_mb_solve_p");
         return CFD_OK;
     }
-    k_solve_p<false><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi,
-                                                with_div ? c->div : nullptr, c->cs, c->mean_diag, 0.0);
+    const dim3 gp((d.ncol + c->SNT - 1) / c->SNT);
+    k_solve_p<false><<<gp, c->SNT, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi,
+                                                   with_div ? c->div : nullptr, c->cs, c->mean_diag, 0.0);
     LK("k_solve_p");
     return CFD_OK;
 }
@@ -859,8 +862,9 @@ int substep(cfd_ctx* c, int krk) {
         LK("k_mb_solve_p_vcorr");
         return CFD_OK;
     }
-    k_solve_p<true><<<gb, 256, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, nullptr, c->cs,
-                                               c->mean_diag, dtrk);
+    const dim3 gp((d.ncol + c->SNT - 1) / c->SNT);
+    k_solve_p<true><<<gp, c->SNT, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, nullptr,
+                                                  c->cs, c->mean_diag, dtrk);
     LK("k_solve_p_vcorr");
     return CFD_OK;
 }
@@ -1260,6 +1264,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     AL(c->cs, double, nc * nyu);
     AL(c->cs_v, double, nc * nyv);
     c->JC = tune_int(&cfd_tuning::rhs_chunk, "CFD_RHS_CHUNK", 4, 2, 64);
+    c->SNT = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_THREADS", 256, 32, 256));
+    c->PAIR = env_int("CFD_IB_PAIR", 1, 0, 1) != 0;
     c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;
     AL(c->scal, double, 4);
     AL(c->mf_work, double, 4 * (size_t)(cfg->ny + 4));
@@ -1474,7 +1480,7 @@ int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
     t->xline_rows = c->RW4 ? c->RW4 : (c->RW2 ? c->RW2 : 0);
     t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
     t->solve_kind = 1;
-    t->solve_cols = 0;
+    t->solve_cols = c->SNT;
     t->rhs_chunk = c->JC;
     t->xsplit = c->XALT ? 2 : 1;
     t->zsplit = c->ZALT ? 2 : 1;

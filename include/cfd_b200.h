@@ -142,7 +142,8 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
  *   solve_kind   1: thread-per-column Thomas sweeps (the only kind; other values fall back
  *                to it)
- *   solve_cols   reported as 0 (kept so that the structure's layout stays fixed)
+ *   solve_cols   threads (columns) per CTA of the column sweeps k_solve_uvw and k_solve_p:
+ *                32, 64, 128 or 256
  *   rhs_chunk    y-planes per thread of the right-hand-side kernel: 2 .. 64
  *   xsplit       radix order of the x-line transforms (x-line path 1): 1 = the split
  *                N = N1*N2 of 64 = 8*8, 96 = 8*12, 128 = 8*16, 192 = 16*12, 384 = 16*24,

@@ -20,7 +20,7 @@ def torch_cuda():
 
 SHAPES = [dict(xline_path=2), dict(xline_path=1, xline_rows=2, zlines=4), dict(xline_path=3),
           dict(xline_path=3, xline_rows=2, rhs_chunk=16),
-          dict(xline_rows=4, zlines=8), dict(xsplit=2, zsplit=2)]
+          dict(xline_rows=4, zlines=8, solve_cols=64), dict(xsplit=2, zsplit=2, solve_cols=32)]
 
 
 def rel(a, b):
