@@ -80,8 +80,7 @@ struct cfd_ctx {
     double* cs = nullptr;
     double* cs_v = nullptr;
     int JC = 16;
-    int SNT = 256;          // threads per CTA of the column sweeps (k_solve_uvw, k_solve_p)
-    bool PAIR = true;       // IB round trip + solve of the u/w and v grids as two graph branches
+    int SNT = 64;           // threads per CTA of the column sweeps (k_solve_uvw, k_solve_p)
     int nch = 1;
     double* scal = nullptr;
     double* mf_work = nullptr;
@@ -747,38 +746,18 @@ int launch_solve(cfd_ctx* c, cudaStream_t st, double beta, int part0, int nsys) 
     return launched(c, "k_solve_uvw");
 }
 
-// The IB round trips and the Helmholtz solves of one substep as two graph branches: the
-// v grid's round trip and v solve on the side stream while the u/w grid's round trip and
-// u/w solve run on the context stream (the two systems are independent).  Otherwise the
-// round trips, then one solve launch.
 int solve_kernel(cfd_ctx* c, int krk);
 
+// The IB round trips (u/w and v grids on two streams inside ib_all), then one solve launch
+// over both systems.  Measured at re550: running the v solve beside the u/w round trip as
+// a second graph branch split the solve into two launches of half the CTAs and lost 4.5 %
+// (FP32-mixed) and 3.8 % (FP64) of the step rate.
 template <typename T2>
 int ib_solve_all(cfd_ctx* c, int krk) {
-    const bool par = c->PAIR && c->side && c->ibu.npl > 0 && c->ibv.npl > 0 && !c->profiling && !c->mb;
-    if (!par) {
-        int s = ib_all<T2>(c);
-        if (s != CFD_OK) return s;
-        c->hx_valid = false;  // the solve changes u, v, w
-        return solve_kernel(c, krk);
-    }
-    const Dims& d = c->d;
-    const double beta = kRKb[krk - 1] * c->dt / c->re;
-    CK(cudaEventRecord(c->ev_fork, c->stream));
-    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
-    cudaStream_t main = c->stream;
-    c->stream = c->side;
-    int s = ib_grid<T2>(c, c->ibv, d.jv0, 1, c->du2, c->u2, nullptr, nullptr, c->Hib_v, c->phys_v, 2 * d.nyu, 0);
-    if (s == CFD_OK) s = launch_solve(c, c->side, beta, 1, 1);
-    c->stream = main;
-    const cudaError_t ej = cudaEventRecord(c->ev_join, c->side);  // join even after a failure
-    if (ej == cudaSuccess) cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    int s = ib_all<T2>(c);
     if (s != CFD_OK) return s;
-    CK(ej);
-    s = ib_grid<T2>(c, c->ibu, d.ju0, 2, c->du1, c->u1, c->du3, c->u3, c->Hib, c->phys, 0, d.nyu);
-    if (s != CFD_OK) return s;
-    c->hx_valid = false;
-    return launch_solve(c, c->stream, beta, 0, 1);
+    c->hx_valid = false;  // the solve changes u, v, w
+    return solve_kernel(c, krk);
 }
 
 int solve_kernel(cfd_ctx* c, int krk) {
@@ -1264,8 +1243,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     AL(c->cs, double, nc * nyu);
     AL(c->cs_v, double, nc * nyv);
     c->JC = tune_int(&cfd_tuning::rhs_chunk, "CFD_RHS_CHUNK", 4, 2, 64);
-    c->SNT = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_THREADS", 256, 32, 256));
-    c->PAIR = env_int("CFD_IB_PAIR", 1, 0, 1) != 0;
+    c->SNT = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_THREADS", 64, 32, 256));
     c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;
     AL(c->scal, double, 4);
     AL(c->mf_work, double, 4 * (size_t)(cfg->ny + 4));

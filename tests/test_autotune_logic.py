@@ -6,13 +6,13 @@ import pytest
 
 from cfd_b200 import autotune
 
-DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "solve_cols": 256, "rhs_chunk": 16,
+DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "solve_cols": 64, "rhs_chunk": 16,
            "xsplit": 1, "zsplit": 1}
 
 
 def fake_model(calls, bad=()):
     """Seconds per step: a separable cost with its minimum at xline_rows 4, zlines 16,
-    rhs_chunk 4, 64 threads per column-sweep CTA, the transposed x split and the default z
+    rhs_chunk 4, 128 threads per column-sweep CTA, the transposed x split and the default z
     split; path 2 is slow; shapes in
     `bad` raise."""
     def time_step(setup, precision, device, tuning, steps=5, warmup=2):
@@ -28,7 +28,7 @@ def fake_model(calls, bad=()):
         t += {2: 0.4, 4: 0.0, 8: 0.2}[eff["xline_rows"]]
         t += {4: 0.5, 8: 0.3, 16: 0.0}[eff["zlines"]]
         t += {2: 0.2, 4: 0.0, 8: 0.1, 16: 0.3}[eff["rhs_chunk"]]
-        t += {64: 0.0, 128: 0.05, 256: 0.1}[eff["solve_cols"]]
+        t += {64: 0.1, 128: 0.0, 256: 0.05}[eff["solve_cols"]]
         t += {1: 0.1, 2: 0.0}[eff["xsplit"]] + {1: 0.0, 2: 0.2}[eff["zsplit"]]
         return t * 1e-3, eff
     return time_step
@@ -39,7 +39,7 @@ def test_coordinate_search_finds_the_separable_minimum(monkeypatch):
     monkeypatch.setattr(autotune, "time_step", fake_model(calls))
     best, t = autotune.autotune(None, "mixed")
     assert best["xline_path"] == 1 and best["xline_rows"] == 4 and best["zlines"] == 16
-    assert best["solve_kind"] == 1 and best["rhs_chunk"] == 4 and best["solve_cols"] == 64
+    assert best["solve_kind"] == 1 and best["rhs_chunk"] == 4 and best["solve_cols"] == 128
     assert best["xsplit"] == 2 and best["zsplit"] == 1
     assert t == pytest.approx(10.0e-3)
     assert len(calls) == len(set(calls)), "a shape was timed twice"
