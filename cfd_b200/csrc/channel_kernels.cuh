@@ -1872,42 +1872,60 @@ __global__ void __launch_bounds__(256) k_vcorr(Dims d, Geo g, double dtrk, doubl
 // --------------------------------------------------------------------------------------
 __global__ void k_meanflow(Dims d, Geo g, double beta, double bdt, double qxt, int ctpress, double2* __restrict__ u1,
                            double* __restrict__ scal, double* __restrict__ work) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    // one warp: the flow-rate sums and the final update spread over the lanes (strided
+    // reads of the mean-mode column), the tridiagonal solve of the mean mode on lane 0
+    if (blockIdx.x != 0) return;
+    const int lane = threadIdx.x & 31;
     const int nn = d.ny - 2;
     auto YV = [&](int j) { return g.yv[j - d.jv0]; };
+    auto wsum = [](double v) {
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    };
     double Qx0 = 0.0;
-    for (int j = 1; j <= nn + 1; ++j) Qx0 += (YV(j) - YV(j - 1)) * u1[(size_t)(j - d.ju0) * d.ncol].x;
-    if (ctpress == 1) { scal[1] = Qx0; return; }
+    for (int j = 1 + lane; j <= nn + 1; j += 32) Qx0 += (YV(j) - YV(j - 1)) * u1[(size_t)(j - d.ju0) * d.ncol].x;
+    Qx0 = wsum(Qx0);
+    if (ctpress == 1) {
+        if (lane == 0) scal[1] = Qx0;
+        return;
+    }
     const int n = nn + 3;
     double* a1 = work;
     double* a2 = work + n;
     double* a3 = work + 2 * n;
     double* x = work + 3 * n;
-    a1[0] = 0.0; a2[0] = 1.0; a3[0] = g.gwb;
-    for (int j = 1; j <= nn + 1; ++j) {
+    for (int j = 1 + lane; j <= nn + 1; j += 32) {
         const int jj = j - d.ju0;
         a1[j] = -beta * g.dyu2i[3 * jj + 0];
         a2[j] = 1.0 - beta * g.dyu2i[3 * jj + 1];
         a3[j] = -beta * g.dyu2i[3 * jj + 2];
     }
-    a1[nn + 2] = g.gwt; a2[nn + 2] = 1.0; a3[nn + 2] = 0.0;
-    a2[0] = 1.0 / a2[0];
-    for (int j = 1; j < n; ++j) {
-        a3[j - 1] = a3[j - 1] * a2[j - 1];
-        a2[j] = 1.0 / (a2[j] - a1[j] * a3[j - 1]);
+    __syncwarp();
+    if (lane == 0) {
+        a1[0] = 0.0; a2[0] = 1.0; a3[0] = g.gwb;
+        a1[nn + 2] = g.gwt; a2[nn + 2] = 1.0; a3[nn + 2] = 0.0;
+        a2[0] = 1.0 / a2[0];
+        for (int j = 1; j < n; ++j) {
+            a3[j - 1] = a3[j - 1] * a2[j - 1];
+            a2[j] = 1.0 / (a2[j] - a1[j] * a3[j - 1]);
+        }
+        x[0] = 0.0 * a2[0];
+        for (int j = 1; j < n; ++j) {
+            const double rj = (j <= nn + 1) ? bdt : 0.0;
+            x[j] = (rj - a1[j] * x[j - 1]) * a2[j];
+        }
+        for (int j = n - 2; j >= 0; --j) x[j] = x[j] - a3[j] * x[j + 1];
     }
-    x[0] = 0.0 * a2[0];
-    for (int j = 1; j < n; ++j) {
-        const double rj = (j <= nn + 1) ? bdt : 0.0;
-        x[j] = (rj - a1[j] * x[j - 1]) * a2[j];
-    }
-    for (int j = n - 2; j >= 0; --j) x[j] = x[j] - a3[j] * x[j + 1];
+    __syncwarp();
     double Qx1 = 0.0;
-    for (int j = 1; j <= nn + 1; ++j) Qx1 += (YV(j) - YV(j - 1)) * x[j];
+    for (int j = 1 + lane; j <= nn + 1; j += 32) Qx1 += (YV(j) - YV(j - 1)) * x[j];
+    Qx1 = wsum(Qx1);
     const double gg = (qxt - Qx0) / Qx1;
-    scal[0] = scal[0] + gg;
-    scal[2] = gg;
-    for (int j = 0; j <= nn + 2; ++j) u1[(size_t)(j - d.ju0) * d.ncol].x += gg * x[j];
+    if (lane == 0) {
+        scal[0] = scal[0] + gg;
+        scal[2] = gg;
+    }
+    for (int j = lane; j <= nn + 2; j += 32) u1[(size_t)(j - d.ju0) * d.ncol].x += gg * x[j];
 }
 
 // --------------------------------------------------------------------------------------
