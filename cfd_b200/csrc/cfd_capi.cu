@@ -81,7 +81,6 @@ struct cfd_ctx {
     double* cs_v = nullptr;
     int JC = 16;
     int SNT = 64;           // threads per CTA of the column sweeps (k_solve_uvw, k_solve_p)
-    bool PDL = true;        // programmatic dependent launches along the step's kernel chain
     int nch = 1;
     double* scal = nullptr;
     double* mf_work = nullptr;
@@ -247,27 +246,6 @@ int dalloc(cfd_ctx* c, T** p, size_t n) {
     } while (0)
 
 size_t zsmem(int n, int CH, size_t esz) { return (size_t)(2 * n * CH + n) * esz; }
-
-// Kernel launch with programmatic stream serialisation when pdl (the kernel starts with
-// pdl_entry): its CTAs may be scheduled while its predecessor in the stream drains.  Errors
-// surface through cudaGetLastError like those of a <<<>>> launch.
-template <typename... KArgs, typename... Args>
-void launch_k(bool pdl, void (*kern)(KArgs...), dim3 g, dim3 b, size_t sm, cudaStream_t st, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = g;
-    cfg.blockDim = b;
-    cfg.dynamicSmemBytes = sm;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, kern, args...);
-}
-// programmatic launches in captured or direct stream order, not under the per-kernel
-// profiler (its events sit between the kernels)
-bool pdl_on(const cfd_ctx* c) { return c->PDL && !c->profiling; }
 
 int ilog2(int b) {
     int s = 0;
@@ -522,8 +500,8 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gz2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 3);
         bool ok = true;
         TWO_SWITCH_SEL(c->ZALT, d.ngal2, ok, {
-            launch_k(pdl_on(c), k_zinv2s<T2, TN1, TN2>, gz2, dim3(c->NTZN), c->SMZN, c->stream, d, c->u1, c->u2,
-                     c->u3, (T2*)c->Hx, twz<T2>(c), c->LZ2);
+            k_zinv2s<T2, TN1, TN2><<<gz2, c->NTZN, c->SMZN, c->stream>>>(d, c->u1, c->u2, c->u3, (T2*)c->Hx,
+                                                                      twz<T2>(c), c->LZ2);
         });
         LK("k_zinv2s");
         c->hx_valid = true;
@@ -574,9 +552,9 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
         TWO_SWITCH_SEL(c->XALT, d.ngal1, ok, {
-            launch_k(pdl_on(c), k_xline2<T2, TN1, TN2>, gx2, dim3(c->NT2), c->SM2, c->stream, d, c->g,
-                     (const T2*)c->Hx, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], twx<T2>(c), c->RW2,
-                     ilog2(c->RW2));
+            k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0],
+                                                                    (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
+                                                                    twx<T2>(c), c->RW2, ilog2(c->RW2));
         });
         LK("k_xline2");
     } else {
@@ -593,9 +571,9 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gf2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 4, 2);
         bool ok = true;
         TWO_SWITCH_SEL(c->ZALT, d.ngal2, ok, {
-            launch_k(pdl_on(c), k_zfwd2<T2, TN1, TN2>, gf2, dim3(c->NTZN), c->SMZN, c->stream, d, (T2*)c->H[0],
-                     (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
-                     (T2*)c->S[3], twz<T2>(c), c->LZ2);
+            k_zfwd2<T2, TN1, TN2><<<gf2, c->NTZN, c->SMZN, c->stream>>>(
+                d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
+                (T2*)c->S[3], twz<T2>(c), c->LZ2);
         });
         LK("k_zfwd2");
     } else {
@@ -624,9 +602,9 @@ int rhs_kernel(cfd_ctx* c, int krk) {
         return CFD_OK;
     }
     gb.y = c->nch;
-    launch_k(pdl_on(c), k_rhs<T2, MODE>, gb, dim3(256), 0, c->stream, d, c->g, coef(c, krk), c->scal, c->u1, c->u2,
-             c->u3, c->p, (T2*)c->Nu1, (T2*)c->Nu2, (T2*)c->Nu3, c->du1, c->du2, c->du3, (const T2*)c->S[0],
-             (const T2*)c->S[1], (const T2*)c->S[2], (const T2*)c->S[3], c->JC);
+    k_rhs<T2, MODE><<<gb, 256, 0, c->stream>>>(d, c->g, coef(c, krk), c->scal, c->u1, c->u2, c->u3, c->p, (T2*)c->Nu1,
+                                               (T2*)c->Nu2, (T2*)c->Nu3, c->du1, c->du2, c->du3, (const T2*)c->S[0],
+                                               (const T2*)c->S[1], (const T2*)c->S[2], (const T2*)c->S[3], c->JC);
     LK("k_rhs");
     return CFD_OK;
 }
@@ -671,8 +649,9 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         bool ok = true;
         if (ib.nact > 0) {
             TWO_SWITCH(d.ngal1, ok, {
-                launch_k(pdl_on(c), k_ib_xinv2<T2, TN1, TN2>, g2, dim3(c->NTIX2), c->SMIX2, c->stream, d,
-                         (const T2*)Hib, ib.npl, (R*)phys, ib.arow, ib.nact, twx<T2>(c), c->RWIX2, vel);
+                k_ib_xinv2<T2, TN1, TN2><<<g2, c->NTIX2, c->SMIX2, c->stream>>>(d, (T2*)Hib, ib.npl, (R*)phys,
+                                                                              ib.arow, ib.nact, twx<T2>(c), c->RWIX2,
+                                                                              vel);
             });
             LK("k_ib_xinv2");
         }
@@ -687,8 +666,7 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
     if (ib.n > 0) {
         dim3 g3((ib.n + 255) / 256, nb);
         prof_mark(c);
-        launch_k(pdl_on(c), k_ib_force<R>, g3, dim3(256), 0, c->stream, d, ib.idx, ib.w, ib.n, ib.slot_of_j, j0,
-                 ib.npl, (R*)phys);
+        k_ib_force<R><<<g3, 256, 0, c->stream>>>(d, ib.idx, ib.w, ib.n, ib.slot_of_j, j0, ib.npl, (R*)phys);
         LK("k_ib_force");
     }
     prof_mark(c);
@@ -697,8 +675,8 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         bool ok = true;
         if (ib.nact > 0) {
             TWO_SWITCH(d.ngal1, ok, {
-                launch_k(pdl_on(c), k_ib_xfwd2<T2, TN1, TN2>, g4, dim3(c->NTFX2), c->SMFX2, c->stream, d,
-                         (T2*)Hib, ib.npl, (const R*)phys, ib.arow, ib.nact, twx<T2>(c), c->RWFX2);
+                k_ib_xfwd2<T2, TN1, TN2><<<g4, c->NTFX2, c->SMFX2, c->stream>>>(
+                    d, (T2*)Hib, ib.npl, (const R*)phys, ib.arow, ib.nact, twx<T2>(c), c->RWFX2);
             });
             LK("k_ib_xfwd2");
         }
@@ -716,9 +694,9 @@ int ib_grid(cfd_ctx* c, const IBDev& ib, int j0, int nb, double2* rhs_a, double2
         dim3 g5((ib.npl * d.nkx + CH2 - 1) / CH2, 1, nb);
         bool ok = true;
         TWO_SWITCH(d.ngal2, ok, {
-            launch_k(pdl_on(c), k_ib_zfwd2<T2, TN1, TN2>, g5, dim3(c->NTZ2), c->SMZ2, c->stream, d, (const T2*)Hib,
-                     ib.npl, dst, j0, ib.planes, c->RWIX2 ? ib.rowflag : (const unsigned char*)nullptr,
-                     twz<T2>(c), c->LZ2);
+            k_ib_zfwd2<T2, TN1, TN2><<<g5, c->NTZ2, c->SMZ2, c->stream>>>(d, (const T2*)Hib, ib.npl, dst, j0,
+                                                                        ib.planes, c->RWIX2 ? ib.rowflag : nullptr,
+                                                                        twz<T2>(c), c->LZ2);
         });
         LK("k_ib_zfwd2");
     } else {
@@ -800,8 +778,7 @@ int meanflow_kernel(cfd_ctx* c, int krk) {
     const double beta = kRKb[krk - 1] * c->dt / c->re;
     const double bdt = -kRKd[krk - 1] * c->dt;
     prof_mark(c);
-    launch_k(pdl_on(c), k_meanflow, dim3(1), dim3(32), 0, c->stream, c->d, c->g, beta, bdt, c->qxt, c->ctpress,
-             c->u1, c->scal, c->mf_work);
+    k_meanflow<<<1, 32, 0, c->stream>>>(c->d, c->g, beta, bdt, c->qxt, c->ctpress, c->u1, c->scal, c->mf_work);
     LK("k_meanflow");
     return CFD_OK;
 }
@@ -865,8 +842,8 @@ int substep(cfd_ctx* c, int krk) {
         return CFD_OK;
     }
     const dim3 gp((d.ncol + c->SNT - 1) / c->SNT);
-    launch_k(pdl_on(c), k_solve_p<true>, gp, dim3(c->SNT), 0, c->stream, d, c->g, dtirk, c->u1, c->u2, c->u3, c->p,
-             c->psi, (double2*)nullptr, c->cs, c->mean_diag, dtrk);
+    k_solve_p<true><<<gp, c->SNT, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, nullptr,
+                                                  c->cs, c->mean_diag, dtrk);
     LK("k_solve_p_vcorr");
     return CFD_OK;
 }
@@ -1267,7 +1244,6 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     AL(c->cs_v, double, nc * nyv);
     c->JC = tune_int(&cfd_tuning::rhs_chunk, "CFD_RHS_CHUNK", 4, 2, 64);
     c->SNT = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_THREADS", 64, 32, 256));
-    c->PDL = env_int("CFD_PDL", 1, 0, 1) != 0;
     c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;
     AL(c->scal, double, 4);
     AL(c->mf_work, double, 4 * (size_t)(cfg->ny + 4));

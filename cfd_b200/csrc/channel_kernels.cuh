@@ -47,16 +47,6 @@ __device__ __forceinline__ size_t scol(const Dims& d, int i, int q) {
 }
 
 // Grid and wavenumber tables on the device (array index = j - j0 of the grid).
-// Programmatic dependent launch: a kernel launched with programmatic stream serialisation
-// may be scheduled while its predecessor in the stream drains.  pdl_entry() lets the next
-// kernel be scheduled early (its CTAs wait in their own pdl_entry) and then waits until
-// the predecessor grid has completed and its writes are visible, so everything after it
-// reads the predecessor's results.  For an ordinary launch both instructions return at once.
-__device__ __forceinline__ void pdl_entry() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-
 struct Geo {
     const double* yu;
     const double* yv;
@@ -296,7 +286,6 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 template <typename T2, int N1, int N2>
 __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && (N1 > N2 ? N1 : N2) <= 24) ? 2 : 1) k_xline2(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
-    pdl_entry();
     using R = decltype(T2::x);
     constexpr int N = N1 * N2;
     constexpr int HX = N / 3;               // highest retained kx
@@ -960,7 +949,6 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
 template <typename T2, int TN1, int TN2>
 __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zinv2s(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
                          const double2* __restrict__ u3, T2* __restrict__ Hx, const T2* __restrict__ twz, int lb) {
-    pdl_entry();
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     const int f = blockIdx.y;
@@ -995,7 +983,6 @@ template <typename T2, int TN1, int TN2>
 __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zfwd2(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
                         const T2* __restrict__ H3, T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
                         T2* __restrict__ S3, const T2* __restrict__ twz, int lb) {
-    pdl_entry();
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     const int grp = blockIdx.z, f = blockIdx.y;
@@ -1058,7 +1045,6 @@ __global__ void __launch_bounds__(256, sizeof(T2) == 8 ? 3 : 0) k_rhs(Dims d, Ge
                                              double2* __restrict__ du3, const T2* __restrict__ S0,
                                              const T2* __restrict__ S1, const T2* __restrict__ S2,
                                              const T2* __restrict__ S3, int JC) {
-    pdl_entry();
     // one thread = one column and a chunk of JC planes (blockIdx.y); no recurrence in y
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
@@ -1273,7 +1259,6 @@ __global__ void __launch_bounds__(256) k_ib_xinv(Dims d, const T2* __restrict__ 
 template <typename R>
 __global__ void k_ib_force(Dims d, const int* __restrict__ idx, const double* __restrict__ w, int npts,
                            const int* __restrict__ slot_of_j, int j0, int npl, R* __restrict__ phys) {
-    pdl_entry();
     const int pt = blockIdx.x * blockDim.x + threadIdx.x;
     if (pt >= npts) return;
     const int fb = blockIdx.y;
@@ -1368,7 +1353,6 @@ __global__ void __launch_bounds__(256) k_ib_zfwd(Dims d, const T2* __restrict__ 
 template <typename T2, int TN1, int TN2>
 __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_ib_zinv2(Dims d, IBSrc src, int j0, const int* __restrict__ planes, int npl, T2* __restrict__ Hib,
                            const T2* __restrict__ twz, int lb, int sstep) {
-    pdl_entry();
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     const int nlines = npl * d.nkx;
@@ -1411,7 +1395,6 @@ struct IBVel {
 template <typename T2, int TN1, int TN2>
 __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype(T2::x)* __restrict__ phys,
                            const int* __restrict__ arow, int nact, const T2* __restrict__ twx, int RW, IBVel vel) {
-    pdl_entry();
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     constexpr int HX = N / 3;   // highest retained kx (N1 = 2*(Ngal1/3))
@@ -1467,7 +1450,6 @@ __global__ void k_ib_xinv2(Dims d, const T2* __restrict__ Hib, int npl, decltype
 template <typename T2, int TN1, int TN2>
 __global__ void k_ib_xfwd2(Dims d, T2* __restrict__ Hib, int npl, const decltype(T2::x)* __restrict__ phys,
                            const int* __restrict__ arow, int nact, const T2* __restrict__ twx, int RW) {
-    pdl_entry();
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     constexpr int LU = N + 1;
@@ -1506,7 +1488,6 @@ template <typename T2, int TN1, int TN2>
 __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_ib_zfwd2(Dims d, const T2* __restrict__ Hib, int npl, IBDst dst, int j0,
                            const int* __restrict__ planes, const unsigned char* __restrict__ rowflag,
                            const T2* __restrict__ twz, int lb) {
-    pdl_entry();
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
     const int nlines = npl * d.nkx;
@@ -1555,7 +1536,6 @@ __global__ void __launch_bounds__(256) k_solve_uvw(Dims d, Geo g, double beta, d
                                                    const double2* __restrict__ r1, const double2* __restrict__ r2,
                                                    const double2* __restrict__ r3, double* __restrict__ cs_uw,
                                                    double* __restrict__ cs_v, int part0) {
-    pdl_entry();
     // blockIdx.y + part0: 0 = the u/w systems, 1 = the v system
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
@@ -1680,7 +1660,6 @@ __global__ void __launch_bounds__(256) k_solve_p(Dims d, Geo g, double dtirk, do
                                                  double2* __restrict__ p, double2* __restrict__ psi,
                                                  double2* __restrict__ divo, double* __restrict__ cs, double mean_diag,
                                                  double dtrk) {
-    pdl_entry();
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
     const int i = col % d.nkx, q = col / d.nkx;
@@ -1893,7 +1872,6 @@ __global__ void __launch_bounds__(256) k_vcorr(Dims d, Geo g, double dtrk, doubl
 // --------------------------------------------------------------------------------------
 __global__ void k_meanflow(Dims d, Geo g, double beta, double bdt, double qxt, int ctpress, double2* __restrict__ u1,
                            double* __restrict__ scal, double* __restrict__ work) {
-    pdl_entry();
     // one warp: the flow-rate sums and the final update spread over the lanes (strided
     // reads of the mean-mode column), the tridiagonal solve of the mean mode on lane 0
     if (blockIdx.x != 0) return;
