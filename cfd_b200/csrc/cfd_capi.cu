@@ -86,6 +86,12 @@ struct cfd_ctx {
     double* mf_work = nullptr;
     double2* stage0 = nullptr;
     double2* stage1 = nullptr;
+    // reference-layout transfers of u, v, w, p: one staging buffer per field, host-to-device
+    // copies on xin, device-to-host copies on xout, ordered per field by xev (allocated at
+    // the first such transfer)
+    double2* xstage[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t xin = nullptr, xout = nullptr;
+    cudaEvent_t xev[4] = {nullptr, nullptr, nullptr, nullptr};
     double* part = nullptr;
     int npart = 0;
     IBDev ibu, ibv;
@@ -1471,7 +1477,13 @@ int cfd_destroy(cfd_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     destroy_graph(c);
     if (c->side) cudaStreamSynchronize(c->side);
+    if (c->xin) cudaStreamSynchronize(c->xin);
+    if (c->xout) cudaStreamSynchronize(c->xout);
     for (void* p : c->allocs) cudaFree(p);
+    for (int f = 0; f < 4; ++f)
+        if (c->xev[f]) cudaEventDestroy(c->xev[f]);
+    if (c->xin) cudaStreamDestroy(c->xin);
+    if (c->xout) cudaStreamDestroy(c->xout);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->side) cudaStreamDestroy(c->side);
@@ -1508,6 +1520,29 @@ int cfd_field_shape(const cfd_ctx* c, int32_t field, int64_t* ncomplex, int32_t*
     return CFD_OK;
 }
 
+// Staging buffer, copy streams and ordering event of a reference-layout transfer of u, v, w
+// or p.  With them an upload of a field only waits for the download that last used its
+// buffer, so the uploads of the next step run while the downloads of the other fields of
+// this step are still in flight (the two directions of the host link at once).
+int xfer_ready(cfd_ctx* c, int field) {
+    if (!c->xin) {
+        CK(cudaStreamCreateWithFlags(&c->xin, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->xout, cudaStreamNonBlocking));
+    }
+    if (!c->xstage[field]) {
+        FieldInfo fi;
+        field_info(c, field, fi);
+        const size_t n = (size_t)fi.nplanes * c->d.ncol;
+        double2* p = nullptr;
+        CK(cudaMalloc(&p, n * sizeof(double2)));
+        c->allocs.push_back(p);
+        c->xstage[field] = p;
+        CK(cudaEventCreateWithFlags(&c->xev[field], cudaEventDisableTiming));
+        CK(cudaEventRecord(c->xev[field], c->stream));
+    }
+    return CFD_OK;
+}
+
 int cfd_upload_field(cfd_ctx* c, int32_t field, const double* host, int32_t layout) {
     if (!c || !host) return fail(c, CFD_ERR_ARG, "null argument");
     FieldInfo fi;
@@ -1516,6 +1551,23 @@ int cfd_upload_field(cfd_ctx* c, int32_t field, const double* host, int32_t layo
     CK(cudaSetDevice(c->device));
     if (field <= CFD_FIELD_U3) c->hx_valid = false;  // the nonlinear pass's transforms are stale
     const size_t n = (size_t)fi.nplanes * c->d.ncol;
+    if (layout == CFD_LAYOUT_REF && field <= CFD_FIELD_P && !fi.single) {
+        int s = xfer_ready(c, field);
+        if (s != CFD_OK) return s;
+        // the copy waits for the previous use of this field's staging buffer (the download
+        // that last read it), the transpose on the context stream for the copy
+        CK(cudaStreamWaitEvent(c->xin, c->xev[field], 0));
+        CK(cudaMemcpyAsync(c->xstage[field], host, n * sizeof(double2), cudaMemcpyHostToDevice, c->xin));
+        CK(cudaEventRecord(c->xev[field], c->xin));
+        CK(cudaStreamWaitEvent(c->stream, c->xev[field], 0));
+        dim3 grid((fi.nplanes + 31) / 32, (c->d.ncol + 31) / 32);
+        prof_mark(c);
+        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(c->xstage[field], (double2*)fi.ptr, c->d.ncol, fi.nplanes);
+        LK("k_transpose");
+        CK(cudaEventRecord(c->xev[field], c->stream));
+        c->state_loaded = true;
+        return CFD_OK;
+    }
     double2* dst = fi.single ? c->stage1 : (double2*)fi.ptr;
     if (layout == CFD_LAYOUT_PLANE) {
         CK(cudaMemcpyAsync(dst, host, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
@@ -1543,6 +1595,22 @@ int cfd_download_field(cfd_ctx* c, int32_t field, double* host, int32_t layout) 
     CK(cudaSetDevice(c->device));
     const size_t n = (size_t)fi.nplanes * c->d.ncol;
     const double2* src = (const double2*)fi.ptr;
+    if (layout == CFD_LAYOUT_REF && field <= CFD_FIELD_P && !fi.single) {
+        int s = xfer_ready(c, field);
+        if (s != CFD_OK) return s;
+        CK(cudaStreamWaitEvent(c->stream, c->xev[field], 0));  // the last copy out of the buffer
+        dim3 grid((c->d.ncol + 31) / 32, (fi.nplanes + 31) / 32);
+        prof_mark(c);
+        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(src, c->xstage[field], fi.nplanes, c->d.ncol);
+        LK("k_transpose");
+        CK(cudaEventRecord(c->xev[field], c->stream));
+        CK(cudaStreamWaitEvent(c->xout, c->xev[field], 0));
+        CK(cudaMemcpyAsync(host, c->xstage[field], n * sizeof(double2), cudaMemcpyDeviceToHost, c->xout));
+        CK(cudaEventRecord(c->xev[field], c->xout));
+        // work issued later on the context stream (and its synchronisation) follows the copy
+        CK(cudaStreamWaitEvent(c->stream, c->xev[field], 0));
+        return CFD_OK;
+    }
     if (fi.single) {
         prof_mark(c);
         k_f2d<<<1024, 256, 0, c->stream>>>((const float2*)fi.ptr, c->stage1, n);
