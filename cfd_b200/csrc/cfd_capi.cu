@@ -86,12 +86,13 @@ struct cfd_ctx {
     double* mf_work = nullptr;
     double2* stage0 = nullptr;
     double2* stage1 = nullptr;
-    // reference-layout transfers of u, v, w, p: one staging buffer per field, host-to-device
-    // copies on xin, device-to-host copies on xout, ordered per field by xev (allocated at
-    // the first such transfer)
+    // reference-layout transfers of u, v, w, p: one staging buffer per field, moved in
+    // kXC column chunks, host-to-device copies on xin, device-to-host copies on xout,
+    // ordered per field and chunk by xev (allocated at the first such transfer)
+    static constexpr int kXC = 8;
     double2* xstage[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaStream_t xin = nullptr, xout = nullptr;
-    cudaEvent_t xev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t xev[4][kXC] = {};
     double* part = nullptr;
     int npart = 0;
     IBDev ibu, ibv;
@@ -1481,7 +1482,8 @@ int cfd_destroy(cfd_ctx* c) {
     if (c->xout) cudaStreamSynchronize(c->xout);
     for (void* p : c->allocs) cudaFree(p);
     for (int f = 0; f < 4; ++f)
-        if (c->xev[f]) cudaEventDestroy(c->xev[f]);
+        for (int k = 0; k < cfd_ctx::kXC; ++k)
+            if (c->xev[f][k]) cudaEventDestroy(c->xev[f][k]);
     if (c->xin) cudaStreamDestroy(c->xin);
     if (c->xout) cudaStreamDestroy(c->xout);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -1520,10 +1522,11 @@ int cfd_field_shape(const cfd_ctx* c, int32_t field, int64_t* ncomplex, int32_t*
     return CFD_OK;
 }
 
-// Staging buffer, copy streams and ordering event of a reference-layout transfer of u, v, w
-// or p.  With them an upload of a field only waits for the download that last used its
-// buffer, so the uploads of the next step run while the downloads of the other fields of
-// this step are still in flight (the two directions of the host link at once).
+// Staging buffer, copy streams and ordering events of a reference-layout transfer of u, v,
+// w or p.  A field moves in column chunks (contiguous in the f(j,column) layout), and the
+// upload of a chunk only waits for the download that last used that chunk of the buffer,
+// so the uploads of the next step run while this step's downloads are still in flight (the
+// two directions of the host link at once).
 int xfer_ready(cfd_ctx* c, int field) {
     if (!c->xin) {
         CK(cudaStreamCreateWithFlags(&c->xin, cudaStreamNonBlocking));
@@ -1537,10 +1540,19 @@ int xfer_ready(cfd_ctx* c, int field) {
         CK(cudaMalloc(&p, n * sizeof(double2)));
         c->allocs.push_back(p);
         c->xstage[field] = p;
-        CK(cudaEventCreateWithFlags(&c->xev[field], cudaEventDisableTiming));
-        CK(cudaEventRecord(c->xev[field], c->stream));
+        for (int k = 0; k < cfd_ctx::kXC; ++k) {
+            CK(cudaEventCreateWithFlags(&c->xev[field][k], cudaEventDisableTiming));
+            CK(cudaEventRecord(c->xev[field][k], c->stream));
+        }
     }
     return CFD_OK;
+}
+
+// columns [c0, c1) of transfer chunk k
+void xchunk(const cfd_ctx* c, int k, int& c0, int& c1) {
+    const int per = (c->d.ncol + cfd_ctx::kXC - 1) / cfd_ctx::kXC;
+    c0 = std::min(c->d.ncol, k * per);
+    c1 = std::min(c->d.ncol, c0 + per);
 }
 
 int cfd_upload_field(cfd_ctx* c, int32_t field, const double* host, int32_t layout) {
@@ -1554,17 +1566,26 @@ int cfd_upload_field(cfd_ctx* c, int32_t field, const double* host, int32_t layo
     if (layout == CFD_LAYOUT_REF && field <= CFD_FIELD_P && !fi.single) {
         int s = xfer_ready(c, field);
         if (s != CFD_OK) return s;
-        // the copy waits for the previous use of this field's staging buffer (the download
-        // that last read it), the transpose on the context stream for the copy
-        CK(cudaStreamWaitEvent(c->xin, c->xev[field], 0));
-        CK(cudaMemcpyAsync(c->xstage[field], host, n * sizeof(double2), cudaMemcpyHostToDevice, c->xin));
-        CK(cudaEventRecord(c->xev[field], c->xin));
-        CK(cudaStreamWaitEvent(c->stream, c->xev[field], 0));
-        dim3 grid((fi.nplanes + 31) / 32, (c->d.ncol + 31) / 32);
-        prof_mark(c);
-        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(c->xstage[field], (double2*)fi.ptr, c->d.ncol, fi.nplanes);
-        LK("k_transpose");
-        CK(cudaEventRecord(c->xev[field], c->stream));
+        for (int k = 0; k < cfd_ctx::kXC; ++k) {
+            int c0, c1;
+            xchunk(c, k, c0, c1);
+            if (c0 >= c1) continue;
+            cudaEvent_t ev = c->xev[field][k];
+            const size_t off = (size_t)c0 * fi.nplanes, m = (size_t)(c1 - c0) * fi.nplanes;
+            // the copy waits for the last download out of this chunk of the buffer, the
+            // transpose on the context stream for the copy
+            CK(cudaStreamWaitEvent(c->xin, ev, 0));
+            CK(cudaMemcpyAsync(c->xstage[field] + off, host + 2 * off, m * sizeof(double2), cudaMemcpyHostToDevice,
+                               c->xin));
+            CK(cudaEventRecord(ev, c->xin));
+            CK(cudaStreamWaitEvent(c->stream, ev, 0));
+            dim3 grid((fi.nplanes + 31) / 32, (c1 - c0 + 31) / 32);
+            prof_mark(c);
+            k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(c->xstage[field] + off, (double2*)fi.ptr + c0, c1 - c0,
+                                                             fi.nplanes, fi.nplanes, c->d.ncol);
+            LK("k_transpose");
+            CK(cudaEventRecord(ev, c->stream));
+        }
         c->state_loaded = true;
         return CFD_OK;
     }
@@ -1575,7 +1596,8 @@ int cfd_upload_field(cfd_ctx* c, int32_t field, const double* host, int32_t layo
         CK(cudaMemcpyAsync(c->stage0, host, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
         dim3 grid((fi.nplanes + 31) / 32, (c->d.ncol + 31) / 32);
         prof_mark(c);
-        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(c->stage0, dst, c->d.ncol, fi.nplanes);
+        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(c->stage0, dst, c->d.ncol, fi.nplanes, fi.nplanes,
+                                                         c->d.ncol);
         LK("k_transpose");
     }
     if (fi.single) {
@@ -1598,17 +1620,26 @@ int cfd_download_field(cfd_ctx* c, int32_t field, double* host, int32_t layout) 
     if (layout == CFD_LAYOUT_REF && field <= CFD_FIELD_P && !fi.single) {
         int s = xfer_ready(c, field);
         if (s != CFD_OK) return s;
-        CK(cudaStreamWaitEvent(c->stream, c->xev[field], 0));  // the last copy out of the buffer
-        dim3 grid((c->d.ncol + 31) / 32, (fi.nplanes + 31) / 32);
-        prof_mark(c);
-        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(src, c->xstage[field], fi.nplanes, c->d.ncol);
-        LK("k_transpose");
-        CK(cudaEventRecord(c->xev[field], c->stream));
-        CK(cudaStreamWaitEvent(c->xout, c->xev[field], 0));
-        CK(cudaMemcpyAsync(host, c->xstage[field], n * sizeof(double2), cudaMemcpyDeviceToHost, c->xout));
-        CK(cudaEventRecord(c->xev[field], c->xout));
-        // work issued later on the context stream (and its synchronisation) follows the copy
-        CK(cudaStreamWaitEvent(c->stream, c->xev[field], 0));
+        for (int k = 0; k < cfd_ctx::kXC; ++k) {
+            int c0, c1;
+            xchunk(c, k, c0, c1);
+            if (c0 >= c1) continue;
+            cudaEvent_t ev = c->xev[field][k];
+            const size_t off = (size_t)c0 * fi.nplanes, m = (size_t)(c1 - c0) * fi.nplanes;
+            CK(cudaStreamWaitEvent(c->stream, ev, 0));  // the last copy out of this chunk
+            dim3 grid((c1 - c0 + 31) / 32, (fi.nplanes + 31) / 32);
+            prof_mark(c);
+            k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(src + c0, c->xstage[field] + off, fi.nplanes, c1 - c0,
+                                                             c->d.ncol, fi.nplanes);
+            LK("k_transpose");
+            CK(cudaEventRecord(ev, c->stream));
+            CK(cudaStreamWaitEvent(c->xout, ev, 0));
+            CK(cudaMemcpyAsync(host + 2 * off, c->xstage[field] + off, m * sizeof(double2), cudaMemcpyDeviceToHost,
+                               c->xout));
+            CK(cudaEventRecord(ev, c->xout));
+            // work issued later on the context stream (and its synchronisation) follows the copy
+            CK(cudaStreamWaitEvent(c->stream, ev, 0));
+        }
         return CFD_OK;
     }
     if (fi.single) {
@@ -1622,7 +1653,8 @@ int cfd_download_field(cfd_ctx* c, int32_t field, double* host, int32_t layout) 
     } else {
         dim3 grid((c->d.ncol + 31) / 32, (fi.nplanes + 31) / 32);
         prof_mark(c);
-        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(src, c->stage0, fi.nplanes, c->d.ncol);
+        k_transpose<<<grid, dim3(32, 8), 0, c->stream>>>(src, c->stage0, fi.nplanes, c->d.ncol, c->d.ncol,
+                                                         fi.nplanes);
         LK("k_transpose");
         CK(cudaMemcpyAsync(host, c->stage0, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     }

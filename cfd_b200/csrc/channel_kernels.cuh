@@ -1931,18 +1931,19 @@ __global__ void k_meanflow(Dims d, Geo g, double beta, double bdt, double qxt, i
 // --------------------------------------------------------------------------------------
 // Layout conversion f(j,column) <-> [j][column] (32x32 tiles through shared memory).
 // --------------------------------------------------------------------------------------
-__global__ void k_transpose(const double2* __restrict__ in, double2* __restrict__ out, int rows, int cols) {
-    // in: [rows][cols] -> out: [cols][rows]
+__global__ void k_transpose(const double2* __restrict__ in, double2* __restrict__ out, int rows, int cols,
+                            int ldi, int ldo) {
+    // in: [rows][cols] with row stride ldi -> out: [cols][rows] with row stride ldo
     __shared__ double2 tile[32][33];
     const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
     for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
         const int r = by + yy, c = bx + threadIdx.x;
-        if (r < rows && c < cols) tile[yy][threadIdx.x] = in[(size_t)r * cols + c];
+        if (r < rows && c < cols) tile[yy][threadIdx.x] = in[(size_t)r * ldi + c];
     }
     __syncthreads();
     for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
         const int c = bx + yy, r = by + threadIdx.x;
-        if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][yy];
+        if (r < rows && c < cols) out[(size_t)c * ldo + r] = tile[threadIdx.x][yy];
     }
 }
 

@@ -173,11 +173,12 @@ int cfd_field_shape(const cfd_ctx *ctx, int32_t field, int64_t *ncomplex,
 /* Host <-> device copy of one field (complex(8) interleaved).  host must hold
  * ncomplex complex values in `layout` order.  Stream-ordered; call cfd_synchronize
  * before reading a downloaded buffer.  Pinned host memory makes the copy async.
- * U1, U2, U3 and P in CFD_LAYOUT_REF go through a staging buffer per field and two copy
- * streams of their own (one per direction): an upload waits only for the download that
- * last used its field's buffer, so a loop of upload / cfd_step / download without host
- * synchronisation overlaps the next step's uploads with this step's downloads.  The
- * first such transfer of a field allocates its buffer (one field's size). */
+ * U1, U2, U3 and P in CFD_LAYOUT_REF go through a staging buffer per field, in 8 column
+ * chunks, on two copy streams of their own (one per direction): the upload of a chunk
+ * waits only for the download that last used that chunk of the buffer, so a loop of
+ * upload / cfd_step / download without host synchronisation overlaps the next step's
+ * uploads with this step's downloads.  The first such transfer of a field allocates its
+ * buffer (one field's size). */
 int cfd_upload_field(cfd_ctx *ctx, int32_t field, const double *host, int32_t layout);
 int cfd_download_field(cfd_ctx *ctx, int32_t field, double *host, int32_t layout);
 /* Device pointer of a field (FP64 [j][column] complex; NU* are FP32 complex in

@@ -25,11 +25,12 @@ def pinned(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a).view(np.float64).copy()).pin_memory()
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_unsynchronised_round_trips_equal_device_steps(torch_cuda, prec):
+@pytest.mark.parametrize("prec,grid", [("fp64", (64, 96, 17)), ("mixed", (64, 96, 17)), ("fp64", (24, 18, 17))])
+def test_unsynchronised_round_trips_equal_device_steps(torch_cuda, prec, grid):
+    """(24, 18, 17) has 108 columns: transfer chunks of 14 and a last one of 10."""
     from cfd_b200.channel import Channel, build_channel
     from cfd_b200.config import tiny
-    s = build_channel(tiny(64, 96, 17, cyl_diameter=0.3, cyl_spacing=1.5, seed=21))
+    s = build_channel(tiny(*grid, cyl_diameter=0.3, cyl_spacing=1.5, seed=21))
     ref = Channel(s, device=0, precision=prec)
     ref.upload_state()
     ref.step(4)
