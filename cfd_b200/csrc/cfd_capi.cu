@@ -112,6 +112,7 @@ struct cfd_ctx {
     int RW2 = 0, NT2 = 0;
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
     bool XALT = false, ZALT = false;  // transposed two-step splits (x-line; nonlinear z kernels)
+    bool XR64 = false;      // FP32 x-line kernel held to 64 registers (k_xline2r)
     // three bands: the launch dimensions of the nonlinear pass over the bottom wall band,
     // the middle band and the top wall band; the middle band's transforms
     bool mb = false;
@@ -393,6 +394,9 @@ int set_smem_attrs(cfd_ctx* c) {
         TWO_SWITCH_SEL(c->XALT, n1, ok, {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
+            if constexpr (std::is_same<T2, float2>::value)
+                if (e == cudaSuccess && c->XR64)
+                    e = cudaFuncSetAttribute(k_xline2r<TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
         });
         TWO_SWITCH(n1, ok, {
             if (e == cudaSuccess && c->XL3)
@@ -559,9 +563,20 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
         TWO_SWITCH_SEL(c->XALT, d.ngal1, ok, {
-            k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0],
-                                                                    (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
-                                                                    twx<T2>(c), c->RW2, ilog2(c->RW2));
+            bool capped = false;
+            if constexpr (std::is_same<T2, float2>::value) {
+                if (c->XR64) {
+                    k_xline2r<TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const float2*)c->Hx,
+                                                                          (float2*)c->H[0], (float2*)c->H[1],
+                                                                          (float2*)c->H[2], (float2*)c->H[3],
+                                                                          twx<float2>(c), c->RW2, ilog2(c->RW2));
+                    capped = true;
+                }
+            }
+            if (!capped)
+                k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0],
+                                                                        (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
+                                                                        twx<T2>(c), c->RW2, ilog2(c->RW2));
         });
         LK("k_xline2");
     } else {
@@ -1176,6 +1191,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (c->LZ2 < 0) c->RW2 = 0;  // the two-step x-line kernels read the output of k_zinv2s
     if (!c->RW2) c->RW4 = 0;
     c->XALT = c->RW2 && xalt;  // (xalt implies path 1: neither k_xline3 nor k_xline4)
+    c->XR64 = c->RW2 && !c->XL3 && !c->RW4 && c->precision == CFD_PREC_MIXED && env_int("CFD_XLINE_R64", 0, 0, 1);
     if (c->RW2 && c->LZ2 >= 0 && tune_int(&cfd_tuning::zsplit, "CFD_ZSPLIT", 1, 1, 2) == 2) {
         bool ok = true;
         int n1s = 0, n2s = 0;
@@ -1206,7 +1222,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (c->mb) {
         // three bands: the per-slot interpolating z pass, the Stockham x-line kernel and the
         // two-step forward z pass, launched once per band; thread-per-column solves
-        c->RW2 = 0; c->XL3 = false; c->RW4 = 0; c->XALT = c->ZALT = false;
+        c->RW2 = 0; c->XL3 = false; c->RW4 = 0; c->XALT = c->ZALT = false; c->XR64 = false;
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(cfg->ngal2_mid, ok, { n1s = TN1; n2s = TN2; });

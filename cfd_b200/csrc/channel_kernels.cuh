@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // elements of a subsequence are zero, direct or conjugated is resolved at compile time
 // except in the two blocks that straddle a boundary.
 template <typename T2, int N1, int N2>
-__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && (N1 > N2 ? N1 : N2) <= 24) ? 2 : 1) k_xline2(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+__device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
     using R = decltype(T2::x);
     constexpr int N = N1 * N2;
@@ -469,6 +469,21 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
         da[o] = cx<T2>((Pk.x + Qc.x) * hs, (Pk.y + Qc.y) * hs);
         db[o] = cx<T2>((Pk.y - Qc.y) * hs, -(Pk.x - Qc.x) * hs);
     }
+}
+
+template <typename T2, int N1, int N2>
+__global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && (N1 > N2 ? N1 : N2) <= 24) ? 2 : 1) k_xline2(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
+                         T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
+    xline2_body<T2, N1, N2>(d, g, Hx, H0, H1, H2, H3, twx, RW, lrw);
+}
+
+// The FP32 x-line kernel held to 64 registers per thread: with 4 rows per CTA (192 threads
+// at the 24 x 16 split of 384) five CTAs fit on an SM instead of four.
+template <int N1, int N2>
+__global__ void __maxnreg__(64) k_xline2r(Dims d, Geo g, const float2* __restrict__ Hx, float2* __restrict__ H0,
+                                          float2* __restrict__ H1, float2* __restrict__ H2, float2* __restrict__ H3,
+                                          const float2* __restrict__ twx, int RW, int lrw) {
+    xline2_body<float2, N1, N2>(d, g, Hx, H0, H1, H2, H3, twx, RW, lrw);
 }
 
 // Pass 2 on packed line pairs (FP32 only).  The two lines of a row (u + i v, w + i 0) travel

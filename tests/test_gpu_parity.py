@@ -423,3 +423,25 @@ def test_transposed_splits(torch_cuda, ng1, ng2, ny):
         for k in ("u1", "u2", "u3", "p"):
             assert rel(st[k], ref[k]) < tol, (prec, k, rel(st[k], ref[k]))
         g.close()
+
+
+@pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
+@pytest.mark.parametrize("xsplit", [1, 2])
+def test_register_capped_xline(torch_cuda, monkeypatch, ng1, ng2, ny, xsplit):
+    """The FP32 x-line kernel held to 64 registers (CFD_XLINE_R64=1, k_xline2r) on every
+    two-step length and both radix orders, against the oracle after one RK3 step (FP32-mixed
+    within 1e-5 on u, v, w, p)."""
+    from cfd_b200.channel import Channel, build_channel
+    from cfd_b200.config import tiny
+    monkeypatch.setenv("CFD_XLINE_R64", "1")
+    s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=5 * ng1 + ng2))
+    o = oracle(s)
+    o.step(1)
+    ref = o.download_state()
+    g = Channel(s, device=0, precision="mixed", tuning=dict(xline_path=1, xsplit=xsplit))
+    g.upload_state()
+    g.step(1)
+    st = g.download_state()
+    for k in ("u1", "u2", "u3", "p"):
+        assert rel(st[k], ref[k]) < 1e-5, (k, rel(st[k], ref[k]))
+    g.close()
