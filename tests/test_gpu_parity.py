@@ -428,9 +428,9 @@ def test_transposed_splits(torch_cuda, ng1, ng2, ny):
 @pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
 @pytest.mark.parametrize("xsplit", [1, 2])
 def test_register_capped_xline(torch_cuda, monkeypatch, ng1, ng2, ny, xsplit):
-    """The FP32 x-line kernel held to 64 registers (CFD_XLINE_R64=1, k_xline2r) on every
-    two-step length and both radix orders, against the oracle after one RK3 step (FP32-mixed
-    within 1e-5 on u, v, w, p)."""
+    """The x-line kernel held to 64 (FP32) / 112 (FP64) registers (CFD_XLINE_R64=1,
+    k_xline2rf / k_xline2rd) on every two-step length and both radix orders, against the
+    oracle after one RK3 step (FP64 within 1e-10, FP32-mixed within 1e-5 on u, v, w, p)."""
     from cfd_b200.channel import Channel, build_channel
     from cfd_b200.config import tiny
     monkeypatch.setenv("CFD_XLINE_R64", "1")
@@ -438,10 +438,11 @@ def test_register_capped_xline(torch_cuda, monkeypatch, ng1, ng2, ny, xsplit):
     o = oracle(s)
     o.step(1)
     ref = o.download_state()
-    g = Channel(s, device=0, precision="mixed", tuning=dict(xline_path=1, xsplit=xsplit))
-    g.upload_state()
-    g.step(1)
-    st = g.download_state()
-    for k in ("u1", "u2", "u3", "p"):
-        assert rel(st[k], ref[k]) < 1e-5, (k, rel(st[k], ref[k]))
-    g.close()
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-5)):
+        g = Channel(s, device=0, precision=prec, tuning=dict(xline_path=1, xsplit=xsplit))
+        g.upload_state()
+        g.step(1)
+        st = g.download_state()
+        for k in ("u1", "u2", "u3", "p"):
+            assert rel(st[k], ref[k]) < tol, (prec, k, rel(st[k], ref[k]))
+        g.close()
