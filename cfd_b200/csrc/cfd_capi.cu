@@ -113,6 +113,7 @@ struct cfd_ctx {
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
     bool XALT = false, ZALT = false;  // transposed two-step splits (x-line; nonlinear z kernels)
     bool XR64 = false;      // x-line kernel held to 64 (FP32) / 112 (FP64) registers (k_xline2r)
+    bool ZR = false;        // FP64 nonlinear z kernels held to 112 registers (k_zinv2sd, k_zfwd2d)
     // three bands: the launch dimensions of the nonlinear pass over the bottom wall band,
     // the middle band and the top wall band; the middle band's transforms
     bool mb = false;
@@ -369,6 +370,12 @@ int set_smem_attrs(cfd_ctx* c) {
                 e = cudaFuncSetAttribute(k_zinv2s<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZN);
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_zfwd2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZN);
+            if constexpr (std::is_same<T2, double2>::value) {
+                if (e == cudaSuccess && c->ZR)
+                    e = cudaFuncSetAttribute(k_zinv2sd<TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZN);
+                if (e == cudaSuccess && c->ZR)
+                    e = cudaFuncSetAttribute(k_zfwd2d<TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SMZN);
+            }
         });
     }
     if (c->LZ2 >= 0) {
@@ -511,8 +518,17 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gz2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 3);
         bool ok = true;
         TWO_SWITCH_SEL(c->ZALT, d.ngal2, ok, {
-            k_zinv2s<T2, TN1, TN2><<<gz2, c->NTZN, c->SMZN, c->stream>>>(d, c->u1, c->u2, c->u3, (T2*)c->Hx,
-                                                                      twz<T2>(c), c->LZ2);
+            bool capped = false;
+            if constexpr (std::is_same<T2, double2>::value) {
+                if (c->ZR) {
+                    k_zinv2sd<TN1, TN2><<<gz2, c->NTZN, c->SMZN, c->stream>>>(d, c->u1, c->u2, c->u3, (double2*)c->Hx,
+                                                                            twz<double2>(c), c->LZ2);
+                    capped = true;
+                }
+            }
+            if (!capped)
+                k_zinv2s<T2, TN1, TN2><<<gz2, c->NTZN, c->SMZN, c->stream>>>(d, c->u1, c->u2, c->u3, (T2*)c->Hx,
+                                                                          twz<T2>(c), c->LZ2);
         });
         LK("k_zinv2s");
         c->hx_valid = true;
@@ -587,9 +603,20 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gf2((std::max(d.nyu, d.nyv) * d.nkx + CH2 - 1) / CH2, 4, 2);
         bool ok = true;
         TWO_SWITCH_SEL(c->ZALT, d.ngal2, ok, {
-            k_zfwd2<T2, TN1, TN2><<<gf2, c->NTZN, c->SMZN, c->stream>>>(
-                d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1], (T2*)c->S[2],
-                (T2*)c->S[3], twz<T2>(c), c->LZ2);
+            bool capped = false;
+            if constexpr (std::is_same<T2, double2>::value) {
+                if (c->ZR) {
+                    k_zfwd2d<TN1, TN2><<<gf2, c->NTZN, c->SMZN, c->stream>>>(
+                        d, (double2*)c->H[0], (double2*)c->H[1], (double2*)c->H[2], (double2*)c->H[3],
+                        (double2*)c->S[0], (double2*)c->S[1], (double2*)c->S[2], (double2*)c->S[3], twz<double2>(c),
+                        c->LZ2);
+                    capped = true;
+                }
+            }
+            if (!capped)
+                k_zfwd2<T2, TN1, TN2><<<gf2, c->NTZN, c->SMZN, c->stream>>>(
+                    d, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], (T2*)c->S[0], (T2*)c->S[1],
+                    (T2*)c->S[2], (T2*)c->S[3], twz<T2>(c), c->LZ2);
         });
         LK("k_zfwd2");
     } else {
@@ -1186,6 +1213,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (!c->RW2) c->RW4 = 0;
     c->XALT = c->RW2 && xalt;  // (xalt implies path 1: neither k_xline3 nor k_xline4)
     c->XR64 = c->RW2 && !c->XL3 && !c->RW4 && env_int("CFD_XLINE_R64", 0, 0, 1);
+    c->ZR = c->RW2 && c->precision == CFD_PREC_FP64 && env_int("CFD_Z_R112", 0, 0, 1);
     if (c->RW2 && c->LZ2 >= 0 && tune_int(&cfd_tuning::zsplit, "CFD_ZSPLIT", 1, 1, 2) == 2) {
         bool ok = true;
         int n1s = 0, n2s = 0;
@@ -1216,7 +1244,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (c->mb) {
         // three bands: the per-slot interpolating z pass, the Stockham x-line kernel and the
         // two-step forward z pass, launched once per band; thread-per-column solves
-        c->RW2 = 0; c->XL3 = false; c->RW4 = 0; c->XALT = c->ZALT = false; c->XR64 = false;
+        c->RW2 = 0; c->XL3 = false; c->RW4 = 0; c->XALT = c->ZALT = false; c->XR64 = false; c->ZR = false;
         bool ok = true;
         int n1s = 0, n2s = 0;
         TWO_SWITCH(cfg->ngal2_mid, ok, { n1s = TN1; n2s = TN2; });

@@ -978,7 +978,7 @@ __global__ void k_zinv2(Dims d, Geo g, const double2* __restrict__ u1, const dou
 // planes gives the transform of the interpolated planes (FOU3D.f90:261-308).
 // grid: x = line chunk (line = plane * nkx + kx), y = field (u, w, v).
 template <typename T2, int TN1, int TN2>
-__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zinv2s(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
+__device__ __forceinline__ void zinv2s_body(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
                          const double2* __restrict__ u3, T2* __restrict__ Hx, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
     constexpr int N = TN1 * TN2;
@@ -1009,9 +1009,15 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
     two_step_lines<T2, TN1, TN2, +1>(lb, ex, twt, load, store);
 }
 
+template <typename T2, int TN1, int TN2>
+__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zinv2s(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
+                         const double2* __restrict__ u3, T2* __restrict__ Hx, const T2* __restrict__ twz, int lb) {
+    zinv2s_body<T2, TN1, TN2>(d, u1, u2, u3, Hx, twz, lb);
+}
+
 // Pass 3: grid x = line chunk, y = field 0..3, z = group (v-planes carry fields 0, 1 only).
 template <typename T2, int TN1, int TN2>
-__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zfwd2(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
+__device__ __forceinline__ void zfwd2_body(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
                         const T2* __restrict__ H3, T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
                         T2* __restrict__ S3, const T2* __restrict__ twz, int lb) {
     using R = decltype(T2::x);
@@ -1042,6 +1048,28 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
         if (q >= 0 && live) S[scol(d, 0, q)] = cscale(v, sc);
     };
     two_step_lines<T2, TN1, TN2, -1>(lb, ex, twt, load, store);
+}
+
+template <typename T2, int TN1, int TN2>
+__global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8 && (TN1 > TN2 ? TN1 : TN2) <= 24) ? 3 : 1) k_zfwd2(Dims d, const T2* __restrict__ H0, const T2* __restrict__ H1, const T2* __restrict__ H2,
+                        const T2* __restrict__ H3, T2* __restrict__ S0, T2* __restrict__ S1, T2* __restrict__ S2,
+                        T2* __restrict__ S3, const T2* __restrict__ twz, int lb) {
+    zfwd2_body<T2, TN1, TN2>(d, H0, H1, H2, H3, S0, S1, S2, S3, twz, lb);
+}
+
+
+// The FP64 z kernels of the nonlinear pass held to 112 registers per thread: with 8 lines
+// per CTA (192 threads at the 384-point splits) three CTAs fit on an SM instead of two.
+template <int TN1, int TN2>
+__global__ void __maxnreg__(112) k_zinv2sd(Dims d, const double2* __restrict__ u1, const double2* __restrict__ u2,
+                         const double2* __restrict__ u3, double2* __restrict__ Hx, const double2* __restrict__ twz, int lb) {
+    zinv2s_body<double2, TN1, TN2>(d, u1, u2, u3, Hx, twz, lb);
+}
+template <int TN1, int TN2>
+__global__ void __maxnreg__(112) k_zfwd2d(Dims d, const double2* __restrict__ H0, const double2* __restrict__ H1, const double2* __restrict__ H2,
+                        const double2* __restrict__ H3, double2* __restrict__ S0, double2* __restrict__ S1, double2* __restrict__ S2,
+                        double2* __restrict__ S3, const double2* __restrict__ twz, int lb) {
+    zfwd2_body<double2, TN1, TN2>(d, H0, H1, H2, H3, S0, S1, S2, S3, twz, lb);
 }
 
 // --------------------------------------------------------------------------------------
