@@ -1,11 +1,12 @@
 """Autotuner of the launch shapes (cfd_tuning): for one grid, precision and GPU it builds a
 context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
 
-Candidates: the x-line path (register two-step; the same with 1.5 complex lines per row;
-the same on packed FP32 line pairs; or shared-memory Stockham), rows per CTA of the two-step
-x-line kernel, lines per CTA of the two-step z kernels, the radix order of the x and z
-two-step transforms (N = N1*N2 or N2*N1: which register DFT runs first), the y-planes
-per thread of the right-hand-side kernel, and the threads per CTA of the column sweeps.
+Candidates: the x-line path (register two-step; the same held to 64 registers; with 1.5
+complex lines per row; on packed FP32 line pairs; or shared-memory Stockham) searched
+jointly with the radix order of its two-step transform (N = N1*N2 or N2*N1: which register
+DFT runs first), rows per CTA of the two-step x-line kernel, lines per CTA of the two-step
+z kernels, the radix order of the z transforms, the y-planes per thread of the
+right-hand-side kernel, and the threads per CTA of the column sweeps.
 The search is coordinate-wise from the library default, one knob at a time, so it costs a
 dozen short timings.  Results are cached in a JSON file keyed by grid, precision and GPU
 name (CFD_TUNE_CACHE, default ~/.cache/cfd_b200/tuning.json).
@@ -15,14 +16,17 @@ from __future__ import annotations
 import json
 import os
 
-KNOBS = (("xline_path", (1, 2, 3, 4)), ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)),
-         ("xsplit", (1, 2)), ("zsplit", (1, 2)), ("rhs_chunk", (2, 4, 8, 16)), ("solve_cols", (64, 128, 256)))
+# A knob is one setting or a tuple of settings searched jointly: the x-line kernel and its
+# radix order interact (the register-capped kernel, path 5, only pays at one split), so a
+# one-at-a-time search from path 1 would not reach their best pair.
+KNOBS = ((("xline_path", "xsplit"), ((1, 1), (1, 2), (5, 1), (5, 2), (2, 1), (3, 1), (4, 1))),
+         ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)), ("zsplit", (1, 2)), ("rhs_chunk", (2, 4, 8, 16)),
+         ("solve_cols", (64, 128, 256)))
 
 
 # knobs that only act with another setting (the library reports them as 0 or 1 otherwise)
 RELEVANT = {"xline_rows": lambda t: t.get("xline_path") != 2,
-            "xsplit": lambda t: t.get("xline_path") == 1,
-            "zsplit": lambda t: t.get("xline_path") == 1}
+            "zsplit": lambda t: t.get("xline_path") in (1, 5)}
 
 
 def _cache_path() -> str:
@@ -32,7 +36,7 @@ def _cache_path() -> str:
 
 def _key(setup, precision: str, gpu: str) -> str:
     c, g = setup.cfg, setup.grid
-    return f"v7|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+    return f"v8|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
 
 
 def time_step(setup, precision, device, tuning, steps=5, warmup=2):
@@ -64,7 +68,7 @@ def autotune(setup, precision: str, device: int = 0, steps: int = 5, log=None):
         for v in values:
             if name in RELEVANT and not RELEVANT[name](best):
                 continue
-            cand = dict(best, **{name: v})
+            cand = dict(best, **(dict(zip(name, v)) if isinstance(name, tuple) else {name: v}))
             k = json.dumps(cand, sort_keys=True)
             if k in tried:
                 continue

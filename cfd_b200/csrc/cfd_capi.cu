@@ -112,7 +112,7 @@ struct cfd_ctx {
     int RW2 = 0, NT2 = 0;
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
     bool XALT = false, ZALT = false;  // transposed two-step splits (x-line; nonlinear z kernels)
-    bool XR64 = false;      // x-line kernel held to 64 (FP32) / 112 (FP64) registers (k_xline2r)
+    bool XR64 = false;      // FP32 x-line kernel held to 64 registers (k_xline2r, path 5)
     bool ZR = false;        // FP64 nonlinear z kernels held to 112 registers (k_zinv2sd, k_zfwd2d)
     // three bands: the launch dimensions of the nonlinear pass over the bottom wall band,
     // the middle band and the top wall band; the middle band's transforms
@@ -401,9 +401,9 @@ int set_smem_attrs(cfd_ctx* c) {
         TWO_SWITCH_SEL(c->XALT, n1, ok, {
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k_xline2<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
-            if (e == cudaSuccess && c->XR64)
-                e = cudaFuncSetAttribute(XLine2R<T2, TN1, TN2>::kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)c->SM2);
+            if constexpr (std::is_same<T2, float2>::value)
+                if (e == cudaSuccess && c->XR64)
+                    e = cudaFuncSetAttribute(k_xline2r<TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
         });
         TWO_SWITCH(n1, ok, {
             if (e == cudaSuccess && c->XL3)
@@ -579,11 +579,16 @@ int nl_transforms(cfd_ctx* c) {
         dim3 gx2(d.ngal2 / c->RW2, d.nslot);
         bool ok = true;
         TWO_SWITCH_SEL(c->XALT, d.ngal1, ok, {
-            if (c->XR64)
-                XLine2R<T2, TN1, TN2>::kernel<<<gx2, c->NT2, c->SM2, c->stream>>>(
-                    d, c->g, (const T2*)c->Hx, (T2*)c->H[0], (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3], twx<T2>(c),
-                    c->RW2, ilog2(c->RW2));
-            else
+            bool capped = false;
+            if constexpr (std::is_same<T2, float2>::value) {
+                if (c->XR64) {
+                    k_xline2r<TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(
+                        d, c->g, (const float2*)c->Hx, (float2*)c->H[0], (float2*)c->H[1], (float2*)c->H[2],
+                        (float2*)c->H[3], twx<float2>(c), c->RW2, ilog2(c->RW2));
+                    capped = true;
+                }
+            }
+            if (!capped)
                 k_xline2<T2, TN1, TN2><<<gx2, c->NT2, c->SM2, c->stream>>>(d, c->g, (const T2*)c->Hx, (T2*)c->H[0],
                                                                         (T2*)c->H[1], (T2*)c->H[2], (T2*)c->H[3],
                                                                         twx<T2>(c), c->RW2, ilog2(c->RW2));
@@ -1153,8 +1158,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         c->RWibf /= 2;
     if (d.ngal2 % c->RWibf) return fail(c, CFD_ERR_SIZE, "Ngal2 must be even");
     // the transposed split of the x-line transform (tuning xsplit = 2) is for path 1 only
-    const int xpath = g_tuning && g_tuning->xline_path ? g_tuning->xline_path : env_int("CFD_XLINE_PATH", 1, 1, 4);
-    const bool xalt = xpath == 1 && tune_int(&cfd_tuning::xsplit, "CFD_XSPLIT", 1, 1, 2) == 2;
+    const int xpath = g_tuning && g_tuning->xline_path ? g_tuning->xline_path : env_int("CFD_XLINE_PATH", 1, 1, 5);
+    const bool xalt = (xpath == 1 || xpath == 5) && tune_int(&cfd_tuning::xsplit, "CFD_XSPLIT", 1, 1, 2) == 2;
     {
         bool ok = true;
         int n1s = 0, n2s = 0;
@@ -1192,7 +1197,8 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         }
     }
     if ((g_tuning && g_tuning->xline_path == 2) ||
-        (!(g_tuning && (g_tuning->xline_path == 1 || g_tuning->xline_path == 3 || g_tuning->xline_path == 4)) &&
+        (!(g_tuning && (g_tuning->xline_path == 1 || g_tuning->xline_path == 3 || g_tuning->xline_path == 4 ||
+                         g_tuning->xline_path == 5)) &&
          env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)))
         c->RW2 = 0;
     {
@@ -1212,7 +1218,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (c->LZ2 < 0) c->RW2 = 0;  // the two-step x-line kernels read the output of k_zinv2s
     if (!c->RW2) c->RW4 = 0;
     c->XALT = c->RW2 && xalt;  // (xalt implies path 1: neither k_xline3 nor k_xline4)
-    c->XR64 = c->RW2 && !c->XL3 && !c->RW4 && env_int("CFD_XLINE_R64", 0, 0, 1);
+    c->XR64 = c->RW2 && !c->XL3 && !c->RW4 && mixed && xpath == 5;
     c->ZR = c->RW2 && c->precision == CFD_PREC_FP64 && env_int("CFD_Z_R112", 0, 0, 1);
     if (c->RW2 && c->LZ2 >= 0 && tune_int(&cfd_tuning::zsplit, "CFD_ZSPLIT", 1, 1, 2) == 2) {
         bool ok = true;
@@ -1499,7 +1505,7 @@ int cfd_create_tuned(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib
 
 int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
     if (!c || !t) return CFD_ERR_ARG;
-    t->xline_path = c->RW2 ? (c->RW4 ? 4 : (c->XL3 ? 3 : 1)) : 2;
+    t->xline_path = c->RW2 ? (c->RW4 ? 4 : (c->XL3 ? 3 : (c->XR64 ? 5 : 1))) : 2;
     t->xline_rows = c->RW4 ? c->RW4 : (c->RW2 ? c->RW2 : 0);
     t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
     t->solve_kind = 1;

@@ -477,30 +477,16 @@ __global__ void __launch_bounds__(16 * (N1 > N2 ? N1 : N2), (sizeof(T2) == 8 && 
     xline2_body<T2, N1, N2>(d, g, Hx, H0, H1, H2, H3, twx, RW, lrw);
 }
 
-// The x-line kernel held to 64 (FP32) or 112 (FP64) registers per thread: with 4 rows per
-// CTA (192 threads at the 24 x 16 split of 384) five CTAs (FP32) or three (FP64) fit on an
-// SM instead of four or two.  (A register cap is a constant of the kernel, not of its
-// template arguments, hence one kernel per precision.)
+// The FP32 x-line kernel held to 64 registers per thread: with 4 rows per CTA (192 threads
+// at the 24 x 16 split of 384) five CTAs fit on an SM instead of four (x-line path 5).  The
+// FP64 kernel capped at 112 registers (three CTAs instead of two) measured slower at re550
+// (1.72 against 1.53 ms per launch) and is not built.
 template <int N1, int N2>
-__global__ void __maxnreg__(64) k_xline2rf(Dims d, Geo g, const float2* __restrict__ Hx, float2* __restrict__ H0,
-                                           float2* __restrict__ H1, float2* __restrict__ H2, float2* __restrict__ H3,
-                                           const float2* __restrict__ twx, int RW, int lrw) {
+__global__ void __maxnreg__(64) k_xline2r(Dims d, Geo g, const float2* __restrict__ Hx, float2* __restrict__ H0,
+                                          float2* __restrict__ H1, float2* __restrict__ H2, float2* __restrict__ H3,
+                                          const float2* __restrict__ twx, int RW, int lrw) {
     xline2_body<float2, N1, N2>(d, g, Hx, H0, H1, H2, H3, twx, RW, lrw);
 }
-template <int N1, int N2>
-__global__ void __maxnreg__(112) k_xline2rd(Dims d, Geo g, const double2* __restrict__ Hx,
-                                            double2* __restrict__ H0, double2* __restrict__ H1,
-                                            double2* __restrict__ H2, double2* __restrict__ H3,
-                                            const double2* __restrict__ twx, int RW, int lrw) {
-    xline2_body<double2, N1, N2>(d, g, Hx, H0, H1, H2, H3, twx, RW, lrw);
-}
-template <typename T2, int N1, int N2> struct XLine2R;
-template <int N1, int N2> struct XLine2R<float2, N1, N2> {
-    static constexpr auto kernel = k_xline2rf<N1, N2>;
-};
-template <int N1, int N2> struct XLine2R<double2, N1, N2> {
-    static constexpr auto kernel = k_xline2rd<N1, N2>;
-};
 
 // Pass 2 on packed line pairs (FP32 only).  The two lines of a row (u + i v, w + i 0) travel
 // together, one cpair per element (fft_pair.cuh), so every DFT instruction of k_xline2

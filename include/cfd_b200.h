@@ -137,7 +137,9 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *                2: shared-memory Stockham x-line kernel with the per-slot z pass,
  *                3: as 1 with three real inputs packed into 1.5 complex lines per row,
  *                4: as 1 with the two lines of a row in packed FP32 pairs (.f32x2
- *                   instructions; FP32-mixed only, FP64 contexts run path 1)
+ *                   instructions; FP32-mixed only, FP64 contexts run path 1),
+ *                5: as 1 with the kernel held to 64 registers per thread (more CTAs per
+ *                   SM; FP32-mixed only, FP64 contexts run path 1)
  *   xline_rows   rows per CTA of the two-step x-line kernel: 2, 4 or 8
  *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
  *   solve_kind   1: thread-per-column Thomas sweeps (the only kind; other values fall back
@@ -145,7 +147,7 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *   solve_cols   threads (columns) per CTA of the column sweeps k_solve_uvw and k_solve_p:
  *                32, 64, 128 or 256
  *   rhs_chunk    y-planes per thread of the right-hand-side kernel: 2 .. 64
- *   xsplit       radix order of the x-line transforms (x-line path 1): 1 = the split
+ *   xsplit       radix order of the x-line transforms (x-line paths 1, 5): 1 = the split
  *                N = N1*N2 of 64 = 8*8, 96 = 8*12, 128 = 8*16, 192 = 16*12, 384 = 16*24,
  *                768 = 32*24 (first step N1 points); 2 = the transposed split (16*4, 12*8,
  *                16*8, 12*16, 24*16, 24*32)

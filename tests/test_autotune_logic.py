@@ -11,20 +11,22 @@ DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "sol
 
 
 def fake_model(calls, bad=()):
-    """Seconds per step: a separable cost with its minimum at xline_rows 4, zlines 16,
-    rhs_chunk 4, 128 threads per column-sweep CTA, the transposed x split and the default z
-    split; path 2 is slow; shapes in
-    `bad` raise."""
+    """Seconds per step: a cost with its minimum at x-line path 5 with the transposed x split
+    (path 5 alone and the split alone are each worse than path 1 with the default split),
+    xline_rows 4, zlines 16, rhs_chunk 4, 128 threads per column-sweep CTA and the default z
+    split; path 2 is slow; shapes in `bad` raise."""
     def time_step(setup, precision, device, tuning, steps=5, warmup=2):
         eff = dict(DEFAULT, **(tuning or {}))
-        if eff["xline_path"] != 1:
-            eff["xsplit"] = eff["zsplit"] = 1  # the splits act on path 1 only
+        if eff["xline_path"] not in (1, 5):
+            eff["xsplit"] = eff["zsplit"] = 1  # the splits act on paths 1 and 5 only
         for k, v in bad:
             if eff.get(k) == v:
                 raise RuntimeError(f"{k}={v} does not fit")
         calls.append(json.dumps(eff, sort_keys=True))
         t = 10.0
-        t += {1: 0.0, 2: 3.0, 3: 0.5, 4: 0.8}[eff["xline_path"]]
+        t += {1: 0.0, 2: 3.0, 3: 0.5, 4: 0.8, 5: 0.2}[eff["xline_path"]]
+        if eff["xline_path"] == 5 and eff["xsplit"] == 2:
+            t -= 0.5   # an interaction a one-knob-at-a-time search from path 1 would miss
         t += {2: 0.4, 4: 0.0, 8: 0.2}[eff["xline_rows"]]
         t += {4: 0.5, 8: 0.3, 16: 0.0}[eff["zlines"]]
         t += {2: 0.2, 4: 0.0, 8: 0.1, 16: 0.3}[eff["rhs_chunk"]]
@@ -38,10 +40,10 @@ def test_coordinate_search_finds_the_separable_minimum(monkeypatch):
     calls = []
     monkeypatch.setattr(autotune, "time_step", fake_model(calls))
     best, t = autotune.autotune(None, "mixed")
-    assert best["xline_path"] == 1 and best["xline_rows"] == 4 and best["zlines"] == 16
+    assert best["xline_path"] == 5 and best["xline_rows"] == 4 and best["zlines"] == 16
     assert best["solve_kind"] == 1 and best["rhs_chunk"] == 4 and best["solve_cols"] == 128
     assert best["xsplit"] == 2 and best["zsplit"] == 1
-    assert t == pytest.approx(10.0e-3)
+    assert t == pytest.approx(9.7e-3)
     assert len(calls) == len(set(calls)), "a shape was timed twice"
 
 

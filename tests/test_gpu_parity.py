@@ -428,20 +428,20 @@ def test_transposed_splits(torch_cuda, ng1, ng2, ny):
 @pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
 @pytest.mark.parametrize("xsplit", [1, 2])
 def test_register_capped_xline(torch_cuda, monkeypatch, ng1, ng2, ny, xsplit):
-    """The x-line kernel held to 64 (FP32) / 112 (FP64) registers (CFD_XLINE_R64=1,
-    k_xline2rf / k_xline2rd) and the FP64 nonlinear z kernels held to 112 (CFD_Z_R112=1,
-    k_zinv2sd / k_zfwd2d) on every two-step length and both radix orders, against the
-    oracle after one RK3 step (FP64 within 1e-10, FP32-mixed within 1e-5 on u, v, w, p)."""
+    """The FP32 x-line kernel held to 64 registers (x-line path 5, k_xline2r; FP64 contexts
+    run path 1) and the FP64 nonlinear z kernels held to 112 (CFD_Z_R112=1, k_zinv2sd /
+    k_zfwd2d) on every two-step length and both radix orders, against the oracle after one
+    RK3 step (FP64 within 1e-10, FP32-mixed within 1e-5 on u, v, w, p)."""
     from cfd_b200.channel import Channel, build_channel
     from cfd_b200.config import tiny
-    monkeypatch.setenv("CFD_XLINE_R64", "1")
     monkeypatch.setenv("CFD_Z_R112", "1")
     s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=5 * ng1 + ng2))
     o = oracle(s)
     o.step(1)
     ref = o.download_state()
     for prec, tol in (("fp64", 1e-10), ("mixed", 1e-5)):
-        g = Channel(s, device=0, precision=prec, tuning=dict(xline_path=1, xsplit=xsplit, zsplit=xsplit))
+        g = Channel(s, device=0, precision=prec, tuning=dict(xline_path=5, xsplit=xsplit, zsplit=xsplit))
+        assert g.tuning()["xline_path"] == (5 if prec == "mixed" else 1)
         g.upload_state()
         g.step(1)
         st = g.download_state()
