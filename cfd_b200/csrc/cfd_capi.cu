@@ -1219,7 +1219,9 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (!c->RW2) c->RW4 = 0;
     c->XALT = c->RW2 && xalt;  // (xalt implies path 1: neither k_xline3 nor k_xline4)
     c->XR64 = c->RW2 && !c->XL3 && !c->RW4 && mixed && xpath == 5;
-    c->ZR = c->RW2 && c->precision == CFD_PREC_FP64 && env_int("CFD_Z_R112", 0, 0, 1);
+    // FP64 z kernels at 112 registers (3 CTAs of 8 lines per SM): measured 0.31 / 0.59 against
+    // 0.34 / 0.61 ms per launch at re550; the 768-point split spills at that cap
+    c->ZR = c->RW2 && c->precision == CFD_PREC_FP64 && d.ngal2 <= 384 && env_int("CFD_Z_R112", 1, 0, 1);
     if (c->RW2 && c->LZ2 >= 0 && tune_int(&cfd_tuning::zsplit, "CFD_ZSPLIT", 1, 1, 2) == 2) {
         bool ok = true;
         int n1s = 0, n2s = 0;

@@ -429,9 +429,9 @@ def test_transposed_splits(torch_cuda, ng1, ng2, ny):
 @pytest.mark.parametrize("xsplit", [1, 2])
 def test_register_capped_xline(torch_cuda, monkeypatch, ng1, ng2, ny, xsplit):
     """The FP32 x-line kernel held to 64 registers (x-line path 5, k_xline2r; FP64 contexts
-    run path 1) and the FP64 nonlinear z kernels held to 112 (CFD_Z_R112=1, k_zinv2sd /
-    k_zfwd2d) on every two-step length and both radix orders, against the oracle after one
-    RK3 step (FP64 within 1e-10, FP32-mixed within 1e-5 on u, v, w, p)."""
+    run path 1) and the FP64 nonlinear z kernels held to 112 (k_zinv2sd / k_zfwd2d, the
+    default for z lengths up to 384) on every two-step length and both radix orders, against
+    the oracle after one RK3 step (FP64 within 1e-10, FP32-mixed within 1e-5 on u, v, w, p)."""
     from cfd_b200.channel import Channel, build_channel
     from cfd_b200.config import tiny
     monkeypatch.setenv("CFD_Z_R112", "1")
