@@ -335,7 +335,8 @@ int tune_int(int32_t cfd_tuning::*field, const char* env, int dflt, int lo, int 
 
 size_t xline2_smem(int n1s, int n2s, int rw, size_t esz) {
     const int N = n1s * n2s;
-    const int L1 = n1s * (n2s + 1) + 1, L2 = n2s * (n1s + 1) + 1, LU = N + 1;
+    const int S = 128 / (int)esz;
+    const int L1 = xline2_pitch(n1s * (n2s + 1), rw, S), L2 = xline2_pitch(n2s * (n1s + 1), rw, S), LU = N + 1;
     const int LX = std::max(L1, std::max(L2, LU));
     return ((size_t)2 * rw * LX + N) * esz;
 }
@@ -1167,7 +1168,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         int n1s = 0, n2s = 0;
         TWO_SWITCH_SEL(xalt, d.ngal1, ok, { n1s = TN1; n2s = TN2; });
         if (ok) {
-            int rw = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", mixed ? 8 : 4, 2, 8);
+            int rw = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", 4, 2, 8);
             rw = 1 << (31 - __builtin_clz(rw));  // a power of two
             while (rw >= 2 && ((d.ngal2 % rw) || xline2_smem(n1s, n2s, rw, esz) > budget)) rw /= 2;
             if (rw >= 2 && d.ngal2 % rw == 0 && (2 * rw * n1s) % 32 == 0) {

@@ -6,7 +6,7 @@ import pytest
 
 from cfd_b200 import autotune
 
-DEFAULT = {"xline_path": 1, "xline_rows": 8, "zlines": 16, "solve_kind": 1, "solve_cols": 64, "rhs_chunk": 16,
+DEFAULT = {"xline_path": 1, "xline_rows": 4, "zlines": 16, "solve_kind": 1, "solve_cols": 64, "rhs_chunk": 16,
            "xsplit": 1, "zsplit": 1}
 
 
