@@ -49,10 +49,10 @@ def test_coordinate_search_finds_the_separable_minimum(monkeypatch):
 
 def test_shapes_that_do_not_fit_are_skipped(monkeypatch):
     calls = []
-    monkeypatch.setattr(autotune, "time_step", fake_model(calls, bad=(("xline_rows", 4),)))
+    monkeypatch.setattr(autotune, "time_step", fake_model(calls, bad=(("xline_rows", 2),)))
     logs = []
     best, _ = autotune.autotune(None, "mixed", log=logs.append)
-    assert best["xline_rows"] == 8 and best["rhs_chunk"] == 4
+    assert best["xline_rows"] == 4 and best["rhs_chunk"] == 4
     assert any(m.startswith("skip") for m in logs)
 
 
