@@ -1298,7 +1298,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     AL(c->cs, double, nc * nyu);
     AL(c->cs_v, double, nc * nyv);
-    AL(c->ck_uw, double, sweep_ck_doubles(nyu, 2, nc));
+    AL(c->ck_uw, double, std::max(sweep_ck_doubles(nyu, 2, nc), sweep_ck_doubles(d.nyp, 1, nc, CFD_SKP)));
     AL(c->ck_v, double, sweep_ck_doubles(nyv, 1, nc));
     c->JC = tune_int(&cfd_tuning::rhs_chunk, "CFD_RHS_CHUNK", 4, 2, 64);
     c->SNT = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_THREADS", 64, 32, 256));

@@ -1592,13 +1592,14 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
 // several independent loads in flight while the recurrence runs on registers.
 // --------------------------------------------------------------------------------------
 #define CFD_UB 8
-#define CFD_SK 8
+#define CFD_SK 16   // rows per segment of the Helmholtz sweeps
+#define CFD_SKP 8   // rows per segment of the pressure sweep (more live values per row)
 
 // checkpoint store of one system with NF fields: e[nseg][ncol] then y[nseg][NF][ncol]
-__host__ __device__ __forceinline__ int sweep_segments(int n) { return (n + CFD_SK - 1) / CFD_SK; }
-__host__ __device__ __forceinline__ size_t sweep_ck_doubles(int n, int nf, size_t ncol) {
-    const size_t e = (size_t)sweep_segments(n) * ncol;
-    return ((e + 1) & ~(size_t)1) + (size_t)2 * nf * sweep_segments(n) * ncol;
+__host__ __device__ __forceinline__ int sweep_segments(int n, int k = CFD_SK) { return (n + k - 1) / k; }
+__host__ __device__ __forceinline__ size_t sweep_ck_doubles(int n, int nf, size_t ncol, int k = CFD_SK) {
+    const size_t e = (size_t)sweep_segments(n, k) * ncol;
+    return ((e + 1) & ~(size_t)1) + (size_t)2 * nf * sweep_segments(n, k) * ncol;
 }
 
 // rows (a1, a2, a3) of LU_buildU (uw: ghost rows (0, 1, gwb) / (gwt, 1, 0)) or LU_buildV
@@ -1886,7 +1887,7 @@ __global__ void __launch_bounds__(256) k_solve_p_ck(Dims d, Geo g, double dtirk,
     const double k2x = -kxv * kxv, k2z = -kzv * kzv;
     const size_t nc = d.ncol;
     const int n = d.nyp;
-    const int nseg = sweep_segments(n);
+    const int nseg = sweep_segments(n, CFD_SKP);
     double* ck_e = ck;
     double2* ck_y = reinterpret_cast<double2*>(ck + ((((size_t)nseg * nc) + 1) & ~(size_t)1));
     auto UO = [&](int jj) { return (size_t)(d.jp0 + jj - d.ju0) * nc + col; };  // u, w at p-row jj
@@ -1896,17 +1897,17 @@ __global__ void __launch_bounds__(256) k_solve_p_ck(Dims d, Geo g, double dtirk,
     double2 y = dc(0, 0);
     double2 vb = u2[VO(-1)];
     for (int m = 0; m < nseg; ++m) {
-        const int j0 = m * CFD_SK;
+        const int j0 = m * CFD_SKP;
         if (m > 0) {
             ck_e[(size_t)m * nc + col] = e;
             ck_y[(size_t)m * nc + col] = y;
         }
-        double2 A[CFD_SK], W[CFD_SK], VA[CFD_SK];
+        double2 A[CFD_SKP], W[CFD_SKP], VA[CFD_SKP];
 #pragma unroll
-        for (int t = 0; t < CFD_SK; ++t)
+        for (int t = 0; t < CFD_SKP; ++t)
             if (j0 + t < n) { A[t] = u1[UO(j0 + t)]; W[t] = u3[UO(j0 + t)]; VA[t] = u2[VO(j0 + t)]; }
 #pragma unroll
-        for (int t = 0; t < CFD_SK; ++t) {
+        for (int t = 0; t < CFD_SKP; ++t) {
             const int jj = j0 + t;
             if (jj >= n) break;
             const double2 dv = dadd(dadd(dik(kxv, A[t]), dik(kzv, W[t])),
@@ -1924,17 +1925,17 @@ __global__ void __launch_bounds__(256) k_solve_p_ck(Dims d, Geo g, double dtirk,
     // back sweep by segments from the top: recompute, substitute, correct
     double2 x = dc(0, 0);
     for (int m = nseg - 1; m >= 0; --m) {
-        const int j0 = m * CFD_SK;
+        const int j0 = m * CFD_SKP;
         double es = m > 0 ? ck_e[(size_t)m * nc + col] : 0.0;
         double2 ys = m > 0 ? ck_y[(size_t)m * nc + col] : dc(0, 0);
         double2 vbs = u2[VO(j0 - 1)];
-        double2 A[CFD_SK], W[CFD_SK], VA[CFD_SK], Y[CFD_SK];
-        double E[CFD_SK];
+        double2 A[CFD_SKP], W[CFD_SKP], VA[CFD_SKP], Y[CFD_SKP];
+        double E[CFD_SKP];
 #pragma unroll
-        for (int t = 0; t < CFD_SK; ++t)
+        for (int t = 0; t < CFD_SKP; ++t)
             if (j0 + t < n) { A[t] = u1[UO(j0 + t)]; W[t] = u3[UO(j0 + t)]; VA[t] = u2[VO(j0 + t)]; }
 #pragma unroll
-        for (int t = 0; t < CFD_SK; ++t) {
+        for (int t = 0; t < CFD_SKP; ++t) {
             const int jj = j0 + t;
             if (jj >= n) break;
             const double2 dv = dadd(dadd(dik(kxv, A[t]), dik(kzv, W[t])),
@@ -1951,7 +1952,7 @@ __global__ void __launch_bounds__(256) k_solve_p_ck(Dims d, Geo g, double dtirk,
             E[t] = es;
         }
 #pragma unroll
-        for (int t = CFD_SK - 1; t >= 0; --t) {
+        for (int t = CFD_SKP - 1; t >= 0; --t) {
             const int jj = j0 + t;
             if (jj >= n) continue;
             const double2 xp = x;  // psi(jj + 1)
