@@ -90,8 +90,6 @@ struct cfd_ctx {
     // kXC column chunks, host-to-device copies on xin, device-to-host copies on xout,
     // ordered per field and chunk by xev (allocated at the first such transfer)
     static constexpr int kXC = 8;
-    double* ck_uw = nullptr;  // checkpoints of the column sweeps (k_solve_uvw; k_solve_p_ck uses ck_uw)
-    double* ck_v = nullptr;
     double2* xstage[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaStream_t xin = nullptr, xout = nullptr;
     cudaEvent_t xev[4][kXC] = {};
@@ -792,8 +790,8 @@ int ib_all(cfd_ctx* c) {
 int launch_solve(cfd_ctx* c, cudaStream_t st, double beta, int part0, int nsys) {
     const Dims& d = c->d;
     const dim3 gb((d.ncol + c->SNT - 1) / c->SNT, nsys);
-    k_solve_uvw<<<gb, c->SNT, 0, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->ck_uw,
-                                       c->ck_v, part0);
+    k_solve_uvw<<<gb, c->SNT, 0, st>>>(d, c->g, beta, c->u1, c->u2, c->u3, c->du1, c->du2, c->du3, c->cs, c->cs_v,
+                                       part0);
     return launched(c, "k_solve_uvw");
 }
 
@@ -893,8 +891,8 @@ int substep(cfd_ctx* c, int krk) {
         return CFD_OK;
     }
     const dim3 gp((d.ncol + c->SNT - 1) / c->SNT);
-    k_solve_p_ck<<<gp, c->SNT, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->ck_uw, c->mean_diag,
-                                               dtrk);
+    k_solve_p<true><<<gp, c->SNT, 0, c->stream>>>(d, c->g, dtirk, c->u1, c->u2, c->u3, c->p, c->psi, nullptr,
+                                                  c->cs, c->mean_diag, dtrk);
     LK("k_solve_p_vcorr");
     return CFD_OK;
 }
@@ -1298,8 +1296,6 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     AL(c->cs, double, nc * nyu);
     AL(c->cs_v, double, nc * nyv);
-    AL(c->ck_uw, double, std::max(sweep_ck_doubles(nyu, 2, nc), sweep_ck_doubles(d.nyp, 1, nc, CFD_SKP)));
-    AL(c->ck_v, double, sweep_ck_doubles(nyv, 1, nc));
     c->JC = tune_int(&cfd_tuning::rhs_chunk, "CFD_RHS_CHUNK", 4, 2, 64);
     c->SNT = 1 << ilog2(tune_int(&cfd_tuning::solve_cols, "CFD_SOLVE_THREADS", 64, 32, 256));
     c->nch = (d.nyu - 2 + c->JC - 1) / c->JC;

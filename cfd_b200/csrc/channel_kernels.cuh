@@ -1581,126 +1581,19 @@ __global__ void __launch_bounds__(16 * (TN1 > TN2 ? TN1 : TN2), (sizeof(T2) == 8
 
 // --------------------------------------------------------------------------------------
 // Implicit Helmholtz solves: LUsolU/LUsolV with LU_buildU/V + LU_dec computed on the fly
-// (tridLU_3D_IB.f90:50-160, 349-413, 521-559).  One thread per (kx,kz) column; u and w
-// share the matrix and its factorisation.  The forward sweep keeps only a checkpoint of its
-// recurrence (e_{j-1} = a3_{j-1} d_{j-1} and y_{j-1}) every CFD_SK rows; the back sweep
-// walks the segments from the top, re-reads a segment's right-hand sides, recomputes its
-// pivots and forward values from the checkpoint into registers (the same expressions as
-// the forward sweep, so the same values) and substitutes.  The right-hand side is read
-// twice and the solution written once; neither y nor the scaled upper diagonal goes
-// through HBM.  Loads are batched CFD_UB planes at a time so that each thread keeps
-// several independent loads in flight while the recurrence runs on registers.
+// (tridLU_3D_IB.f90:50-160, 349-413, 521-559).  One thread per (kx,kz) column; the
+// forward sweep leaves y_j in the solution array and the scaled upper diagonal in `cs`.
+// u and w share the matrix and its factorisation.
 // --------------------------------------------------------------------------------------
+// Loads of the sweeps are batched UB planes at a time so that each thread keeps several
+// independent loads in flight while the recurrence runs on registers.
 #define CFD_UB 8
-#define CFD_SK 16   // rows per segment of the Helmholtz sweeps
-#define CFD_SKP 8   // rows per segment of the pressure sweep (more live values per row)
-
-// checkpoint store of one system with NF fields: e[nseg][ncol] then y[nseg][NF][ncol]
-__host__ __device__ __forceinline__ int sweep_segments(int n, int k = CFD_SK) { return (n + k - 1) / k; }
-__host__ __device__ __forceinline__ size_t sweep_ck_doubles(int n, int nf, size_t ncol, int k = CFD_SK) {
-    const size_t e = (size_t)sweep_segments(n, k) * ncol;
-    return ((e + 1) & ~(size_t)1) + (size_t)2 * nf * sweep_segments(n, k) * ncol;
-}
-
-// rows (a1, a2, a3) of LU_buildU (uw: ghost rows (0, 1, gwb) / (gwt, 1, 0)) or LU_buildV
-// (identity wall rows)
-__device__ __forceinline__ void sweep_coef(const Geo& g, bool uw, int n, int j, double beta, double k2x, double k2z,
-                                           double& a1, double& a2, double& a3) {
-    const double* D2 = uw ? g.dyu2i : g.dyv2i;
-    if (j == 0) {
-        a1 = 0.0; a2 = 1.0; a3 = uw ? g.gwb : 0.0;
-    } else if (j < n - 1) {
-        a1 = -beta * D2[3 * j + 0];
-        a2 = 1.0 - beta * (D2[3 * j + 1] + k2x + k2z);
-        a3 = -beta * D2[3 * j + 2];
-    } else {
-        a1 = uw ? g.gwt : 0.0; a2 = 1.0; a3 = 0.0;
-    }
-}
-
-template <int NF>
-__device__ __forceinline__ void sweep_ck(const Geo& g, bool uw, int n, int col, size_t nc, double beta, double k2x,
-                                         double k2z, const double2* const (&r)[2], double2* const (&x)[2],
-                                         double* __restrict__ ck) {
-    const int nseg = sweep_segments(n);
-    double* ck_e = ck;
-    double2* ck_y = reinterpret_cast<double2*>(ck + ((((size_t)nseg * nc) + 1) & ~(size_t)1));
-    // forward: pivots and y, a checkpoint at every segment start
-    double e = 0.0;  // e_{j-1}
-    double2 y[NF];
-    for (int f = 0; f < NF; ++f) y[f] = dc(0, 0);
-    for (int m = 0; m < nseg; ++m) {
-        const int j0 = m * CFD_SK;
-        if (m > 0) {
-            ck_e[(size_t)m * nc + col] = e;
-            for (int f = 0; f < NF; ++f) ck_y[((size_t)m * NF + f) * nc + col] = y[f];
-        }
-        double2 ra[NF][CFD_SK];
-#pragma unroll
-        for (int t = 0; t < CFD_SK; ++t)
-            if (j0 + t < n)
-                for (int f = 0; f < NF; ++f) ra[f][t] = r[f][(size_t)(j0 + t) * nc + col];
-#pragma unroll
-        for (int t = 0; t < CFD_SK; ++t) {
-            const int j = j0 + t;
-            if (j >= n) break;
-            double a1, a2, a3;
-            sweep_coef(g, uw, n, j, beta, k2x, k2z, a1, a2, a3);
-            const double dj = j == 0 ? 1.0 : 1.0 / (a2 - a1 * e);
-            for (int f = 0; f < NF; ++f) y[f] = j == 0 ? ra[f][t] : dscl(dj, dsub(ra[f][t], dscl(a1, y[f])));
-            e = a3 * dj;
-        }
-    }
-    // back: segments from the top, each recomputed from its checkpoint
-    double2 xn[NF];
-    for (int f = 0; f < NF; ++f) xn[f] = dc(0, 0);
-    for (int m = nseg - 1; m >= 0; --m) {
-        const int j0 = m * CFD_SK;
-        double es = 0.0;
-        double2 ys[NF];
-        if (m > 0) {
-            es = ck_e[(size_t)m * nc + col];
-            for (int f = 0; f < NF; ++f) ys[f] = ck_y[((size_t)m * NF + f) * nc + col];
-        } else {
-            for (int f = 0; f < NF; ++f) ys[f] = dc(0, 0);
-        }
-        double2 ya[NF][CFD_SK];
-        double ea[CFD_SK];
-#pragma unroll
-        for (int t = 0; t < CFD_SK; ++t)
-            if (j0 + t < n)
-                for (int f = 0; f < NF; ++f) ya[f][t] = r[f][(size_t)(j0 + t) * nc + col];
-#pragma unroll
-        for (int t = 0; t < CFD_SK; ++t) {
-            const int j = j0 + t;
-            if (j >= n) break;
-            double a1, a2, a3;
-            sweep_coef(g, uw, n, j, beta, k2x, k2z, a1, a2, a3);
-            const double dj = j == 0 ? 1.0 : 1.0 / (a2 - a1 * es);
-            for (int f = 0; f < NF; ++f) {
-                ys[f] = j == 0 ? ya[f][t] : dscl(dj, dsub(ya[f][t], dscl(a1, ys[f])));
-                ya[f][t] = ys[f];
-            }
-            es = a3 * dj;
-            ea[t] = es;
-        }
-#pragma unroll
-        for (int t = CFD_SK - 1; t >= 0; --t) {
-            const int j = j0 + t;
-            if (j >= n) continue;
-            for (int f = 0; f < NF; ++f) {
-                xn[f] = j == n - 1 ? ya[f][t] : dsub(ya[f][t], dscl(ea[t], xn[f]));
-                x[f][(size_t)j * nc + col] = xn[f];
-            }
-        }
-    }
-}
 
 __global__ void __launch_bounds__(256) k_solve_uvw(Dims d, Geo g, double beta, double2* __restrict__ u1,
                                                    double2* __restrict__ u2, double2* __restrict__ u3,
                                                    const double2* __restrict__ r1, const double2* __restrict__ r2,
-                                                   const double2* __restrict__ r3, double* __restrict__ ck_uw,
-                                                   double* __restrict__ ck_v, int part0) {
+                                                   const double2* __restrict__ r3, double* __restrict__ cs_uw,
+                                                   double* __restrict__ cs_v, int part0) {
     // blockIdx.y + part0: 0 = the u/w systems, 1 = the v system
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
@@ -1708,13 +1601,109 @@ __global__ void __launch_bounds__(256) k_solve_uvw(Dims d, Geo g, double beta, d
     const double k2x = -g.kx[i] * g.kx[i], k2z = -g.kz[q] * g.kz[q];
     const size_t nc = d.ncol;
     if (blockIdx.y + part0 == 0) {
-        const double2* const r[2] = {r1, r3};
-        double2* const x[2] = {u1, u3};
-        sweep_ck<2>(g, true, d.nyu, col, nc, beta, k2x, k2z, r, x, ck_uw);
+        // u and w share the matrix: rows (0,1,gwb), interior, (gwt,1,0)
+        const int n = d.nyu;
+        double dprev = 1.0, a3prev = g.gwb;
+        double2 y1 = r1[col], y3 = r3[col];
+        u1[col] = y1;
+        u3[col] = y3;
+        for (int j0 = 1; j0 < n; j0 += CFD_UB) {
+            double2 ra[CFD_UB], rc[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 + t < n) { ra[t] = r1[(size_t)(j0 + t) * nc + col]; rc[t] = r3[(size_t)(j0 + t) * nc + col]; }
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                const int jj = j0 + t;
+                if (jj >= n) break;
+                double a1, a2, a3;
+                if (jj < n - 1) {
+                    a1 = -beta * g.dyu2i[3 * jj + 0];
+                    a2 = 1.0 - beta * (g.dyu2i[3 * jj + 1] + k2x + k2z);
+                    a3 = -beta * g.dyu2i[3 * jj + 2];
+                } else {
+                    a1 = g.gwt; a2 = 1.0; a3 = 0.0;
+                }
+                const double csm = a3prev * dprev;  // a(3,j-1) * a(2,j-1)
+                cs_uw[(size_t)(jj - 1) * nc + col] = csm;
+                const double dj = 1.0 / (a2 - a1 * csm);
+                y1 = dscl(dj, dsub(ra[t], dscl(a1, y1)));
+                y3 = dscl(dj, dsub(rc[t], dscl(a1, y3)));
+                u1[(size_t)jj * nc + col] = y1;
+                u3[(size_t)jj * nc + col] = y3;
+                dprev = dj;
+                a3prev = a3;
+            }
+        }
+        double2 x1 = y1, x3 = y3;
+        for (int j0 = n - 2; j0 >= 0; j0 -= CFD_UB) {
+            double cc[CFD_UB];
+            double2 ya[CFD_UB], yc[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 - t >= 0) {
+                    const size_t o = (size_t)(j0 - t) * nc + col;
+                    cc[t] = cs_uw[o]; ya[t] = u1[o]; yc[t] = u3[o];
+                }
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                if (j0 - t < 0) break;
+                const size_t o = (size_t)(j0 - t) * nc + col;
+                x1 = dsub(ya[t], dscl(cc[t], x1));
+                x3 = dsub(yc[t], dscl(cc[t], x3));
+                u1[o] = x1;
+                u3[o] = x3;
+            }
+        }
     } else {
-        const double2* const r[2] = {r2, r2};
-        double2* const x[2] = {u2, u2};
-        sweep_ck<1>(g, false, d.nyv, col, nc, beta, k2x, k2z, r, x, ck_v);
+        // v: identity wall rows
+        const int n = d.nyv;
+        double dprev = 1.0, a3prev = 0.0;
+        double2 y = r2[col];
+        u2[col] = y;
+        for (int j0 = 1; j0 < n; j0 += CFD_UB) {
+            double2 ra[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 + t < n) ra[t] = r2[(size_t)(j0 + t) * nc + col];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                const int jj = j0 + t;
+                if (jj >= n) break;
+                double a1, a2, a3;
+                if (jj < n - 1) {
+                    a1 = -beta * g.dyv2i[3 * jj + 0];
+                    a2 = 1.0 - beta * (g.dyv2i[3 * jj + 1] + k2x + k2z);
+                    a3 = -beta * g.dyv2i[3 * jj + 2];
+                } else {
+                    a1 = 0.0; a2 = 1.0; a3 = 0.0;
+                }
+                const double csm = a3prev * dprev;
+                cs_v[(size_t)(jj - 1) * nc + col] = csm;
+                const double dj = 1.0 / (a2 - a1 * csm);
+                y = dscl(dj, dsub(ra[t], dscl(a1, y)));
+                u2[(size_t)jj * nc + col] = y;
+                dprev = dj;
+                a3prev = a3;
+            }
+        }
+        double2 x = y;
+        for (int j0 = n - 2; j0 >= 0; j0 -= CFD_UB) {
+            double cc[CFD_UB];
+            double2 ya[CFD_UB];
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t)
+                if (j0 - t >= 0) {
+                    const size_t o = (size_t)(j0 - t) * nc + col;
+                    cc[t] = cs_v[o]; ya[t] = u2[o];
+                }
+#pragma unroll
+            for (int t = 0; t < CFD_UB; ++t) {
+                if (j0 - t < 0) break;
+                x = dsub(ya[t], dscl(cc[t], x));
+                u2[(size_t)(j0 - t) * nc + col] = x;
+            }
+        }
     }
 }
 
@@ -1841,140 +1830,6 @@ __global__ void __launch_bounds__(256) k_solve_p(Dims d, Geo g, double dtirk, do
         u2[col] = dc(0, 0);
         u2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
     }
-}
-
-// --------------------------------------------------------------------------------------
-// solveP + v_corr in one column sweep (the fused substep; littleharsh.f90:556-611, 796-907,
-// LU_buildP/LU_decP/LUsolP tridLU_3D_IB.f90:284-318, 417-491, 562-603): as k_solve_p<true>,
-// but the forward sweep keeps only a checkpoint of its recurrence (e_{j-1}, y_{j-1}) every
-// CFD_SK rows, and the back sweep walks the segments from the top, re-reads a segment's u,
-// w and v (which the velocity correction needs anyway), recomputes its divergence, pivots
-// and forward values from the checkpoint (the same expressions, so the same values) and
-// substitutes, correcting u, w, v and p.  u, v, w are read twice and written once, p read
-// and written once; psi and the scaled upper diagonal never go through HBM.
-// --------------------------------------------------------------------------------------
-__device__ __forceinline__ void dg_coef(const Dims& d, const Geo& g, int n, int jj, int col, double k2x, double k2z,
-                                        double mean_diag, double& a1, double& a2, double& a3) {
-    const int j = d.jp0 + jj;
-    const double du = g.dthdyu[j - d.ju0];
-    const double dv = g.dthdyv[j - d.jv0];
-    if (jj == 0) {
-        a1 = 0.0;
-        a2 = (du * -dv) + k2x + k2z;
-        a3 = (du * dv);
-        if (col == 0) { a2 = mean_diag; a3 = 0.0; }
-    } else if (jj == n - 1) {
-        const double dvm = g.dthdyv[j - 1 - d.jv0];
-        a1 = (-du) * (-dvm);
-        a2 = ((-du) * dvm) + k2x + k2z;
-        a3 = 0.0;
-    } else {
-        const double dvm = g.dthdyv[j - 1 - d.jv0];
-        a2 = ((-du) * dvm) + (du * -dv) + k2x + k2z;
-        a1 = ((-du) * (-dvm));
-        a3 = (du * dv);
-    }
-}
-
-__global__ void __launch_bounds__(256) k_solve_p_ck(Dims d, Geo g, double dtirk, double2* __restrict__ u1,
-                                                    double2* __restrict__ u2, double2* __restrict__ u3,
-                                                    double2* __restrict__ p, double* __restrict__ ck,
-                                                    double mean_diag, double dtrk) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= d.ncol) return;
-    const int i = col % d.nkx, q = col / d.nkx;
-    const double kxv = g.kx[i], kzv = g.kz[q];
-    const double k2x = -kxv * kxv, k2z = -kzv * kzv;
-    const size_t nc = d.ncol;
-    const int n = d.nyp;
-    const int nseg = sweep_segments(n, CFD_SKP);
-    double* ck_e = ck;
-    double2* ck_y = reinterpret_cast<double2*>(ck + ((((size_t)nseg * nc) + 1) & ~(size_t)1));
-    auto UO = [&](int jj) { return (size_t)(d.jp0 + jj - d.ju0) * nc + col; };  // u, w at p-row jj
-    auto VO = [&](int jj) { return (size_t)(d.jp0 + jj - d.jv0) * nc + col; };  // v at the face of p-row jj
-    // forward sweep of D.G psi = div / (dt (a+b)), checkpoints only
-    double e = 0.0;
-    double2 y = dc(0, 0);
-    double2 vb = u2[VO(-1)];
-    for (int m = 0; m < nseg; ++m) {
-        const int j0 = m * CFD_SKP;
-        if (m > 0) {
-            ck_e[(size_t)m * nc + col] = e;
-            ck_y[(size_t)m * nc + col] = y;
-        }
-        double2 A[CFD_SKP], W[CFD_SKP], VA[CFD_SKP];
-#pragma unroll
-        for (int t = 0; t < CFD_SKP; ++t)
-            if (j0 + t < n) { A[t] = u1[UO(j0 + t)]; W[t] = u3[UO(j0 + t)]; VA[t] = u2[VO(j0 + t)]; }
-#pragma unroll
-        for (int t = 0; t < CFD_SKP; ++t) {
-            const int jj = j0 + t;
-            if (jj >= n) break;
-            const double2 dv = dadd(dadd(dik(kxv, A[t]), dik(kzv, W[t])),
-                                    dscl(g.dthdyu[d.jp0 + jj - d.ju0], dsub(VA[t], vb)));
-            vb = VA[t];
-            double2 r = dscl(dtirk, dv);
-            double a1, a2, a3;
-            dg_coef(d, g, n, jj, col, k2x, k2z, mean_diag, a1, a2, a3);
-            if (jj == 0 && col == 0) r = dc(0, 0);
-            const double dj = jj == 0 ? 1.0 / a2 : 1.0 / (a2 - a1 * e);
-            y = jj == 0 ? dscl(dj, r) : dscl(dj, dsub(r, dscl(a1, y)));
-            e = a3 * dj;
-        }
-    }
-    // back sweep by segments from the top: recompute, substitute, correct
-    double2 x = dc(0, 0);
-    for (int m = nseg - 1; m >= 0; --m) {
-        const int j0 = m * CFD_SKP;
-        double es = m > 0 ? ck_e[(size_t)m * nc + col] : 0.0;
-        double2 ys = m > 0 ? ck_y[(size_t)m * nc + col] : dc(0, 0);
-        double2 vbs = u2[VO(j0 - 1)];
-        double2 A[CFD_SKP], W[CFD_SKP], VA[CFD_SKP], Y[CFD_SKP];
-        double E[CFD_SKP];
-#pragma unroll
-        for (int t = 0; t < CFD_SKP; ++t)
-            if (j0 + t < n) { A[t] = u1[UO(j0 + t)]; W[t] = u3[UO(j0 + t)]; VA[t] = u2[VO(j0 + t)]; }
-#pragma unroll
-        for (int t = 0; t < CFD_SKP; ++t) {
-            const int jj = j0 + t;
-            if (jj >= n) break;
-            const double2 dv = dadd(dadd(dik(kxv, A[t]), dik(kzv, W[t])),
-                                    dscl(g.dthdyu[d.jp0 + jj - d.ju0], dsub(VA[t], vbs)));
-            vbs = VA[t];
-            double2 r = dscl(dtirk, dv);
-            double a1, a2, a3;
-            dg_coef(d, g, n, jj, col, k2x, k2z, mean_diag, a1, a2, a3);
-            if (jj == 0 && col == 0) r = dc(0, 0);
-            const double dj = jj == 0 ? 1.0 / a2 : 1.0 / (a2 - a1 * es);
-            ys = jj == 0 ? dscl(dj, r) : dscl(dj, dsub(r, dscl(a1, ys)));
-            Y[t] = ys;
-            es = a3 * dj;
-            E[t] = es;
-        }
-#pragma unroll
-        for (int t = CFD_SKP - 1; t >= 0; --t) {
-            const int jj = j0 + t;
-            if (jj >= n) continue;
-            const double2 xp = x;  // psi(jj + 1)
-            x = jj == n - 1 ? Y[t] : dsub(Y[t], dscl(E[t], x));
-            const size_t po = (size_t)jj * nc + col;
-            p[po] = dadd(p[po], x);
-            u1[UO(jj)] = dsub(A[t], dik(dtrk * kxv, x));
-            u3[UO(jj)] = dsub(W[t], dik(dtrk * kzv, x));
-            if (jj == n - 1) {
-                // ghost centre above the top p-row (v_corr, littleharsh.f90:796-907)
-                u1[UO(jj + 1)] = dscl(-g.gwt, u1[UO(jj)]);
-                u3[UO(jj + 1)] = dscl(-g.gwt, u3[UO(jj)]);
-            } else {
-                const size_t jv = (size_t)(d.jp0 + jj - d.jv0);
-                u2[VO(jj)] = dsub(VA[t], dscl(dtrk * g.dthdyv[jv], dsub(xp, x)));
-            }
-        }
-    }
-    u1[col] = dscl(-g.gwb, u1[nc + col]);
-    u3[col] = dscl(-g.gwb, u3[nc + col]);
-    u2[col] = dc(0, 0);
-    u2[(size_t)(d.nyv - 1) * nc + col] = dc(0, 0);
 }
 
 // v_corr without the closing divergence, one thread per column and a chunk of JC planes
