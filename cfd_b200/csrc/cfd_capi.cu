@@ -333,8 +333,7 @@ int tune_int(int32_t cfd_tuning::*field, const char* env, int dflt, int lo, int 
 
 size_t xline2_smem(int n1s, int n2s, int rw, size_t esz) {
     const int N = n1s * n2s;
-    const int S = 128 / (int)esz;
-    const int L1 = xline2_pitch(n1s * (n2s + 1), rw, S), L2 = xline2_pitch(n2s * (n1s + 1), rw, S), LU = N + 1;
+    const int L1 = n1s * (n2s + 1) + 1, L2 = n2s * (n1s + 1) + 1, LU = N + 1;
     const int LX = std::max(L1, std::max(L2, LU));
     return ((size_t)2 * rw * LX + N) * esz;
 }

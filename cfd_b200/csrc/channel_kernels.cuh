@@ -283,18 +283,6 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // The retained modes are kx = 0..N/3 (N1 = 2*(Ngal1/3)), a compile-time bound, so which
 // elements of a subsequence are zero, direct or conjugated is resolved at compile time
 // except in the two blocks that straddle a boundary.
-// Row pitch (values) of the x-line exchange buffers.  In step 2 a shared-memory wavefront
-// (S complex values: 16 in FP32, 8 in FP64) serves lanes of 2*RW lines times S/(2*RW)
-// positions k1 of one row, one position apart; a pitch L = s (mod 2s), s = S/(2*RW) (at
-// least 1), puts all of them in distinct banks.
-__host__ __device__ __forceinline__ int xline2_pitch(int L0, int RW, int S) {
-    int s = S / (2 * RW);
-    if (s < 1) s = 1;
-    int L = L0;
-    while (L % (2 * s) != s) ++L;
-    return L;
-}
-
 template <typename T2, int N1, int N2>
 __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
@@ -302,11 +290,10 @@ __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict_
     constexpr int N = N1 * N2;
     constexpr int HX = N / 3;               // highest retained kx
     constexpr int NK = HX + 1;              // kx columns per row (= d.nkx)
-    constexpr int S = 128 / (int)sizeof(T2);              // values per shared-memory wavefront
-    const int L1 = xline2_pitch(N1 * (N2 + 1), RW, S);    // inverse exchange, per line: [k1][n2]
-    const int L2 = xline2_pitch(N2 * (N1 + 1), RW, S);    // forward exchange, per line: [kb][na]
-    constexpr int LU = N + 1;                              // unpack buffer, per line
-    const int LX = L1 > L2 ? (L1 > LU ? L1 : LU) : (L2 > LU ? L2 : LU);
+    constexpr int L1 = N1 * (N2 + 1) + 1;  // inverse exchange, per line: [k1][n2]
+    constexpr int L2 = N2 * (N1 + 1) + 1;  // forward exchange, per line: [kb][na]
+    constexpr int LU = N + 1;               // unpack buffer, per line
+    constexpr int LX = (L1 > L2 ? (L1 > LU ? L1 : LU) : (L2 > LU ? L2 : LU));
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = 2 * RW;
     T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX
