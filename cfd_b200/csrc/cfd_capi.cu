@@ -335,7 +335,7 @@ size_t xline2_smem(int n1s, int n2s, int rw, size_t esz) {
     const int N = n1s * n2s;
     const int L1 = n1s * (n2s + 1) + 1, L2 = n2s * (n1s + 1) + 1, LU = N + 1;
     const int LX = std::max(L1, std::max(L2, LU));
-    return ((size_t)2 * rw * LX + N) * esz;
+    return ((size_t)2 * rw * LX + (size_t)n1s * (n2s + 1)) * esz;  // exchange rows + twiddle table
 }
 
 // ---------------------------------------------------------------------------------------

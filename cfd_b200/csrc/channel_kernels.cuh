@@ -297,7 +297,10 @@ __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = 2 * RW;
     T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX
-    T2* twt = ex + (size_t)B * LX;                   // N1 * N2: twt[b*N2 + a] = w^(a*b), a < N2, b < N1
+    // twt[b*(N2+1) + a] = w^(a*b), a < N2, b < N1; the odd row pitch keeps the lanes of a
+    // step-2 wavefront, which read two or more rows b at once, in distinct banks
+    constexpr int TP = N2 + 1;
+    T2* twt = ex + (size_t)B * LX;
     // u- and v-slots interleaved in y (nyu = nyv + 1), so that the y-neighbour planes read
     // by the interpolation are still in L2 from the adjacent slots
     const int slot = (blockIdx.y & 1) ? d.nyu + (blockIdx.y >> 1) : (blockIdx.y >> 1);
@@ -306,7 +309,7 @@ __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict_
     const int t = threadIdx.x;
     for (int i = t; i < N; i += blockDim.x) {
         const int b = i / N2, a = i - b * N2;
-        twt[i] = twx[(a * b) % N];
+        twt[b * TP + a] = twx[(a * b) % N];
     }
     const size_t pbase = (size_t)slot * d.ngal2 * NK;
     // y-interpolated sources of this slot, each ca * plane a + cb * plane b of Hx:
@@ -392,7 +395,7 @@ __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict_
         rdft_z<N1, +1, gap_blocks<N1, N2, HX>()>(v);
         T2* o = ex + (size_t)b * L1 + n2;
 #pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) o[k1 * (N2 + 1)] = k1 == 0 ? v[0] : cmulc(v[k1], twt[k1 * N2 + n2]);
+        for (int k1 = 0; k1 < N1; ++k1) o[k1 * (N2 + 1)] = k1 == 0 ? v[0] : cmulc(v[k1], twt[k1 * TP + n2]);
     }
     __syncthreads();
 
@@ -418,7 +421,7 @@ __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict_
         }
         rdft<N2, -1>(y);
 #pragma unroll
-        for (int kb = 1; kb < N2; ++kb) y[kb] = cmul(y[kb], twt[k1 * N2 + kb]);
+        for (int kb = 1; kb < N2; ++kb) y[kb] = cmul(y[kb], twt[k1 * TP + kb]);
     }
     __syncthreads();  // every lane has read the inverse exchange
     if (act2) {
