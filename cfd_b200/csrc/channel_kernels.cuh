@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(256) k_xline(Dims d, T2* __restrict__ H0, T2* 
 // The retained modes are kx = 0..N/3 (N1 = 2*(Ngal1/3)), a compile-time bound, so which
 // elements of a subsequence are zero, direct or conjugated is resolved at compile time
 // except in the two blocks that straddle a boundary.
-template <typename T2, int N1, int N2>
+template <typename T2, int N1, int N2, int TPAD = 1>
 __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0, T2* __restrict__ H1, T2* __restrict__ H2,
                          T2* __restrict__ H3, const T2* __restrict__ twx, int RW, int lrw) {
     using R = decltype(T2::x);
@@ -297,9 +297,9 @@ __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int B = 2 * RW;
     T2* ex = reinterpret_cast<T2*>(smem_raw);       // B * LX
-    // twt[b*(N2+1) + a] = w^(a*b), a < N2, b < N1; the odd row pitch keeps the lanes of a
-    // step-2 wavefront, which read two or more rows b at once, in distinct banks
-    constexpr int TP = N2 + 1;
+    // twt[b*(N2+TPAD) + a] = w^(a*b), a < N2, b < N1; an odd row pitch (TPAD = 1) keeps the
+    // lanes of a step-2 wavefront, which read two or more rows b at once, in distinct banks
+    constexpr int TP = N2 + TPAD;
     T2* twt = ex + (size_t)B * LX;
     // u- and v-slots interleaved in y (nyu = nyv + 1), so that the y-neighbour planes read
     // by the interpolation are still in L2 from the adjacent slots
@@ -309,7 +309,7 @@ __device__ __forceinline__ void xline2_body(Dims d, Geo g, const T2* __restrict_
     const int t = threadIdx.x;
     for (int i = t; i < N; i += blockDim.x) {
         const int b = i / N2, a = i - b * N2;
-        twt[b * TP + a] = twx[(a * b) % N];
+        twt[TPAD ? b * TP + a : i] = twx[(a * b) % N];
     }
     const size_t pbase = (size_t)slot * d.ngal2 * NK;
     // y-interpolated sources of this slot, each ca * plane a + cb * plane b of Hx:
@@ -488,7 +488,7 @@ template <int N1, int N2>
 __global__ void __maxnreg__(64) k_xline2r(Dims d, Geo g, const float2* __restrict__ Hx, float2* __restrict__ H0,
                                           float2* __restrict__ H1, float2* __restrict__ H2, float2* __restrict__ H3,
                                           const float2* __restrict__ twx, int RW, int lrw) {
-    xline2_body<float2, N1, N2>(d, g, Hx, H0, H1, H2, H3, twx, RW, lrw);
+    xline2_body<float2, N1, N2, 0>(d, g, Hx, H0, H1, H2, H3, twx, RW, lrw);  // unpadded: no spill at 64
 }
 
 // Pass 2 on packed line pairs (FP32 only).  The two lines of a row (u + i v, w + i 0) travel
