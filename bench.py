@@ -60,6 +60,8 @@ def kernel_bytes(name, setup, mixed):
         # reads every transformed field plane once (y-neighbours of the interpolation from L2)
         "k_xline2": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,
         "k_xline4": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,   # the same pass on packed line pairs
+        # the pass marching in y: every field plane read once, the products written once
+        "k_xmarch": (nfp + 4 * nyu + 2 * nyv) * hpl * ct,
         "k_zfwd": (4 * nyu + 2 * nyv) * (hpl + ncol) * ct,
         "k_rhs": ncol * ((2 * nyu + nyv + nyp) * cs + (2 * nyu + nyv) * ct + (4 * nyu + 2 * nyv) * ct
                          + (2 * nyu + nyv) * cs + (2 * nyu + nyv) * ct),

@@ -1,10 +1,10 @@
 """Autotuner of the launch shapes (cfd_tuning): for one grid, precision and GPU it builds a
 context per candidate, times RK3 steps with CUDA events, and keeps the fastest.
 
-Candidates: the x-line path (register two-step; the same held to 64 registers; with 1.5
-complex lines per row; on packed FP32 line pairs; or shared-memory Stockham) searched
-jointly with the radix order of its two-step transform (N = N1*N2 or N2*N1: which register
-DFT runs first), rows per CTA of the two-step x-line kernel, lines per CTA of the two-step
+Candidates: the x-line path (marching in y; register two-step; the same held to 64
+registers; with 1.5 complex lines per row; on packed FP32 line pairs; or shared-memory
+Stockham) searched jointly with the radix order of its two-step transform (N = N1*N2 or
+N2*N1: which register DFT runs first), rows per CTA of the two-step x-line kernel, lines per CTA of the two-step
 z kernels, the radix order of the z transforms, the y-planes per thread of the
 right-hand-side kernel, and the threads per CTA of the column sweeps.
 The search is coordinate-wise from the library default, one knob at a time, so it costs a
@@ -19,14 +19,14 @@ import os
 # A knob is one setting or a tuple of settings searched jointly: the x-line kernel and its
 # radix order interact (the register-capped kernel, path 5, only pays at one split), so a
 # one-at-a-time search from path 1 would not reach their best pair.
-KNOBS = ((("xline_path", "xsplit"), ((1, 1), (1, 2), (5, 1), (5, 2), (2, 1), (3, 1), (4, 1))),
+KNOBS = ((("xline_path", "xsplit"), ((6, 1), (1, 1), (1, 2), (5, 1), (5, 2), (2, 1), (3, 1), (4, 1))),
          ("xline_rows", (2, 4, 8)), ("zlines", (4, 8, 16)), ("zsplit", (1, 2)), ("rhs_chunk", (2, 4, 8, 16)),
          ("solve_cols", (64, 128, 256)))
 
 
 # knobs that only act with another setting (the library reports them as 0 or 1 otherwise)
 RELEVANT = {"xline_rows": lambda t: t.get("xline_path") != 2,
-            "zsplit": lambda t: t.get("xline_path") in (1, 5)}
+            "zsplit": lambda t: t.get("xline_path") in (1, 5, 6)}
 
 
 def _cache_path() -> str:
@@ -36,7 +36,7 @@ def _cache_path() -> str:
 
 def _key(setup, precision: str, gpu: str) -> str:
     c, g = setup.cfg, setup.grid
-    return f"v8|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
+    return f"v9|{gpu}|{c.ngal1}x{g.nyu}x{c.ngal2}|{precision}|ib{setup.ibu.n > 0}"
 
 
 def time_step(setup, precision, device, tuning, steps=5, warmup=2):

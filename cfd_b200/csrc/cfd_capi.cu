@@ -20,6 +20,7 @@
 #include "channel_kernels.cuh"
 #include "bands_kernels.cuh"
 #include "stats_kernels.cuh"
+#include "xmarch.cuh"
 
 using namespace cfd;
 
@@ -113,6 +114,10 @@ struct cfd_ctx {
     bool XL3 = false;       // packed two-step x-line kernel (k_xline3) instead of k_xline2
     bool XALT = false, ZALT = false;  // transposed two-step splits (x-line; nonlinear z kernels)
     bool XR64 = false;      // FP32 x-line kernel held to 64 registers (k_xline2r, path 5)
+    // x-line pass marching in y (k_xmarch, path 6, FP32): rows per CTA, threads, emission
+    // steps per CTA (the y-chunk), shared memory
+    int XMRW = 0, NTXM = 0, XMC = 0;
+    size_t SMXM = 0;
     bool ZR = false;        // FP64 nonlinear z kernels held to 112 registers (k_zinv2sd, k_zfwd2d)
     // three bands: the launch dimensions of the nonlinear pass over the bottom wall band,
     // the middle band and the top wall band; the middle band's transforms
@@ -286,6 +291,18 @@ int ilog2(int b) {
         default: ok = false; break;                                          \
     }
 
+// Splits of the marching x-line kernel (x-line path 6): its second step holds N2 = 8 or 16
+// points per lane, so that the unpack partners kb and N2 - kb share a warp
+#define MARCH_SWITCH(n, ok, ...)                                             \
+    switch (n) {                                                             \
+        case 64: { constexpr int TN1 = 8, TN2 = 8; __VA_ARGS__; } break;     \
+        case 96: { constexpr int TN1 = 12, TN2 = 8; __VA_ARGS__; } break;    \
+        case 128: { constexpr int TN1 = 8, TN2 = 16; __VA_ARGS__; } break;   \
+        case 192: { constexpr int TN1 = 12, TN2 = 16; __VA_ARGS__; } break;  \
+        case 384: { constexpr int TN1 = 24, TN2 = 16; __VA_ARGS__; } break;  \
+        default: ok = false; break;                                          \
+    }
+
 // The transposed splits (the other radix order), selected by cfd_tuning.xsplit/zsplit = 2
 // for the x-line kernel and the nonlinear pass's z kernels.
 #define TWO_SWITCH_ALT(n, ok, ...)                                           \
@@ -405,6 +422,14 @@ int set_smem_attrs(cfd_ctx* c) {
                 if (e == cudaSuccess && c->XR64)
                     e = cudaFuncSetAttribute(k_xline2r<TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM2);
         });
+        if constexpr (std::is_same<T2, float2>::value)
+            if (c->XMRW) {
+                MARCH_SWITCH(n1, ok, {
+                    if (e == cudaSuccess)
+                        e = cudaFuncSetAttribute(k_xmarch<float2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)c->SMXM);
+                });
+            }
         TWO_SWITCH(n1, ok, {
             if (e == cudaSuccess && c->XL3)
                 e = cudaFuncSetAttribute(k_xline3<T2, TN1, TN2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->SM3);
@@ -562,6 +587,19 @@ int nl_transforms(cfd_ctx* c) {
                                                                      (float2*)c->H[3], twx<float2>(c), c->RW4);
             });
             LK("k_xline4");
+            xdone = true;
+        }
+    }
+    if constexpr (std::is_same<T2, float2>::value) {
+        if (!xdone && c->XMRW) {
+            dim3 gxm(d.ngal2 / c->XMRW, (d.nyu - 1 + c->XMC - 1) / c->XMC);
+            bool ok = true;
+            MARCH_SWITCH(d.ngal1, ok, {
+                k_xmarch<float2, TN1, TN2><<<gxm, c->NTXM, c->SMXM, c->stream>>>(
+                    d, c->g, (const float2*)c->Hx, (float2*)c->H[0], (float2*)c->H[1], (float2*)c->H[2],
+                    (float2*)c->H[3], twx<float2>(c), c->XMRW, c->XMC);
+            });
+            LK("k_xmarch");
             xdone = true;
         }
     }
@@ -1158,7 +1196,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         c->RWibf /= 2;
     if (d.ngal2 % c->RWibf) return fail(c, CFD_ERR_SIZE, "Ngal2 must be even");
     // the transposed split of the x-line transform (tuning xsplit = 2) is for path 1 only
-    const int xpath = g_tuning && g_tuning->xline_path ? g_tuning->xline_path : env_int("CFD_XLINE_PATH", 1, 1, 5);
+    const int xpath = g_tuning && g_tuning->xline_path ? g_tuning->xline_path : env_int("CFD_XLINE_PATH", mixed ? 6 : 1, 1, 6);
     const bool xalt = (xpath == 1 || xpath == 5) && tune_int(&cfd_tuning::xsplit, "CFD_XSPLIT", 1, 1, 2) == 2;
     {
         bool ok = true;
@@ -1198,7 +1236,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     }
     if ((g_tuning && g_tuning->xline_path == 2) ||
         (!(g_tuning && (g_tuning->xline_path == 1 || g_tuning->xline_path == 3 || g_tuning->xline_path == 4 ||
-                         g_tuning->xline_path == 5)) &&
+                         g_tuning->xline_path == 5 || g_tuning->xline_path == 6)) &&
          env_int("CFD_XLINE_STOCKHAM", 0, 0, 1)))
         c->RW2 = 0;
     {
@@ -1219,6 +1257,26 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (!c->RW2) c->RW4 = 0;
     c->XALT = c->RW2 && xalt;  // (xalt implies path 1: neither k_xline3 nor k_xline4)
     c->XR64 = c->RW2 && !c->XL3 && !c->RW4 && mixed && xpath == 5;
+    // the x-line pass marching in y (FP32-mixed, one band, the default there; FP64 contexts
+    // and lengths without its split run path 1): rows per CTA from xline_rows (2 or 4),
+    // emission steps per CTA from CFD_XMARCH_STEPS (16: 0.62 ms per launch at re550,
+    // against 0.63 at 8, 12 and 20 and 0.65 at 32)
+    if (c->RW2 && mixed && xpath == 6 && !c->mb && d.nyu >= 4) {
+        bool ok = true;
+        int n1s = 0, n2s = 0;
+        MARCH_SWITCH(d.ngal1, ok, { n1s = TN1; n2s = TN2; });
+        if (ok) {
+            int rw = tune_int(&cfd_tuning::xline_rows, "CFD_XLINE_ROWS", 2, 2, 8) >= 4 ? 4 : 2;
+            auto smx = [&](int r) { return (size_t)xmarch_smem_elems(n1s, n2s, r) * sizeof(float2); };
+            if (rw == 4 && (d.ngal2 % 4 || smx(4) > budget)) rw = 2;
+            if (d.ngal2 % rw == 0 && smx(rw) <= budget) {
+                c->XMRW = rw;
+                c->NTXM = xmarch_threads(n1s, n2s, rw);
+                c->SMXM = smx(rw);
+                c->XMC = env_int("CFD_XMARCH_STEPS", 16, 2, 1 << 20);
+            }
+        }
+    }
     // FP64 z kernels at 112 registers (3 CTAs of 8 lines per SM): measured 0.31 / 0.59 against
     // 0.34 / 0.61 ms per launch at re550; the 768-point split spills at that cap
     c->ZR = c->RW2 && c->precision == CFD_PREC_FP64 && d.ngal2 <= 384 && env_int("CFD_Z_R112", 1, 0, 1);
@@ -1507,8 +1565,8 @@ int cfd_create_tuned(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib
 
 int cfd_get_tuning(const cfd_ctx* c, cfd_tuning* t) {
     if (!c || !t) return CFD_ERR_ARG;
-    t->xline_path = c->RW2 ? (c->RW4 ? 4 : (c->XL3 ? 3 : (c->XR64 ? 5 : 1))) : 2;
-    t->xline_rows = c->RW4 ? c->RW4 : (c->RW2 ? c->RW2 : 0);
+    t->xline_path = c->RW2 ? (c->XMRW ? 6 : (c->RW4 ? 4 : (c->XL3 ? 3 : (c->XR64 ? 5 : 1)))) : 2;
+    t->xline_rows = c->XMRW ? c->XMRW : (c->RW4 ? c->RW4 : (c->RW2 ? c->RW2 : 0));
     t->zlines = c->LZ2 >= 0 ? (1 << c->LZ2) : 0;
     t->solve_kind = 1;
     t->solve_cols = c->SNT;

@@ -139,8 +139,14 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *                4: as 1 with the two lines of a row in packed FP32 pairs (.f32x2
  *                   instructions; FP32-mixed only, FP64 contexts run path 1),
  *                5: as 1 with the kernel held to 64 registers per thread (more CTAs per
- *                   SM; FP32-mixed only, FP64 contexts run path 1)
- *   xline_rows   rows per CTA of the two-step x-line kernel: 2, 4 or 8
+ *                   SM; FP32-mixed only, FP64 contexts run path 1),
+ *                6: x-line pass marching in y: a CTA walks a pair of z rows up the channel,
+ *                   transforms u, w and v of each plane pair once and interpolates in
+ *                   physical space (2 inverse and 3 forward lines per row and plane pair
+ *                   instead of 4 and 3); FP32-mixed one-band contexts with x lengths 64,
+ *                   96, 128, 192, 384, where it is the default (FP64 contexts, other
+ *                   lengths and three-band channels run path 1)
+ *   xline_rows   rows per CTA of the two-step x-line kernel: 2, 4 or 8 (path 6: 2 or 4)
  *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
  *   solve_kind   1: thread-per-column Thomas sweeps (the only kind; other values fall back
  *                to it)

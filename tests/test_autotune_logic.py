@@ -18,13 +18,15 @@ def fake_model(calls, bad=()):
     def time_step(setup, precision, device, tuning, steps=5, warmup=2):
         eff = dict(DEFAULT, **(tuning or {}))
         if eff["xline_path"] not in (1, 5):
-            eff["xsplit"] = eff["zsplit"] = 1  # the splits act on paths 1 and 5 only
+            eff["xsplit"] = 1  # the x split acts on paths 1 and 5 only
+        if eff["xline_path"] not in (1, 5, 6):
+            eff["zsplit"] = 1  # the z split on paths 1, 5 and 6
         for k, v in bad:
             if eff.get(k) == v:
                 raise RuntimeError(f"{k}={v} does not fit")
         calls.append(json.dumps(eff, sort_keys=True))
         t = 10.0
-        t += {1: 0.0, 2: 3.0, 3: 0.5, 4: 0.8, 5: 0.2}[eff["xline_path"]]
+        t += {1: 0.0, 2: 3.0, 3: 0.5, 4: 0.8, 5: 0.2, 6: 0.1}[eff["xline_path"]]
         if eff["xline_path"] == 5 and eff["xsplit"] == 2:
             t -= 0.5   # an interaction a one-knob-at-a-time search from path 1 would miss
         t += {2: 0.4, 4: 0.0, 8: 0.2}[eff["xline_rows"]]

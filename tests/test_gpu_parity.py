@@ -448,3 +448,43 @@ def test_register_capped_xline(torch_cuda, monkeypatch, ng1, ng2, ny, xsplit):
         for k in ("u1", "u2", "u3", "p"):
             assert rel(st[k], ref[k]) < tol, (prec, k, rel(st[k], ref[k]))
         g.close()
+
+
+@pytest.mark.parametrize("ng1,ng2,ny", FIXED_GRIDS)
+def test_marching_xline(torch_cuda, monkeypatch, ng1, ng2, ny):
+    """The x-line pass marching in y (x-line path 6, k_xmarch; FP32-mixed only) on every
+    length it takes (64, 96, 128, 192, 384; 768 and FP64 contexts run path 1), with 2 and 4
+    rows per CTA and y-chunks of 2, 3 and 32 steps (chunk boundaries at every position of
+    the interpolation stencil): within 1e-5 of the oracle after one RK3 step on u, v, w, p,
+    and within 1e-6 of the per-slot FP32 kernel on u, v, w (1e-5 on p)."""
+    from cfd_b200.channel import Channel, build_channel
+    from cfd_b200.config import tiny
+    s = build_channel(tiny(ngal1=ng1, ngal2=ng2, ny=ny, cyl_diameter=0.3, cyl_spacing=1.5, seed=3 * ng1 + ng2))
+    assert s.ibu.n > 0
+    o = oracle(s)
+    o.step(1)
+    ref = o.download_state()
+    g1 = Channel(s, device=0, precision="mixed", tuning=dict(xline_path=1))
+    g1.upload_state()
+    g1.step(1)
+    scalar = g1.download_state()
+    g1.close()
+    for rows in (2, 4):
+        for chunk in (2, 3, 32):
+            monkeypatch.setenv("CFD_XMARCH_STEPS", str(chunk))
+            g = Channel(s, device=0, precision="mixed", tuning=dict(xline_path=6, xline_rows=rows))
+            if ng1 == 768:
+                assert g.tuning()["xline_path"] == 1
+                g.close()
+                return
+            assert g.tuning()["xline_path"] == 6 and g.tuning()["xline_rows"] == rows
+            g.upload_state()
+            g.step(1)
+            st = g.download_state()
+            for k in ("u1", "u2", "u3", "p"):
+                assert rel(st[k], ref[k]) < 1e-5, (rows, chunk, k, rel(st[k], ref[k]))
+                assert rel(st[k], scalar[k]) < (1e-5 if k == "p" else 1e-6), (rows, chunk, k, rel(st[k], scalar[k]))
+            g.close()
+    g = Channel(s, device=0, precision="fp64", tuning=dict(xline_path=6))
+    assert g.tuning()["xline_path"] == 1
+    g.close()
