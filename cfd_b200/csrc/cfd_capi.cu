@@ -1196,7 +1196,7 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
         c->RWibf /= 2;
     if (d.ngal2 % c->RWibf) return fail(c, CFD_ERR_SIZE, "Ngal2 must be even");
     // the transposed split of the x-line transform (tuning xsplit = 2) is for path 1 only
-    const int xpath = g_tuning && g_tuning->xline_path ? g_tuning->xline_path : env_int("CFD_XLINE_PATH", mixed ? 6 : 1, 1, 6);
+    const int xpath = g_tuning && g_tuning->xline_path ? g_tuning->xline_path : env_int("CFD_XLINE_PATH", (mixed && d.ngal1 == 384) ? 6 : 1, 1, 6);
     const bool xalt = (xpath == 1 || xpath == 5) && tune_int(&cfd_tuning::xsplit, "CFD_XSPLIT", 1, 1, 2) == 2;
     {
         bool ok = true;
@@ -1257,10 +1257,12 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
     if (!c->RW2) c->RW4 = 0;
     c->XALT = c->RW2 && xalt;  // (xalt implies path 1: neither k_xline3 nor k_xline4)
     c->XR64 = c->RW2 && !c->XL3 && !c->RW4 && mixed && xpath == 5;
-    // the x-line pass marching in y (FP32-mixed, one band, the default there; FP64 contexts
-    // and lengths without its split run path 1): rows per CTA from xline_rows (2 or 4),
-    // emission steps per CTA from CFD_XMARCH_STEPS (16: 0.62 ms per launch at re550,
-    // against 0.63 at 8, 12 and 20 and 0.65 at 32)
+    // the x-line pass marching in y (FP32-mixed, one band; the default for 384-point x lines,
+    // where it measured 0.607 against 0.811 ms per launch; at 64 and 192 points the per-slot
+    // kernels were faster; FP64 contexts and lengths without its split run path 1): rows per
+    // CTA from xline_rows (2 or 4); emission steps per CTA from CFD_XMARCH_STEPS, by default
+    // the longest chunk that keeps 20 CTAs per SM (re550: 16 steps, 0.621 ms per launch
+    // against 0.625-0.636 at 8, 12, 20 and 0.65 at 32; re395: 8 steps)
     if (c->RW2 && mixed && xpath == 6 && !c->mb && d.nyu >= 4) {
         bool ok = true;
         int n1s = 0, n2s = 0;
@@ -1273,7 +1275,12 @@ int create_impl(const cfd_config* cfg, const cfd_ib_list* ibu, const cfd_ib_list
                 c->XMRW = rw;
                 c->NTXM = xmarch_threads(n1s, n2s, rw);
                 c->SMXM = smx(rw);
-                c->XMC = env_int("CFD_XMARCH_STEPS", 16, 2, 1 << 20);
+                // y-chunk: the longest of 16, 12, 8, 6, 4 steps that still gives 20 CTAs per SM
+                const int nrb = d.ngal2 / rw, ns = d.nyu - 1;
+                int cs = 4;
+                for (int cand : {16, 12, 8, 6})
+                    if ((long long)nrb * ((ns + cand - 1) / cand) >= 20LL * 148) { cs = cand; break; }
+                c->XMC = env_int("CFD_XMARCH_STEPS", cs, 2, 1 << 20);
             }
         }
     }

@@ -144,8 +144,8 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *                   transforms u, w and v of each plane pair once and interpolates in
  *                   physical space (2 inverse and 3 forward lines per row and plane pair
  *                   instead of 4 and 3); FP32-mixed one-band contexts with x lengths 64,
- *                   96, 128, 192, 384, where it is the default (FP64 contexts, other
- *                   lengths and three-band channels run path 1)
+ *                   96, 128, 192, 384 (the default at 384; FP64 contexts, other lengths
+ *                   and three-band channels run path 1); CFD_XMARCH_STEPS sets its y-chunk
  *   xline_rows   rows per CTA of the two-step x-line kernel: 2, 4 or 8 (path 6: 2 or 4)
  *   zlines       lines per CTA of the two-step z kernels: 4, 8 or 16
  *   solve_kind   1: thread-per-column Thomas sweeps (the only kind; other values fall back
