@@ -350,43 +350,65 @@ def plane_profiles(st, npts):
     return out
 
 
-def profile_error(chans, setup, spinup, nsteps, nstat=20, floor=True):
-    """Mean and rms velocity profiles of the mixed and FP64 paths from the same start: each
-    path spins up `spinup` RK3 steps, then accumulates the on-device statistics every
-    `nstat` steps over `nsteps` steps (the reference's cadence, nstat = min(20, nwrite),
-    start.f90:372).  The time step follows the reference's rule dt = min(2.5 dtv, CFL dtc)
-    (FOU3D.f90:178-181), re-chosen from the FP64 state every `nstat` steps (the reference
-    re-chooses it every step); the other runs replay the FP64 run's dt sequence so all
-    integrate with the same steps.  Reported: the largest difference over the planes
-    relative to the largest FP64 value of that profile, against the 1 % bound.  With
-    `floor`, a second FP64 run from the initial state rounded to FP32 measures how far two
-    FP64 trajectories that start one rounding apart drift in the same window (the flow is
-    chaotic, so the profiles of any two runs differ by at least this much)."""
+def profile_error(chans, setup, spinup, nsteps, nstat=20, floor=True, shared=True):
+    """Mean and rms velocity profiles of the mixed and FP64 paths: the flow is spun up
+    `spinup` RK3 steps from the seeded start, then the on-device statistics are accumulated
+    every `nstat` steps over `nsteps` steps (the reference's cadence, nstat = min(20, nwrite),
+    start.f90:372).  With `shared`, one FP64 run makes the spin-up and every path averages
+    from its final state; otherwise each path spins up on its own from the seeded start.
+    The time step follows the reference's rule dt = min(2.5 dtv, CFL dtc) (FOU3D.f90:178-181),
+    re-chosen from the FP64 state every `nstat` steps (the reference re-chooses it every
+    step); the other runs replay the FP64 run's dt sequence so all integrate with the same
+    steps.  Reported: the largest difference over the planes relative to the largest FP64
+    value of that profile, against the 1 % bound.  With `floor`, a second FP64 run from the
+    same start rounded to FP32 measures how far two FP64 trajectories that start one rounding
+    apart drift in the same window (the flow is chaotic, so the profiles of any two runs
+    differ by at least this much)."""
     if nsteps <= 0:
         return None
     npts = setup.cfg.ngal1 * setup.cfg.ngal2
     prof, dts = {}, []
     out = {"spinup_steps": spinup, "steps": nsteps, "nstat": nstat, "bound": 0.01,
+           "spinup": "one FP64 spin-up shared by every run" if shared else "each run spins up on its own",
            "dt_rule": "min(2.5 dtv, CFL dtc) from the FP64 state every nstat steps", "max_rel_diff": {}}
-    runs = [("fp64", chans["fp64"], None), ("mixed", chans["mixed"], None)]
-    if floor:
-        st = setup.state()
-        rounded = {k: v.astype(np.complex64).astype(np.complex128) for k, v in st.items()}
-        runs.append(("fp64_from_fp32_rounded_start", chans["fp64"], rounded))
-    for name, ch, start in runs:
+    start = setup.state()
+    spun = False
+    if shared and spinup > 0:
+        ch = chans["fp64"]
         ch.upload_state(start)
-        blk = 0
+        done = 0
+        try:
+            while done < spinup:
+                n = min(nstat, spinup - done)
+                dts.append(ch.adapt_dt())
+                ch.step(n)
+                done += n
+            ch.cfl()   # raises on a non-finite state
+        except RuntimeError as e:
+            out["error"] = f"fp64 spin-up: {str(e)[:160]}"
+            ch.set_dt(setup.dt)
+            return out
+        start = ch.download_state()
+        spun = True
+    runs = [("fp64", chans["fp64"], start), ("mixed", chans["mixed"], start)]
+    if floor:
+        rounded = {k: v.astype(np.complex64).astype(np.complex128) for k, v in start.items()}
+        runs.append(("fp64_from_fp32_rounded_start", chans["fp64"], rounded))
+    nspin = len(dts)
+    for name, ch, st in runs:
+        ch.upload_state(st)
+        blk = 0 if not spun else nspin
         try:
             def advance(n):
                 nonlocal blk
-                if name == "fp64":
+                if name == "fp64" and blk >= len(dts):
                     dts.append(ch.adapt_dt())
                 else:
                     ch.set_dt(dts[blk])
                 blk += 1
                 ch.step(n)
             done = 0
-            while done < spinup:
+            while not spun and done < spinup:
                 n = min(nstat, spinup - done)
                 advance(n)
                 done += n
@@ -604,6 +626,8 @@ def main():
                     help="averaging steps of the mean/rms profile comparison of mixed vs FP64 (0: skip)")
     ap.add_argument("--spinup-steps", type=int, default=2000,
                     help="spin-up steps before the profile averaging window")
+    ap.add_argument("--independent-spinup", action="store_true",
+                    help="also compare the profiles with each precision spun up on its own")
     ap.add_argument("--sustained-steps", type=int, default=200,
                     help="steps of the longer second timing window per precision (0: skip)")
     args = ap.parse_args()
@@ -651,6 +675,8 @@ def main():
         err[k] = rel_err(states["mixed"][k], states["fp64"][k])
     fp64_div = chans["fp64"].divergence_max()
     prof_err = profile_error(chans, setup, args.spinup_steps, args.profile_steps)
+    prof_err_indep = profile_error(chans, setup, args.spinup_steps, args.profile_steps, shared=False) \
+        if args.independent_spinup else None
     ens = run_ensemble(torch, device, args.steps, args.warmup, None if args.no_autotune else "auto") \
         if (ws == 1 and not args.no_ensemble) else None
 
@@ -712,6 +738,7 @@ def main():
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
         "profile_error_mixed_vs_fp64": prof_err,
+        "profile_error_independent_spinup": prof_err_indep,
         "ensemble": dict(ens, grid_pt_rate_vs_single={
             prec: ens[prec]["grid_pt_updates_per_s"] / (results[prec]["steps_per_s"] * gp)
             for prec in ("mixed", "fp64")}) if ens else None,

@@ -43,13 +43,21 @@ class _FakeChannel:
         self.setup, self.dt, self.log, self.fail_after = setup, setup.dt, [], fail_after
         self.dt_seq = list(dt_seq or [])
         self.acc = None
+        self.nadapt = 0
+        self.uploads = []
 
     def upload_state(self, state=None):
         self.log.clear()
         self.started_from = state
+        self.uploads.append(state)
+
+    def download_state(self):
+        import numpy as np
+        return {k: np.full(3, 1.0 + len(self.log), dtype=np.complex128) for k in ("u1", "u2", "u3", "p")}
 
     def adapt_dt(self):
-        self.dt = self.dt_seq[len(self.log)]
+        self.dt = self.dt_seq[self.nadapt]
+        self.nadapt += 1
         return self.dt
 
     def set_dt(self, dt):
@@ -89,10 +97,10 @@ def test_profile_error_replays_the_fp64_dt_sequence(setup):
     import bench
     seq = [1e-3 * (1 + 0.01 * k) for k in range(10)]
     f64, mix = _FakeChannel(setup, seq), _FakeChannel(setup)
-    out = bench.profile_error({"fp64": f64, "mixed": mix}, setup, spinup=40, nsteps=60, nstat=20)
+    out = bench.profile_error({"fp64": f64, "mixed": mix}, setup, spinup=40, nsteps=60, nstat=20, shared=False)
     assert [n for _, n in f64.log] == [20] * 5 and f64.log == mix.log
     # the chaos-floor run: FP64 again, from the FP32-rounded start, with the same dt sequence
-    assert f64.started_from is not None and mix.started_from is None
+    assert mix.started_from["u1"] is setup.state()["u1"]  # both spin up from the seeded start
     assert f64.started_from["u1"].dtype == "complex128"
     assert max(out["chaos_floor_max_rel_diff"].values()) == 0.0
     assert [d for d, _ in f64.log] == seq[:5]
@@ -101,12 +109,34 @@ def test_profile_error_replays_the_fp64_dt_sequence(setup):
     assert out["dt_first_last_min_max"] == [seq[0], seq[4], seq[0], seq[4]]
 
 
+def test_profile_error_shared_spinup(setup):
+    """With one shared spin-up, FP64 spins up once (re-choosing dt every nstat steps), then
+    FP64, mixed and the FP32-rounded FP64 run each average from the spun-up state with the
+    FP64 averaging window's dt sequence."""
+    import bench
+    seq = [1e-3 * (1 + 0.01 * k) for k in range(10)]
+    f64, mix = _FakeChannel(setup, seq), _FakeChannel(setup)
+    out = bench.profile_error({"fp64": f64, "mixed": mix}, setup, spinup=40, nsteps=60, nstat=20)
+    assert out["spinup"].startswith("one FP64 spin-up")
+    spun = f64.uploads[1]
+    assert f64.uploads[0]["u1"].shape == setup.state()["u1"].shape  # the seeded start
+    assert float(spun["u1"][0].real) == 3.0       # downloaded after the 2 spin-up blocks
+    assert mix.uploads == [spun]
+    assert float(f64.uploads[2]["u1"][0].real) == 3.0 and f64.uploads[2]["u1"].dtype == "complex128"
+    # averaging window: 3 blocks after the 2 spin-up blocks, the same dts in every run
+    assert [d for d, _ in mix.log] == seq[2:5] and f64.log == mix.log
+    assert out["dt_first_last_min_max"] == [seq[0], seq[4], seq[0], seq[4]]
+    assert f64.dt == setup.dt and mix.dt == setup.dt and out["within_bound"]
+
+
 def test_profile_error_reports_a_blow_up(setup):
     """A state that goes non-finite ends the window with the error and the block it
     happened in, instead of NaN profiles."""
     import bench
     seq = [1e-3] * 10
-    f64 = _FakeChannel(setup, seq, fail_after=3)
-    out = bench.profile_error({"fp64": f64, "mixed": _FakeChannel(setup)}, setup, spinup=40, nsteps=60, nstat=20)
-    assert "error" in out and "NONFINITE" in out["error"] and "within_bound" not in out
-    assert f64.dt == setup.dt
+    for shared, fail_after in ((False, 3), (True, 1)):
+        f64 = _FakeChannel(setup, seq, fail_after=fail_after)
+        out = bench.profile_error({"fp64": f64, "mixed": _FakeChannel(setup)}, setup, spinup=40, nsteps=60,
+                                  nstat=20, shared=shared)
+        assert "error" in out and "NONFINITE" in out["error"] and "within_bound" not in out
+        assert f64.dt == setup.dt
