@@ -158,7 +158,8 @@ struct cfd_ctx {
         bool on = false;          // accumulators configured
         int jband = 0, dnx = 0, dnz = 0, nbu = 0, nbv = 0, nbp = 0;
         int istat = 0;
-        int cp = 16;              // planes per field in one chunk
+        int cp = 48;              // planes per field in one chunk
+        int ns = 8;               // CTAs per plane of the plane sums
         double* su = nullptr;     // [6][nyu]
         double* sv = nullptr;     // [5][nyv]
         double* sp = nullptr;     // [2][nyp]
@@ -167,7 +168,10 @@ struct cfd_ctx {
         double* cp_ = nullptr;    // [2][2][nbp][dnz][dnx]
         double* planes = nullptr; // [3][cp] physical planes
         double* mx = nullptr;     // [3][nyu]: |u|, |w| per u plane, |v| dthdyv per v plane
-        cfd::PlaneSrc* src = nullptr;  // [3*cp]
+        // the sources of every plane of a pass, [kind u, v, p][chunk][field][cp], built once
+        // per context (the state pointers and the y weights do not change)
+        cfd::PlaneSrc* src = nullptr;
+        double* part = nullptr;   // [cp][ns][8] partial plane sums
         // spectra (spectra.f90): [plane][column] each; null when not configured
         double *spu = nullptr, *spv = nullptr, *spw = nullptr, *spuv = nullptr, *spp = nullptr;
     } st;
@@ -1444,40 +1448,29 @@ int stats_scratch(cfd_ctx* c) {
     const Dims& d = c->d;
     AL(c->st.planes, double, (size_t)3 * c->st.cp * (d.ngal1 + 2) * d.ngal2);
     AL(c->st.mx, double, (size_t)3 * d.nyu);
-    AL(c->st.src, PlaneSrc, (size_t)3 * c->st.cp);
-    return CFD_OK;
-}
-
-// One pass over the u, v and p planes in chunks of cp planes per field: build the planes
-// of the chunk from the spectral state, transform them to physical space (FP64), reduce.
-// acc = false computes only the CFL maxima (u, w on u planes, v on v planes).
-int stats_pass(cfd_ctx* c, bool acc) {
-    const Dims& d = c->d;
+    AL(c->st.part, double, (size_t)c->st.cp * c->st.ns * 8);
+    // plane sources of the whole pass
     const Geo& g = c->g;
-    auto& st = c->st;
     const size_t nc = d.ncol;
-    const long long ps = (long long)(d.ngal1 + 2) * d.ngal2;
-    const int rowc = (d.ngal1 + 2) / 2;
-    std::vector<PlaneSrc> hs(3 * st.cp);
-    // host copies of the y weights (small, read once per pass)
+    const int cp = c->st.cp;
     std::vector<double> hvca(d.nyu), hvcb(d.nyu), ufa(d.nyv), ufb(d.nyv), dthv(d.nyv);
     CK(cudaMemcpy(hvca.data(), g.vca, sizeof(double) * d.nyu, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(hvcb.data(), g.vcb, sizeof(double) * d.nyu, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(ufa.data(), g.ufa, sizeof(double) * d.nyv, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(ufb.data(), g.ufb, sizeof(double) * d.nyv, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(dthv.data(), g.dthdyv, sizeof(double) * d.nyv, cudaMemcpyDeviceToHost));
+    std::vector<PlaneSrc> hs;
     for (int kind = 0; kind < 3; ++kind) {
         const int nyg = kind == 0 ? d.nyu : (kind == 1 ? d.nyv : d.nyp);
-        const int nf = kind == 2 ? 1 : 3;
-        if (!acc && kind == 2) break;
-        for (int j0 = 0; j0 < nyg; j0 += st.cp) {
-            const int nch = std::min(st.cp, nyg - j0);
+        for (int j0 = 0; j0 < nyg; j0 += cp) {
+            const int nch = std::min(cp, nyg - j0);
+            const size_t base = hs.size();
+            hs.resize(base + (size_t)3 * cp, PlaneSrc{nullptr, nullptr, nullptr, 1.0, 0.0, 0.0});
             for (int pl = 0; pl < nch; ++pl) {
                 const int jr = j0 + pl;
-                PlaneSrc* f = &hs[pl];
-                PlaneSrc* f1 = &hs[nch + pl];
-                PlaneSrc* f2 = &hs[2 * nch + pl];
-                *f = *f1 = *f2 = PlaneSrc{nullptr, nullptr, nullptr, 1.0, 0.0, 0.0};
+                PlaneSrc* f = &hs[base + pl];
+                PlaneSrc* f1 = &hs[base + nch + pl];
+                PlaneSrc* f2 = &hs[base + 2 * nch + pl];
                 if (kind == 0) {  // u, w, v interpolated to the centre (interp_v, FOU3D.f90:285-308)
                     f->a = c->u1 + (size_t)jr * nc;
                     f1->a = c->u3 + (size_t)jr * nc;
@@ -1502,10 +1495,32 @@ int stats_pass(cfd_ctx* c, bool acc) {
                     f->a = c->p + (size_t)jr * nc;
                 }
             }
-            CK(cudaMemcpyAsync(st.src, hs.data(), sizeof(PlaneSrc) * nf * nch, cudaMemcpyHostToDevice, c->stream));
+        }
+    }
+    AL(c->st.src, PlaneSrc, hs.size());
+    CK(cudaMemcpy(c->st.src, hs.data(), sizeof(PlaneSrc) * hs.size(), cudaMemcpyHostToDevice));
+    return CFD_OK;
+}
+
+// One pass over the u, v and p planes in chunks of cp planes per field: build the planes
+// of the chunk from the spectral state, transform them to physical space (FP64), reduce.
+// acc = false computes only the CFL maxima (u, w on u planes, v on v planes).
+int stats_pass(cfd_ctx* c, bool acc) {
+    const Dims& d = c->d;
+    const Geo& g = c->g;
+    auto& st = c->st;
+    const long long ps = (long long)(d.ngal1 + 2) * d.ngal2;
+    const int rowc = (d.ngal1 + 2) / 2;
+    const PlaneSrc* src = st.src;  // advances by 3*cp entries per chunk, in pass order
+    for (int kind = 0; kind < 3; ++kind) {
+        const int nyg = kind == 0 ? d.nyu : (kind == 1 ? d.nyv : d.nyp);
+        const int nf = kind == 2 ? 1 : 3;
+        if (!acc && kind == 2) break;
+        for (int j0 = 0; j0 < nyg; j0 += st.cp, src += 3 * st.cp) {
+            const int nch = std::min(st.cp, nyg - j0);
             prof_mark(c);
             dim3 gb((rowc * d.ngal2 + 255) / 256, nf * nch);
-            k_st_build<<<gb, 256, 0, c->stream>>>(d, g, st.src, st.planes);
+            k_st_build<<<gb, 256, 0, c->stream>>>(d, g, src, st.planes);
             LK("k_st_build");
             // four_to_phys (the oddball row Ngal2/2 zeroed by four_to_phys_u lies inside the
             // dealiasing gap, which the build leaves zero)
@@ -1514,13 +1529,18 @@ int stats_pass(cfd_ctx* c, bool acc) {
             s = strided_rft(c, st.planes, d.ngal1, d.ngal1 + 2, d.ngal2, ps, nf * nch, +1);
             if (s) return s;
             prof_mark(c);
+            dim3 gs(st.ns, nch);
+            const int fb = (nch + 63) / 64;
             if (kind == 0) {
-                k_st_sums<0><<<nch, 256, 0, c->stream>>>(d, g, st.planes, nch, j0, acc ? st.su : nullptr, d.nyu, st.mx);
+                k_st_sums<0><<<gs, 256, 0, c->stream>>>(d, st.planes, nch, st.part);
+                k_st_fin<0><<<fb, 64, 0, c->stream>>>(d, g, st.part, nch, st.ns, j0, acc ? st.su : nullptr, d.nyu, st.mx);
             } else if (kind == 1) {
-                k_st_sums<1><<<nch, 256, 0, c->stream>>>(d, g, st.planes, nch, j0, acc ? st.sv : nullptr, d.nyv,
-                                                        st.mx + 2 * d.nyu);
+                k_st_sums<1><<<gs, 256, 0, c->stream>>>(d, st.planes, nch, st.part);
+                k_st_fin<1><<<fb, 64, 0, c->stream>>>(d, g, st.part, nch, st.ns, j0, acc ? st.sv : nullptr, d.nyv,
+                                                      st.mx + 2 * d.nyu);
             } else {
-                k_st_sums<2><<<nch, 256, 0, c->stream>>>(d, g, st.planes, nch, j0, st.sp, d.nyp, nullptr);
+                k_st_sums<2><<<gs, 256, 0, c->stream>>>(d, st.planes, nch, st.part);
+                k_st_fin<2><<<fb, 64, 0, c->stream>>>(d, g, st.part, nch, st.ns, j0, st.sp, d.nyp, nullptr);
             }
             LK("k_st_sums");
             if (acc && st.dnx > 0) {
@@ -1537,8 +1557,6 @@ int stats_pass(cfd_ctx* c, bool acc) {
                     k_st_cond<2><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, cb, cb + half);
                 LK("k_st_cond");
             }
-            // the host array hs is reused by the next chunk: wait for the copy
-            CK(cudaStreamSynchronize(c->stream));
         }
     }
     return CFD_OK;
@@ -2224,6 +2242,7 @@ int cfd_cfl(cfd_ctx* c, double* dtc, double* terms) {
     if (!s) s = stats_pass(c, false);
     if (s) return s;
     std::vector<double> h((size_t)3 * d.nyu);
+    CK(cudaStreamSynchronize(c->stream));  // the pass runs on the (non-blocking) context stream
     CK(cudaMemcpy(h.data(), c->st.mx, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
     double um = 0.0, wm = 0.0, vm = 1e-6;
     bool bad = false;

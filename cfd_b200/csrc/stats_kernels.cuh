@@ -8,7 +8,8 @@
 //   k_st_build   spectral columns -> plane layout, as a y-combination of up to two planes
 //                plus an optional i*kz term (the interpolations of interp_u/interp_v and
 //                omega_x = dw/dy - dv/dz at the faces)
-//   k_st_sums    one CTA per plane: plane sums (deterministic tree) and |.| maxima
+//   k_st_sums    ns CTAs per plane: partial plane sums (deterministic tree) and |.| maxima
+//   k_st_fin     the partials of each plane added in slice order into the accumulators
 //   k_st_cond    one thread per tile point: the tile-folded (conditional) sums, added in
 //                the reference's loop order so that each call's rounding matches
 #pragma once
@@ -60,13 +61,11 @@ __global__ void __launch_bounds__(256) k_st_build(Dims d, Geo g, const PlaneSrc*
 // kind 2: p planes -> Pm P2m.  Each plane j0+pl of the chunk adds its sums to acc[q][j]
 // (one writer per entry) and stores its maxima in mx[q][j].
 template <int KIND>
-__global__ void __launch_bounds__(256) k_st_sums(Dims d, Geo g, const double* __restrict__ planes, int nchunk,
-                                                 int jrel0, double* __restrict__ acc, int nyg,
-                                                 double* __restrict__ mx) {
+__global__ void __launch_bounds__(256) k_st_sums(Dims d, const double* __restrict__ planes, int nchunk,
+                                                 double* __restrict__ part) {
     constexpr int NQ = KIND == 0 ? 6 : (KIND == 1 ? 5 : 2);
-    constexpr int NM = KIND == 0 ? 2 : (KIND == 1 ? 1 : 0);
-    const int pl = blockIdx.x;
-    const int jr = jrel0 + pl;  // plane index within its grid (j - j0 of the grid)
+    const int sl = blockIdx.x, ns = gridDim.x;   // slice of the plane
+    const int pl = blockIdx.y;
     const size_t ps = (size_t)(d.ngal1 + 2) * d.ngal2;
     const double* f0 = planes + (size_t)pl * ps;
     const double* f1 = planes + (size_t)(nchunk + pl) * ps;
@@ -77,7 +76,7 @@ __global__ void __launch_bounds__(256) k_st_sums(Dims d, Geo g, const double* __
     double m0 = 0.0, m1 = 0.0;
     const int L = d.ngal1 + 2;
     const int npts = d.ngal1 * d.ngal2;
-    for (int t = threadIdx.x; t < npts; t += blockDim.x) {
+    for (int t = sl * blockDim.x + threadIdx.x; t < npts; t += ns * blockDim.x) {
         const int k = t / d.ngal1, i = t - k * d.ngal1;
         const size_t o = (size_t)k * L + i;
         const double x0 = f0[o];
@@ -110,17 +109,38 @@ __global__ void __launch_bounds__(256) k_st_sums(Dims d, Geo g, const double* __
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        if (acc)
+    if (threadIdx.x < NQ + 2) part[((size_t)pl * ns + sl) * (NQ + 2) + threadIdx.x] = red[threadIdx.x * 256];
+}
+
+// The partial sums of the slices of each plane, added in slice order (deterministic), into
+// the plane accumulators; the maxima of |.| per plane for the CFL query.  One thread per plane.
+template <int KIND>
+__global__ void k_st_fin(Dims d, Geo g, const double* __restrict__ part, int nchunk, int ns, int jrel0,
+                         double* __restrict__ acc, int nyg, double* __restrict__ mx) {
+    constexpr int NQ = KIND == 0 ? 6 : (KIND == 1 ? 5 : 2);
+    constexpr int NM = KIND == 0 ? 2 : (KIND == 1 ? 1 : 0);
+    const int pl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pl >= nchunk) return;
+    const int jr = jrel0 + pl;  // plane index within its grid (j - j0 of the grid)
+    double s[NQ + 2];
 #pragma unroll
-            for (int k = 0; k < NQ; ++k) acc[(size_t)k * nyg + jr] += red[k * 256];
-        if (NM >= 1) {
-            double v = red[NQ * 256];
-            if (KIND == 1) v = (jr > 0 && jr < nyg - 1) ? v * g.dthdyv[jr] : 0.0;
-            mx[jr] = v;
-        }
-        if (NM >= 2) mx[nyg + jr] = red[(NQ + 1) * 256];
+    for (int k = 0; k < NQ + 2; ++k) s[k] = 0.0;
+    for (int sl = 0; sl < ns; ++sl) {
+        const double* q = part + ((size_t)pl * ns + sl) * (NQ + 2);
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) s[k] += q[k];
+        s[NQ] = nan_max(s[NQ], q[NQ]);
+        s[NQ + 1] = nan_max(s[NQ + 1], q[NQ + 1]);
     }
+    if (acc)
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) acc[(size_t)k * nyg + jr] += s[k];
+    if (NM >= 1) {
+        double v = s[NQ];
+        if (KIND == 1) v = (jr > 0 && jr < nyg - 1) ? v * g.dthdyv[jr] : 0.0;
+        mx[jr] = v;
+    }
+    if (NM >= 2) mx[nyg + jr] = s[NQ + 1];
 }
 
 // Conditional sums of one chunk.  grid: x = tile-point blocks, y = plane of the chunk.
