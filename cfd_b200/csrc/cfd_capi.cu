@@ -172,6 +172,8 @@ struct cfd_ctx {
         // per context (the state pointers and the y weights do not change)
         cfd::PlaneSrc* src = nullptr;
         double* part = nullptr;   // [cp][ns][8] partial plane sums
+        int nseg = 1;             // segments of tile rows of the conditional sums
+        double* cpart = nullptr;  // [cp][2][nseg][6][dnx*dnz] their partial sums (nseg > 1)
         // spectra (spectra.f90): [plane][column] each; null when not configured
         double *spu = nullptr, *spv = nullptr, *spw = nullptr, *spuv = nullptr, *spp = nullptr;
     } st;
@@ -1547,14 +1549,25 @@ int stats_pass(cfd_ctx* c, bool acc) {
                 const int nb = kind == 0 ? st.nbu : (kind == 1 ? st.nbv : st.nbp);
                 const size_t half = (size_t)(kind == 0 ? 6 : (kind == 1 ? 5 : 2)) * nb * st.dnx * st.dnz;
                 double* cb = kind == 0 ? st.cu : (kind == 1 ? st.cv : st.cp_);
-                dim3 gc((st.dnx * st.dnz + 255) / 256, nch);
+                const int tsz = st.dnx * st.dnz, nseg = st.nseg;
+                dim3 gc((tsz * nseg + 255) / 256, nch), gf((tsz + 255) / 256, nch);
                 prof_mark(c);
-                if (kind == 0)
-                    k_st_cond<0><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, cb, cb + half);
-                else if (kind == 1)
-                    k_st_cond<1><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, cb, cb + half);
-                else
-                    k_st_cond<2><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, cb, cb + half);
+                if (kind == 0) {
+                    k_st_cond<0><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, nseg,
+                                                            st.cpart, cb, cb + half);
+                    if (nseg > 1)
+                        k_st_cond_fin<0><<<gf, 256, 0, c->stream>>>(st.cpart, j0, nyg, nb, tsz, nseg, cb, cb + half);
+                } else if (kind == 1) {
+                    k_st_cond<1><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, nseg,
+                                                            st.cpart, cb, cb + half);
+                    if (nseg > 1)
+                        k_st_cond_fin<1><<<gf, 256, 0, c->stream>>>(st.cpart, j0, nyg, nb, tsz, nseg, cb, cb + half);
+                } else {
+                    k_st_cond<2><<<gc, 256, 0, c->stream>>>(d, st.planes, nch, j0, nyg, nb, st.dnx, st.dnz, nseg,
+                                                            st.cpart, cb, cb + half);
+                    if (nseg > 1)
+                        k_st_cond_fin<2><<<gf, 256, 0, c->stream>>>(st.cpart, j0, nyg, nb, tsz, nseg, cb, cb + half);
+                }
                 LK("k_st_cond");
             }
         }
@@ -1938,8 +1951,9 @@ int cfd_stats_configure(cfd_ctx* c, const cfd_stats_config* sc) {
             return fail(c, CFD_ERR_ARG, "tile %d x %d must divide Ngal1 x Ngal2", sc->dnx, sc->dnz);
         if (sc->jband + 1 > d.ju1) return fail(c, CFD_ERR_ARG, "jband %d above the channel", sc->jband);
     }
-    for (double* p : {st.su, st.sv, st.sp, st.cu, st.cv, st.cp_, st.spu, st.spv, st.spw, st.spuv, st.spp}) dfree(c, p);
-    st.su = st.sv = st.sp = st.cu = st.cv = st.cp_ = nullptr;
+    for (double* p : {st.su, st.sv, st.sp, st.cu, st.cv, st.cp_, st.spu, st.spv, st.spw, st.spuv, st.spp, st.cpart})
+        dfree(c, p);
+    st.su = st.sv = st.sp = st.cu = st.cv = st.cp_ = st.cpart = nullptr;
     st.spu = st.spv = st.spw = st.spuv = st.spp = nullptr;
     int s = stats_scratch(c);
     if (s) return s;
@@ -1957,6 +1971,9 @@ int cfd_stats_configure(cfd_ctx* c, const cfd_stats_config* sc) {
     AL(st.cu, double, 2 * 6 * st.nbu * tsz);
     AL(st.cv, double, 2 * 5 * st.nbv * tsz);
     AL(st.cp_, double, 2 * 2 * st.nbp * tsz);
+    // conditional sums: tile rows split into segments so that a plane has about 1024 threads
+    st.nseg = tsz ? (int)std::max<size_t>(1, std::min<size_t>({16, (size_t)(d.ngal2 / st.dnz), 1024 / tsz})) : 1;
+    if (st.nseg > 1) AL(st.cpart, double, (size_t)st.cp * 2 * st.nseg * 6 * tsz);
     if (sc->spectra) {
         AL(st.spu, double, (size_t)d.nyu * d.ncol);
         AL(st.spv, double, (size_t)d.nyv * d.ncol);

@@ -10,8 +10,9 @@
 //                omega_x = dw/dy - dv/dz at the faces)
 //   k_st_sums    ns CTAs per plane: partial plane sums (deterministic tree) and |.| maxima
 //   k_st_fin     the partials of each plane added in slice order into the accumulators
-//   k_st_cond    one thread per tile point: the tile-folded (conditional) sums, added in
-//                the reference's loop order so that each call's rounding matches
+//   k_st_cond    one thread per tile point and segment of tile rows: the tile-folded
+//                (conditional) sums of the segment in the reference's loop order
+//   k_st_cond_fin the segments added in order to the band accumulators
 #pragma once
 
 #include "channel_kernels.cuh"
@@ -143,38 +144,47 @@ __global__ void k_st_fin(Dims d, Geo g, const double* __restrict__ part, int nch
     if (NM >= 2) mx[nyg + jr] = s[NQ + 1];
 }
 
-// Conditional sums of one chunk.  grid: x = tile-point blocks, y = plane of the chunk.
-// Plane j (index jr in its grid) is a bottom-band plane when jr < nb (j1 = jr) and a
-// top-band plane when nyg-1-jr < nb (j1 = nyg-1-jr, v sign-flipped: condup1/condup2).
-// Accumulators: cb/ct [NQ][nb][dnz][dnx] for the bottom and the top band.
+// Conditional sums of one chunk.  grid: x = blocks of (segment, tile point), y = plane of
+// the chunk.  Plane j (index jr in its grid) is a bottom-band plane when jr < nb (j1 = jr)
+// and a top-band plane when nyg-1-jr < nb (j1 = nyg-1-jr, v sign-flipped: condup1/condup2).
+// The nseg segments split the tile rows iz; each thread adds the points of its tile point
+// in its segment in the reference's loop order (iz, then ix) and writes the partial sums
+// part[((pl*2 + side)*nseg + seg)*NQ + k][t]; k_st_cond_fin adds the segments in order to
+// the accumulators cb/ct [NQ][nb][dnz][dnx] of the bottom and the top band.  With one
+// segment the thread adds straight onto the accumulator.
 template <int KIND>
 __global__ void __launch_bounds__(256) k_st_cond(Dims d, const double* __restrict__ planes, int nchunk, int jrel0,
-                                                 int nyg, int nb, int dnx, int dnz, double* __restrict__ cbot,
+                                                 int nyg, int nb, int dnx, int dnz, int nseg,
+                                                 double* __restrict__ part, double* __restrict__ cbot,
                                                  double* __restrict__ ctop) {
     constexpr int NQ = KIND == 0 ? 6 : (KIND == 1 ? 5 : 2);
     const int pl = blockIdx.y;
     const int jr = jrel0 + pl;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= dnx * dnz) return;
+    const int tsz = dnx * dnz;
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= tsz * nseg) return;
+    if (jr >= nb && nyg - 1 - jr >= nb) return;   // a plane of neither band
+    const int seg = u / tsz, t = u - seg * tsz;
     const int tk = t / dnx, ti = t - tk * dnx;
     const int ntx = d.ngal1 / dnx, ntz = d.ngal2 / dnz;
+    const int iz0 = (int)((long long)ntz * seg / nseg), iz1 = (int)((long long)ntz * (seg + 1) / nseg);
     const size_t ps = (size_t)(d.ngal1 + 2) * d.ngal2;
     const int L = d.ngal1 + 2;
     const double* f0 = planes + (size_t)pl * ps;
     const double* f1 = planes + (size_t)(nchunk + pl) * ps;
     const double* f2 = planes + (size_t)(2 * nchunk + pl) * ps;
-    const size_t tsz = (size_t)dnx * dnz;
     for (int side = 0; side < 2; ++side) {
         const int j1 = side == 0 ? jr : nyg - 1 - jr;
         if (j1 < 0 || j1 >= nb) continue;
         // sign of v in the top band (condup1 xsign = -1 for v, condup2 -1 on the v factor)
         const double sv = (side == 1) ? -1.0 : 1.0;
+        // one segment: add straight onto the accumulator (the reference's order throughout)
         double* C = (side == 0 ? cbot : ctop) + (size_t)j1 * tsz + t;
         const size_t qs = (size_t)nb * tsz;  // stride between quantities
         double a[NQ];
 #pragma unroll
-        for (int k = 0; k < NQ; ++k) a[k] = C[k * qs];
-        for (int iz = 0; iz < ntz; ++iz) {
+        for (int k = 0; k < NQ; ++k) a[k] = nseg == 1 ? C[k * qs] : 0.0;
+        for (int iz = iz0; iz < iz1; ++iz) {
             const size_t ro = (size_t)(tk + dnz * iz) * L + ti;
             for (int ix = 0; ix < ntx; ++ix) {
                 const size_t o = ro + (size_t)dnx * ix;
@@ -200,8 +210,40 @@ __global__ void __launch_bounds__(256) k_st_cond(Dims d, const double* __restric
                 }
             }
         }
+        if (nseg == 1) {
 #pragma unroll
-        for (int k = 0; k < NQ; ++k) C[k * qs] = a[k];
+            for (int k = 0; k < NQ; ++k) C[k * qs] = a[k];
+        } else {
+            double* P = part + ((size_t)(pl * 2 + side) * nseg + seg) * NQ * tsz + t;
+#pragma unroll
+            for (int k = 0; k < NQ; ++k) P[(size_t)k * tsz] = a[k];
+        }
+    }
+}
+
+// The segments of k_st_cond added in segment order to the band accumulators.  grid: x =
+// tile-point blocks, y = plane of the chunk.
+template <int KIND>
+__global__ void __launch_bounds__(256) k_st_cond_fin(const double* __restrict__ part, int jrel0, int nyg, int nb,
+                                                     int tsz, int nseg, double* __restrict__ cbot,
+                                                     double* __restrict__ ctop) {
+    constexpr int NQ = KIND == 0 ? 6 : (KIND == 1 ? 5 : 2);
+    const int pl = blockIdx.y;
+    const int jr = jrel0 + pl;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tsz) return;
+    for (int side = 0; side < 2; ++side) {
+        const int j1 = side == 0 ? jr : nyg - 1 - jr;
+        if (j1 < 0 || j1 >= nb) continue;
+        double* C = (side == 0 ? cbot : ctop) + (size_t)j1 * tsz + t;
+        const size_t qs = (size_t)nb * tsz;  // stride between quantities
+        const double* P = part + (size_t)(pl * 2 + side) * nseg * NQ * tsz + t;
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) {
+            double sum = P[(size_t)k * tsz];
+            for (int seg = 1; seg < nseg; ++seg) sum += P[((size_t)seg * NQ + k) * tsz];
+            C[k * qs] += sum;
+        }
     }
 }
 
