@@ -442,6 +442,41 @@ def profile_error(chans, setup, spinup, nsteps, nstat=20, floor=True, shared=Tru
     return out
 
 
+def stats_pass_timing(torch, ch, setup, stream, reps=5):
+    """The statistics pass of the reference (stats.f90, every nstat steps at kRK = 1) on the
+    current state: CUDA-event ms per cfd_stats_accumulate with plane sums only and with the
+    conditional sums over the cylinder lattice's tile (bottom band up to the canopy top,
+    as the reference's conddown/condup), its per-kernel split, and the host-timed CFL query."""
+    from cfd_b200.geometry import lattice_params
+    _, _, dnx, dnz, *_ = lattice_params(setup.cfg)
+    g = setup.grid
+    jtop = setup.ibv.jhi[0] if setup.ibv.n else g.jv0 + g.nyv // 4   # top of the bottom canopy
+    out = {"tile": [dnx, dnz], "jband": int(min(jtop, g.jv1 - 1))}
+    for name, jband in (("plane_sums_ms", g.jv0 - 1), ("with_conditional_ms", out["jband"])):
+        ch.stats_configure(jband, dnx, dnz)
+        ch.stats_accumulate()
+        ch.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(reps):
+            ch.stats_accumulate()
+        e.record(stream)
+        e.synchronize()
+        out[name] = s.elapsed_time(e) / reps
+    ch.lib.cfd_profile(ch.ctx, 1)
+    ch.stats_accumulate()
+    ch.lib.cfd_profile(ch.ctx, 0)
+    buf = C.create_string_buffer(1 << 16)
+    ch.lib.cfd_profile_read(ch.ctx, buf, len(buf))
+    out["kernels_ms"] = {ln.split()[0]: float(ln.split()[2]) for ln in buf.value.decode().splitlines()}
+    ch.stats_reset()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ch.cfl()
+    out["cfl_query_ms"] = (time.perf_counter() - t0) / reps * 1e3
+    return out
+
+
 def run_ensemble(torch, device, nsteps, warmup, tuning):
     """The 16-member batched ensemble (4 x 96x97x96, 8 x 128x129x128, 4 x 192x161x192, own
     seeds and cylinder diameters) in both precisions: RK3 steps/s of the whole ensemble with
@@ -690,6 +725,7 @@ def main():
     per_launch_s = kms / kcalls / 1e3
     achieved = kb / per_launch_s / 1e9 if kb else None
     prof64 = profile_step(chans["fp64"])
+    stats_t = stats_pass_timing(torch, chans["mixed"], setup, stream) if ws == 1 else None
 
     # end-to-end through the C ABI with pinned host buffers: H2D state, step, D2H state,
     # for both precisions (FP64 is the reference's arithmetic)
@@ -739,6 +775,7 @@ def main():
         "error_mixed_vs_fp64": {"steps": args.error_steps, "rel_l2": err},
         "profile_error_mixed_vs_fp64": prof_err,
         "profile_error_independent_spinup": prof_err_indep,
+        "statistics_pass": stats_t,
         "ensemble": dict(ens, grid_pt_rate_vs_single={
             prec: ens[prec]["grid_pt_updates_per_s"] / (results[prec]["steps_per_s"] * gp)
             for prec in ("mixed", "fp64")}) if ens else None,
