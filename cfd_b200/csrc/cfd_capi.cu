@@ -1430,7 +1430,9 @@ int strided_rft(cfd_ctx* c, double* dptr, int n, int isa, int m, long long bstri
     const int CH = 8;
     const int sm = fft_generic_smem(n, CH);
     CK(cudaFuncSetAttribute(k_rft_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    dim3 grid((m + CH - 1) / CH, nb);
+    // the inverse transforms two lines per complex transform
+    const int lines = iopt > 0 ? (m + 1) / 2 : m;
+    dim3 grid((lines + CH - 1) / CH, nb);
     prof_mark(c);
     k_rft_strided<<<grid, 256, sm, c->stream>>>(dptr, isa, m, bstride, fd, tw, iopt, CH);
     LK("k_rft_strided");

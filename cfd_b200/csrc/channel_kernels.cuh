@@ -2063,7 +2063,8 @@ __global__ void __launch_bounds__(256) k_cft_strided(double* __restrict__ c, int
 
 __global__ void __launch_bounds__(256) k_rft_strided(double* __restrict__ c, int isa, int m, long long bstride,
                                                      FFTDesc fd, const double2* __restrict__ tw_g, int iopt, int CH) {
-    // each line: complex transform of length n of (real, 0) data; FFTPACK storage
+    // forward: each line a complex transform of length n of (real, 0) data, FFTPACK
+    // storage; inverse: two lines per complex transform
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = fd.n;
     double2* buf0 = reinterpret_cast<double2*>(smem_raw);
@@ -2072,36 +2073,47 @@ __global__ void __launch_bounds__(256) k_rft_strided(double* __restrict__ c, int
     double* base = c + (size_t)blockIdx.y * bstride;
     const int l0 = blockIdx.x * CH;
     for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = tw_g[t];
+    if (iopt > 0) {
+        // inverse: CTA line slot b carries the line pair (2(l0+b), 2(l0+b)+1) as one complex
+        // transform of X_a + i X_b (both Hermitian extensions of cc(0..n/2), Im cc(0) and
+        // Im cc(n/2) ignored), whose output is x_a + i x_b
+        for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+            const int b = t % CH, k = t / CH, la = 2 * (l0 + b), lb = la + 1;
+            double2 A = dc(0, 0), B = dc(0, 0);
+            const int kk = k <= n / 2 ? k : n - k;
+            const bool edge = kk == 0 || kk == n / 2;
+            if (la < m) { const double* x = base + (size_t)la * isa; A = dc(x[2 * kk], edge ? 0.0 : x[2 * kk + 1]); }
+            if (lb < m) { const double* x = base + (size_t)lb * isa; B = dc(x[2 * kk], edge ? 0.0 : x[2 * kk + 1]); }
+            if (k > n / 2) { A.y = -A.y; B.y = -B.y; }
+            buf0[swz(k, b, __ffs(CH) - 1)] = dc(A.x - B.y, A.y + B.x);
+        }
+        __syncthreads();
+        double2* res = fft_lines<double2>(buf0, buf1, CH, fd, tw, +1);
+        for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
+            const int b = t % CH, e = t / CH, la = 2 * (l0 + b), lb = la + 1;
+            const double2 v = res[swz(e, b, __ffs(CH) - 1)];
+            if (la < m) base[(size_t)la * isa + e] = v.x;
+            if (lb < m) base[(size_t)lb * isa + e] = v.y;
+        }
+        return;
+    }
     for (int t = threadIdx.x; t < n * CH; t += blockDim.x) {
         const int b = t % CH, k = t / CH, l = l0 + b;
         double2 v = dc(0, 0);
-        if (l < m) {
-            const double* x = base + (size_t)l * isa;
-            if (iopt < 0) {
-                v = dc(x[k], 0.0);
-            } else {
-                // Hermitian extension of cc(0..n/2); Im cc(0), Im cc(n/2) ignored
-                if (k <= n / 2) v = dc(x[2 * k], (k == 0 || k == n / 2) ? 0.0 : x[2 * k + 1]);
-                else v = dc(x[2 * (n - k)], -x[2 * (n - k) + 1]);
-            }
-        }
+        if (l < m) v = dc(base[(size_t)l * isa + k], 0.0);
         buf0[swz(k, b, __ffs(CH) - 1)] = v;
     }
     __syncthreads();
-    double2* res = fft_lines<double2>(buf0, buf1, CH, fd, tw, iopt < 0 ? -1 : +1);
+    double2* res = fft_lines<double2>(buf0, buf1, CH, fd, tw, -1);
     for (int t = threadIdx.x; t < (n + 2) * CH; t += blockDim.x) {
         const int b = t % CH, e = t / CH, l = l0 + b;
         if (l >= m) continue;
         double* x = base + (size_t)l * isa;
-        if (iopt < 0) {
-            const int k = e >> 1;
-            const double2 v = res[swz(k, b, __ffs(CH) - 1)];
-            double val = (e & 1) ? v.y : v.x;
-            if ((e & 1) && (k == 0 || k == n / 2)) val = 0.0;
-            x[e] = val / n;
-        } else if (e < n) {
-            x[e] = res[swz(e, b, __ffs(CH) - 1)].x;
-        }
+        const int k = e >> 1;
+        const double2 v = res[swz(k, b, __ffs(CH) - 1)];
+        double val = (e & 1) ? v.y : v.x;
+        if ((e & 1) && (k == 0 || k == n / 2)) val = 0.0;
+        x[e] = val / n;
     }
 }
 

@@ -173,6 +173,14 @@ def test_rft_cft_entry_points(torch_cuda):
     g.synchronize()
     exp = O.rft(x.ravel().copy(), n1, isa, m, -1).reshape(m, isa)
     np.testing.assert_allclose(d.cpu().numpy()[:, :n1 + 2], exp[:, :n1 + 2], atol=1e-14)
+    # inverse of the same 5 lines (transformed two per complex FFT, the last one alone):
+    # against the oracle and back to the input
+    dy = torch.tensor(exp, device="cuda")
+    assert g.lib.cfd_rft(g.ctx, C.c_void_p(dy.data_ptr()), isa, m, +1) == 0
+    g.synchronize()
+    expi = O.rft(exp.ravel().copy(), n1, isa, m, +1).reshape(m, isa)
+    np.testing.assert_allclose(dy.cpu().numpy()[:, :n1], expi[:, :n1], atol=1e-13)
+    np.testing.assert_allclose(dy.cpu().numpy()[:, :n1], x[:, :n1], atol=1e-12)
     ise, isa2, m2 = 6, 2, 3
     c = rng.standard_normal(ise * n2 + 8)
     dc = torch.tensor(c, device="cuda")
