@@ -17,7 +17,8 @@
 //            C: (ww_r + i ww_r+1), (uw_r + i uw_r+1) [u-plane t]
 // In the physical phase the three lanes of a (pair, k1) triple are adjacent (10 triples per
 // warp, lanes 30 and 31 idle) and pass u (A, B -> C) and the face value of w (C -> A, B)
-// with two shuffles, so every lane runs two forward lines.  The forward N1-point step holds
+// with two shuffles, so every lane runs two forward lines, as one packed-pair transform
+// (fft_pair.cuh: each .f32x2 instruction serves both lines).  The forward N1-point step holds
 // X[kb + N2 ka] in registers; the unpack of the two real spectra pairs X_k with X_N-k, which
 // lane N2 - kb of the same warp holds (N2 divides 32), so it needs no shared memory.
 //
@@ -29,7 +30,10 @@
 // spectral space, since no v-plane t exists; the weights are those of the per-slot kernels.
 #pragma once
 
+#include <type_traits>
+
 #include "fft_reg.cuh"
+#include "fft_pair.cuh"
 
 namespace cfd {
 
@@ -67,6 +71,7 @@ __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restr
                                                  const T2* __restrict__ twx, int RW, int csteps) {
     using R = decltype(T2::x);
     static_assert(N2 == 8 || N2 == 16, "the shuffle unpack pairs lanes kb and N2-kb inside a warp");
+    static_assert(std::is_same<T2, float2>::value, "FP32 only: the forward step runs on packed FP32 pairs");
     constexpr int N = N1 * N2;
     constexpr int HX = N / 3;               // highest retained kx
     constexpr int NK = HX + 1;              // kx columns per row
@@ -211,7 +216,7 @@ __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restr
 #pragma unroll
                 for (int k2 = 0; k2 < N2; ++k2) hist[k2 * NT + t] = y[k2];
             } else {
-                T2 la[N2], lb[N2];
+                cpair P[N2];  // the lane's two forward lines: x = (Re la, Re lb), y = (Im la, Im lb)
 #pragma unroll
                 for (int k2 = 0; k2 < N2; ++k2) {
                     const T2 h = hist[k2 * NT + t];
@@ -222,20 +227,24 @@ __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restr
                     const R r2 = __shfl_sync(0xffffffffu, isC ? f2 : y[k2].x, src2);
                     // A/B: (u u, vc vc) with vc = pa v + pb v(t-1); C: (w w, w' w')
                     const R x2 = isC ? y[k2].y : pa * y[k2].y + pb * h.y;
-                    la[k2] = cx<T2>(y[k2].x * y[k2].x, x2 * x2);
-                    // A/B: (uf v(t-1), v(t-1) wf); C: (u w, u' w')
-                    lb[k2] = cx<T2>((isC ? r1 : f) * (isC ? y[k2].x : h.y),
-                                    (isC ? r2 : h.y) * (isC ? y[k2].y : (isA ? r1 : r2)));
+                    // la: A/B (u u, vc vc); C (w w, w' w').  lb: A/B (uf v(t-1), v(t-1) wf); C (u w, u' w')
+                    const R lbx = (isC ? r1 : f) * (isC ? y[k2].x : h.y);
+                    const R lby = (isC ? r2 : h.y) * (isC ? y[k2].y : (isA ? r1 : r2));
+                    P[k2] = cpair{f2p(y[k2].x * y[k2].x, lbx), f2p(x2 * x2, lby)};
                 }
-                rdft<N2, -1>(la);
-                rdft<N2, -1>(lb);
+                rdft<N2, -1>(P);
                 if (act2) {
                     T2* oa = exf + (size_t)(6 * p2 + 2 * role) * L2 + k1;
                     T2* ob = oa + L2;
 #pragma unroll
                     for (int q = 0; q < N2; ++q) {
-                        oa[q * (N1 + 1)] = q == 0 ? la[0] : cmul(la[q], twt[k1 * TP + q]);
-                        ob[q * (N1 + 1)] = q == 0 ? lb[0] : cmul(lb[q], twt[k1 * TP + q]);
+                        cpair v = P[q];
+                        if (q > 0) {
+                            const T2 w = twt[k1 * TP + q];
+                            v = cmul(v, cpair{f2b(w.x), f2b(w.y)});
+                        }
+                        oa[q * (N1 + 1)] = cx<T2>(v.x.v.x, v.y.v.x);
+                        ob[q * (N1 + 1)] = cx<T2>(v.x.v.y, v.y.v.y);
                     }
                 }
             }
