@@ -205,7 +205,8 @@ __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restr
         __syncthreads();
 
         // ---- step 2: inverse N2-point DFT -> physical x = k1 + N1*k2; products with the
-        // previous step's values; forward N2-point DFTs of the two output lines of the lane
+        // previous step's values; the forward N2-point DFT of the lane's two output lines, la
+        // and lb, as one transform on packed FP32 pairs
         {
             T2 y[N2];
             const T2* o = exi + (size_t)b2 * L1 + k1 * (N2 + 1);
@@ -225,9 +226,9 @@ __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restr
                     const R f = fa * y[k2].x + fb * h.x, f2 = fa * y[k2].y + fb * h.y;
                     const R r1 = __shfl_sync(0xffffffffu, isC ? f : y[k2].x, src1);
                     const R r2 = __shfl_sync(0xffffffffu, isC ? f2 : y[k2].x, src2);
-                    // A/B: (u u, vc vc) with vc = pa v + pb v(t-1); C: (w w, w' w')
+                    // la: A/B (u u, vc vc) with vc = pa v + pb v(t-1); C (w w, w' w')
                     const R x2 = isC ? y[k2].y : pa * y[k2].y + pb * h.y;
-                    // la: A/B (u u, vc vc); C (w w, w' w').  lb: A/B (uf v(t-1), v(t-1) wf); C (u w, u' w')
+                    // lb: A/B (uf v(t-1), v(t-1) wf); C (u w, u' w')
                     const R lbx = (isC ? r1 : f) * (isC ? y[k2].x : h.y);
                     const R lby = (isC ? r2 : h.y) * (isC ? y[k2].y : (isA ? r1 : r2));
                     P[k2] = cpair{f2p(y[k2].x * y[k2].x, lbx), f2p(x2 * x2, lby)};
