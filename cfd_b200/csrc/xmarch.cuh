@@ -34,36 +34,9 @@
 
 #include "fft_reg.cuh"
 #include "fft_pair.cuh"
+#include "xmarch_plan.cuh"
 
 namespace cfd {
-
-// Row pitches (in 8-byte words for FP32 complex) of the two exchanges: the physical phase
-// reads the inverse exchange and writes the forward one with the three lines of a triple
-// side by side, so the line pitches put the three roles of a warp 10 and 20 = 4 bank pairs
-// apart (inverse) and 2*5 and 4*5 apart (forward, where a lane's lines are 2 apart): each
-// bank pair then sees at most two of the 30 lanes, the minimum for 8-byte accesses.
-__host__ __device__ constexpr int xmarch_pitch(int x, int r) { return x + (((r - x % 16) % 16) + 16) % 16; }
-__host__ __device__ constexpr int xmarch_l1(int n1, int n2) { return xmarch_pitch(n1 * (n2 + 1), 10); }
-__host__ __device__ constexpr int xmarch_l2(int n1, int n2) { return xmarch_pitch(n2 * (n1 + 1), 5); }
-
-// threads of a k_xmarch CTA with RW rows (RW/2 row pairs) and the split N1 x N2
-__host__ __device__ constexpr int xmarch_threads(int n1, int n2, int rw) {
-    const int pairs = rw / 2;
-    int nt = 3 * pairs * n2;                          // step 1: 3 lines per pair
-    if (6 * pairs * n2 > nt) nt = 6 * pairs * n2;     // step 2': 6 lines per pair
-    const int tw = 32 * ((pairs * n1 + 9) / 10);      // triples, 10 per warp
-    if (tw > nt) nt = tw;
-    return (nt + 31) / 32 * 32;
-}
-
-// dynamic shared memory (elements of the complex type): inverse and forward exchanges,
-// the per-thread history and the twiddle table
-__host__ __device__ constexpr long long xmarch_smem_elems(int n1, int n2, int rw) {
-    const int pairs = rw / 2;
-    const long long l1 = xmarch_l1(n1, n2), l2 = xmarch_l2(n1, n2);
-    return 3LL * pairs * l1 + 6LL * pairs * l2 + (long long)n2 * xmarch_threads(n1, n2, rw) +
-           (long long)n1 * (n2 + 1);
-}
 
 template <typename T2, int N1, int N2>
 __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restrict__ Hx, T2* __restrict__ H0,
@@ -81,7 +54,7 @@ __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restr
     constexpr int KA = HX / N2 + 1;         // output blocks ka holding some k <= HX
     const int NT = blockDim.x;
     const int pairs = RW >> 1;
-    const int NLI = 3 * pairs, NLF = 6 * pairs, NTRI = pairs * N1;
+    const int NLI = 3 * pairs, NLF = 6 * pairs;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T2* exi = reinterpret_cast<T2*>(smem_raw);
     T2* exf = exi + (size_t)NLI * L1;
@@ -99,56 +72,37 @@ __global__ void __launch_bounds__(256) k_xmarch(Dims d, Geo g, const T2* __restr
     const T2* Hu = Hx;
     const T2* Hw = Hx + (size_t)d.nyu * pls;
     const T2* Hv = Hx + (size_t)(2 * d.nyu) * pls;
-    const int ta = 1 + blockIdx.y * csteps;
-    const int tb = min(ta + csteps, d.nyu);
-    const int it0 = blockIdx.y == 0 ? -1 : ta - 1;
+    int it0, ta, tb;
+    xmarch_chunk(blockIdx.y, csteps, d.nyu, it0, ta, tb);
 
-    // step 1: thread (line b1, n2), 3 lines per pair
-    const bool act1 = t < NLI * N2;
-    const int b1 = t / N2, n2 = t - b1 * N2;
-    const int p1 = b1 / 3, role1 = b1 - 3 * p1;
-    // physical phase: lane triples
-    const int lane = t & 31;
-    const int g3 = (t >> 5) * 10 + lane / 3, role = lane - 3 * (lane / 3);
-    const bool act2 = lane < 30 && g3 < NTRI;
-    const int gq = act2 ? g3 : 0;
-    const int p2 = gq / N1, k1 = gq - p2 * N1;
-    const int b2 = 3 * p2 + (act2 ? role : 0);
+    // thread roles of step 1 (line b1, column n2), the physical phase (lane triples) and
+    // step 2' (forward line bf, column kb)
+    const XMRoles ro = xmarch_roles(t, RW, N1, N2);
+    const bool act1 = ro.act1, act2 = ro.act2, act3 = ro.act3;
+    const int b1 = ro.b1, n2 = ro.n2, p1 = ro.p1, role1 = ro.role1;
+    const int role = ro.role, p2 = ro.p2, k1 = ro.k1, b2 = ro.b2, src1 = ro.src1, src2 = ro.src2;
     const bool isA = role == 0, isC = role == 2;
-    const int src1 = isA ? lane + 2 : (isC ? lane - 2 : lane);
-    const int src2 = role == 1 ? lane + 1 : (isC ? lane - 1 : lane);
-    // step 2': thread (forward line bf, kb)
-    const int bf = t / N2, kb = t - bf * N2;
-    const bool act3 = bf < NLF;
-    const int bfc = act3 ? bf : NLF - 1;
-    const int partner = (lane - kb) + ((N2 - kb) & (N2 - 1));
-    const int p3 = bfc / 6, rem3 = bfc - 6 * p3, role3 = rem3 >> 1, j3 = rem3 & 1;
+    const int kb = ro.kb, bfc = ro.bfc, partner = ro.partner, p3 = ro.p3, role3 = ro.role3, j3 = ro.j3;
     __syncthreads();
 
     for (int it = it0; it < tb; ++it) {
         // ---- step parameters (uniform over the CTA)
-        const bool emit = it == -1 || it >= ta;
-        const int tu = it < 0 ? 0 : it;
-        int va = tu, vb = tu;
-        R ca = 1, cb = 0;
-        bool combo = false;
-        R pa = 1, pb = 0, fa = 0, fb = 0;
-        bool emit_v = false;
-        if (it == -1) {  // u-plane 0: v at the bottom ghost centre
-            combo = true; va = 1; vb = 0;
+        const XMStep sp = xmarch_step(it, ta, d.nyu);
+        const bool emit = sp.emit, emit_v = sp.emit_v, combo = sp.combo != 0;
+        const int tu = sp.tu, va = sp.va, vb = sp.vb;
+        R ca = 1, cb = 0, pa = 1, pb = 0, fa = 0, fb = 0;
+        if (sp.combo < 0) {  // u-plane 0: v at the bottom ghost centre
             ca = (R)((1.0 - g.gwib) * g.vca[1]);
             cb = (R)(g.gwib + (1.0 - g.gwib) * g.vcb[1]);
-        } else if (it == d.nyu - 1) {  // u-plane nyu-1: v at the top ghost centre
-            combo = true; va = it - 1; vb = it - 2;
+        } else if (sp.combo > 0) {  // u-plane nyu-1: v at the top ghost centre
             ca = (R)(g.gwit + (1.0 - g.gwit) * g.vca[it - 1]);
             cb = (R)((1.0 - g.gwit) * g.vcb[it - 1]);
         }
-        if (emit && it >= 1) {
-            emit_v = true;
-            fa = (R)g.ufa[it - 1];
-            fb = (R)g.ufb[it - 1];
-            if (it <= d.nyu - 2) { pa = (R)g.vca[it]; pb = (R)g.vcb[it]; }
+        if (emit_v) {
+            fa = (R)g.ufa[tu - 1];
+            fb = (R)g.ufb[tu - 1];
         }
+        if (sp.vc >= 0) { pa = (R)g.vca[sp.vc]; pb = (R)g.vcb[sp.vc]; }
 
         // ---- step 1: inverse N1-point DFTs of the Hermitian-extended spectra, thread (b1, n2)
         if (act1) {
