@@ -24,6 +24,9 @@ KNOBS = ((("xline_path", "xsplit"), ((6, 1), (1, 1), (1, 2), (5, 1), (5, 2), (2,
          ("solve_cols", (64, 128, 256)))
 
 
+# x-line paths that only FP32-mixed contexts run (FP64 contexts asked for them run path 1)
+MIXED_ONLY_XLINE = (4, 5, 6)
+
 # knobs that only act with another setting (the library reports them as 0 or 1 otherwise)
 RELEVANT = {"xline_rows": lambda t: t.get("xline_path") != 2,
             "zsplit": lambda t: t.get("xline_path") in (1, 5, 6)}
@@ -69,6 +72,8 @@ def autotune(setup, precision: str, device: int = 0, steps: int = 5, log=None):
             if name in RELEVANT and not RELEVANT[name](best):
                 continue
             cand = dict(best, **(dict(zip(name, v)) if isinstance(name, tuple) else {name: v}))
+            if precision == "fp64" and cand.get("xline_path") in MIXED_ONLY_XLINE:
+                continue
             k = json.dumps(cand, sort_keys=True)
             if k in tried:
                 continue

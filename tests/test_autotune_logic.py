@@ -87,4 +87,19 @@ def test_cache_is_written_once_and_reused(monkeypatch, tmp_path):
     assert "FAKE B200" in key and "64x33x96" in key and key.endswith("ibTrue")
     other = autotune.tuned(S, "fp64")
     assert len(calls) > n and len(json.load(open(tmp_path / "sub" / "tune.json"))) == 2
-    assert other == first
+    # FP64 searches the x-line paths it runs (1-3) and otherwise reaches the same shape
+    assert other["xline_path"] == 1 and first["xline_path"] == 5
+    assert {k: v for k, v in other.items() if k != "xline_path"} == {k: v for k, v in first.items() if k != "xline_path"}
+
+
+def test_fp64_skips_the_mixed_only_xline_paths(monkeypatch):
+    """FP64 contexts run x-line path 1 when asked for paths 4, 5 or 6, so the FP64 search
+    does not time them."""
+    calls = []
+    monkeypatch.setattr(autotune, "time_step", fake_model(calls))
+    autotune.autotune(None, "fp64")
+    assert not any(json.loads(c)["xline_path"] in (4, 5, 6) for c in calls)
+    calls.clear()
+    autotune.autotune(None, "mixed")
+    assert {json.loads(c)["xline_path"] for c in calls} >= {1, 2, 3, 4, 5, 6}
+
