@@ -8,7 +8,7 @@
 // pair of z-rows and walks up the channel: each step transforms u, w of u-plane t and v of
 // v-plane t once (1.5 complex lines per row), keeps the previous step's physical values in
 // shared memory, and forms the products of u-plane t and v-plane t-1 from the two steps'
-// values in physical space: 2 inverse + 3 forward complex lines per row and step instead
+// values in physical space: 1.5 inverse + 3 forward complex lines per row and step instead
 // of 4 + 3, and each spectral plane is read once.
 //
 // Lines of a row pair (rows r, r+1) and their lanes:

@@ -142,7 +142,7 @@ const char *cfd_last_error(const cfd_ctx *ctx);
  *                   SM; FP32-mixed only, FP64 contexts run path 1),
  *                6: x-line pass marching in y: a CTA walks a pair of z rows up the channel,
  *                   transforms u, w and v of each plane pair once and interpolates in
- *                   physical space (2 inverse and 3 forward lines per row and plane pair
+ *                   physical space (1.5 inverse and 3 forward lines per row and plane pair
  *                   instead of 4 and 3); FP32-mixed one-band contexts with x lengths 64,
  *                   96, 128, 192, 384 (the default at 384; FP64 contexts, other lengths
  *                   and three-band channels run path 1); CFD_XMARCH_STEPS sets its y-chunk
