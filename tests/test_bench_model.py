@@ -1,5 +1,6 @@
-"""bench.py's compulsory-traffic model covers every kernel of the default RK3 step, so the
-per-kernel HBM fractions of the bench line are never empty (CPU)."""
+"""bench.py's compulsory-traffic model covers every kernel of the default RK3 step (both
+x-line kernels: the marching one of FP32-mixed, the per-slot one of FP64), so the per-kernel
+HBM fractions of the bench line are never empty (CPU)."""
 import os
 import sys
 
@@ -8,8 +9,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
-STEP_KERNELS = ("k_zinv2s", "k_xline2", "k_zfwd2", "k_rhs", "k_solve_uvw", "k_solve_p_vcorr", "k_meanflow",
-                "k_ib_zinv2", "k_ib_xinv2", "k_ib_force", "k_ib_xfwd2", "k_ib_zfwd2")
+STEP_KERNELS = ("k_zinv2s", "k_xline2", "k_xmarch", "k_zfwd2", "k_rhs", "k_solve_uvw", "k_solve_p_vcorr",
+                "k_meanflow", "k_ib_zinv2", "k_ib_xinv2", "k_ib_force", "k_ib_xfwd2", "k_ib_zfwd2")
 
 
 @pytest.fixture(scope="module")
@@ -140,3 +141,13 @@ def test_profile_error_reports_a_blow_up(setup):
                                   nstat=20, shared=shared)
         assert "error" in out and "NONFINITE" in out["error"] and "within_bound" not in out
         assert f64.dt == setup.dt
+
+
+def test_top_kernel_profile_rows():
+    """The roofline's ncu traffic and FP32-pipe rows of the default top kernels are committed
+    (profiles/dram_traffic_re550.md, profiles/fp32_ops_re550.md)."""
+    import bench
+    for k in ("k_xmarch", "k_xline2"):
+        assert bench.ncu_traffic("re550", k) > 0, k
+        assert bench.fp32_pipe("re550", k, 0.5, {"sm_mhz": 1965.0})["fp32_ops_per_launch"] > 0, k
+
